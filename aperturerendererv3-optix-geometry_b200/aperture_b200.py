@@ -1,0 +1,230 @@
+"""Python binding of the C ABI in include/aperture_b200.h (ctypes).
+
+The shipped product is libaperture_b200.so; this module only marshals
+arguments.  It never falls back to CPU code: if the shared library is missing
+or no CUDA device is visible the calls raise.
+
+Layouts mirror the C structs field by field; `OBJECT_DTYPE` is the numpy view
+of ar_object_desc used to build large scenes without per-object Python work.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int32, c_int64, c_size_t, c_uint64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libaperture_b200.so")
+
+AR_OK = 0
+STATUS_NAMES = {0: "AR_OK", 1: "AR_ERR_INVALID_ARGUMENT", 2: "AR_ERR_CUDA", 3: "AR_ERR_OUT_OF_MEMORY",
+                4: "AR_ERR_UNSUPPORTED", 5: "AR_ERR_DEVICE_FAULT", 6: "AR_ERR_NO_DEVICE"}
+OBJ_CUBE, OBJ_SPHERE, OBJ_SDF, OBJ_TRIANGLE = 0, 1, 2, 3
+MAT_DIFFUSE, MAT_LIGHT, MAT_GLASS, MAT_GGX = 0, 1, 2, 3
+MEM_HOST, MEM_DEVICE = 0, 1
+DEBUG_MAX_HITS = 16
+REFERENCE_SEED = 0x9E3779B97F4A7C15
+
+
+class Vec3(ctypes.Structure):
+    _fields_ = [("x", c_float), ("y", c_float), ("z", c_float)]
+
+
+class Material(ctypes.Structure):
+    _fields_ = [("shading_model", c_int32), ("albedo", Vec3), ("emissive", Vec3), ("specular", c_float),
+                ("metallic", c_float), ("roughness", c_float), ("ior", c_float), ("sigma_a", c_float),
+                ("abbe_number", c_float), ("tilt_number", c_float)]
+
+
+class Vertex(ctypes.Structure):
+    _fields_ = [("position", Vec3), ("normal", Vec3), ("u", c_float), ("v", c_float)]
+
+
+class ObjectDesc(ctypes.Structure):
+    _fields_ = [("type", c_int32), ("center", Vec3), ("extent", Vec3), ("rotation_deg", Vec3),
+                ("material", Material), ("tri", Vertex * 3), ("visible", c_int32), ("reserved", c_int32 * 3)]
+
+
+class Camera(ctypes.Structure):
+    _fields_ = [("position", Vec3), ("direction", Vec3), ("fov_y_deg", c_float), ("width", c_int32),
+                ("height", c_int32)]
+
+
+class RenderParams(ctypes.Structure):
+    _fields_ = [("spp", c_int32), ("max_depth", c_int32), ("rr_depth", c_int32), ("use_nee", c_int32),
+                ("sky", c_int32), ("frame_offset", c_int32), ("seed", c_uint64), ("sort_rays", c_int32),
+                ("wave_paths", c_int32)]
+
+
+class PathRecord(ctypes.Structure):
+    _fields_ = [("radiance", c_float * 3), ("segments", c_int32), ("uniforms", c_int32), ("nee_rays", c_int32),
+                ("reserved", c_int32 * 2), ("hit_object", c_int32 * DEBUG_MAX_HITS)]
+
+
+class SceneInfo(ctypes.Structure):
+    _fields_ = [("objects", c_int64), ("triangles", c_int64), ("lights", c_int64), ("wide_nodes", c_int64),
+                ("prim_refs", c_int64), ("device_bytes", c_int64), ("device", c_int32), ("camera_inside", c_int32)]
+
+
+class RenderStats(ctypes.Structure):
+    _fields_ = [("paths", c_int64), ("extension_rays", c_int64), ("shadow_rays", c_int64),
+                ("kernel_launches", c_int64), ("trace_ms", c_float), ("total_ms", c_float)]
+
+
+assert ctypes.sizeof(ObjectDesc) == 208
+assert ctypes.sizeof(PathRecord) == 96
+OBJECT_DTYPE = np.dtype(ObjectDesc)
+RECORD_DTYPE = np.dtype(PathRecord)
+
+EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create", "ar_scene_destroy",
+                    "ar_scene_get_info", "ar_render", "ar_trace_rays", "ar_render_debug_paths", "ar_rng_tape")
+
+
+class ArError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libaperture_b200.so and declare the prototypes; raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built; run `make -C {HERE}`")
+    lib = ctypes.CDLL(path)
+    lib.ar_version.restype = c_int32
+    lib.ar_get_last_error_string.restype = c_char_p
+    lib.ar_scene_create.argtypes = [c_void_p, c_size_t, c_int32, POINTER(c_void_p)]
+    lib.ar_scene_create.restype = c_int32
+    lib.ar_scene_destroy.argtypes = [c_void_p]
+    lib.ar_scene_destroy.restype = None
+    lib.ar_scene_get_info.argtypes = [c_void_p, POINTER(SceneInfo)]
+    lib.ar_scene_get_info.restype = c_int32
+    lib.ar_render.argtypes = [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p, c_int32,
+                              c_void_p, POINTER(RenderStats)]
+    lib.ar_render.restype = c_int32
+    lib.ar_trace_rays.argtypes = [c_void_p, c_void_p, c_size_t, c_int32, c_void_p, c_void_p, c_int32, c_void_p]
+    lib.ar_trace_rays.restype = c_int32
+    lib.ar_render_debug_paths.argtypes = [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_int32,
+                                          c_void_p]
+    lib.ar_render_debug_paths.restype = c_int32
+    lib.ar_rng_tape.argtypes = [POINTER(Camera), POINTER(RenderParams), c_int32, c_void_p, c_int32, c_void_p]
+    lib.ar_rng_tape.restype = c_int32
+    _lib = lib
+    return lib
+
+
+def _check(status: int) -> None:
+    if status != AR_OK:
+        msg = _lib.ar_get_last_error_string().decode(errors="replace")
+        raise ArError(status, msg)
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def make_camera(position, direction, fov_y_deg, width, height) -> Camera:
+    return Camera(Vec3(*map(float, position)), Vec3(*map(float, direction)), float(fov_y_deg), int(width),
+                  int(height))
+
+
+def make_params(spp=1, max_depth=8, rr_depth=3, use_nee=1, sky=1, frame_offset=0, seed=REFERENCE_SEED,
+                sort_rays=0, wave_paths=0) -> RenderParams:
+    return RenderParams(int(spp), int(max_depth), int(rr_depth), int(use_nee), int(sky), int(frame_offset),
+                        int(seed) & 0xFFFFFFFFFFFFFFFF, int(sort_rays), int(wave_paths))
+
+
+class Scene:
+    """Owns one ar_scene handle (the SceneRenderer of the reference)."""
+
+    def __init__(self, objects: np.ndarray, device: int = 0):
+        lib = load_library()
+        objects = np.ascontiguousarray(objects, dtype=OBJECT_DTYPE)
+        self._objects_keepalive = objects
+        h = c_void_p()
+        _check(lib.ar_scene_create(_ptr(objects) if len(objects) else None, len(objects), device, ctypes.byref(h)))
+        self._h = h
+        self.num_objects = len(objects)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.ar_scene_destroy(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def info(self) -> SceneInfo:
+        si = SceneInfo()
+        _check(_lib.ar_scene_get_info(self._h, ctypes.byref(si)))
+        return si
+
+    def render(self, camera: Camera, params: RenderParams, accum: np.ndarray | None = None,
+               stream: int = 0, want_stats: bool = True):
+        """Host-buffer render; returns (image[h, w, 3] float32, RenderStats)."""
+        out = np.empty((camera.height, camera.width, 3), np.float32)
+        st = RenderStats()
+        acc_ptr = None
+        if accum is not None:
+            assert accum.dtype == np.float64 and accum.flags.c_contiguous
+            acc_ptr = _ptr(accum)
+        _check(_lib.ar_render(self._h, ctypes.byref(camera), ctypes.byref(params), _ptr(out), acc_ptr, MEM_HOST,
+                              c_void_p(stream), ctypes.byref(st) if want_stats else None))
+        return out, st
+
+    def render_device(self, camera: Camera, params: RenderParams, out_ptr: int, accum_ptr: int | None = None,
+                      stream: int = 0, stats: RenderStats | None = None) -> None:
+        """Device-buffer render into caller-owned device memory (pointers)."""
+        _check(_lib.ar_render(self._h, ctypes.byref(camera), ctypes.byref(params), c_void_p(out_ptr),
+                              c_void_p(accum_ptr) if accum_ptr else None, MEM_DEVICE, c_void_p(stream),
+                              ctypes.byref(stats) if stats is not None else None))
+
+    def trace_rays(self, rays: np.ndarray, any_hit: bool = False):
+        """rays: float32 [n, 8] (origin, tmin, direction, tmax) -> (hit_object int32[n], t float32[n])."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        obj = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        _check(_lib.ar_trace_rays(self._h, _ptr(rays), n, int(any_hit), _ptr(obj), _ptr(t), MEM_HOST, None))
+        return obj, t
+
+    def trace_rays_device(self, rays_ptr: int, n: int, any_hit: bool, obj_ptr: int, t_ptr: int | None,
+                          stream: int = 0) -> None:
+        _check(_lib.ar_trace_rays(self._h, c_void_p(rays_ptr), n, int(any_hit), c_void_p(obj_ptr),
+                                  c_void_p(t_ptr) if t_ptr else None, MEM_DEVICE, c_void_p(stream)))
+
+    def debug_paths(self, camera: Camera, params: RenderParams) -> np.ndarray:
+        n = camera.width * camera.height * params.spp
+        rec = np.zeros(n, RECORD_DTYPE)
+        _check(_lib.ar_render_debug_paths(self._h, ctypes.byref(camera), ctypes.byref(params), _ptr(rec), MEM_HOST,
+                                          None))
+        return rec
+
+
+def rng_tape(camera: Camera, params: RenderParams, per_path: int) -> np.ndarray:
+    load_library()
+    n = camera.width * camera.height * params.spp
+    out = np.empty((n, per_path), np.float32)
+    _check(_lib.ar_rng_tape(ctypes.byref(camera), ctypes.byref(params), int(per_path), _ptr(out), MEM_HOST, None))
+    return out

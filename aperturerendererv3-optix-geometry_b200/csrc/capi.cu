@@ -1,0 +1,533 @@
+// capi.cu -- implementation of the C ABI declared in include/aperture_b200.h.
+//
+// Host orchestration only: scene upload, workspace management and the order of
+// kernel launches.  All arithmetic on scene data happens in scene_build.cpp
+// (host, once per scene) and render.cu (device).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/aperture_b200.h"
+#include "render_kernels.h"
+#include "scene_build.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+ar_status fail(ar_status s, const std::string& msg)
+{
+    g_last_error = msg;
+    return s;
+}
+
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t c, const std::string& where)
+        : std::runtime_error(where + ": " + cudaGetErrorString(c)), code(c) {}
+};
+
+void ck(cudaError_t e, const char* where)
+{
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw CudaError(e, where);
+    }
+}
+
+template <class T>
+T* dalloc(size_t count, const char* what)
+{
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw CudaError(e, std::string("cudaMalloc ") + what);
+    }
+    return static_cast<T*>(p);
+}
+
+template <class T>
+T* upload(const std::vector<T>& v, const char* what)
+{
+    T* p = dalloc<T>(v.size(), what);
+    if (!v.empty()) ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), what);
+    return p;
+}
+
+class DeviceGuard {
+public:
+    explicit DeviceGuard(int dev)
+    {
+        ck(cudaGetDevice(&prev_), "cudaGetDevice");
+        if (prev_ != dev) ck(cudaSetDevice(dev), "cudaSetDevice");
+        changed_ = prev_ != dev;
+    }
+    ~DeviceGuard() { if (changed_) cudaSetDevice(prev_); }
+private:
+    int prev_ = 0;
+    bool changed_ = false;
+};
+
+constexpr int64_t kMaxWave = int64_t(1) << 22;
+
+}  // namespace
+
+struct ar_scene {
+    int device = 0;
+    int sm_count = 148;
+    ar::SceneView view{};
+    int stack_depth = 32;
+    int64_t objects = 0, triangles = 0, lights = 0, nodes = 0, prims = 0;
+    int64_t device_bytes = 0;
+    std::vector<void*> owned;
+    // host copy for the camera overlap test (intersection::Overlap)
+    std::vector<ar::ObjInfo> h_objects;
+    std::vector<ar::Analytic> h_analytic;
+    // render workspace
+    char* ws = nullptr;
+    size_t ws_bytes = 0;
+    int64_t ws_wave = 0;
+    int64_t ws_pix = 0;
+    ar::PathSoA paths{};
+    uint4* base0 = nullptr;
+    uint2* base1 = nullptr;
+    double* accum = nullptr;
+    float* fout = nullptr;
+    int32_t* counts = nullptr;
+    unsigned long long* stats = nullptr;
+    int* err = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    ~ar_scene()
+    {
+        DeviceGuard g(device);
+        for (void* p : owned) cudaFree(p);
+        if (ws) cudaFree(ws);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+namespace {
+
+// Carve the per-path SoA arrays, queues and per-pixel buffers from one allocation.
+void ensure_workspace(ar_scene* s, int64_t wave, int64_t npix, bool debug)
+{
+    if (s->ws && s->ws_wave >= wave && s->ws_pix >= npix && (!debug || s->paths.ucount)) return;
+    if (s->ws) { cudaFree(s->ws); s->ws = nullptr; }
+    wave = std::max(wave, s->ws_wave);
+    npix = std::max(npix, s->ws_pix);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
+    const size_t W = static_cast<size_t>(wave), N = static_cast<size_t>(npix);
+    const size_t o_o = take(16 * W), o_d = take(16 * W), o_mask = take(16 * W), o_rad = take(16 * W);
+    const size_t o_r0 = take(16 * W), o_r1 = take(8 * W), o_info = take(16 * W), o_prev = take(16 * W);
+    const size_t o_media = take(16 * W), o_hit = take(16 * W), o_nee = take(16 * W), o_s0 = take(16 * W);
+    const size_t o_s1 = take(16 * W), o_q0 = take(4 * W), o_q1 = take(4 * W), o_qs = take(4 * W), o_uc = take(4 * W);
+    const size_t o_b0 = take(16 * N), o_b1 = take(8 * N), o_acc = take(24 * N), o_fout = take(12 * N);
+    const size_t o_cnt = take(64), o_stats = take(64), o_err = take(64);
+    s->ws = dalloc<char>(off, "render workspace");
+    s->ws_bytes = off;
+    s->ws_wave = wave;
+    s->ws_pix = npix;
+    char* b = s->ws;
+    ar::PathSoA& P = s->paths;
+    P.o = reinterpret_cast<float4*>(b + o_o); P.d = reinterpret_cast<float4*>(b + o_d);
+    P.mask = reinterpret_cast<float4*>(b + o_mask); P.rad = reinterpret_cast<float4*>(b + o_rad);
+    P.rng0 = reinterpret_cast<uint4*>(b + o_r0); P.rng1 = reinterpret_cast<uint2*>(b + o_r1);
+    P.info = reinterpret_cast<int4*>(b + o_info); P.prev = reinterpret_cast<float4*>(b + o_prev);
+    P.media = reinterpret_cast<float4*>(b + o_media); P.hit = reinterpret_cast<int4*>(b + o_hit);
+    P.nee = reinterpret_cast<float4*>(b + o_nee); P.sseg0 = reinterpret_cast<float4*>(b + o_s0);
+    P.sseg1 = reinterpret_cast<float4*>(b + o_s1);
+    P.q[0] = reinterpret_cast<int32_t*>(b + o_q0); P.q[1] = reinterpret_cast<int32_t*>(b + o_q1);
+    P.qs = reinterpret_cast<int32_t*>(b + o_qs);
+    P.ucount = reinterpret_cast<int32_t*>(b + o_uc);
+    s->base0 = reinterpret_cast<uint4*>(b + o_b0);
+    s->base1 = reinterpret_cast<uint2*>(b + o_b1);
+    s->accum = reinterpret_cast<double*>(b + o_acc);
+    s->fout = reinterpret_cast<float*>(b + o_fout);
+    s->counts = reinterpret_cast<int32_t*>(b + o_cnt);
+    s->stats = reinterpret_cast<unsigned long long*>(b + o_stats);
+    s->err = reinterpret_cast<int*>(b + o_err);
+}
+
+// intersection::Overlap (intersection.cuh:399-414) at the camera position; the
+// reference scans every object per path, here it is done once per render.
+bool camera_inside(const ar_scene* s, ar::f3 p)
+{
+    using namespace ar;
+    for (size_t i = 0; i < s->h_objects.size(); ++i) {
+        const ObjInfo& oi = s->h_objects[i];
+        if (oi.type != AR_OBJ_CUBE && oi.type != AR_OBJ_SPHERE) continue;
+        const Analytic& an = s->h_analytic[oi.aux];
+        m3 w2o;
+        w2o.x = mk(an.w2o[0], an.w2o[1], an.w2o[2]);
+        w2o.y = mk(an.w2o[3], an.w2o[4], an.w2o[5]);
+        w2o.z = mk(an.w2o[6], an.w2o[7], an.w2o[8]);
+        const f3 l = mul(w2o, p - mk(an.center[0], an.center[1], an.center[2]));
+        if (oi.type == AR_OBJ_CUBE) {
+            const f3 e = mk(an.extent[0], an.extent[1], an.extent[2]);
+            if (-e.x < l.x && -e.y < l.y && -e.z < l.z && e.x > l.x && e.y > l.y && e.z > l.z) return true;
+        } else {
+            if (dot(l, l) < an.radius * an.radius) return true;
+        }
+    }
+    return false;
+}
+
+ar_status check_camera(const ar_camera* c)
+{
+    if (!c) return fail(AR_ERR_INVALID_ARGUMENT, "camera is NULL");
+    if (c->width <= 0 || c->height <= 0) return fail(AR_ERR_INVALID_ARGUMENT, "camera width/height must be positive");
+    if (static_cast<int64_t>(c->width) * c->height > (int64_t(1) << 28))
+        return fail(AR_ERR_INVALID_ARGUMENT, "image larger than 2^28 pixels");
+    if (!(c->fov_y_deg > 0.0f && c->fov_y_deg < 180.0f)) return fail(AR_ERR_INVALID_ARGUMENT, "fov_y_deg must be in (0, 180)");
+    return AR_OK;
+}
+
+ar_status check_params(const ar_render_params* p)
+{
+    if (!p) return fail(AR_ERR_INVALID_ARGUMENT, "params is NULL");
+    if (p->spp <= 0) return fail(AR_ERR_INVALID_ARGUMENT, "spp must be positive");
+    if (p->max_depth <= 0 || p->max_depth > 4096) return fail(AR_ERR_INVALID_ARGUMENT, "max_depth must be in [1, 4096]");
+    if (p->rr_depth < 0) return fail(AR_ERR_INVALID_ARGUMENT, "rr_depth must be >= 0");
+    if (p->frame_offset < 0) return fail(AR_ERR_INVALID_ARGUMENT, "frame_offset must be >= 0");
+    return AR_OK;
+}
+
+ar::FrameParams make_frame(const ar_scene* s, const ar_camera* c, const ar_render_params* p)
+{
+    using namespace ar;
+    FrameParams fp;
+    std::memset(&fp, 0, sizeof(fp));
+    const f3 cd = mk(c->direction.x, c->direction.y, c->direction.z);
+    // RenderCamera (scene.cu:218-230) with the field of view as a parameter
+    const float fov = c->fov_y_deg * 3.1415926f / 180.0f;
+    const float aspect = static_cast<float>(c->width) / std::max(1.0f, static_cast<float>(c->height));
+    const float tanHalfY = tan_det(0.5f * fov);
+    fp.tan_half_y = tanHalfY;
+    fp.tan_half_x = tanHalfY * aspect;
+    const f3 right = normalize(cross(cd, mk(0.0f, 1.0f, 0.0f)));
+    const f3 up = normalize(cross(cd, right));
+    fp.cam_o[0] = c->position.x; fp.cam_o[1] = c->position.y; fp.cam_o[2] = c->position.z;
+    fp.cam_d[0] = cd.x; fp.cam_d[1] = cd.y; fp.cam_d[2] = cd.z;
+    fp.right[0] = right.x; fp.right[1] = right.y; fp.right[2] = right.z;
+    fp.up[0] = up.x; fp.up[1] = up.y; fp.up[2] = up.z;
+    fp.width = c->width;
+    fp.height = c->height;
+    fp.grid_x = (c->width + 7) / 8;
+    fp.npix = c->width * c->height;
+    fp.camera_inside = camera_inside(s, mk(c->position.x, c->position.y, c->position.z)) ? 1 : 0;
+    if (p) {
+        fp.max_depth = p->max_depth;
+        fp.rr_depth = p->rr_depth;
+        fp.use_nee = p->use_nee;
+        fp.sky = p->sky;
+        fp.seed = p->seed;
+        fp.frame0 = static_cast<uint64_t>(p->frame_offset);
+    }
+    for (int d = 0; d <= 8; ++d) fp.eps_tab[d] = 1.0e-3f * exp_det(fminf(static_cast<float>(d) * 0.5f, 4.0f));
+    return fp;
+}
+
+ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* p, ar_path_record* rec_dev,
+                     cudaStream_t st, ar_render_stats* stats)
+{
+    using namespace ar;
+    ar::FrameParams fp = make_frame(s, cam, p);
+    const int64_t npix = fp.npix;
+    int64_t wave = p->wave_paths > 0 ? std::min<int64_t>(p->wave_paths, kMaxWave) : kMaxWave;
+    wave = std::min<int64_t>(wave, npix);
+    ensure_workspace(s, wave, npix, rec_dev != nullptr);
+    PathSoA P = s->paths;
+    if (!rec_dev) P.ucount = nullptr;
+    ck(cudaMemsetAsync(s->accum, 0, sizeof(double) * 3 * npix, st), "memset accum");
+    ck(cudaMemsetAsync(s->stats, 0, 64, st), "memset stats");
+    ck(cudaMemsetAsync(s->err, 0, 64, st), "memset err");
+    if (!s->ev0) { ck(cudaEventCreate(&s->ev0), "event"); ck(cudaEventCreate(&s->ev1), "event"); }
+    ck(cudaEventRecord(s->ev0, st), "event record");
+    ck(launch_rng_init(fp, s->base0, s->base1, st), "rng init");
+    int64_t launches = 1;
+    const int grid_trace = s->sm_count * 8;
+    const int grid_shade = s->sm_count * 4;
+    for (int sidx = 0; sidx < p->spp; ++sidx) {
+        for (int64_t first = 0; first < npix; first += wave) {
+            fp.spp_index = sidx;
+            fp.first_pixel = static_cast<int32_t>(first);
+            fp.wave = static_cast<int32_t>(std::min<int64_t>(wave, npix - first));
+            ck(launch_wave(s->view, s->stack_depth, fp, P, s->base0, s->base1, s->counts, s->stats, s->err, s->accum,
+                           rec_dev, grid_trace, grid_shade, st, &launches),
+               "render launch");
+        }
+    }
+    ck(cudaEventRecord(s->ev1, st), "event record");
+    if (stats) {
+        unsigned long long h[2];
+        ck(cudaMemcpyAsync(h, s->stats, sizeof(h), cudaMemcpyDeviceToHost, st), "stats copy");
+        ck(cudaStreamSynchronize(st), "sync");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+        stats->paths = npix * p->spp;
+        stats->extension_rays = static_cast<int64_t>(h[0]);
+        stats->shadow_rays = static_cast<int64_t>(h[1]);
+        stats->kernel_launches = launches;
+        stats->trace_ms = -1.0f;
+        stats->total_ms = ms;
+    }
+    return AR_OK;
+}
+
+ar_status check_err(ar_scene* s, cudaStream_t st)
+{
+    int e = 0;
+    ck(cudaMemcpyAsync(&e, s->err, sizeof(int), cudaMemcpyDeviceToHost, st), "error word copy");
+    ck(cudaStreamSynchronize(st), "sync");
+    if (e != 0) return fail(AR_ERR_DEVICE_FAULT, "traversal stack overflow reported by a kernel");
+    return AR_OK;
+}
+
+#define AR_GUARD_BEGIN try {
+#define AR_GUARD_END                                                              \
+    }                                                                             \
+    catch (const CudaError& e) {                                                  \
+        return fail(e.code == cudaErrorMemoryAllocation ? AR_ERR_OUT_OF_MEMORY    \
+                                                        : AR_ERR_CUDA, e.what()); \
+    }                                                                             \
+    catch (const std::bad_alloc&) { return fail(AR_ERR_OUT_OF_MEMORY, "host allocation failed"); } \
+    catch (const std::domain_error& e) { return fail(AR_ERR_UNSUPPORTED, e.what()); } \
+    catch (const std::invalid_argument& e) { return fail(AR_ERR_INVALID_ARGUMENT, e.what()); } \
+    catch (const std::exception& e) { return fail(AR_ERR_CUDA, e.what()); }
+
+}  // namespace
+
+extern "C" {
+
+int32_t ar_version(void) { return AR_ABI_VERSION; }
+
+const char* ar_get_last_error_string(void) { return g_last_error.c_str(); }
+
+ar_status ar_scene_create(const ar_object_desc* objects, size_t count, int32_t device, ar_scene** out_scene)
+{
+    g_last_error.clear();
+    if (!out_scene) return fail(AR_ERR_INVALID_ARGUMENT, "out_scene is NULL");
+    *out_scene = nullptr;
+    if (count > 0 && !objects) return fail(AR_ERR_INVALID_ARGUMENT, "objects is NULL");
+    AR_GUARD_BEGIN
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(AR_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(AR_ERR_INVALID_ARGUMENT, "device index out of range");
+    ar::HostScene hs = ar::build_scene(objects, count);
+    DeviceGuard g(device);
+    ar_scene* s = new ar_scene();
+    s->device = device;
+    cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device);
+    try {
+        auto own = [&](void* p, size_t bytes) { s->owned.push_back(p); s->device_bytes += static_cast<int64_t>(bytes); return p; };
+        ar::SceneView& v = s->view;
+        v.nodes = static_cast<const ar::WideNode*>(own(upload(hs.nodes, "nodes"), hs.nodes.size() * sizeof(ar::WideNode)));
+        v.prims = static_cast<const ar::PrimRec*>(own(upload(hs.prims, "prims"), hs.prims.size() * sizeof(ar::PrimRec)));
+        v.objects = static_cast<const ar::ObjInfo*>(own(upload(hs.objects, "objects"), hs.objects.size() * sizeof(ar::ObjInfo)));
+        v.trishade = static_cast<const ar::TriShade*>(own(upload(hs.trishade, "trishade"), hs.trishade.size() * sizeof(ar::TriShade)));
+        v.analytic = static_cast<const ar::Analytic*>(own(upload(hs.analytic, "analytic"), hs.analytic.size() * sizeof(ar::Analytic)));
+        v.materials = static_cast<const ar::MaterialRec*>(own(upload(hs.materials, "materials"), hs.materials.size() * sizeof(ar::MaterialRec)));
+        v.light_object = static_cast<const int32_t*>(own(upload(hs.light_object, "lights"), hs.light_object.size() * 4));
+        v.light_prob = static_cast<const float*>(own(upload(hs.light_prob, "lights"), hs.light_prob.size() * 4));
+        v.num_nodes = static_cast<int32_t>(hs.prims.empty() ? 0 : hs.nodes.size());
+        v.num_objects = static_cast<int32_t>(hs.objects.size());
+        v.num_lights = static_cast<int32_t>(hs.light_object.size());
+        s->stack_depth = hs.stack_bound <= 32 ? 32 : (hs.stack_bound <= 64 ? 64 : 128);
+        if (hs.stack_bound > 128) throw std::domain_error("BVH too deep for the traversal stack");
+        s->objects = static_cast<int64_t>(count);
+        s->triangles = hs.triangles;
+        s->lights = static_cast<int64_t>(hs.light_object.size());
+        s->nodes = static_cast<int64_t>(hs.nodes.size());
+        s->prims = static_cast<int64_t>(hs.prims.size());
+        s->h_objects = std::move(hs.objects);
+        s->h_analytic = std::move(hs.analytic);
+    } catch (...) {
+        delete s;
+        throw;
+    }
+    *out_scene = s;
+    return AR_OK;
+    AR_GUARD_END
+}
+
+void ar_scene_destroy(ar_scene* scene)
+{
+    try { delete scene; } catch (...) {}
+}
+
+ar_status ar_scene_get_info(const ar_scene* s, ar_scene_info* info)
+{
+    if (!s || !info) return fail(AR_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::memset(info, 0, sizeof(*info));
+    info->objects = s->objects;
+    info->triangles = s->triangles;
+    info->lights = s->lights;
+    info->wide_nodes = s->nodes;
+    info->prim_refs = s->prims;
+    info->device_bytes = s->device_bytes;
+    info->device = s->device;
+    return AR_OK;
+}
+
+ar_status ar_render(ar_scene* s, const ar_camera* cam, const ar_render_params* p, float* out_rgb, double* accum,
+                    int32_t mem_kind, void* stream, ar_render_stats* stats)
+{
+    g_last_error.clear();
+    if (!s) return fail(AR_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (ar_status e = check_camera(cam)) return e;
+    if (ar_status e = check_params(p)) return e;
+    if (!out_rgb && !accum) return fail(AR_ERR_INVALID_ARGUMENT, "out_rgb and accum are both NULL");
+    if (mem_kind != AR_MEM_HOST && mem_kind != AR_MEM_DEVICE) return fail(AR_ERR_INVALID_ARGUMENT, "bad mem_kind");
+    AR_GUARD_BEGIN
+    DeviceGuard g(s->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (ar_status e = run_render(s, cam, p, nullptr, st, stats)) return e;
+    const int64_t n = static_cast<int64_t>(cam->width) * cam->height * 3;
+    const double inv = 1.0 / static_cast<double>(p->spp);
+    if (mem_kind == AR_MEM_DEVICE) {
+        if (out_rgb) ck(ar::launch_mean(s->accum, n, inv, out_rgb, st), "mean");
+        if (accum) ck(ar::launch_add(s->accum, n, accum, st), "accumulate");
+    } else {
+        if (out_rgb) {
+            ck(ar::launch_mean(s->accum, n, inv, s->fout, st), "mean");
+            ck(cudaMemcpyAsync(out_rgb, s->fout, n * sizeof(float), cudaMemcpyDeviceToHost, st), "copy image");
+        }
+        if (accum) {
+            std::vector<double> tmp(static_cast<size_t>(n));
+            ck(cudaMemcpyAsync(tmp.data(), s->accum, n * sizeof(double), cudaMemcpyDeviceToHost, st), "copy accum");
+            ck(cudaStreamSynchronize(st), "sync");
+            for (int64_t i = 0; i < n; ++i) accum[i] += tmp[static_cast<size_t>(i)];
+        }
+    }
+    return check_err(s, st);
+    AR_GUARD_END
+}
+
+ar_status ar_trace_rays(ar_scene* s, const float* rays, size_t n, int32_t any_hit, int32_t* hit_object, float* hit_t,
+                        int32_t mem_kind, void* stream)
+{
+    g_last_error.clear();
+    if (!s) return fail(AR_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (n == 0) return AR_OK;
+    if (!rays || !hit_object) return fail(AR_ERR_INVALID_ARGUMENT, "rays/hit_object is NULL");
+    if (mem_kind != AR_MEM_HOST && mem_kind != AR_MEM_DEVICE) return fail(AR_ERR_INVALID_ARGUMENT, "bad mem_kind");
+    if (mem_kind == AR_MEM_DEVICE && (reinterpret_cast<uintptr_t>(rays) & 15u))
+        return fail(AR_ERR_INVALID_ARGUMENT, "device ray buffer must be 16-byte aligned");
+    AR_GUARD_BEGIN
+    DeviceGuard g(s->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!s->err) ensure_workspace(s, 1, 1, false);
+    ck(cudaMemsetAsync(s->err, 0, 64, st), "memset err");
+    const float4* drays;
+    int32_t* dobj;
+    float* dt;
+    std::vector<void*> tmp;
+    if (mem_kind == AR_MEM_HOST) {
+        float4* rr = dalloc<float4>(2 * n, "rays");
+        tmp.push_back(rr);
+        ck(cudaMemcpyAsync(rr, rays, n * 32, cudaMemcpyHostToDevice, st), "copy rays");
+        drays = rr;
+        dobj = dalloc<int32_t>(n, "hits"); tmp.push_back(dobj);
+        dt = hit_t ? dalloc<float>(n, "t") : nullptr;
+        if (dt) tmp.push_back(dt);
+    } else {
+        drays = reinterpret_cast<const float4*>(rays);
+        dobj = hit_object;
+        dt = hit_t;
+    }
+    const int grid = s->sm_count * 8;
+    cudaError_t e = ar::launch_trace_rays(s->view, s->stack_depth, drays, static_cast<int64_t>(n), any_hit ? 1 : 0, dobj, dt,
+                                          s->err, grid, st);
+    if (e == cudaSuccess && mem_kind == AR_MEM_HOST) {
+        e = cudaMemcpyAsync(hit_object, dobj, n * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && hit_t) e = cudaMemcpyAsync(hit_t, dt, n * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    for (void* p : tmp) cudaFree(p);
+    ck(e, "trace rays");
+    return check_err(s, st);
+    AR_GUARD_END
+}
+
+ar_status ar_render_debug_paths(ar_scene* s, const ar_camera* cam, const ar_render_params* p, ar_path_record* records,
+                                int32_t mem_kind, void* stream)
+{
+    g_last_error.clear();
+    if (!s || !records) return fail(AR_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (ar_status e = check_camera(cam)) return e;
+    if (ar_status e = check_params(p)) return e;
+    if (mem_kind != AR_MEM_HOST && mem_kind != AR_MEM_DEVICE) return fail(AR_ERR_INVALID_ARGUMENT, "bad mem_kind");
+    AR_GUARD_BEGIN
+    DeviceGuard g(s->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t nrec = static_cast<size_t>(cam->width) * cam->height * p->spp;
+    ar_path_record* drec = records;
+    if (mem_kind == AR_MEM_HOST) drec = dalloc<ar_path_record>(nrec, "path records");
+    cudaError_t e = cudaMemsetAsync(drec, 0, nrec * sizeof(ar_path_record), st);
+    ar_status rs = AR_OK;
+    if (e == cudaSuccess) {
+        try { rs = run_render(s, cam, p, drec, st, nullptr); } catch (...) { if (mem_kind == AR_MEM_HOST) cudaFree(drec); throw; }
+    }
+    if (e == cudaSuccess && rs == AR_OK && mem_kind == AR_MEM_HOST) {
+        e = cudaMemcpyAsync(records, drec, nrec * sizeof(ar_path_record), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (mem_kind == AR_MEM_HOST) cudaFree(drec);
+    ck(e, "debug render");
+    if (rs != AR_OK) return rs;
+    return check_err(s, st);
+    AR_GUARD_END
+}
+
+ar_status ar_rng_tape(const ar_camera* cam, const ar_render_params* p, int32_t per_path, float* out, int32_t mem_kind,
+                      void* stream)
+{
+    g_last_error.clear();
+    if (ar_status e = check_camera(cam)) return e;
+    if (ar_status e = check_params(p)) return e;
+    if (per_path <= 0 || !out) return fail(AR_ERR_INVALID_ARGUMENT, "per_path must be positive and out non-NULL");
+    if (mem_kind != AR_MEM_HOST && mem_kind != AR_MEM_DEVICE) return fail(AR_ERR_INVALID_ARGUMENT, "bad mem_kind");
+    AR_GUARD_BEGIN
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(AR_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ar::FrameParams fp;
+    std::memset(&fp, 0, sizeof(fp));
+    fp.width = cam->width;
+    fp.height = cam->height;
+    fp.grid_x = (cam->width + 7) / 8;
+    fp.npix = cam->width * cam->height;
+    fp.seed = p->seed;
+    fp.frame0 = static_cast<uint64_t>(p->frame_offset);
+    const size_t n = static_cast<size_t>(fp.npix) * p->spp * per_path;
+    float* dout = out;
+    if (mem_kind == AR_MEM_HOST) dout = dalloc<float>(n, "tape");
+    cudaError_t e = ar::launch_rng_tape(fp, p->spp, per_path, dout, st);
+    if (e == cudaSuccess && mem_kind == AR_MEM_HOST) {
+        e = cudaMemcpyAsync(out, dout, n * 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (mem_kind == AR_MEM_HOST) cudaFree(dout);
+    ck(e, "rng tape");
+    return AR_OK;
+    AR_GUARD_END
+}
+
+}  // extern "C"

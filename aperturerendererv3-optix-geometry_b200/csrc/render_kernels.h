@@ -1,0 +1,25 @@
+// render_kernels.h -- host-side launchers of the sm_100a kernels (render.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "wavefront.cuh"
+
+namespace ar {
+
+constexpr int kTraceBlock = 128;  // threads per traversal block (4 warps)
+constexpr int kShadeBlock = 256;
+
+cudaError_t launch_trace_rays(const SceneView& s, int stack_depth, const float4* rays, int64_t n, int any, int32_t* obj,
+                              float* t, int* err, int grid, cudaStream_t st);
+cudaError_t launch_rng_init(const FrameParams& fp, uint4* b0, uint2* b1, cudaStream_t st);
+cudaError_t launch_rng_tape(const FrameParams& fp, int spp, int per_path, float* out, cudaStream_t st);
+cudaError_t launch_wave(const SceneView& s, int stack_depth, const FrameParams& fp, const PathSoA& P, uint4* b0, uint2* b1,
+                        int32_t* counts, unsigned long long* stats, int* err, double* accum, ar_path_record* rec,
+                        int grid_trace, int grid_shade, cudaStream_t st, int64_t* launches);
+cudaError_t launch_mean(const double* accum, int64_t n, double inv, float* out, cudaStream_t st);
+cudaError_t launch_add(const double* src, int64_t n, double* dst, cudaStream_t st);
+
+}  // namespace ar

@@ -1,0 +1,276 @@
+// traverse.cuh -- sm_100a BVH traversal and primitive intersection.
+//
+// Replaces intersection::TraverseBVH (core/render/intersection.cuh:235-370) and
+// the per-shape intersectors it calls.  One thread per ray; the traversal stack
+// of each warp lives in shared memory, interleaved by lane (entry k of lane l at
+// [k * 32 + l]) so pushes and pops are bank-conflict free.  Nodes are 80-byte
+// 8-wide records read with five 128-bit read-only loads; the child boxes are
+// decoded from 8-bit grid coordinates with one FMA per plane:
+//     t(q) = fma(q, scale * inv_dir, (origin - ray_origin) * inv_dir).
+// The box test is conservative (far distance widened by 2^-20 relative), so the
+// set of primitives tested is a superset of the exact one and the closest hit
+// equals a brute-force search.  Ties in t go to the lowest object index; the
+// reference keeps the first primitive its traversal happens to find.
+#pragma once
+
+#include <cstdint>
+
+#include "detmath.h"
+#include "scene_types.h"
+
+namespace ar {
+
+struct SceneView {
+    const WideNode* nodes;
+    const PrimRec* prims;
+    const ObjInfo* objects;
+    const TriShade* trishade;
+    const Analytic* analytic;
+    const MaterialRec* materials;
+    const int32_t* light_object;
+    const float* light_prob;
+    int32_t num_nodes;
+    int32_t num_objects;
+    int32_t num_lights;
+    int32_t pad;
+};
+
+constexpr float kSlabWiden = 1.000001f;
+constexpr float kMinDir = 0x1p-64f;
+
+__device__ __forceinline__ float4 ldg4(const void* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ uint4 ldgu4(const void* p) { return __ldg(reinterpret_cast<const uint4*>(p)); }
+
+// Moller-Trumbore exactly as IntersectTriangleObject (intersection.cuh:31-57),
+// operands precomputed with the same expressions.  Returns t or -1.
+__device__ __forceinline__ float mt_triangle(f3 o, f3 d, f3 v0, f3 e1, f3 e2)
+{
+    const f3 h = cross(d, e2);
+    const float a = dot(e1, h);
+    if (a > -1e-6f && a < 1e-6f) return -1.0f;
+    const float f = __frcp_rn(a);  // == 1.0f / a, IEEE
+    const f3 s = o - v0;
+    const float u = f * dot(s, h);
+    if (u < 0.0f || u > 1.0f) return -1.0f;
+    const f3 q = cross(s, e1);
+    const float v = f * dot(d, q);
+    if (v < 0.0f || u + v > 1.0f) return -1.0f;
+    const float t = f * dot(e2, q);
+    return (t > 1e-5f) ? t : -1.0f;
+}
+
+__device__ __forceinline__ m3 load_m3(const float* m)
+{
+    m3 r;
+    r.x = mk(m[0], m[1], m[2]); r.y = mk(m[3], m[4], m[5]); r.z = mk(m[6], m[7], m[8]);
+    return r;
+}
+
+// IntersectAABBObject (object/aabb.cuh:28-89).  Fills pos/nrm when wanted.
+template <bool kDetail>
+__device__ __forceinline__ float isect_cube(const Analytic& an, f3 ro, f3 rd, f3* pos, f3* nrm)
+{
+    const f3 c = mk(an.center[0], an.center[1], an.center[2]);
+    const f3 e = mk(an.extent[0], an.extent[1], an.extent[2]);
+    const m3 w2o = load_m3(an.w2o);
+    const f3 lo = mul(w2o, ro - c);
+    const f3 ld = normalize(mul(w2o, rd));
+    const f3 dv = mk(inv_safe(ld.x), inv_safe(ld.y), inv_safe(ld.z));
+    const f3 t1 = (-e - lo) * dv;
+    const f3 t2 = (e - lo) * dv;
+    const f3 tmn = vmin(t1, t2), tmx = vmax(t1, t2);
+    const float tEnter = fmaxf(fmaxf(tmn.x, tmn.y), tmn.z);
+    const float tExit = fminf(fminf(tmx.x, tmx.y), tmx.z);
+    if (tEnter > tExit) return -1.0f;
+    if (tExit <= 0.0f) return -1.0f;
+    const bool inside = (tEnter < 0.0f);
+    const float tHit = inside ? tExit : tEnter;
+    if (kDetail) {
+        const m3 o2w = load_m3(an.o2w);
+        const f3 lp = lo + ld * tHit;
+        *pos = mul(o2w, lp) + c;
+        const float rx = fabsf(lp.x) / e.x;
+        const float ry = fabsf(lp.y) / e.y;
+        const float rz = fabsf(lp.z) / e.z;
+        f3 ln;
+        if (rx >= ry && rx >= rz) ln = mk((lp.x > 0.0f) ? 1.0f : -1.0f, 0.0f, 0.0f);
+        else if (ry >= rz) ln = mk(0.0f, (lp.y > 0.0f) ? 1.0f : -1.0f, 0.0f);
+        else ln = mk(0.0f, 0.0f, (lp.z > 0.0f) ? 1.0f : -1.0f);
+        if (inside) ln = -ln;
+        *nrm = normalize(mul(o2w, ln));
+    }
+    return tHit;
+}
+
+// IntersectSphereObject (object/sphere.cuh:9-70)
+template <bool kDetail>
+__device__ __forceinline__ float isect_sphere(const Analytic& an, f3 ro, f3 rd, f3* pos, f3* nrm)
+{
+    const f3 c = mk(an.center[0], an.center[1], an.center[2]);
+    const m3 w2o = load_m3(an.w2o);
+    const f3 lo = mul(w2o, ro - c);
+    const f3 ld = normalize(mul(w2o, rd));
+    const float r = an.radius;
+    const float b = dot(lo, ld);
+    const float cc = dot(lo, lo) - r * r;
+    const float disc = b * b - 1.0f * cc;
+    if (disc < 0.0f) return -1.0f;
+    const float sq = sqrtf(disc);
+    float t = -b - sq;
+    bool inside = false;
+    if (t <= 0.0f) { t = -b + sq; inside = true; }
+    if (t <= 0.0f) return -1.0f;
+    if (kDetail) {
+        const m3 o2w = load_m3(an.o2w);
+        const f3 lp = lo + ld * t;
+        const f3 ln = normalize(lp) * (inside ? -1.0f : 1.0f);
+        *pos = mul(o2w, lp) + c;
+        *nrm = normalize(mul(o2w, ln));
+    }
+    return t;
+}
+
+__device__ __forceinline__ float isect_analytic_t(const SceneView& s, int obj, f3 ro, f3 rd)
+{
+    const ObjInfo oi = s.objects[obj];
+    const Analytic& an = s.analytic[oi.aux];
+    f3 p, n;
+    if (oi.type == 0) return isect_cube<false>(an, ro, rd, &p, &n);
+    if (oi.type == 1) return isect_sphere<false>(an, ro, rd, &p, &n);
+    return -1.0f;
+}
+
+struct Hit {
+    float t;
+    int32_t obj;   // object index, -1 = miss
+    int32_t prim;  // leaf-order primitive slot, -1 = none
+};
+
+__device__ __forceinline__ uint32_t byte_of(uint32_t w, int k) { return (w >> (8 * k)) & 0xFFu; }
+
+__device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b)
+{
+    const uint32_t lo = min(a, b), hi = max(a, b);
+    a = lo; b = hi;
+}
+
+// Closest hit (kAny = false) or any hit (kAny = true) on [tmin, tmax).
+// stack: this lane's first stack entry in shared memory; entries are 32 apart.
+template <bool kAny, int kDepth>
+__device__ __forceinline__ Hit trace_ray(const SceneView& s, f3 o, f3 d, float tmin, float tmax,
+                                         uint32_t* stack, int* err)
+{
+    Hit best;
+    best.t = tmax; best.obj = -1; best.prim = -1;
+    if (s.num_nodes == 0) return best;
+    const float dx = fabsf(d.x) < kMinDir ? copysignf(kMinDir, d.x) : d.x;
+    const float dy = fabsf(d.y) < kMinDir ? copysignf(kMinDir, d.y) : d.y;
+    const float dz = fabsf(d.z) < kMinDir ? copysignf(kMinDir, d.z) : d.z;
+    const float idx = __frcp_rn(dx), idy = __frcp_rn(dy), idz = __frcp_rn(dz);
+    const bool nx = idx < 0.0f, ny = idy < 0.0f, nz = idz < 0.0f;
+    int sp = 0;
+    uint32_t node = 0;
+    for (;;) {
+        const WideNode* np = s.nodes + node;
+        const float4 w0 = ldg4(reinterpret_cast<const char*>(np));
+        const uint4 w1 = ldgu4(reinterpret_cast<const char*>(np) + 16);
+        const uint4 w2 = ldgu4(reinterpret_cast<const char*>(np) + 32);
+        const uint4 w3 = ldgu4(reinterpret_cast<const char*>(np) + 48);
+        const uint4 w4 = ldgu4(reinterpret_cast<const char*>(np) + 64);
+        const uint32_t exps = __float_as_uint(w0.w);
+        const float sx = __uint_as_float((exps & 0xFFu) << 23);
+        const float sy = __uint_as_float(((exps >> 8) & 0xFFu) << 23);
+        const float sz = __uint_as_float(((exps >> 16) & 0xFFu) << 23);
+        const float ax = sx * idx, ay = sy * idy, az = sz * idz;
+        const float bx = (w0.x - o.x) * idx, by = (w0.y - o.y) * idy, bz = (w0.z - o.z) * idz;
+        // quantised planes: w2 = qlo_x[8] | qlo_y[8]; w3 = qlo_z[8] | qhi_x[8]; w4 = qhi_y[8] | qhi_z[8]
+        const uint32_t lox0 = w2.x, lox1 = w2.y, loy0 = w2.z, loy1 = w2.w;
+        const uint32_t loz0 = w3.x, loz1 = w3.y, hix0 = w3.z, hix1 = w3.w;
+        const uint32_t hiy0 = w4.x, hiy1 = w4.y, hiz0 = w4.z, hiz1 = w4.w;
+        const uint32_t nx0 = nx ? hix0 : lox0, nx1 = nx ? hix1 : lox1, fx0 = nx ? lox0 : hix0, fx1 = nx ? lox1 : hix1;
+        const uint32_t ny0 = ny ? hiy0 : loy0, ny1 = ny ? hiy1 : loy1, fy0 = ny ? loy0 : hiy0, fy1 = ny ? loy1 : hiy1;
+        const uint32_t nz0 = nz ? hiz0 : loz0, nz1 = nz ? hiz1 : loz1, fz0 = nz ? loz0 : hiz0, fz1 = nz ? loz1 : hiz1;
+        const uint32_t meta0 = w1.z, meta1 = w1.w;
+        const float limit = fminf(best.t, FLT_MAX);
+        uint32_t key[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t wnx = k < 4 ? nx0 : nx1, wfx = k < 4 ? fx0 : fx1;
+            const uint32_t wny = k < 4 ? ny0 : ny1, wfy = k < 4 ? fy0 : fy1;
+            const uint32_t wnz = k < 4 ? nz0 : nz1, wfz = k < 4 ? fz0 : fz1;
+            const int b = k & 3;
+            const float tnx = fmaf(static_cast<float>(byte_of(wnx, b)), ax, bx);
+            const float tfx = fmaf(static_cast<float>(byte_of(wfx, b)), ax, bx);
+            const float tny = fmaf(static_cast<float>(byte_of(wny, b)), ay, by);
+            const float tfy = fmaf(static_cast<float>(byte_of(wfy, b)), ay, by);
+            const float tnz = fmaf(static_cast<float>(byte_of(wnz, b)), az, bz);
+            const float tfz = fmaf(static_cast<float>(byte_of(wfz, b)), az, bz);
+            const float tnear = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+            const float tfar = fminf(fminf(fminf(tfx, tfy), tfz), limit) * kSlabWiden;
+            const uint32_t meta = byte_of(k < 4 ? meta0 : meta1, b);
+            const bool hit = (tnear <= tfar) && (meta != kMetaEmpty);
+            // tnear >= tmin >= 0, so its bit pattern orders like the value
+            key[k] = hit ? ((__float_as_uint(fmaxf(tnear, 0.0f)) & ~7u) | static_cast<uint32_t>(k)) : 0xFFFFFFFFu;
+        }
+        // sort the 8 keys (Batcher odd-even merge network, 19 comparators)
+        cswap(key[0], key[1]); cswap(key[2], key[3]); cswap(key[4], key[5]); cswap(key[6], key[7]);
+        cswap(key[0], key[2]); cswap(key[1], key[3]); cswap(key[4], key[6]); cswap(key[5], key[7]);
+        cswap(key[1], key[2]); cswap(key[5], key[6]);
+        cswap(key[0], key[4]); cswap(key[1], key[5]); cswap(key[2], key[6]); cswap(key[3], key[7]);
+        cswap(key[2], key[4]); cswap(key[3], key[5]);
+        cswap(key[1], key[2]); cswap(key[3], key[4]); cswap(key[5], key[6]);
+        // leaves, nearest first
+        const uint32_t prim_base = w1.y;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t kk = key[k];
+            if (kk == 0xFFFFFFFFu) break;
+            const int slot = static_cast<int>(kk & 7u);
+            const uint32_t meta = byte_of(slot < 4 ? meta0 : meta1, slot & 3);
+            if (meta & kMetaInternal) continue;
+            const float tn = __uint_as_float(kk & ~7u);
+            if (!(tn <= fminf(best.t, FLT_MAX) * kSlabWiden)) continue;
+            const int count = static_cast<int>(meta >> 5) + 1;
+            const uint32_t first = prim_base + (meta & 31u);
+            for (int p = 0; p < count; ++p) {
+                const PrimRec* pr = s.prims + first + p;
+                const float4 a = ldg4(&pr->v0[0]);
+                const float4 e1 = ldg4(&pr->e1[0]);
+                const int obj = __float_as_int(a.w);
+                float t;
+                if (__float_as_int(e1.w) == kPrimTriangle) {
+                    const float4 e2 = ldg4(&pr->e2[0]);
+                    t = mt_triangle(o, d, mk(a.x, a.y, a.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z));
+                } else {
+                    t = isect_analytic_t(s, obj, o, d);
+                }
+                if (t < 0.0f || t < tmin) continue;
+                if (t < best.t || (best.obj >= 0 && t == best.t && obj < best.obj)) {
+                    best.t = t; best.obj = obj; best.prim = static_cast<int>(first) + p;
+                    if (kAny) return best;
+                }
+            }
+        }
+        // internal children, pushed far to near
+        const uint32_t child_base = w1.x;
+#pragma unroll
+        for (int k = 7; k >= 0; --k) {
+            const uint32_t kk = key[k];
+            if (kk == 0xFFFFFFFFu) continue;
+            const int slot = static_cast<int>(kk & 7u);
+            const uint32_t meta = byte_of(slot < 4 ? meta0 : meta1, slot & 3);
+            if (!(meta & kMetaInternal)) continue;
+            const float tn = __uint_as_float(kk & ~7u);
+            if (!(tn <= fminf(best.t, FLT_MAX) * kSlabWiden)) continue;
+            if (sp >= kDepth) { atomicOr(err, 1); return best; }
+            stack[sp * 32] = child_base + (meta & 7u);
+            ++sp;
+        }
+        if (sp == 0) break;
+        --sp;
+        node = stack[sp * 32];
+    }
+    return best;
+}
+
+}  // namespace ar

@@ -1,0 +1,196 @@
+/*
+ * aperture_b200.h -- C ABI of the B200 (sm_100a) path-tracing core.
+ *
+ * The reference renderer (ApertureRendererV3) exposes its hot path only as the
+ * C++ classes SceneRenderer and Camera (core/scene.hpp:19-154,
+ * core/camera.hpp:14-100), whose scene state lives in module-global
+ * __constant__ symbols (core/render/render.cuh:26-55).  This header is the
+ * drop-in boundary that replaces them: plain C types, plain pointers and sizes,
+ * one handle per scene, no device globals, status codes instead of printed
+ * errors.  Every entry point below names the reference interface it replaces.
+ *
+ * Threading: a scene handle may be used by one host thread at a time.  Work is
+ * issued on the caller's CUDA stream (passed as void*; NULL = legacy default
+ * stream) and every call that returns host data synchronises that stream.
+ */
+#ifndef APERTURE_B200_H
+#define APERTURE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AR_ABI_VERSION 1
+
+typedef enum ar_status {
+    AR_OK = 0,
+    AR_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size, enum value or layout      */
+    AR_ERR_CUDA = 2,             /* a CUDA runtime call failed                   */
+    AR_ERR_OUT_OF_MEMORY = 3,    /* device or host allocation failed             */
+    AR_ERR_UNSUPPORTED = 4,      /* feature not available for this scene/config  */
+    AR_ERR_DEVICE_FAULT = 5,     /* a kernel reported an internal error word     */
+    AR_ERR_NO_DEVICE = 6         /* no CUDA device / extension not usable        */
+} ar_status;
+
+/* EObjectType (core/render/object.cuh:29-35). */
+enum { AR_OBJ_CUBE = 0, AR_OBJ_SPHERE = 1, AR_OBJ_SDF = 2, AR_OBJ_TRIANGLE = 3 };
+/* EShadingModel (core/render/object.cuh:45-52). */
+enum { AR_MAT_DIFFUSE = 0, AR_MAT_LIGHT = 1, AR_MAT_GLASS = 2, AR_MAT_GGX = 3 };
+/* Where a caller-supplied buffer lives. */
+enum { AR_MEM_HOST = 0, AR_MEM_DEVICE = 1 };
+
+typedef struct ar_vec3 { float x, y, z; } ar_vec3;
+
+/* Material = shading model + the GBuffer fields of a pure-colour texture
+ * (core/render/object.cuh:60-91, 124-217).  Textures are not supported. */
+typedef struct ar_material {
+    int32_t shading_model; /* AR_MAT_*                                   */
+    ar_vec3 albedo;        /* linear                                     */
+    ar_vec3 emissive;      /* linear radiance                            */
+    float specular;        /* GGX: F0 = 0.08 * specular                  */
+    float metallic;
+    float roughness;       /* GGX: alpha = roughness^2                   */
+    float ior;             /* glass                                      */
+    float sigma_a;         /* glass Beer-Lambert density                 */
+    float abbe_number;     /* glass dispersion (spectral)                */
+    float tilt_number;
+} ar_material;             /* 56 bytes */
+
+/* Vertex (core/render/object.cuh:233-238), object space. */
+typedef struct ar_vertex { ar_vec3 position; ar_vec3 normal; float u, v; } ar_vertex; /* 32 B */
+
+/* One scene primitive; the fields of the reference SceneObject that its
+ * constructor takes (core/render/object.cuh:344-364).  The world transform is
+ * objectToWorld = Rz * (Ry * Rx) from the Euler angles in degrees, then
+ * + center, exactly as that constructor builds it. */
+typedef struct ar_object_desc {
+    int32_t type;          /* AR_OBJ_*                                              */
+    ar_vec3 center;
+    ar_vec3 extent;        /* cube half-size; sphere radius = max component         */
+    ar_vec3 rotation_deg;  /* Euler (x, y, z) in degrees                            */
+    ar_material material;
+    ar_vertex tri[3];      /* AR_OBJ_TRIANGLE only, object space                    */
+    int32_t visible;       /* 0 = skipped by intersection (SceneObject::bVisible_)  */
+    int32_t reserved[3];
+} ar_object_desc;          /* 208 bytes */
+
+/* Pinhole camera of RenderCamera (core/scene.cu:201-230) with the field of view
+ * as a parameter instead of the hard-coded 60 degrees. */
+typedef struct ar_camera {
+    ar_vec3 position;
+    ar_vec3 direction;     /* need not be normalised */
+    float fov_y_deg;       /* reference: 60                                         */
+    int32_t width;
+    int32_t height;
+} ar_camera;
+
+/* Knobs the reference fixes at compile time (core/config.cuh). */
+typedef struct ar_render_params {
+    int32_t spp;           /* samples per pixel (frames of the offline Render loop)  */
+    int32_t max_depth;     /* MAX_TRACING_DEPTH (reference: 1000)                    */
+    int32_t rr_depth;      /* MIN_TRACING_DEPTH: RR from this non-delta depth (3)    */
+    int32_t use_nee;       /* SceneSetting::bUseNEE_                                 */
+    int32_t sky;           /* 1 = SkyLighting, 0 = DISABLE_SKYLIGHT                  */
+    int32_t frame_offset;  /* TOTAL_FRAME_INDEX of the first sample                  */
+    uint64_t seed;         /* GLOBAL_SEED (reference: 0x9e3779b97f4a7c15)            */
+    int32_t sort_rays;     /* 1 = sort extension rays by material/direction octant  */
+    int32_t wave_paths;    /* paths in flight per wave; 0 = automatic                */
+} ar_render_params;
+
+/* Per-path record of ar_render_debug_paths (one per pixel and sample). */
+#define AR_DEBUG_MAX_HITS 16
+typedef struct ar_path_record {
+    float radiance[3];     /* CalculateRadiance output before accumulation           */
+    int32_t segments;      /* loop iterations executed (Trace calls)                 */
+    int32_t uniforms;      /* curand_uniform values this path consumed               */
+    int32_t nee_rays;      /* shadow rays cast                                        */
+    int32_t reserved[2];
+    int32_t hit_object[AR_DEBUG_MAX_HITS]; /* closest-hit object per segment, -1 = miss */
+} ar_path_record;          /* 96 bytes */
+
+typedef struct ar_scene_info {
+    int64_t objects;
+    int64_t triangles;
+    int64_t lights;
+    int64_t wide_nodes;    /* 8-wide quantised BVH nodes                              */
+    int64_t prim_refs;     /* leaf primitive records                                  */
+    int64_t device_bytes;  /* bytes held on the device by the scene                   */
+    int32_t device;
+    int32_t camera_inside; /* reserved */
+} ar_scene_info;
+
+typedef struct ar_render_stats {
+    int64_t paths;         /* camera paths traced                                     */
+    int64_t extension_rays;/* closest-hit BVH queries                                 */
+    int64_t shadow_rays;   /* any-hit BVH queries                                     */
+    int64_t kernel_launches;
+    float   trace_ms;      /* device time of the traversal kernels (CUDA events)      */
+    float   total_ms;      /* device time of the whole render call                    */
+} ar_render_stats;
+
+typedef struct ar_scene ar_scene;
+
+/* Library ABI version (AR_ABI_VERSION). */
+int32_t ar_version(void);
+
+/* Message of the last error on the calling thread; "" when none.
+ * Replaces the printing CHECK_ERROR macro (core/vector.cuh:22-31). */
+const char* ar_get_last_error_string(void);
+
+/* Build a scene on `device`: world-space triangle records, SAH BVH collapsed to
+ * 8-wide quantised nodes, light table.  Replaces SceneRenderer::SceneRenderer
+ * (core/scene.hpp:113, core/scene.cu:1120-1156) together with the upload it
+ * defers to the first Render, UpdateSceneToDeviceIfDirty (core/scene.cu:1025-1118). */
+ar_status ar_scene_create(const ar_object_desc* objects, size_t count, int32_t device,
+                          ar_scene** out_scene);
+
+/* Release every device allocation of the scene (SceneRenderer::~SceneRenderer,
+ * core/scene.cu:1158-1163).  NULL is accepted. */
+void ar_scene_destroy(ar_scene* scene);
+
+ar_status ar_scene_get_info(const ar_scene* scene, ar_scene_info* info);
+
+/* Offline render: spp samples per pixel, FP64 accumulation, mean written as
+ * linear RGB float3 rows (index j*width+i).  Replaces
+ * std::vector<float3> SceneRenderer::Render(int2, float3, float3, int)
+ * (core/scene.hpp:126, core/scene.cu:276-306).
+ *   out_rgb   width*height*3 floats (may be NULL if accum is given)
+ *   accum     width*height*3 doubles holding running sums, or NULL; when given it
+ *             is ADDED to (resume/extend a render), never cleared
+ *   mem_kind  AR_MEM_HOST or AR_MEM_DEVICE for both buffers
+ *   stats     optional counters (NULL to skip)                                 */
+ar_status ar_render(ar_scene* scene, const ar_camera* camera, const ar_render_params* params,
+                    float* out_rgb, double* accum, int32_t mem_kind, void* stream,
+                    ar_render_stats* stats);
+
+/* Closest-hit (any_hit = 0) or any-hit (any_hit = 1) queries for n rays laid out
+ * as 8 floats each: origin.xyz, tmin, direction.xyz, tmax.  A hit is accepted
+ * when tmin <= t < tmax (intersection.cuh:160) and ties in t go to the lowest
+ * object index.  hit_t may be NULL.  Replaces intersection::TraverseBVH
+ * (core/render/intersection.cuh:235-370) as used by Trace and SegmentTrace. */
+ar_status ar_trace_rays(ar_scene* scene, const float* rays, size_t n, int32_t any_hit,
+                        int32_t* hit_object, float* hit_t, int32_t mem_kind, void* stream);
+
+/* Render spp samples and record every path (width*height*spp records, sample
+ * major: record[(s*height + j)*width + i]).  Debug/parity entry; same kernels
+ * as ar_render. */
+ar_status ar_render_debug_paths(ar_scene* scene, const ar_camera* camera,
+                                const ar_render_params* params, ar_path_record* records,
+                                int32_t mem_kind, void* stream);
+
+/* The first `per_path` uniforms of the random stream of every path of
+ * ar_render (curand XORWOW, seed params->seed, subsequence = the reference's
+ * block-linear pixel index of 8x4 blocks, offset = frame * 2^32;
+ * core/random.cuh:31-39).  out has spp*height*width*per_path floats, sample
+ * major.  Lets a CPU replay consume exactly the GPU's sample sequence. */
+ar_status ar_rng_tape(const ar_camera* camera, const ar_render_params* params, int32_t per_path,
+                      float* out, int32_t mem_kind, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APERTURE_B200_H */

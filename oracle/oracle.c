@@ -1,0 +1,1538 @@
+/*
+ * oracle.c -- CPU restatement of ApertureRendererV3's path-tracing hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see oracle.h).  Scalar C, IEEE single precision,
+ * compiled with -ffp-contract=off so that every a*b+c rounds twice, exactly
+ * like the reference's source expressions read and like the CUDA core built
+ * with --fmad=false.  Expression order follows the reference token by token;
+ * each function cites the reference lines it restates (paths relative to the
+ * reference's core/ directory).
+ *
+ * Deliberate, documented choices where the reference's exact arithmetic cannot
+ * be reproduced on two machines:
+ *   - sinf/cosf/sincosf/expf/logf/powf -> oracle_math.h (fixed definitions);
+ *   - rsqrtf(x) -> 1/sqrtf(x) (IEEE);
+ *   - INTERSECT_EPS(d) = 1e-3f * expf(min(d/2, 4)) -> 9-entry table of the same.
+ */
+#define _GNU_SOURCE
+#include "oracle.h"
+#include "oracle_math.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* float3 helpers (vector.cuh:127-262)                                       */
+/* ------------------------------------------------------------------------ */
+typedef struct { float x, y, z; } V3;
+typedef struct { V3 x, y, z; } M3; /* rows, float3x3 (vector.cuh:320-420) */
+
+static inline V3 v3(float x, float y, float z) { V3 r = {x, y, z}; return r; }
+static inline V3 vadd(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline V3 vsub(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline V3 vmul(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline V3 vscale(V3 a, float b) { return v3(a.x * b, a.y * b, a.z * b); }
+static inline V3 vdivs(V3 a, float b) { return v3(a.x / b, a.y / b, a.z / b); }
+static inline V3 vneg(V3 a) { return v3(-a.x, -a.y, -a.z); }
+static inline V3 vadds(V3 a, float b) { return v3(a.x + b, a.y + b, a.z + b); }
+static inline float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V3 cross3(V3 a, V3 b)
+{
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static inline float len3(V3 a) { return sqrtf(dot3(a, a)); }
+static inline V3 vmin3(V3 a, V3 b) { return v3(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)); }
+static inline V3 vmax3(V3 a, V3 b) { return v3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)); }
+static inline V3 vmaxs(V3 a, float b) { return v3(fmaxf(a.x, b), fmaxf(a.y, b), fmaxf(a.z, b)); }
+static inline float max3f(V3 a) { return fmaxf(a.x, fmaxf(a.y, a.z)); }
+static inline V3 vabs(V3 a) { return v3(fabsf(a.x), fabsf(a.y), fabsf(a.z)); }
+static inline int all_zero(V3 a) { return a.x == 0.0f && a.y == 0.0f && a.z == 0.0f; }
+
+/* vector.cuh:222-231 with rsqrtf -> 1/sqrtf */
+static inline V3 vnormalize(V3 v)
+{
+    const float l2 = dot3(v, v);
+    if (l2 <= 1e-20f) return v3(0.0f, 0.0f, 0.0f);
+    const float inv = om_rsqrtf(l2);
+    return vscale(v, inv);
+}
+static inline float clampf_(float v, float a, float b) { return isnan(v) ? 0.0f : fminf(fmaxf(v, a), b); }
+static inline float saturatef_(float v) { return isnan(v) ? 0.0f : fminf(fmaxf(v, 0.0f), 1.0f); }
+static inline float signf_(float a) { return a > 0.0f ? 1.0f : (a < 0.0f ? -1.0f : 0.0f); }
+static inline float lerpf_(float a, float b, float v) { return a * (1.0f - v) + b * v; }
+static inline V3 vlerp(V3 a, V3 b, float v) { return v3(lerpf_(a.x, b.x, v), lerpf_(a.y, b.y, v), lerpf_(a.z, b.z, v)); }
+static inline float luminance3(V3 c) { return dot3(c, v3(0.2126f, 0.7152f, 0.0722f)); }
+/* v - 2*dot(v,n)*n (vector.cuh:296-299) */
+static inline V3 vreflect(V3 v, V3 n) { return vsub(v, vscale(n, 2.0f * dot3(v, n))); }
+/* vector.cuh:254-262 */
+static inline V3 vrefract(V3 in, V3 normal, float eta)
+{
+    const V3 n = (dot3(normal, in) > 0.0f) ? vneg(normal) : normal;
+    const float cosI = -dot3(n, in);
+    const float k = 1.0f - (eta * eta) * fmaxf(0.0f, 1.0f - cosI * cosI);
+    const float cosT = sqrtf(fmaxf(0.0f, k));
+    return vadd(vscale(in, eta), vscale(n, eta * cosI - cosT));
+}
+static inline float inv_safe(float x) { return (x == 0.0f) ? (x >= 0 ? FLT_MAX : -FLT_MAX) : 1.0f / x; }
+static inline V3 mmul(const M3* m, V3 v) { return v3(dot3(m->x, v), dot3(m->y, v), dot3(m->z, v)); }
+static inline float fix_nan_inf(float x)
+{
+    if (isnan(x)) return 0.0f;
+    if (isinf(x)) return x > 0.0f ? 0.0f : -0.0f;
+    return x;
+}
+
+/* BuildTangentBasis (vector.cuh:264-269) */
+static inline void tangent_basis(V3 n, V3* t, V3* b)
+{
+    const V3 a = (fabsf(n.z) < 0.999f) ? v3(0.0f, 0.0f, 1.0f) : v3(1.0f, 0.0f, 0.0f);
+    *t = vnormalize(cross3(a, n));
+    *b = cross3(n, *t);
+}
+/* BuildTangentBasisRandom (vector.cuh:271-283) */
+static inline void tangent_basis_random(V3 n, V3* t, V3* b, float e)
+{
+    const V3 a = (fabsf(n.z) < 0.999f) ? v3(0.0f, 0.0f, 1.0f) : v3(1.0f, 0.0f, 0.0f);
+    const V3 t0 = vnormalize(cross3(a, n));
+    const V3 b0 = cross3(n, t0);
+    float s, c;
+    om_sincosf(e * 3.14159265358979f * 2.0f, &s, &c);
+    *t = vadd(vscale(t0, c), vscale(b0, s));
+    *b = vadd(vscale(t0, -s), vscale(b0, c));
+}
+
+#define OR_PI 3.14159265358979f /* CUDART_PI_F rounds to the same float */
+
+/* ------------------------------------------------------------------------ */
+/* Scene                                                                      */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int type, visible, light_index;
+    V3 center, extent;
+    M3 o2w, w2o;
+    ar_material mat;
+    V3 p0, p1, p2;        /* world-space triangle vertices */
+    V3 n0, n1, n2;        /* objectToWorld * vertex normal */
+    V3 bmin, bmax, pc;    /* PrimitiveProxy */
+} OObj;
+
+typedef struct { V3 bmin, bmax; int left, right, first, count; } ONode;
+
+struct or_scene {
+    int n;
+    OObj* o;
+    ONode* nodes;
+    int nn, cap;
+    int* idx;
+    int nl;
+    int* lobj;
+    float* lprob;
+    int flags;
+    int fallbacks;
+    float eps_tab[9];
+};
+
+/* float3x3::rotX/Y/Z and mul (vector.cuh:378-416), host libm as in the
+ * reference's SceneObject constructor (object.cuh:344-364). */
+static M3 mat_mul(const M3* a, const M3* m)
+{
+    const V3 c0 = v3(m->x.x, m->y.x, m->z.x);
+    const V3 c1 = v3(m->x.y, m->y.y, m->z.y);
+    const V3 c2 = v3(m->x.z, m->y.z, m->z.z);
+    M3 r;
+    r.x = v3(dot3(a->x, c0), dot3(a->x, c1), dot3(a->x, c2));
+    r.y = v3(dot3(a->y, c0), dot3(a->y, c1), dot3(a->y, c2));
+    r.z = v3(dot3(a->z, c0), dot3(a->z, c1), dot3(a->z, c2));
+    return r;
+}
+static void euler_to_matrix(V3 deg, M3* o2w, M3* w2o)
+{
+    const float k = 3.14159265358979f / 180.0f; /* deg2rad (vector.cuh:76-80) */
+    const float ax = deg.x * k, ay = deg.y * k, az = deg.z * k;
+    M3 rx, ry, rz;
+    float c = cosf(ax), s = sinf(ax);
+    rx.x = v3(1, 0, 0); rx.y = v3(0, c, -s); rx.z = v3(0, s, c);
+    c = cosf(ay); s = sinf(ay);
+    ry.x = v3(c, 0, s); ry.y = v3(0, 1, 0); ry.z = v3(-s, 0, c);
+    c = cosf(az); s = sinf(az);
+    rz.x = v3(c, -s, 0); rz.y = v3(s, c, 0); rz.z = v3(0, 0, 1);
+    const M3 yx = mat_mul(&ry, &rx);
+    *o2w = mat_mul(&rz, &yx);
+    w2o->x = v3(o2w->x.x, o2w->y.x, o2w->z.x);
+    w2o->y = v3(o2w->x.y, o2w->y.y, o2w->z.y);
+    w2o->z = v3(o2w->x.z, o2w->y.z, o2w->z.z);
+}
+
+static V3 from_ar(ar_vec3 a) { return v3(a.x, a.y, a.z); }
+
+/* SceneObject::GetArea (object.cuh:278-302) */
+static float object_area(const OObj* o, const ar_object_desc* d)
+{
+    if (o->type == AR_OBJ_CUBE || o->type == AR_OBJ_SDF) {
+        const float ex = fabsf(o->extent.x), ey = fabsf(o->extent.y), ez = fabsf(o->extent.z);
+        return 8.0f * (ex * ey + ex * ez + ey * ez);
+    } else if (o->type == AR_OBJ_SPHERE) {
+        const float r = fabsf(o->extent.x);
+        return 4.0f * OR_PI * r * r;
+    } else if (o->type == AR_OBJ_TRIANGLE) {
+        const V3 e1 = vsub(from_ar(d->tri[1].position), from_ar(d->tri[0].position));
+        const V3 e2 = vsub(from_ar(d->tri[2].position), from_ar(d->tri[0].position));
+        return 0.5f * len3(cross3(e1, e2));
+    }
+    return 0.0f;
+}
+
+/* SceneObject::UpdateProxy (object.cuh:309-342) */
+static void update_proxy(OObj* o, int object_center)
+{
+    o->pc = o->center;
+    if (o->type == AR_OBJ_CUBE || o->type == AR_OBJ_SDF) {
+        const V3 ax = mmul(&o->o2w, v3(1.0f, 0.0f, 0.0f));
+        const V3 ay = mmul(&o->o2w, v3(0.0f, 1.0f, 0.0f));
+        const V3 az = mmul(&o->o2w, v3(0.0f, 0.0f, 1.0f));
+        V3 h;
+        h.x = fabsf(ax.x) * o->extent.x + fabsf(ay.x) * o->extent.y + fabsf(az.x) * o->extent.z;
+        h.y = fabsf(ax.y) * o->extent.x + fabsf(ay.y) * o->extent.y + fabsf(az.y) * o->extent.z;
+        h.z = fabsf(ax.z) * o->extent.x + fabsf(ay.z) * o->extent.y + fabsf(az.z) * o->extent.z;
+        o->bmin = v3(o->center.x - h.x, o->center.y - h.y, o->center.z - h.z);
+        o->bmax = v3(o->center.x + h.x, o->center.y + h.y, o->center.z + h.z);
+    } else if (o->type == AR_OBJ_SPHERE) {
+        const float r = max3f(o->extent);
+        const V3 h = v3(r, r, r);
+        o->bmin = vsub(o->center, h);
+        o->bmax = vadd(o->center, h);
+    } else if (o->type == AR_OBJ_TRIANGLE) {
+        const V3 p0 = o->p0, p1 = o->p1, p2 = o->p2;
+        o->bmin = v3(fminf(fminf(p0.x, p1.x), p2.x), fminf(fminf(p0.y, p1.y), p2.y), fminf(fminf(p0.z, p1.z), p2.z));
+        o->bmax = v3(fmaxf(fmaxf(p0.x, p1.x), p2.x), fmaxf(fmaxf(p0.y, p1.y), p2.y), fmaxf(fmaxf(p0.z, p1.z), p2.z));
+        if (!object_center)
+            o->pc = v3(0.5f * (o->bmin.x + o->bmax.x), 0.5f * (o->bmin.y + o->bmax.y), 0.5f * (o->bmin.z + o->bmax.z));
+    } else {
+        o->bmin = o->center;
+        o->bmax = o->center;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* BuildBVH (bvh/bvh.cuh:142-422), 32-bit node layout                        */
+/* ------------------------------------------------------------------------ */
+static float aabb_area(V3 mn, V3 mx)
+{
+    const V3 d = v3(fmaxf(0.0f, mx.x - mn.x), fmaxf(0.0f, mx.y - mn.y), fmaxf(0.0f, mx.z - mn.z));
+    return 2.0f * (d.x * d.y + d.y * d.z + d.z * d.x);
+}
+static float axis_of(V3 v, int axis) { return axis == 0 ? v.x : (axis == 1 ? v.y : v.z); }
+
+typedef struct { or_scene* s; int leaf, bins; } BuildCtx;
+
+static int bin_of(const OObj* p, int axis, float cmin, float invW, int bins)
+{
+    const float key = axis_of(p->pc, axis);
+    int b = invW > 0.0f ? (int)((key - cmin) * invW) : 0;
+    b = (b < 0) ? 0 : (b >= bins ? bins - 1 : b);
+    return b;
+}
+
+static int cmp_key_axis;
+static const OObj* cmp_objs;
+static int cmp_idx_key(const void* a, const void* b)
+{
+    const int ia = *(const int*)a, ib = *(const int*)b;
+    const float ka = axis_of(cmp_objs[ia].pc, cmp_key_axis), kb = axis_of(cmp_objs[ib].pc, cmp_key_axis);
+    if (ka < kb) return -1;
+    if (ka > kb) return 1;
+    return (ia < ib) ? -1 : (ia > ib);
+}
+
+static int new_node(or_scene* s)
+{
+    if (s->nn == s->cap) {
+        s->cap = s->cap ? 2 * s->cap : 1024;
+        s->nodes = (ONode*)realloc(s->nodes, (size_t)s->cap * sizeof(ONode));
+    }
+    memset(&s->nodes[s->nn], 0, sizeof(ONode));
+    return s->nn++;
+}
+
+static void make_leaf(ONode* node, int start, int count)
+{
+    node->left = -1; node->right = -1; node->first = start; node->count = count;
+}
+
+static int build_rec(BuildCtx* c, int start, int end)
+{
+    or_scene* s = c->s;
+    const int count = end - start;
+    const int ni = new_node(s);
+    V3 bmin = v3(FLT_MAX, FLT_MAX, FLT_MAX), bmax = v3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+    V3 cmin = bmin, cmax = bmax;
+    for (int i = start; i < end; ++i) {
+        const OObj* p = &s->o[s->idx[i]];
+        bmin = vmin3(bmin, p->bmin); bmax = vmax3(bmax, p->bmax);
+        cmin = vmin3(cmin, p->pc); cmax = vmax3(cmax, p->pc);
+    }
+    s->nodes[ni].bmin = bmin; s->nodes[ni].bmax = bmax;
+    if (count <= c->leaf) { make_leaf(&s->nodes[ni], start, count); return ni; }
+    const V3 ce = v3(cmax.x - cmin.x, cmax.y - cmin.y, cmax.z - cmin.z);
+    int axis = 0;
+    if (ce.y > ce.x && ce.y >= ce.z) axis = 1;
+    else if (ce.z > ce.x && ce.z >= ce.y) axis = 2;
+    if (ce.x <= 1e-6f && ce.y <= 1e-6f && ce.z <= 1e-6f) { make_leaf(&s->nodes[ni], start, count); return ni; }
+    const float cminA = axis_of(cmin, axis), cmaxA = axis_of(cmax, axis);
+    const int B = c->bins;
+    const float invW = (cmaxA > cminA) ? (float)B / (cmaxA - cminA) : 0.0f;
+    V3 binMin[64], binMax[64];
+    int binCount[64];
+    float leftArea[64], rightArea[64];
+    int leftCount[64], rightCount[64];
+    for (int b = 0; b < B; ++b) {
+        binMin[b] = v3(FLT_MAX, FLT_MAX, FLT_MAX); binMax[b] = v3(-FLT_MAX, -FLT_MAX, -FLT_MAX); binCount[b] = 0;
+    }
+    for (int i = start; i < end; ++i) {
+        const OObj* p = &s->o[s->idx[i]];
+        const int b = bin_of(p, axis, cminA, invW, B);
+        binMin[b] = vmin3(binMin[b], p->bmin); binMax[b] = vmax3(binMax[b], p->bmax); binCount[b]++;
+    }
+    V3 rmin = v3(FLT_MAX, FLT_MAX, FLT_MAX), rmax = v3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+    int run = 0;
+    for (int b = 0; b < B; ++b) {
+        if (binCount[b] > 0) { rmin = vmin3(rmin, binMin[b]); rmax = vmax3(rmax, binMax[b]); }
+        run += binCount[b];
+        leftArea[b] = (run > 0) ? aabb_area(rmin, rmax) : 0.0f;
+        leftCount[b] = run;
+    }
+    rmin = v3(FLT_MAX, FLT_MAX, FLT_MAX); rmax = v3(-FLT_MAX, -FLT_MAX, -FLT_MAX); run = 0;
+    for (int b = B - 1; b >= 0; --b) {
+        if (binCount[b] > 0) { rmin = vmin3(rmin, binMin[b]); rmax = vmax3(rmax, binMax[b]); }
+        run += binCount[b];
+        rightArea[b] = (run > 0) ? aabb_area(rmin, rmax) : 0.0f;
+        rightCount[b] = run;
+    }
+    const float parentArea = aabb_area(bmin, bmax);
+    float bestCost = FLT_MAX;
+    int bestSplit = -1;
+    for (int b = 0; b < B - 1; ++b) {
+        const int nl = leftCount[b], nr = rightCount[b + 1];
+        if (nl == 0 || nr == 0) continue;
+        const float sah = 1.0f + (leftArea[b] * (float)nl + rightArea[b + 1] * (float)nr) / fmaxf(parentArea, 1e-20f) * 1.0f;
+        if (sah < bestCost) { bestCost = sah; bestSplit = b; }
+    }
+    int mid = -1;
+    if (bestSplit >= 0) {
+        /* std::partition on a random-access range: the classic two-pointer
+         * (Hoare) scheme -- advance from the front past elements that satisfy
+         * the predicate, retreat from the back past those that do not, swap. */
+        int* first = s->idx + start;
+        int* last = s->idx + end;
+        for (;;) {
+            for (;;) {
+                if (first == last) goto done;
+                if (bin_of(&s->o[*first], axis, cminA, invW, B) <= bestSplit) ++first; else break;
+            }
+            --last;
+            for (;;) {
+                if (first == last) goto done;
+                if (!(bin_of(&s->o[*last], axis, cminA, invW, B) <= bestSplit)) --last; else break;
+            }
+            { const int t = *first; *first = *last; *last = t; }
+            ++first;
+        }
+    done:
+        mid = (int)(first - s->idx);
+        if (mid == start || mid == end) bestSplit = -1;
+    }
+    if (bestSplit < 0) {
+        /* Median fallback (bvh.cuh:357-392).  The reference uses
+         * std::nth_element, whose placement of the other elements is
+         * implementation defined; this restatement sorts instead and counts the
+         * event so that pinned scenes can assert it never happens. */
+        s->fallbacks++;
+        const int m = start + count / 2;
+        cmp_key_axis = axis; cmp_objs = s->o;
+        qsort(s->idx + start, (size_t)count, sizeof(int), cmp_idx_key);
+        mid = m;
+        if (mid == start || mid == end) { make_leaf(&s->nodes[ni], start, count); return ni; }
+    }
+    const int l = build_rec(c, start, mid);
+    const int r = build_rec(c, mid, end);
+    s->nodes[ni].left = l; s->nodes[ni].right = r; s->nodes[ni].first = -1; s->nodes[ni].count = 0;
+    return ni;
+}
+
+or_scene* or_scene_create(const ar_object_desc* objects, size_t count, int flags, int leaf_size, int bin_count)
+{
+    or_scene* s = (or_scene*)calloc(1, sizeof(or_scene));
+    s->n = (int)count;
+    s->flags = flags;
+    s->o = (OObj*)calloc(count ? count : 1, sizeof(OObj));
+    for (int d = 0; d <= 8; ++d)   /* INTERSECT_EPS (config.cuh:3) */
+        s->eps_tab[d] = 1.0e-3f * om_expf(fminf((float)d * 0.5f, 4.0f));
+    for (size_t i = 0; i < count; ++i) {
+        const ar_object_desc* d = &objects[i];
+        OObj* o = &s->o[i];
+        o->type = d->type;
+        o->visible = d->visible;
+        o->center = from_ar(d->center);
+        o->extent = vabs(from_ar(d->extent));
+        o->mat = d->material;
+        euler_to_matrix(from_ar(d->rotation_deg), &o->o2w, &o->w2o);
+        if (o->type == AR_OBJ_TRIANGLE) {
+            /* intersection.cuh:27-29 and 75-77 */
+            o->p0 = vadd(mmul(&o->o2w, from_ar(d->tri[0].position)), o->center);
+            o->p1 = vadd(mmul(&o->o2w, from_ar(d->tri[1].position)), o->center);
+            o->p2 = vadd(mmul(&o->o2w, from_ar(d->tri[2].position)), o->center);
+            o->n0 = mmul(&o->o2w, from_ar(d->tri[0].normal));
+            o->n1 = mmul(&o->o2w, from_ar(d->tri[1].normal));
+            o->n2 = mmul(&o->o2w, from_ar(d->tri[2].normal));
+        }
+        update_proxy(o, (flags & OR_PROXY_OBJECT_CENTER) != 0);
+    }
+    /* BuildBVH */
+    if (leaf_size <= 0) leaf_size = 8;
+    if (bin_count <= 0) bin_count = 12;
+    BuildCtx c;
+    c.s = s;
+    c.bins = bin_count < 4 ? 4 : (bin_count > 64 ? 64 : bin_count);
+    c.leaf = leaf_size < 1 ? 1 : (leaf_size > 16 ? 16 : leaf_size);
+    s->idx = (int*)malloc((count ? count : 1) * sizeof(int));
+    for (size_t i = 0; i < count; ++i) s->idx[i] = (int)i;
+    if (count > 0) build_rec(&c, 0, (int)count);
+    /* Light table (scene.cu:1056-1080) */
+    s->lobj = (int*)malloc((count ? count : 1) * sizeof(int));
+    s->lprob = (float*)malloc((count ? count : 1) * sizeof(float));
+    float total = 0.0f;
+    for (size_t i = 0; i < count; ++i) {
+        OObj* o = &s->o[i];
+        if (o->mat.shading_model == AR_MAT_LIGHT) {
+            o->light_index = s->nl;
+            const float w = fmaxf(object_area(o, &objects[i]) * luminance3(from_ar(o->mat.emissive)), 1.0e-20f);
+            s->lobj[s->nl] = (int)i;
+            s->lprob[s->nl] = w;
+            total += w;
+            s->nl++;
+        } else {
+            o->light_index = -1;
+        }
+    }
+    for (int l = 0; l < s->nl; ++l) s->lprob[l] = s->lprob[l] / total;
+    return s;
+}
+
+void or_scene_destroy(or_scene* s)
+{
+    if (!s) return;
+    free(s->o); free(s->nodes); free(s->idx); free(s->lobj); free(s->lprob); free(s);
+}
+
+int64_t or_scene_node_count(const or_scene* s) { return s->nn; }
+void or_scene_nodes(const or_scene* s, float* b6, int32_t* l4)
+{
+    for (int i = 0; i < s->nn; ++i) {
+        const ONode* n = &s->nodes[i];
+        b6[6 * i + 0] = n->bmin.x; b6[6 * i + 1] = n->bmin.y; b6[6 * i + 2] = n->bmin.z;
+        b6[6 * i + 3] = n->bmax.x; b6[6 * i + 4] = n->bmax.y; b6[6 * i + 5] = n->bmax.z;
+        l4[4 * i + 0] = n->left; l4[4 * i + 1] = n->right; l4[4 * i + 2] = n->first; l4[4 * i + 3] = n->count;
+    }
+}
+void or_scene_indices(const or_scene* s, int32_t* idx) { memcpy(idx, s->idx, (size_t)s->n * sizeof(int32_t)); }
+int64_t or_scene_light_count(const or_scene* s) { return s->nl; }
+void or_scene_lights(const or_scene* s, int32_t* obj, float* prob)
+{
+    for (int l = 0; l < s->nl; ++l) { obj[l] = s->lobj[l]; prob[l] = s->lprob[l]; }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Intersection (intersection.cuh:15-113, object/aabb.cuh, object/sphere.cuh) */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int hit, obj, light;
+    float dist;
+    V3 pos, nrm;
+    int inside;
+    /* GBuffer fields used by shading */
+    V3 albedo, emissive;
+    float specular, metallic, roughness, ior, sigma_a;
+} Isect;
+
+static void gbuffer_default(Isect* c)
+{
+    c->albedo = v3(1.0f, 1.0f, 1.0f); c->emissive = v3(0.0f, 0.0f, 0.0f);
+    c->specular = 0.0f; c->metallic = 0.0f; c->roughness = 0.0f; c->ior = 1.5f; c->sigma_a = 100.0f;
+}
+static void gbuffer_material(Isect* c, const ar_material* m)
+{
+    c->albedo = from_ar(m->albedo); c->emissive = from_ar(m->emissive);
+    c->specular = m->specular; c->metallic = m->metallic; c->roughness = m->roughness;
+    c->ior = m->ior; c->sigma_a = m->sigma_a;
+}
+
+/* IntersectTriangleObject (intersection.cuh:15-89); world vertices precomputed
+ * with the same expression as lines 27-29. */
+static int isect_triangle(const or_scene* s, const OObj* o, V3 ro, V3 rd, Isect* out)
+{
+    if (!o->visible) return 0;
+    const V3 e1 = vsub(o->p1, o->p0);
+    const V3 e2 = vsub(o->p2, o->p0);
+    const V3 h = cross3(rd, e2);
+    const float a = dot3(e1, h);
+    if (a > -1e-6f && a < 1e-6f) return 0;
+    const float f = 1.0f / a;
+    const V3 sv = vsub(ro, o->p0);
+    const float u = f * dot3(sv, h);
+    if (u < 0.0f || u > 1.0f) return 0;
+    const V3 q = cross3(sv, e1);
+    const float v = f * dot3(rd, q);
+    if (v < 0.0f || u + v > 1.0f) return 0;
+    const float t = f * dot3(e2, q);
+    if (!(t > 1e-5f)) return 0;
+    out->hit = 1;
+    out->dist = t;
+    if (out->obj != -2) { /* -2: caller wants only t */
+        out->pos = vadd(ro, vscale(rd, t));
+        const float w = 1.0f - u - v;
+        const V3 ni = vnormalize(vadd(vadd(vscale(o->n0, w), vscale(o->n1, u)), vscale(o->n2, v)));
+        out->inside = dot3(rd, ni) > 0.0f;
+        out->nrm = out->inside ? vneg(ni) : ni;
+        if (s->flags & OR_TRIANGLE_DEFAULT_GBUFFER) gbuffer_default(out); else gbuffer_material(out, &o->mat);
+    }
+    return 1;
+}
+
+/* IntersectAABBObject (object/aabb.cuh:9-89) */
+static int isect_cube(const OObj* o, V3 ro, V3 rd, Isect* out)
+{
+    const V3 lo = mmul(&o->w2o, vsub(ro, o->center));
+    const V3 ld = vnormalize(mmul(&o->w2o, rd));
+    const V3 bmin = vneg(o->extent), bmax = o->extent;
+    const V3 dv = v3(inv_safe(ld.x), inv_safe(ld.y), inv_safe(ld.z));
+    const V3 t1 = vmul(vsub(bmin, lo), dv);
+    const V3 t2 = vmul(vsub(bmax, lo), dv);
+    const V3 tmn = vmin3(t1, t2), tmx = vmax3(t1, t2);
+    const float tEnter = fmaxf(fmaxf(tmn.x, tmn.y), tmn.z);
+    const float tExit = fminf(fminf(tmx.x, tmx.y), tmx.z);
+    if (tEnter > tExit) return 0;
+    if (tExit <= 0.0f) return 0;
+    const int inside = (tEnter < 0.0f);
+    const float tHit = inside ? tExit : tEnter;
+    out->hit = 1;
+    out->dist = tHit;
+    if (out->obj != -2) {
+        const V3 lp = vadd(lo, vscale(ld, tHit));
+        out->pos = vadd(mmul(&o->o2w, lp), o->center);
+        const float rx = fabsf(lp.x) / o->extent.x;
+        const float ry = fabsf(lp.y) / o->extent.y;
+        const float rz = fabsf(lp.z) / o->extent.z;
+        V3 ln;
+        if (rx >= ry && rx >= rz) ln = v3((lp.x > 0.0f) ? 1.0f : -1.0f, 0.0f, 0.0f);
+        else if (ry >= rz) ln = v3(0.0f, (lp.y > 0.0f) ? 1.0f : -1.0f, 0.0f);
+        else ln = v3(0.0f, 0.0f, (lp.z > 0.0f) ? 1.0f : -1.0f);
+        if (inside) ln = vneg(ln);
+        out->nrm = vnormalize(mmul(&o->o2w, ln));
+        out->inside = 0;
+        gbuffer_material(out, &o->mat);
+    }
+    return 1;
+}
+
+/* IntersectSphereObject (object/sphere.cuh:9-70) */
+static int isect_sphere(const OObj* o, V3 ro, V3 rd, Isect* out)
+{
+    const V3 lo = mmul(&o->w2o, vsub(ro, o->center));
+    const V3 ld = vnormalize(mmul(&o->w2o, rd));
+    const float r = max3f(o->extent);
+    const float b = dot3(lo, ld);
+    const float c = dot3(lo, lo) - r * r;
+    const float disc = b * b - 1.0f * c;
+    if (disc < 0.0f) return 0;
+    const float sq = sqrtf(disc);
+    float t = -b - sq;
+    int inside = 0;
+    if (t <= 0.0f) { t = -b + sq; inside = 1; }
+    if (t <= 0.0f) return 0;
+    out->hit = 1;
+    out->dist = t;
+    if (out->obj != -2) {
+        const V3 lp = vadd(lo, vscale(ld, t));
+        const V3 ln = vscale(vnormalize(lp), inside ? -1.0f : 1.0f);
+        out->pos = vadd(mmul(&o->o2w, lp), o->center);
+        out->nrm = vnormalize(mmul(&o->o2w, ln));
+        out->inside = 0;
+        gbuffer_material(out, &o->mat);
+    }
+    return 1;
+}
+
+/* IntersectBase (intersection.cuh:93-113).  SDF objects are not part of this
+ * restatement; they never hit. */
+static int isect_object(const or_scene* s, int i, V3 ro, V3 rd, Isect* out)
+{
+    const OObj* o = &s->o[i];
+    switch (o->type) {
+    case AR_OBJ_CUBE: return isect_cube(o, ro, rd, out);
+    case AR_OBJ_SPHERE: return isect_sphere(o, ro, rd, out);
+    case AR_OBJ_TRIANGLE: return isect_triangle(s, o, ro, rd, out);
+    default: return 0;
+    }
+}
+
+/* distance of a hit only (same arithmetic) */
+static int isect_t(const or_scene* s, int i, V3 ro, V3 rd, float* t)
+{
+    Isect c;
+    c.hit = 0; c.obj = -2;
+    if (!isect_object(s, i, ro, rd, &c)) return 0;
+    *t = c.dist;
+    return 1;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Traversal (intersection.cuh:235-370, bvh.cuh:424-470)                      */
+/* ------------------------------------------------------------------------ */
+static inline int slab_ref(V3 ro, V3 inv, V3 mn, V3 mx, float tMin, float tMax, float* tEnterOut)
+{
+    float t0 = (mn.x - ro.x) * inv.x, t1 = (mx.x - ro.x) * inv.x;
+    float te = fminf(t0, t1), tx = fmaxf(t0, t1);
+    t0 = (mn.y - ro.y) * inv.y; t1 = (mx.y - ro.y) * inv.y;
+    te = fmaxf(te, fminf(t0, t1)); tx = fminf(tx, fmaxf(t0, t1));
+    t0 = (mn.z - ro.z) * inv.z; t1 = (mx.z - ro.z) * inv.z;
+    te = fmaxf(te, fminf(t0, t1)); tx = fminf(tx, fmaxf(t0, t1));
+    if (tx >= fmaxf(0.0f, tMin) && te <= tMax) { *tEnterOut = te; return 1; }
+    return 0;
+}
+static inline int slab_std(V3 ro, V3 inv, V3 mn, V3 mx, float tMin, float tMax, float* tEnterOut)
+{
+    float t0 = (mn.x - ro.x) * inv.x, t1 = (mx.x - ro.x) * inv.x;
+    float te = fminf(t0, t1), tx = fmaxf(t0, t1);
+    t0 = (mn.y - ro.y) * inv.y; t1 = (mx.y - ro.y) * inv.y;
+    te = fmaxf(te, fminf(t0, t1)); tx = fminf(tx, fmaxf(t0, t1));
+    t0 = (mn.z - ro.z) * inv.z; t1 = (mx.z - ro.z) * inv.z;
+    te = fmaxf(te, fminf(t0, t1)); tx = fminf(tx, fmaxf(t0, t1));
+    te = fmaxf(te, fmaxf(0.0f, tMin));
+    tx = fminf(tx * 1.0000004f, tMax);
+    if (te <= tx) { *tEnterOut = te; return 1; }
+    return 0;
+}
+
+typedef struct { int obj; float t; int visits, tests; } TraceResult;
+
+static TraceResult traverse(const or_scene* s, V3 ro, V3 rd, float tMin, float tMax, int any, int mode)
+{
+    TraceResult r;
+    r.obj = -1; r.t = tMax; r.visits = 0; r.tests = 0;
+    if (s->nn == 0) return r;
+    const int tie_lowest = (mode & OR_TIE_LOWEST_INDEX) != 0;
+    const int std_slab = (mode & OR_SLAB_STANDARD) != 0;
+    int stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    const V3 inv = v3(inv_safe(rd.x), inv_safe(rd.y), inv_safe(rd.z));
+    while (sp) {
+        const ONode* n = &s->nodes[stack[--sp]];
+        r.visits++;
+        float te;
+        const int ok = std_slab ? slab_std(ro, inv, n->bmin, n->bmax, tMin, r.t, &te)
+                                : slab_ref(ro, inv, n->bmin, n->bmax, tMin, r.t, &te);
+        if (!ok) continue;
+        if (n->count > 0) {
+            for (int i = 0; i < n->count; ++i) {
+                const int oi = s->idx[n->first + i];
+                float t;
+                r.tests++;
+                if (!isect_t(s, oi, ro, rd, &t)) continue;
+                if (t < tMin) continue;
+                if (t < r.t || (tie_lowest && r.obj >= 0 && t == r.t && oi < r.obj)) {
+                    r.t = t; r.obj = oi;
+                    if (any) return r;
+                }
+            }
+        } else {
+            const ONode* L = &s->nodes[n->left];
+            const ONode* R = &s->nodes[n->right];
+            float tL = 0.0f, tR = 0.0f;
+            const int hL = std_slab ? slab_std(ro, inv, L->bmin, L->bmax, tMin, r.t, &tL)
+                                    : slab_ref(ro, inv, L->bmin, L->bmax, tMin, r.t, &tL);
+            const int hR = std_slab ? slab_std(ro, inv, R->bmin, R->bmax, tMin, r.t, &tR)
+                                    : slab_ref(ro, inv, R->bmin, R->bmax, tMin, r.t, &tR);
+            if (hL && hR) {
+                if (tL > tR) { if (sp < 128) stack[sp++] = n->left; if (sp < 128) stack[sp++] = n->right; }
+                else { if (sp < 128) stack[sp++] = n->right; if (sp < 128) stack[sp++] = n->left; }
+            } else if (hL) { if (sp < 128) stack[sp++] = n->left; }
+            else if (hR) { if (sp < 128) stack[sp++] = n->right; }
+        }
+    }
+    return r;
+}
+
+static TraceResult brute(const or_scene* s, V3 ro, V3 rd, float tMin, float tMax, int any)
+{
+    TraceResult r;
+    r.obj = -1; r.t = tMax; r.visits = 0; r.tests = 0;
+    for (int i = 0; i < s->n; ++i) {
+        float t;
+        if (!isect_t(s, i, ro, rd, &t)) continue;
+        if (t < tMin || t >= r.t) continue;
+        r.t = t; r.obj = i;
+        if (any) return r;
+    }
+    return r;
+}
+
+void or_trace_rays(const or_scene* s, const float* rays, int64_t n, int any_hit, int mode,
+                   int32_t* hit_object, float* hit_t, int32_t* node_visits, int32_t* prim_tests, int threads)
+{
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 256)
+#endif
+    for (int64_t i = 0; i < n; ++i) {
+        const float* q = rays + 8 * i;
+        const TraceResult r = traverse(s, v3(q[0], q[1], q[2]), v3(q[4], q[5], q[6]), q[3], q[7], any_hit, mode);
+        hit_object[i] = r.obj;
+        if (hit_t) hit_t[i] = r.obj >= 0 ? r.t : q[7];
+        if (node_visits) node_visits[i] = r.visits;
+        if (prim_tests) prim_tests[i] = r.tests;
+    }
+}
+
+void or_trace_rays_brute(const or_scene* s, const float* rays, int64_t n, int any_hit,
+                         int32_t* hit_object, float* hit_t, int threads)
+{
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+    for (int64_t i = 0; i < n; ++i) {
+        const float* q = rays + 8 * i;
+        const TraceResult r = brute(s, v3(q[0], q[1], q[2]), v3(q[4], q[5], q[6]), q[3], q[7], any_hit);
+        hit_object[i] = r.obj;
+        if (hit_t) hit_t[i] = r.obj >= 0 ? r.t : q[7];
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Random numbers: a tape of curand uniforms, or an own generator             */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    const float* tape;
+    int limit, pos, overflow;
+    uint64_t state; /* own generator when tape == NULL */
+} Rng;
+
+static inline float rng1(Rng* g)
+{
+    if (g->tape) {
+        if (g->pos >= g->limit) { g->overflow = 1; g->pos++; return 0.5f; }
+        return g->tape[g->pos++];
+    }
+    /* splitmix64 -> uniform in (0, 1] (for the CPU baseline only) */
+    uint64_t z = (g->state += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z = z ^ (z >> 31);
+    g->pos++;
+    return (float)((z >> 40) + 1) * 0x1p-24f;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Sampling and BSDFs (render/sample.cuh, render/brdf.cuh, render/material.cuh) */
+/* ------------------------------------------------------------------------ */
+typedef struct { V3 dir; float pdf; } Smp;
+
+/* ConcentricSampleDisk (sample.cuh:63-86) */
+static void concentric_disk(float ux, float uy, float* dx, float* dy)
+{
+    const float sx = 2.0f * ux - 1.0f;
+    const float sy = 2.0f * uy - 1.0f;
+    if (sx == 0.0f && sy == 0.0f) { *dx = 0.0f; *dy = 0.0f; return; }
+    float r, phi;
+    if (fabsf(sx) > fabsf(sy)) {
+        r = sx;
+        phi = (OR_PI / 4.0f) * (sy / fmaxf(fabsf(sx), 1e-20f));
+    } else {
+        r = sy;
+        phi = (OR_PI / 2.0f) - (OR_PI / 4.0f) * (sx / fmaxf(fabsf(sy), 1e-20f));
+    }
+    float sn, cs;
+    om_sincosf(phi, &sn, &cs);
+    *dx = r * cs; *dy = r * sn;
+}
+
+/* SampleCosineWeightedHemisphere (sample.cuh:88-108) */
+static Smp sample_cosine(float e0, float e1, float e2, V3 n)
+{
+    V3 T, Bv;
+    tangent_basis_random(n, &T, &Bv, e2);
+    float x, y;
+    concentric_disk(e0, e1, &x, &y);
+    const float z = sqrtf(fmaxf(0.0f, 1.0f - x * x - y * y));
+    const V3 dir = vadd(vadd(vscale(T, x), vscale(Bv, y)), vscale(n, z));
+    Smp s;
+    s.pdf = z / OR_PI;
+    s.dir = vnormalize(dir);
+    return s;
+}
+
+/* FresnelDielectricExact (brdf.cuh:25-32) */
+static float fresnel_exact(float cosI, float cosT, float eta)
+{
+    const float invE = 1.0f / eta;
+    const float rPar = (invE * cosI - cosT) / (invE * cosI + cosT);
+    const float rPerp = (cosI - invE * cosT) / (cosI + invE * cosT);
+    return 0.5f * (rPar * rPar + rPerp * rPerp);
+}
+static V3 fresnel_schlick3(V3 F0, float cosX)
+{
+    const float c = clampf_(1.0f - cosX, 0.0f, 1.0f);
+    const float c5 = c * c * c * c * c;
+    return v3(F0.x + (1.0f - F0.x) * c5, F0.y + (1.0f - F0.y) * c5, F0.z + (1.0f - F0.z) * c5);
+}
+static float ggx_g_correlated(float alpha, float NoL, float NoV)
+{
+    const float a2 = alpha * alpha;
+    const float gv = NoL * sqrtf(a2 + (1.0f - a2) * NoV * NoV);
+    const float gl = NoV * sqrtf(a2 + (1.0f - a2) * NoL * NoL);
+    const float denom = gv + gl;
+    return (denom > 0.0f) ? (2.0f * NoL * NoV) / denom : 0.0f;
+}
+static float f0_ue(float spec) { const float s = clampf_(spec, 0.0f, 1.0f); return 0.08f * s; }
+static float ggx_d(float alpha, float NoH)
+{
+    const float a2 = alpha * alpha;
+    const float d = NoH * NoH * (a2 - 1.0f) + 1.0f;
+    return a2 / fmaxf(OR_PI * d * d, 1e-12f);
+}
+/* GGXLambert_BRDF (brdf.cuh:96-112) */
+static V3 ggx_lambert(V3 V, V3 L, V3 N, V3 F0, float NoV, float kD, float alpha, V3 albedo)
+{
+    const float NoL = fmaxf(0.0f, dot3(N, L));
+    const V3 Hn = vnormalize(vadd(V, L));
+    const float NoH = fmaxf(0.0f, dot3(N, Hn));
+    const float LoH = fmaxf(0.0f, dot3(L, Hn));
+    const V3 F = fresnel_schlick3(F0, LoH);
+    const float D = ggx_d(alpha, NoH);
+    const float G = ggx_g_correlated(alpha, NoL, NoV);
+    V3 spec;
+    if (NoL > 0.0f) spec = vdivs(vscale(vscale(F, D), G), fmaxf(4.0f * NoV, 1e-7f));
+    else spec = v3(0.0f, 0.0f, 0.0f);
+    const V3 omF = v3(1.0f - F.x, 1.0f - F.y, 1.0f - F.z);
+    const V3 diff = vscale(vmul(vscale(omF, kD), albedo), NoL / OR_PI);
+    return vadd(spec, diff);
+}
+/* SampleGGXBoundedVNDF (sample.cuh:179-222) */
+static Smp sample_ggx_vndf(V3 V, V3 N, float alpha, float r0, float r1, float r2)
+{
+    V3 X, Y;
+    tangent_basis_random(N, &X, &Y, r2);
+    const float XoV = dot3(X, V), YoV = dot3(Y, V), NoV = dot3(N, V);
+    const V3 localV = v3(XoV, YoV, NoV);
+    const float NoV2 = fminf(1.0f, NoV * NoV);
+    const float a2 = alpha * alpha;
+    const V3 lstd = vdivs(v3(XoV * alpha, YoV * alpha, NoV), sqrtf(a2 + (1.0f - a2) * NoV2));
+    const float phi = 2.0f * OR_PI * r0;
+    const float sv = 1.0f + sqrtf(1.0f - NoV2);
+    const float s2 = sv * sv;
+    const float k = (1.0f - a2) * s2 / (s2 + a2 * NoV2);
+    const float b = NoV > 0 ? k * lstd.z : lstd.z;
+    const float z = fmaf(1.0f - r1, 1.0f + b, -b);
+    const float sinT = sqrtf(saturatef_(1.0f - z * z));
+    float sp, cp;
+    om_sincosf(phi, &sp, &cp);
+    const V3 ostd = v3(sinT * cp, sinT * sp, z);
+    const V3 mstd = vadd(lstd, ostd);
+    const V3 lh = vnormalize(v3(mstd.x * alpha, mstd.y * alpha, mstd.z));
+    const V3 ll = vreflect(vneg(localV), lh);
+    const V3 dir = vadd(vadd(vscale(X, ll.x), vscale(Y, ll.y)), vscale(N, ll.z));
+    const float ndf = ggx_d(alpha, lh.z);
+    const float len2 = (1.0f - NoV2) * a2;
+    const float t = sqrtf(len2 + NoV2);
+    Smp s;
+    s.dir = dir;
+    s.pdf = ndf / (2.0f * (k * NoV + t));
+    return s;
+}
+/* GGXBoundedVNDF_PDF (sample.cuh:224-248) */
+static float ggx_vndf_pdf(V3 V, V3 N, V3 L, float alpha)
+{
+    const float NoV = dot3(N, V), NoL = dot3(N, L);
+    if (NoV <= 0.0f || NoL <= 0.0f) return 0.0f;
+    const V3 H = vnormalize(vadd(V, L));
+    const float NoV2 = fminf(1.0f, NoV * NoV);
+    const float a2 = alpha * alpha;
+    const float sv = 1.0f + sqrtf(1.0f - NoV2);
+    const float s2 = sv * sv;
+    const float k = (1.0f - a2) * s2 / (s2 + a2 * NoV2);
+    const float NoH = fmaxf(0.0f, dot3(N, H));
+    const float ndf = ggx_d(alpha, NoH);
+    const float len2 = (1.0f - NoV2) * a2;
+    const float t = sqrtf(len2 + NoV2);
+    const float pdf = ndf / (2.0f * (k * NoV + t));
+    return fmaxf(pdf, 1e-12f);
+}
+
+typedef struct { int inside; V3 vloc; int obj; int depth; } Media; /* MediaContext (material.cuh:12-18) */
+typedef struct {
+    V3 next; float pdf; V3 emis; V3 brdf;
+    int terminate, pure_light, delta, miss_thin;
+    Media media;
+} SCtx; /* SampleContext (material.cuh:19-37) */
+
+static void sctx_init(SCtx* c)
+{
+    memset(c, 0, sizeof(*c));
+    c->pdf = 1.0f;
+    c->media.obj = -1;
+}
+
+static V3 bsdf_ggx_params(const Isect* g, float* alpha, float* kD, V3* F0)
+{
+    *alpha = g->roughness * g->roughness;
+    const float f0d = f0_ue(g->specular);
+    *F0 = vlerp(v3(f0d, f0d, f0d), g->albedo, g->metallic);
+    *kD = 1.0f - g->metallic;
+    return *F0;
+}
+
+/* EvaluateBSDFWithCos, RGB (material.cuh:48-175) */
+static V3 eval_bsdf_cos(int model, V3 rayDir, V3 L, const Isect* ic, const Media* m)
+{
+    const V3 N = ic->nrm;
+    const float NoL = fmaxf(0.0f, dot3(N, L));
+    if (model == AR_MAT_DIFFUSE) return vscale(ic->albedo, NoL / OR_PI);
+    if (model == AR_MAT_LIGHT) return v3(0.0f, 0.0f, 0.0f);
+    if (model == AR_MAT_GGX) {
+        const V3 V = vnormalize(vneg(rayDir));
+        const float NoV = fmaxf(0.0f, dot3(N, V));
+        if (NoV <= 0.0f || NoL <= 0.0f) return v3(0.0f, 0.0f, 0.0f);
+        float alpha, kD; V3 F0;
+        bsdf_ggx_params(ic, &alpha, &kD, &F0);
+        return ggx_lambert(V, L, N, F0, NoV, kD, alpha, ic->albedo);
+    }
+    if (model == AR_MAT_GLASS) {
+        const float IOR = ic->ior;
+        V3 tr = v3(1.0f, 1.0f, 1.0f);
+        if (m->inside) {
+            /* BeerLambert (brdf.cuh:15-18): exp(d * sigmaA * log(clamp(albedo))) */
+            const float d = len3(vsub(m->vloc, ic->pos));
+            const V3 al = vmin3(vmaxs(ic->albedo, 1.0e-12f), v3(1.0f, 1.0f, 1.0f));
+            const float ds = d * ic->sigma_a;
+            tr = v3(om_expf(ds * om_logf(al.x)), om_expf(ds * om_logf(al.y)), om_expf(ds * om_logf(al.z)));
+        }
+        const V3 nIn = (dot3(N, rayDir) > 0.0f) ? vneg(N) : N;
+        const float eta = m->inside ? IOR : 1.0f / IOR;
+        const float cosI = -dot3(nIn, rayDir);
+        const float sin2I = fmaxf(0.0f, 1.0f - cosI * cosI);
+        const float k = 1.0f - sin2I * (eta * eta);
+        if (k <= 0.0f) return vscale(tr, 0.99f);
+        const float cosT = sqrtf(k);
+        const float Fr = fresnel_exact(cosI, cosT, eta);
+        const V3 R = vreflect(rayDir, nIn);
+        const V3 T = vrefract(rayDir, nIn, eta);
+        const float dR = dot3(L, R), dT = dot3(L, T);
+        if (dR >= dT) return vscale(tr, Fr);
+        const float weight = (eta * eta) * (fabsf(cosT) / fmaxf(1e-6f, cosI));
+        return vscale(vscale(tr, 1.0f - Fr), weight);
+    }
+    return v3(0.0f, 0.0f, 0.0f);
+}
+
+/* SampleBSDF, RGB (material.cuh:177-330) */
+static SCtx sample_bsdf(Rng* g, int model, V3 rayDir, const Isect* ic, const Media* m)
+{
+    SCtx r;
+    sctx_init(&r);
+    const V3 N = ic->nrm;
+    const V3 V = vneg(rayDir);
+    if (model == AR_MAT_DIFFUSE) {
+        const float e0 = rng1(g), e1 = rng1(g), e2 = rng1(g);
+        const Smp s = sample_cosine(e0, e1, e2, N);
+        r.next = s.dir; r.pdf = s.pdf; r.emis = ic->emissive;
+        r.media.inside = m->inside; r.media.vloc = ic->pos;
+        return r;
+    }
+    if (model == AR_MAT_LIGHT) {
+        r.pdf = 1.0f; r.emis = ic->emissive; r.terminate = 1; r.pure_light = 1;
+        return r;
+    }
+    if (model == AR_MAT_GLASS) {
+        const float IOR = ic->ior;
+        r.delta = 1;
+        const int inside = m->inside;
+        const float eta = inside ? IOR : 1.0f / IOR;
+        const V3 nIn = (dot3(N, rayDir) > 0.0f) ? vneg(N) : N;
+        const float cosI = -dot3(nIn, rayDir);
+        const float sin2I = fmaxf(0.0f, 1.0f - cosI * cosI);
+        const float k = 1.0f - sin2I * (eta * eta);
+        r.emis = v3(0.0f, 0.0f, 0.0f);
+        if (k <= 0.0f) {
+            if (m->depth < 1024) {
+                r.next = vreflect(rayDir, nIn); r.pdf = 1.0f; r.media.inside = inside; r.media.vloc = ic->pos;
+            } else {
+                r.next = rayDir; r.pdf = 1.0f; r.media.inside = !inside; r.media.vloc = ic->pos;
+            }
+            return r;
+        }
+        const float cosT = sqrtf(k);
+        const float Fr = fresnel_exact(cosI, cosT, eta);
+        if (rng1(g) < Fr) {
+            r.next = vreflect(rayDir, nIn); r.pdf = Fr; r.media.inside = inside; r.media.vloc = ic->pos;
+        } else {
+            r.next = vrefract(rayDir, nIn, eta); r.pdf = 1.0f - Fr; r.media.inside = !inside; r.media.vloc = ic->pos;
+        }
+        return r;
+    }
+    if (model == AR_MAT_GGX) {
+        r.emis = ic->emissive;
+        const float NoV = fmaxf(0.0f, dot3(N, V));
+        if (NoV <= 0.0f) { r.terminate = 1; return r; }
+        float alpha, kD; V3 F0;
+        bsdf_ggx_params(ic, &alpha, &kD, &F0);
+        const float pSpec = clampf_(luminance3(F0), 0.1f, 0.9f);
+        const float u = rng1(g);
+        if (u < pSpec) {
+            const float e0 = rng1(g), e1 = rng1(g), e2 = rng1(g);
+            const Smp s = sample_ggx_vndf(V, N, alpha, e0, e1, e2);
+            const V3 L = s.dir;
+            const float NoL = fmaxf(0.0f, dot3(N, L));
+            if (NoL <= 0.0f) { r.terminate = 1; return r; }
+            const float pdfSpec = s.pdf;
+            const float pdfDiff = NoL / OR_PI;
+            r.next = L; r.pdf = pSpec * pdfSpec + (1.0f - pSpec) * pdfDiff;
+        } else {
+            const float e0 = rng1(g), e1 = rng1(g), e2 = rng1(g);
+            const Smp s = sample_cosine(e0, e1, e2, N);
+            const V3 L = s.dir;
+            const float pdfDiff = s.pdf;
+            const float pdfSpec = ggx_vndf_pdf(V, N, L, alpha);
+            r.next = L; r.pdf = pSpec * pdfSpec + (1.0f - pSpec) * pdfDiff;
+        }
+        r.media.inside = m->inside; r.media.vloc = ic->pos;
+        return r;
+    }
+    return r;
+}
+
+/* BSDF_PDF, RGB (material.cuh:332-387) */
+static float bsdf_pdf(int model, const Isect* ic, V3 N, V3 rayDir, V3 L)
+{
+    const V3 V = vneg(rayDir);
+    const float NoL = fmaxf(0.0f, dot3(N, L));
+    if (model == AR_MAT_DIFFUSE) return NoL > 0.0f ? (NoL * (1.0f / OR_PI)) : 0.0f;
+    if (model == AR_MAT_GGX) {
+        const float NoV = fmaxf(0.0f, dot3(N, V));
+        if (NoV <= 0.0f || NoL <= 0.0f) return 0.0f;
+        float alpha, kD; V3 F0;
+        bsdf_ggx_params(ic, &alpha, &kD, &F0);
+        const float pSpec = clampf_(luminance3(F0), 0.1f, 0.9f);
+        const float pdfSpec = ggx_vndf_pdf(V, N, L, alpha);
+        const float pdfDiff = NoL * (1.0f / OR_PI);
+        return fmaxf(0.0f, pSpec * pdfSpec + (1.0f - pSpec) * pdfDiff);
+    }
+    return 0.0f;
+}
+
+/* ------------------------------------------------------------------------ */
+/* NEE (nee/nee.cuh)                                                          */
+/* ------------------------------------------------------------------------ */
+typedef struct { int obj; V3 p, n, emis; float pFacet, pA; int valid; } LSmp;
+
+static void obb_axes(const OObj* o, V3* ux, V3* uy, V3* uz)
+{
+    const M3* M = &o->o2w;
+    *ux = vnormalize(v3(M->x.x, M->y.x, M->z.x));
+    *uy = vnormalize(v3(M->x.y, M->y.y, M->z.y));
+    *uz = vnormalize(v3(M->x.z, M->y.z, M->z.z));
+}
+static float area_to_solid_angle(V3 sp, V3 lp, V3 ln, float pA)
+{
+    const V3 s2l = vsub(lp, sp);
+    const float d2 = fmaxf(dot3(s2l, s2l), 1e-20f);
+    const V3 dir = vscale(s2l, om_rsqrtf(d2));
+    const float cosY = fmaxf(0.0f, dot3(ln, vneg(dir)));
+    if (cosY <= 0.0f) return 0.0f;
+    return pA * (d2 / cosY);
+}
+static float facing_weight(V3 fn, V3 fc, V3 sp, float area)
+{
+    const V3 l2s = vnormalize(vsub(sp, fc));
+    const float c = fmaxf(0.0f, dot3(fn, l2s));
+    return area * c;
+}
+static void box_facets(const OObj* o, V3 fn[6], V3 fc[6], V3 ft[6], V3 fb[6], float s1[6], float s2[6], float area[6])
+{
+    V3 ux, uy, uz;
+    obb_axes(o, &ux, &uy, &uz);
+    const V3 c = o->center, e = o->extent;
+    fn[0] = ux; fn[1] = vneg(ux); fn[2] = uy; fn[3] = vneg(uy); fn[4] = uz; fn[5] = vneg(uz);
+    fc[0] = vadd(c, vscale(ux, e.x)); fc[1] = vsub(c, vscale(ux, e.x));
+    fc[2] = vadd(c, vscale(uy, e.y)); fc[3] = vsub(c, vscale(uy, e.y));
+    fc[4] = vadd(c, vscale(uz, e.z)); fc[5] = vsub(c, vscale(uz, e.z));
+    ft[0] = uy; ft[1] = uy; ft[2] = ux; ft[3] = ux; ft[4] = ux; ft[5] = ux;
+    fb[0] = uz; fb[1] = uz; fb[2] = uz; fb[3] = uz; fb[4] = uy; fb[5] = uy;
+    s1[0] = e.y; s1[1] = e.y; s1[2] = e.x; s1[3] = e.x; s1[4] = e.x; s1[5] = e.x;
+    s2[0] = e.z; s2[1] = e.z; s2[2] = e.z; s2[3] = e.z; s2[4] = e.y; s2[5] = e.y;
+    for (int f = 0; f < 6; ++f) area[f] = 4.0f * s1[f] * s2[f];
+}
+
+/* NEEPDFOmegaFromHit_Box (nee.cuh:64-151) */
+static float pdf_box(const OObj* o, float selectProb, V3 sp, V3 lp, V3 ln)
+{
+    V3 fn[6], fc[6], ft[6], fb[6];
+    float s1[6], s2[6], area[6];
+    box_facets(o, fn, fc, ft, fb, s1, s2, area);
+    int hitFacet = -1;
+    for (int f = 0; f < 6; ++f) if (dot3(fn[f], ln) > 0.999f) { hitFacet = f; break; }
+    if (hitFacet < 0) {
+        float best = 1e30f;
+        for (int f = 0; f < 6; ++f) {
+            const float d = fabsf(dot3(fn[f], vsub(lp, fc[f])));
+            if (d < best) { best = d; hitFacet = f; }
+        }
+    }
+    float sum = 0.0f, wHit = 0.0f, aHit = 0.0f;
+    for (int f = 0; f < 6; ++f) {
+        const float w = facing_weight(fn[f], fc[f], sp, area[f]);
+        sum += w;
+        if (f == hitFacet) { wHit = w; aHit = area[f]; }
+    }
+    if (sum <= 0.0f || wHit <= 0.0f) return 0.0f;
+    const float pA = selectProb * (1.0f / aHit) * (wHit / sum);
+    return area_to_solid_angle(sp, lp, ln, pA);
+}
+
+/* NEESampleBoxAreaFacing (nee.cuh:154-251) */
+static LSmp sample_box(Rng* g, const OObj* o, V3 cp)
+{
+    LSmp ls;
+    memset(&ls, 0, sizeof(ls));
+    V3 fn[6], fc[6], ft[6], fb[6];
+    float s1[6], s2[6], area[6];
+    box_facets(o, fn, fc, ft, fb, s1, s2, area);
+    int vi[6];
+    float vw[6];
+    int nv = 0;
+    float wsum = 0.0f;
+    for (int f = 0; f < 6; ++f) {
+        const float w = facing_weight(fn[f], fc[f], cp, area[f]);
+        if (w > 0.0f) { vi[nv] = f; vw[nv] = w; wsum += w; ++nv; }
+    }
+    if (nv == 0) return ls;
+    int slot = 0, fi = vi[0];
+    {
+        const float r = rng1(g) * wsum;
+        float acc = 0.0f;
+        for (int k = 0; k < nv; ++k) {
+            acc += vw[k];
+            if (r <= acc) { slot = k; fi = vi[k]; break; }
+        }
+    }
+    const float u1 = 2.0f * rng1(g) - 1.0f;
+    const float u2 = 2.0f * rng1(g) - 1.0f;
+    ls.p = vadd(vadd(fc[fi], vscale(ft[fi], u1 * s1[fi])), vscale(fb[fi], u2 * s2[fi]));
+    ls.n = fn[fi];
+    ls.emis = from_ar(o->mat.emissive);
+    ls.pFacet = 1.0f * (vw[slot] / wsum);
+    ls.pA = 1.0f / area[fi];
+    ls.valid = 1;
+    return ls;
+}
+
+/* NEEPDFOmegaFromHit_Sphere (nee.cuh:254-271) */
+static float pdf_sphere(const OObj* o, float selectProb, V3 sp, V3 lp, V3 ln)
+{
+    const float R = max3f(o->extent);
+    const float dist = len3(vsub(sp, o->center));
+    if (dist <= R) return 0.0f;
+    const float cosC = clampf_(R / dist, 0.0f, 1.0f);
+    const float areaCap = 2.0f * OR_PI * R * R * (1.0f - cosC);
+    if (areaCap <= 1e-20f) return 0.0f;
+    const float pA = selectProb / areaCap;
+    return area_to_solid_angle(sp, lp, ln, pA);
+}
+
+/* NEESampleSphereCapArea (nee.cuh:274-310) */
+static LSmp sample_sphere(Rng* g, const OObj* o, V3 cp)
+{
+    LSmp ls;
+    memset(&ls, 0, sizeof(ls));
+    const V3 c = o->center;
+    const float R = max3f(o->extent);
+    const V3 p2c = vsub(cp, c);
+    const float dist = len3(p2c);
+    if (dist <= R) return ls;
+    const V3 axis = vdivs(p2c, dist);
+    const float cosC = clampf_(R / dist, 0.0f, 1.0f);
+    const float areaCap = 2.0f * OR_PI * R * R * (1.0f - cosC);
+    const float u = rng1(g);
+    const float vphi = rng1(g);
+    const float cosT = lerpf_(cosC, 1.0f, u);
+    const float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));
+    const float phi = 2.0f * OR_PI * vphi;
+    V3 t, b;
+    tangent_basis(axis, &t, &b);
+    float sp, cph;
+    om_sincosf(phi, &sp, &cph);
+    const V3 n = vadd(vadd(vscale(t, cph * sinT), vscale(b, sp * sinT)), vscale(axis, cosT));
+    ls.p = vadd(c, vscale(n, R));
+    ls.n = n;
+    ls.emis = from_ar(o->mat.emissive);
+    ls.pFacet = 1.0f;
+    ls.pA = 1.0f / areaCap;
+    ls.valid = 1;
+    return ls;
+}
+
+/* NEESampleLight (nee.cuh:330-377) */
+static LSmp sample_light(const or_scene* s, V3 sp, Rng* g)
+{
+    LSmp none;
+    memset(&none, 0, sizeof(none));
+    if (s->nl <= 0) return none;
+    int pick = s->nl - 1;
+    float pprob = 0.0f;
+    {
+        const float rr = rng1(g);
+        float acc = 0.0f;
+        for (int l = 0; l < s->nl; ++l) {
+            const float p = s->lprob[l];
+            acc += p;
+            if (rr < acc) { pick = l; pprob = p; break; }
+        }
+    }
+    const OObj* lo = &s->o[s->lobj[pick]];
+    LSmp ls = none;
+    if (lo->type == AR_OBJ_CUBE) ls = sample_box(g, lo, sp);
+    else if (lo->type == AR_OBJ_SPHERE) ls = sample_sphere(g, lo, sp);
+    if (!ls.valid) return none;
+    ls.obj = s->lobj[pick];
+    ls.pFacet = ls.pFacet * pprob;
+    return ls;
+}
+
+static float pdf_light_from_hit(const or_scene* s, int obj, V3 sp, V3 lp, V3 ln)
+{
+    const OObj* o = &s->o[obj];
+    const float sel = s->lprob[o->light_index];
+    if (o->type == AR_OBJ_CUBE) return pdf_box(o, sel, sp, lp, ln);
+    if (o->type == AR_OBJ_SPHERE) return pdf_sphere(o, sel, sp, lp, ln);
+    return 0.0f;
+}
+
+static float power_heuristic(float pA, float pB)
+{
+    const float a = pA * pA, b = pB * pB;
+    return a / fmaxf(1e-24f, a + b);
+}
+
+/* SkyLighting (render.cuh:58-73) */
+static V3 sky_lighting(V3 d, int sky)
+{
+    if (!sky) return v3(0.0f, 0.0f, 0.0f);
+    const V3 white = v3(1.0f, 1.0f, 1.0f);
+    const V3 blue = v3(0.05f, 0.45f, 1.0f);
+    const V3 down = vscale(v3(0.2f, 0.6f, 1.0f), 0.125f);
+    const V3 inner = vlerp(blue, white, om_powf(fmaxf(d.y, 0.0f), 0.75f));
+    const V3 l = vlerp(inner, down, fminf(fmaxf(-d.y * 0.5f + 0.5f, 0.0f), 1.0f));
+    return vscale(l, 0.5f);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Path loop                                                                  */
+/* ------------------------------------------------------------------------ */
+typedef struct { int64_t ext_rays, shadow_rays; } Counters;
+
+static int path_mode(const or_scene* s)
+{
+    return (s->flags & OR_REFERENCE_TRAVERSAL) ? (OR_TIE_FIRST_FOUND | OR_SLAB_REFERENCE)
+                                               : (OR_TIE_LOWEST_INDEX | OR_SLAB_STANDARD);
+}
+
+static int closest(const or_scene* s, V3 ro, V3 rd, float tMin, Isect* out)
+{
+    const TraceResult r = traverse(s, ro, rd, tMin, INFINITY, 0, path_mode(s));
+    if (r.obj < 0) return 0;
+    memset(out, 0, sizeof(*out));
+    out->obj = r.obj;
+    isect_object(s, r.obj, ro, rd, out);
+    out->obj = r.obj;
+    out->light = s->o[r.obj].light_index;
+    return 1;
+}
+
+/* AnyHitSegmentBVH (intersection.cuh:372-397) */
+static int segment_occluded(const or_scene* s, float eps_d, V3 src, V3 dst, Counters* cnt)
+{
+    V3 dir = vsub(dst, src);
+    const float dist = len3(dir);
+    if (dist <= 0.0f) return 0;
+    dir = vdivs(dir, dist);
+    const float eps = eps_d * fmaxf(1.0f, fmaxf(len3(src), len3(dst)));
+    const float tMax = fmaxf(0.0f, dist - eps);
+    if (tMax <= 0.0f) return 0;
+    cnt->shadow_rays++;
+    const TraceResult r = traverse(s, src, dir, 0.0f, tMax, 1, path_mode(s));
+    return r.obj >= 0;
+}
+
+typedef struct { V3 radiance; int segments, nee_rays; int hits[AR_DEBUG_MAX_HITS]; } PathOut;
+
+/* CalculateRadiance<bUseBVH=true, bUseNEE, bUsePathGuiding=false>, RGB
+ * (render.cuh:460-999), with camera_inside = intersection::Overlap at the
+ * camera position (render.cuh:536-538). */
+static void calculate_radiance(const or_scene* s, const ar_render_params* p, int camera_inside,
+                               Rng* g, V3 ro, V3 rd, PathOut* po, Counters* cnt)
+{
+    int nonDelta = 0;
+    rd = vnormalize(rd);
+    V3 radiance = v3(0.0f, 0.0f, 0.0f);
+    V3 mask = v3(1.0f, 1.0f, 1.0f);
+    V3 cro = ro, crd = rd;
+    Media media;
+    media.inside = camera_inside; media.vloc = ro; media.obj = -1; media.depth = 0;
+    int prevDidNEE = 0;
+    float prevPdf = 0.0f;
+    V3 prevPos = v3(0.0f, 0.0f, 0.0f);
+    po->segments = 0; po->nee_rays = 0;
+    for (int k = 0; k < AR_DEBUG_MAX_HITS; ++k) po->hits[k] = -1;
+    for (int depth = 0; depth < p->max_depth; depth++) {
+        /* ---- Trace (render.cuh:75-163), depth argument = nonDeltaDepth ---- */
+        const float eps = s->eps_tab[nonDelta < 8 ? nonDelta : 8];
+        Isect ic;
+        memset(&ic, 0, sizeof(ic));
+        ic.obj = -1; ic.light = -1;
+        int hit;
+        cnt->ext_rays++;
+        if (media.inside && media.obj >= 0 &&
+            (s->o[media.obj].type != AR_OBJ_TRIANGLE || (s->flags & OR_TRIANGLE_SOLO_MEDIA))) {
+            /* solo trace (intersection.cuh:185-193) */
+            Isect t;
+            memset(&t, 0, sizeof(t));
+            t.obj = -1;
+            hit = isect_object(s, media.obj, cro, crd, &t) && !(t.dist < eps);
+            if (hit) { ic = t; ic.obj = media.obj; ic.light = s->o[media.obj].light_index; }
+            else { memset(&ic, 0, sizeof(ic)); ic.obj = -1; ic.light = -1; }
+        } else {
+            hit = closest(s, cro, crd, eps, &ic);
+        }
+        if (po->segments < AR_DEBUG_MAX_HITS) po->hits[po->segments] = hit ? ic.obj : -1;
+        po->segments++;
+        SCtx sc;
+        sctx_init(&sc);
+        int model = -1;
+        if (!hit && media.inside) {
+            sc.miss_thin = 1;
+            ic.obj = media.obj; /* traceResult.intersectionContext_.objectIndex_ */
+            sc.media.vloc = cro;  /* hitLocalPosition_ = rayOrigin */
+        }
+        if (hit) {
+            model = s->o[ic.obj].mat.shading_model;
+            const SCtx sb = sample_bsdf(g, model, crd, &ic, &media);
+            sc = sb;
+            sc.media.obj = ic.obj;
+            sc.media.depth = media.depth + 1;
+            sc.brdf = eval_bsdf_cos(model, crd, sc.next, &ic, &media);
+        } else {
+            sc.brdf = v3(1.0f, 1.0f, 1.0f);
+            sc.delta = 0;
+            sc.next = crd;
+            sc.pdf = 1.0f;
+            sc.emis = sky_lighting(crd, p->sky);
+            sc.media.inside = 0;
+        }
+        {
+            /* offset, always one Rand1 (render.cuh:156-160) */
+            const float offEps = eps * fmaxf(1.0f, len3(ic.pos));
+            const float sg = signf_(dot3(ic.nrm, sc.next));
+            const float r = rng1(g);
+            ic.pos = vadd(ic.pos, vscale(vscale(vscale(ic.nrm, sg), offEps), r + 0.5f));
+        }
+        media = sc.media;
+        /* ---- emission (render.cuh:648-723) ---- */
+        if (!hit) {
+            if (!sc.miss_thin) radiance = vadd(radiance, vmul(mask, sc.emis));
+        } else if (ic.light >= 0) {
+            float misW = 1.0f;
+            if (p->use_nee && depth > 0 && prevDidNEE) {
+                const float pB = fmaxf(prevPdf, 0.0f);
+                const float pL = pdf_light_from_hit(s, ic.obj, prevPos, ic.pos, ic.nrm);
+                if (pL >= 0.0f && pB > 0.0f) misW = power_heuristic(pB, pL);
+            }
+            radiance = vadd(radiance, vscale(vmul(mask, sc.emis), misW));
+        }
+        if ((!hit && !sc.miss_thin) || sc.terminate) break;
+        /* ---- NEE (render.cuh:766-827) ---- */
+        if (!sc.miss_thin) {
+            const float lum = luminance3(mask);
+            const float useNEERate = sqrtf(saturatef_(lum));
+            int neeValid = 0;
+            if (p->use_nee && nonDelta < 10 && !sc.delta && !media.inside && rng1(g) < useNEERate) {
+                const LSmp ls = sample_light(s, ic.pos, g);
+                if (ls.valid) {
+                    const float pATotal = fmaxf(1e-20f, ls.pA * ls.pFacet);
+                    const V3 lu = vsub(ls.p, ic.pos);
+                    const float d2 = fmaxf(dot3(lu, lu), 1.0e-12f);
+                    const V3 ld = vscale(lu, om_rsqrtf(d2));
+                    po->nee_rays++;
+                    const int occ = segment_occluded(s, s->eps_tab[depth < 8 ? depth : 8], ic.pos, ls.p, cnt);
+                    if (occ) {
+                        neeValid = 1;
+                    } else {
+                        const float cosX = fmaxf(0.0f, dot3(ic.nrm, ld));
+                        const float cosY = fmaxf(0.0f, dot3(ls.n, vneg(ld)));
+                        if (cosX <= 0.0f || cosY <= 0.0f) {
+                            neeValid = 0;
+                        } else {
+                            Media none;
+                            memset(&none, 0, sizeof(none));
+                            none.obj = -1;
+                            const V3 f = eval_bsdf_cos(model, crd, ld, &ic, &none);
+                            const float G = cosY / d2;
+                            const V3 contrib = vscale(vmul(f, ls.emis), G / pATotal);
+                            neeValid = 1;
+                            const float pL = area_to_solid_angle(ic.pos, ls.p, ls.n, ls.pFacet * ls.pA);
+                            const float pB = fmaxf(bsdf_pdf(model, &ic, ic.nrm, crd, ld), 0.0f);
+                            const float w = power_heuristic(pL, pB);
+                            radiance = vadd(radiance, vmul(mask, vscale(contrib, w)));
+                        }
+                    }
+                }
+            }
+            prevDidNEE = neeValid;
+            prevPdf = sc.pdf;
+            prevPos = ic.pos;
+        }
+        const V3 contrib = v3(sc.brdf.x / fmaxf(sc.pdf, 1e-12f), sc.brdf.y / fmaxf(sc.pdf, 1e-12f),
+                              sc.brdf.z / fmaxf(sc.pdf, 1e-12f));
+        float q = 1.0f;
+        if (nonDelta >= p->rr_depth) {
+            const float lum = luminance3(mask);
+            const float mx = max3f(mask);
+            const float basic = clampf_(lum * 0.5f + mx * 0.5f, 0.05f, 0.95f);
+            q = lerpf_(basic, 1.0f, media.inside ? 0.99f : 0.0f);
+            if (rng1(g) > q) break;
+        }
+        mask = vmul(mask, contrib);
+        mask = vdivs(mask, q);
+        cro = ic.pos;
+        crd = sc.next;
+        if (!sc.delta) nonDelta++;
+    }
+    /* checkNanInf + clamp (render.cuh:969), max(0, .) (scene.cu:238) */
+    V3 out = v3(clampf_(fix_nan_inf(radiance.x), 0.0f, 1.0e3f), clampf_(fix_nan_inf(radiance.y), 0.0f, 1.0e3f),
+                clampf_(fix_nan_inf(radiance.z), 0.0f, 1.0e3f));
+    po->radiance = vmaxs(out, 0.0f);
+}
+
+/* intersection::Overlap (intersection.cuh:399-414) at the camera position */
+static int camera_overlap(const or_scene* s, V3 p)
+{
+    for (int i = 0; i < s->n; ++i) {
+        const OObj* o = &s->o[i];
+        if (o->type == AR_OBJ_CUBE) {
+            const V3 l = mmul(&o->w2o, vsub(p, o->center));
+            const V3 mn = vneg(o->extent), mx = o->extent;
+            if (mn.x < l.x && mn.y < l.y && mn.z < l.z && mx.x > l.x && mx.y > l.y && mx.z > l.z) return 1;
+        } else if (o->type == AR_OBJ_SPHERE) {
+            const V3 l = mmul(&o->w2o, vsub(p, o->center));
+            const float r = max3f(o->extent);
+            if (dot3(l, l) < r * r) return 1;
+        }
+    }
+    return 0;
+}
+
+/* RenderCamera ray generation (scene.cu:213-230), field of view as parameter */
+void or_camera_ray(const ar_camera* cam, int i, int j, float jx, float jy, float* ray8)
+{
+    const float u = ((float)i + jx) / (float)cam->width;
+    const float v = ((float)j + jy) / (float)cam->height;
+    const float ndcx = u * 2.0f - 1.0f;
+    const float ndcy = (float)((1.0 - (double)v) * 2.0 - 1.0);
+    const float fov = cam->fov_y_deg * 3.1415926f / 180.0f;
+    const float aspect = (float)cam->width / fmaxf(1.0f, (float)cam->height);
+    const float tanHalfY = om_tanf(0.5f * fov);
+    const float tanHalfX = tanHalfY * aspect;
+    const float sx = ndcx * tanHalfX;
+    const float sy = ndcy * tanHalfY;
+    const V3 cd = from_ar(cam->direction);
+    const V3 right = vnormalize(cross3(cd, v3(0.0f, 1.0f, 0.0f)));
+    const V3 up = vnormalize(cross3(cd, right));
+    const V3 d = vnormalize(vadd(vadd(cd, vscale(right, sx)), vscale(up, sy)));
+    ray8[0] = cam->position.x; ray8[1] = cam->position.y; ray8[2] = cam->position.z; ray8[3] = 0.0f;
+    ray8[4] = d.x; ray8[5] = d.y; ray8[6] = d.z; ray8[7] = INFINITY;
+}
+
+int64_t or_render_paths(const or_scene* s, const ar_camera* cam, const ar_render_params* p,
+                        const float* tape, int per_path, ar_path_record* rec, int threads)
+{
+    const int64_t W = cam->width, H = cam->height, S = p->spp;
+    const int inside = camera_overlap(s, from_ar(cam->position));
+    int64_t overflow = 0;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : overflow)
+#endif
+    for (int64_t k = 0; k < W * H * S; ++k) {
+        const int i = (int)(k % W), j = (int)((k / W) % H);
+        Rng g;
+        g.tape = tape + k * per_path; g.limit = per_path; g.pos = 0; g.overflow = 0; g.state = 0;
+        const float jx = rng1(&g), jy = rng1(&g);
+        float ray[8];
+        or_camera_ray(cam, i, j, jx, jy, ray);
+        PathOut po;
+        Counters cnt = {0, 0};
+        calculate_radiance(s, p, inside, &g, v3(ray[0], ray[1], ray[2]), v3(ray[4], ray[5], ray[6]), &po, &cnt);
+        ar_path_record* r = &rec[k];
+        memset(r, 0, sizeof(*r));
+        r->radiance[0] = po.radiance.x; r->radiance[1] = po.radiance.y; r->radiance[2] = po.radiance.z;
+        r->segments = po.segments;
+        r->uniforms = g.pos;
+        r->nee_rays = po.nee_rays;
+        for (int h = 0; h < AR_DEBUG_MAX_HITS; ++h) r->hit_object[h] = po.hits[h];
+        if (g.overflow) overflow++;
+    }
+    return overflow;
+}
+
+void or_render_image(const or_scene* s, const ar_camera* cam, const ar_render_params* p,
+                     int64_t pb, int64_t pe, double* accum, int64_t* ext, int64_t* shadow, int threads)
+{
+    const int64_t W = cam->width;
+    const int inside = camera_overlap(s, from_ar(cam->position));
+    int64_t e = 0, sh = 0;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : e, sh)
+#endif
+    for (int64_t pix = pb; pix < pe; ++pix) {
+        const int i = (int)(pix % W), j = (int)(pix / W);
+        double acc[3] = {0.0, 0.0, 0.0};
+        Counters cnt = {0, 0};
+        for (int smp = 0; smp < p->spp; ++smp) {
+            Rng g;
+            g.tape = NULL; g.limit = 0; g.pos = 0; g.overflow = 0;
+            g.state = p->seed ^ ((uint64_t)pix * 0x9e3779b97f4a7c15ull) ^ ((uint64_t)(smp + p->frame_offset) << 40);
+            const float jx = rng1(&g), jy = rng1(&g);
+            float ray[8];
+            or_camera_ray(cam, i, j, jx, jy, ray);
+            PathOut po;
+            calculate_radiance(s, p, inside, &g, v3(ray[0], ray[1], ray[2]), v3(ray[4], ray[5], ray[6]), &po, &cnt);
+            acc[0] += po.radiance.x; acc[1] += po.radiance.y; acc[2] += po.radiance.z;
+        }
+        accum[3 * pix + 0] += acc[0]; accum[3 * pix + 1] += acc[1]; accum[3 * pix + 2] += acc[2];
+        e += cnt.ext_rays; sh += cnt.shadow_rays;
+    }
+    if (ext) *ext = e;
+    if (shadow) *shadow = sh;
+}
+
+float or_sinf(float x) { return om_sinf(x); }
+float or_cosf(float x) { return om_cosf(x); }
+float or_expf(float x) { return om_expf(x); }
+float or_logf(float x) { return om_logf(x); }
+float or_powf(float x, float y) { return om_powf(x, y); }

@@ -1,0 +1,106 @@
+/*
+ * oracle.h -- CPU restatement of the reference path tracer's hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This code is the checker for the CUDA core: only
+ * the test suite, the smoke check and the CPU-baseline leg of bench.py load it.
+ * Nothing in the shipped library links against it.
+ *
+ * It restates, function by function, ApertureRendererV3's CalculateRadiance
+ * stack (core/render/render.cuh:460-999) in scalar C with IEEE single
+ * precision, no FMA contraction (-ffp-contract=off) and the deterministic
+ * transcendental functions of oracle_math.h, so that the GPU kernels -- built
+ * with the same rounding rules -- can be compared bit for bit.  The input
+ * format is the public ar_object_desc of include/aperture_b200.h.
+ *
+ * Pinning: the BVH build and the ray queries are checked against the
+ * reference's own code compiled on the host (oracle/_ref, see oracle/Makefile),
+ * whose outputs are committed as fixtures under tests/golden/.
+ */
+#ifndef APERTURE_ORACLE_H
+#define APERTURE_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../include/aperture_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Scene options. */
+enum {
+    /* BVH proxies of triangles use the SceneObject centre as the reference's
+     * UpdateProxy does (object.cuh:309-342); otherwise the centre of the
+     * triangle's world bounds. */
+    OR_PROXY_OBJECT_CENTER = 1 << 0,
+    /* Triangles hit with the reference's default G-buffer (white, no
+     * emission; intersection.cuh:17,63) instead of their material. */
+    OR_TRIANGLE_DEFAULT_GBUFFER = 1 << 1,
+    /* Inside a medium whose object is a triangle, trace only that triangle
+     * (the reference's solo trace, render.cuh:91-94) instead of the scene. */
+    OR_TRIANGLE_SOLO_MEDIA = 1 << 2,
+    /* Path loop queries use the reference's slab test and first-found tie
+     * rule (for pinning against the reference's own code). */
+    OR_REFERENCE_TRAVERSAL = 1 << 3
+};
+
+/* Query options for or_trace_rays. */
+enum {
+    OR_TIE_FIRST_FOUND = 0,   /* reference: strict t < best (intersection.cuh:160) */
+    OR_TIE_LOWEST_INDEX = 1,  /* this build: equal t goes to the lower object index */
+    OR_SLAB_REFERENCE = 0,    /* FastAABBHit as written (bvh.cuh:424-470)           */
+    OR_SLAB_STANDARD = 2      /* standard slab test (entry <= exit), widened 1 ulp  */
+};
+
+typedef struct or_scene or_scene;
+
+or_scene* or_scene_create(const ar_object_desc* objects, size_t count, int flags,
+                          int leaf_size, int bin_count);
+void or_scene_destroy(or_scene* s);
+
+/* BVH export: per node bmin[3], bmax[3] floats and left, right, first, count. */
+int64_t or_scene_node_count(const or_scene* s);
+void or_scene_nodes(const or_scene* s, float* bounds6, int32_t* links4);
+void or_scene_indices(const or_scene* s, int32_t* indices);
+int64_t or_scene_light_count(const or_scene* s);
+void or_scene_lights(const or_scene* s, int32_t* object_index, float* select_prob);
+
+/* Rays as 8 floats: origin.xyz, tmin, direction.xyz, tmax.  Counters (may be
+ * NULL) receive per-ray node visits and primitive tests. */
+void or_trace_rays(const or_scene* s, const float* rays, int64_t n, int any_hit, int mode,
+                   int32_t* hit_object, float* hit_t, int32_t* node_visits,
+                   int32_t* prim_tests, int threads);
+/* Brute force over all objects, lowest-index tie rule. */
+void or_trace_rays_brute(const or_scene* s, const float* rays, int64_t n, int any_hit,
+                         int32_t* hit_object, float* hit_t, int threads);
+
+/* Camera rays of RenderCamera (scene.cu:213-230) for jitter values taken
+ * from a tape: rays[8] per path, as for or_trace_rays. */
+void or_camera_ray(const ar_camera* cam, int i, int j, float jx, float jy, float* ray8);
+
+/* Replay spp samples of every pixel with uniforms read from `tape`
+ * (ar_rng_tape layout: per path `per_path` floats, sample major).  Writes one
+ * ar_path_record per path.  Returns the number of paths that ran out of tape. */
+int64_t or_render_paths(const or_scene* s, const ar_camera* cam, const ar_render_params* p,
+                        const float* tape, int per_path, ar_path_record* records,
+                        int threads);
+
+/* CPU baseline: render with an own per-path random generator (not curand), FP64
+ * sums added into accum (w*h*3).  Counts closest-hit and shadow queries. */
+void or_render_image(const or_scene* s, const ar_camera* cam, const ar_render_params* p,
+                     int64_t pixel_begin, int64_t pixel_end, double* accum,
+                     int64_t* extension_rays, int64_t* shadow_rays, int threads);
+
+/* Deterministic transcendental functions (exported for their own tests). */
+float or_sinf(float x);
+float or_cosf(float x);
+float or_expf(float x);
+float or_logf(float x);
+float or_powf(float x, float y);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APERTURE_ORACLE_H */

@@ -1,0 +1,151 @@
+"""ctypes wrapper of liboracle.so, the CPU restatement of the reference hot path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py, as the checker.  The input format is
+the public ar_object_desc (aperture_b200.OBJECT_DTYPE).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import POINTER, c_float, c_int, c_int32, c_int64, c_size_t, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+PROXY_OBJECT_CENTER = 1
+TRIANGLE_DEFAULT_GBUFFER = 2
+TRIANGLE_SOLO_MEDIA = 4
+REFERENCE_TRAVERSAL = 8
+TIE_FIRST_FOUND, TIE_LOWEST_INDEX, SLAB_REFERENCE, SLAB_STANDARD = 0, 1, 0, 2
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        build()
+    lib = ctypes.CDLL(LIB)
+    lib.or_scene_create.argtypes = [c_void_p, c_size_t, c_int, c_int, c_int]
+    lib.or_scene_create.restype = c_void_p
+    lib.or_scene_destroy.argtypes = [c_void_p]
+    lib.or_scene_node_count.argtypes = [c_void_p]
+    lib.or_scene_node_count.restype = c_int64
+    lib.or_scene_nodes.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.or_scene_indices.argtypes = [c_void_p, c_void_p]
+    lib.or_scene_light_count.argtypes = [c_void_p]
+    lib.or_scene_light_count.restype = c_int64
+    lib.or_scene_lights.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.or_trace_rays.argtypes = [c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                  c_int]
+    lib.or_trace_rays_brute.argtypes = [c_void_p, c_void_p, c_int64, c_int, c_void_p, c_void_p, c_int]
+    lib.or_camera_ray.argtypes = [c_void_p, c_int, c_int, c_float, c_float, c_void_p]
+    lib.or_render_paths.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int]
+    lib.or_render_paths.restype = c_int64
+    lib.or_render_image.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, POINTER(c_int64),
+                                    POINTER(c_int64), c_int]
+    for f in ("or_sinf", "or_cosf", "or_expf", "or_logf"):
+        getattr(lib, f).argtypes = [c_float]
+        getattr(lib, f).restype = c_float
+    lib.or_powf.argtypes = [c_float, c_float]
+    lib.or_powf.restype = c_float
+    _lib = lib
+    return lib
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class OracleScene:
+    def __init__(self, objects: np.ndarray, flags: int = 0, leaf_size: int = 8, bin_count: int = 12):
+        lib = load()
+        from aperture_b200 import OBJECT_DTYPE
+        self._objs = np.ascontiguousarray(objects, dtype=OBJECT_DTYPE)
+        self._h = lib.or_scene_create(_p(self._objs) if len(self._objs) else None, len(self._objs), flags,
+                                      leaf_size, bin_count)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib.or_scene_destroy(self._h)
+            self._h = None
+
+    def nodes(self):
+        n = _lib.or_scene_node_count(self._h)
+        b = np.zeros((n, 6), np.float32)
+        l = np.zeros((n, 4), np.int32)
+        if n:
+            _lib.or_scene_nodes(self._h, _p(b), _p(l))
+        return b, l
+
+    def indices(self):
+        idx = np.zeros(len(self._objs), np.int32)
+        if len(idx):
+            _lib.or_scene_indices(self._h, _p(idx))
+        return idx
+
+    def lights(self):
+        n = _lib.or_scene_light_count(self._h)
+        o = np.zeros(n, np.int32)
+        p = np.zeros(n, np.float32)
+        if n:
+            _lib.or_scene_lights(self._h, _p(o), _p(p))
+        return o, p
+
+    def trace(self, rays, any_hit=False, mode=TIE_LOWEST_INDEX | SLAB_STANDARD, threads=0, counters=False):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        obj = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        nv = np.empty(n, np.int32) if counters else None
+        pt = np.empty(n, np.int32) if counters else None
+        _lib.or_trace_rays(self._h, _p(rays), n, int(any_hit), mode, _p(obj), _p(t), _p(nv) if counters else None,
+                           _p(pt) if counters else None, threads)
+        if counters:
+            return obj, t, nv, pt
+        return obj, t
+
+    def trace_brute(self, rays, any_hit=False, threads=0):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        obj = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        _lib.or_trace_rays_brute(self._h, _p(rays), n, int(any_hit), _p(obj), _p(t), threads)
+        return obj, t
+
+    def render_paths(self, camera, params, tape: np.ndarray, threads=0):
+        from aperture_b200 import RECORD_DTYPE
+        tape = np.ascontiguousarray(tape, np.float32)
+        n = camera.width * camera.height * params.spp
+        assert tape.shape[0] == n
+        rec = np.zeros(n, RECORD_DTYPE)
+        over = _lib.or_render_paths(self._h, ctypes.byref(camera), ctypes.byref(params), _p(tape), tape.shape[1],
+                                    _p(rec), threads)
+        return rec, over
+
+    def render_image(self, camera, params, pixel_begin=0, pixel_end=None, threads=0):
+        npix = camera.width * camera.height
+        if pixel_end is None:
+            pixel_end = npix
+        acc = np.zeros((npix, 3), np.float64)
+        e, s = c_int64(0), c_int64(0)
+        _lib.or_render_image(self._h, ctypes.byref(camera), ctypes.byref(params), pixel_begin, pixel_end, _p(acc),
+                             ctypes.byref(e), ctypes.byref(s), threads)
+        return acc, e.value, s.value
+
+
+def camera_ray(camera, i, j, jx, jy) -> np.ndarray:
+    lib = load()
+    r = np.zeros(8, np.float32)
+    lib.or_camera_ray(ctypes.byref(camera), i, j, jx, jy, _p(r))
+    return r
