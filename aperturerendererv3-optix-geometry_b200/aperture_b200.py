@@ -70,7 +70,8 @@ class SceneInfo(ctypes.Structure):
 
 class RenderStats(ctypes.Structure):
     _fields_ = [("paths", c_int64), ("extension_rays", c_int64), ("shadow_rays", c_int64),
-                ("kernel_launches", c_int64), ("trace_ms", c_float), ("total_ms", c_float)]
+                ("kernel_launches", c_int64), ("extend_launches", c_int64), ("shadow_launches", c_int64),
+                ("extend_ms", c_float), ("shadow_ms", c_float), ("total_ms", c_float), ("reserved", c_int32)]
 
 
 assert ctypes.sizeof(ObjectDesc) == 208

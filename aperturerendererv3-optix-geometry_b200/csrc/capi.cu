@@ -105,6 +105,7 @@ struct ar_scene {
     unsigned long long* stats = nullptr;
     int* err = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> timer_events;  // 2 kinds x 2 events x launches
 
     ~ar_scene()
     {
@@ -113,6 +114,7 @@ struct ar_scene {
         if (ws) cudaFree(ws);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        for (cudaEvent_t e : timer_events) cudaEventDestroy(e);
     }
 };
 
@@ -258,13 +260,30 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
     int64_t launches = 1;
     const int grid_trace = s->sm_count * 8;
     const int grid_shade = s->sm_count * 4;
+    const int64_t waves = static_cast<int64_t>(p->spp) * ((npix + wave - 1) / wave);
+    LaunchTimers tm;
+    LaunchTimers* tmp = nullptr;
+    if (stats) {
+        const size_t pairs = static_cast<size_t>(waves * p->max_depth);
+        if (pairs <= (size_t(1) << 16)) {
+            while (s->timer_events.size() < 4 * pairs) {
+                cudaEvent_t e;
+                ck(cudaEventCreate(&e), "event create");
+                s->timer_events.push_back(e);
+            }
+            tm.extend_ev = s->timer_events.data();
+            tm.shadow_ev = s->timer_events.data() + 2 * pairs;
+            tm.cap = static_cast<int>(pairs);
+            tmp = &tm;
+        }
+    }
     for (int sidx = 0; sidx < p->spp; ++sidx) {
         for (int64_t first = 0; first < npix; first += wave) {
             fp.spp_index = sidx;
             fp.first_pixel = static_cast<int32_t>(first);
             fp.wave = static_cast<int32_t>(std::min<int64_t>(wave, npix - first));
             ck(launch_wave(s->view, s->stack_depth, fp, P, s->base0, s->base1, s->counts, s->stats, s->err, s->accum,
-                           rec_dev, grid_trace, grid_shade, st, &launches),
+                           rec_dev, grid_trace, grid_shade, st, &launches, tmp),
                "render launch");
         }
     }
@@ -275,12 +294,27 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
         ck(cudaStreamSynchronize(st), "sync");
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+        std::memset(stats, 0, sizeof(*stats));
         stats->paths = npix * p->spp;
         stats->extension_rays = static_cast<int64_t>(h[0]);
         stats->shadow_rays = static_cast<int64_t>(h[1]);
         stats->kernel_launches = launches;
-        stats->trace_ms = -1.0f;
         stats->total_ms = ms;
+        stats->extend_launches = waves * p->max_depth;
+        stats->shadow_launches = waves * p->max_depth;
+        float e_ms = 0.0f, s_ms = 0.0f;
+        for (int k = 0; k < tm.n_extend; ++k) {
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, tm.extend_ev[2 * k], tm.extend_ev[2 * k + 1]);
+            e_ms += t;
+        }
+        for (int k = 0; k < tm.n_shadow; ++k) {
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, tm.shadow_ev[2 * k], tm.shadow_ev[2 * k + 1]);
+            s_ms += t;
+        }
+        stats->extend_ms = tmp ? e_ms : -1.0f;
+        stats->shadow_ms = tmp ? s_ms : -1.0f;
     }
     return AR_OK;
 }
@@ -396,6 +430,7 @@ ar_status ar_render(ar_scene* s, const ar_camera* cam, const ar_render_params* p
     DeviceGuard g(s->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (ar_status e = run_render(s, cam, p, nullptr, st, stats)) return e;
+    if (stats) stats->kernel_launches += (out_rgb ? 1 : 0) + (accum ? 1 : 0);
     const int64_t n = static_cast<int64_t>(cam->width) * cam->height * 3;
     const double inv = 1.0 / static_cast<double>(p->spp);
     if (mem_kind == AR_MEM_DEVICE) {

@@ -955,16 +955,22 @@ cudaError_t launch_rng_tape(const FrameParams& fp, int spp, int per_path, float*
 template <int kDepth>
 static cudaError_t launch_depth_loop_t(const SceneView& s, const FrameParams& fp, const PathSoA& P, int32_t* counts,
                                        unsigned long long* stats, int* err, ar_path_record* rec, int grid_trace,
-                                       int grid_shade, cudaStream_t st, int64_t* launches)
+                                       int grid_shade, cudaStream_t st, int64_t* launches, LaunchTimers* tm)
 {
     const size_t smem = static_cast<size_t>(kDepth) * kTraceBlock * 4;
     cudaFuncSetAttribute(k_extend<kDepth>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     cudaFuncSetAttribute(k_shadow<kDepth>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     int cur = 0;
     for (int depth = 0; depth < fp.max_depth; ++depth) {
+        const bool te = tm && tm->n_extend < tm->cap;
+        if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend], st);
         k_extend<kDepth><<<grid_trace, kTraceBlock, smem, st>>>(s, fp, P, cur, counts, stats, err);
+        if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend++ + 1], st);
         k_shade<<<grid_shade, kShadeBlock, 0, st>>>(s, fp, P, cur, counts, rec);
+        const bool ts = tm && tm->n_shadow < tm->cap;
+        if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow], st);
         k_shadow<kDepth><<<grid_trace, kTraceBlock, smem, st>>>(s, P, counts, stats, err);
+        if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow++ + 1], st);
         *launches += 3;
         cur = 1 - cur;
     }
@@ -973,14 +979,14 @@ static cudaError_t launch_depth_loop_t(const SceneView& s, const FrameParams& fp
 
 cudaError_t launch_wave(const SceneView& s, int stack_depth, const FrameParams& fp, const PathSoA& P, uint4* b0, uint2* b1,
                         int32_t* counts, unsigned long long* stats, int* err, double* accum, ar_path_record* rec,
-                        int grid_trace, int grid_shade, cudaStream_t st, int64_t* launches)
+                        int grid_trace, int grid_shade, cudaStream_t st, int64_t* launches, LaunchTimers* tm)
 {
     k_raygen<<<(fp.wave + 255) / 256, 256, 0, st>>>(fp, P, b0, b1, counts, rec);
     *launches += 1;
     cudaError_t e;
-    if (stack_depth <= 32) e = launch_depth_loop_t<32>(s, fp, P, counts, stats, err, rec, grid_trace, grid_shade, st, launches);
-    else if (stack_depth <= 64) e = launch_depth_loop_t<64>(s, fp, P, counts, stats, err, rec, grid_trace, grid_shade, st, launches);
-    else e = launch_depth_loop_t<128>(s, fp, P, counts, stats, err, rec, grid_trace, grid_shade, st, launches);
+    if (stack_depth <= 32) e = launch_depth_loop_t<32>(s, fp, P, counts, stats, err, rec, grid_trace, grid_shade, st, launches, tm);
+    else if (stack_depth <= 64) e = launch_depth_loop_t<64>(s, fp, P, counts, stats, err, rec, grid_trace, grid_shade, st, launches, tm);
+    else e = launch_depth_loop_t<128>(s, fp, P, counts, stats, err, rec, grid_trace, grid_shade, st, launches, tm);
     if (e != cudaSuccess) return e;
     k_finish<<<(fp.wave + 255) / 256, 256, 0, st>>>(fp, P, accum, rec);
     *launches += 1;

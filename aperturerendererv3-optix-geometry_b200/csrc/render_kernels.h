@@ -16,9 +16,18 @@ cudaError_t launch_trace_rays(const SceneView& s, int stack_depth, const float4*
                               float* t, int* err, int grid, cudaStream_t st);
 cudaError_t launch_rng_init(const FrameParams& fp, uint4* b0, uint2* b1, cudaStream_t st);
 cudaError_t launch_rng_tape(const FrameParams& fp, int spp, int per_path, float* out, cudaStream_t st);
+// Optional event pairs around every traversal launch: ev[2k], ev[2k+1].
+struct LaunchTimers {
+    cudaEvent_t* extend_ev = nullptr;
+    cudaEvent_t* shadow_ev = nullptr;
+    int cap = 0;        // event pairs available per kind
+    int n_extend = 0;   // pairs recorded
+    int n_shadow = 0;
+};
+
 cudaError_t launch_wave(const SceneView& s, int stack_depth, const FrameParams& fp, const PathSoA& P, uint4* b0, uint2* b1,
                         int32_t* counts, unsigned long long* stats, int* err, double* accum, ar_path_record* rec,
-                        int grid_trace, int grid_shade, cudaStream_t st, int64_t* launches);
+                        int grid_trace, int grid_shade, cudaStream_t st, int64_t* launches, LaunchTimers* timers);
 cudaError_t launch_mean(const double* accum, int64_t n, double inv, float* out, cudaStream_t st);
 cudaError_t launch_add(const double* src, int64_t n, double* dst, cudaStream_t st);
 

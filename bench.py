@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark of the sm_100a path-tracing core on the config-2 workload.
+
+Workload (one step): render the seeded 1,024,002-triangle icosphere scene
+(800 icospheres x 1280 triangles + ground quad, 16 emissive spheres) at
+1920x1080, 64 spp, max depth 12, NEE + MIS, FP32 RGB -- the reference's
+offline SceneRenderer::Render call (core/scene.cu:276-306).  The metric is
+Mrays/s: closest-hit plus any-hit BVH queries per second, whole job.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 is launched with torch.distributed.run: every rank renders the same
+image with its own sample streams (frame offset rank * spp) and the FP64
+accumulators are summed to rank 0 with one NCCL reduce per step (weak scaling).
+The reference arm times the reference method's CPU implementation of the path
+on the host cores (the reference compiled for the host when oracle/_ref holds
+it, else the C restatement in oracle/) and prints the same JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "aperturerendererv3-optix-geometry_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+sys.path.insert(0, PKG)
+
+import scenes  # noqa: E402
+from aperture_b200 import Camera, RenderParams, RenderStats, Scene, make_params  # noqa: E402
+
+METRIC = "Mrays/s"
+WIDTH, HEIGHT, SPP, DEPTH = 1920, 1080, 64, 12
+WORKLOAD = ("config2: 800 icospheres x 1280 triangles + 2-triangle ground (1,024,002 triangles) + 16 emissive "
+            "spheres, seed 0xA11CE+2, 1920x1080, 64 spp, max depth 12, NEE+MIS, RR from depth 3, FP32 RGB")
+
+
+def config_block(n_gpus: int) -> dict:
+    return {"workload": WORKLOAD, "triangles": 1024002, "width": WIDTH, "height": HEIGHT, "spp": SPP,
+            "max_depth": DEPTH, "camera": "spheres_camera(): pos (0,30,-150), fov 60",
+            "l2": "flushed between timed steps (256 MiB write); path state 470 MB > L2",
+            "parallelism": f"replicas x{n_gpus}, FP64 accumulators reduced with NCCL" if n_gpus > 1 else "single GPU"}
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ("active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                if self.uuid and self.uuid not in parts[0]:
+                    continue
+                try:
+                    sm.append(float(parts[1].split()[0]))
+                    smax.append(float(parts[2].split()[0]))
+                except ValueError:
+                    continue
+                for name, val in zip(names[1:], parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ----------------------------------------------------------------------------- CPU legs
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_cpu_impl():
+    """The reference's own host build when oracle/_ref has it, else the C restatement."""
+    sys.path.insert(0, ORACLE)
+    import oracle
+    return oracle, "port"
+
+
+def cpu_sample(objs, cam: Camera, params: RenderParams, target_s: float, threads: int, osc=None) -> dict:
+    """Render a bounded, image-wide sample of pixels at 1 spp on the host cores."""
+    oracle, kind = reference_cpu_impl()
+    if osc is None:
+        osc = oracle.OracleScene(objs)
+    p1 = make_params(spp=1, max_depth=params.max_depth, rr_depth=params.rr_depth, use_nee=params.use_nee,
+                     sky=params.sky, seed=params.seed)
+    npix = cam.width * cam.height
+
+    def run(step: int, offset: int):
+        t0 = time.perf_counter()
+        _, e, s = osc.render_image(cam, p1, offset, npix, step=step, threads=threads)
+        return time.perf_counter() - t0, e, s
+
+    step = 4096                              # start with ~506 pixels spread over the image
+    while True:
+        dt, e, s = run(step, 0)
+        if dt >= 0.5 * target_s or step == 1:
+            break
+        step = max(1, int(step * max(dt, 1e-3) / target_s))
+    return {"osc": osc, "value": (e + s) / dt / 1e6, "seconds": dt, "pixels": (npix + step - 1) // step,
+            "ext": e, "shadow": s, "kind": kind, "step": step}
+
+
+# ----------------------------------------------------------------------------- ours
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.gpus != world:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}; launch N>1 with torch.distributed.run")
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    props = torch.cuda.get_device_properties(local)
+    uuid = str(getattr(props, "uuid", "") or "") or None
+
+    objs = scenes.spheres_scene()
+    scene = Scene(objs, device=local)
+    cam = scenes.spheres_camera(WIDTH, HEIGHT)
+    params = make_params(spp=SPP, max_depth=DEPTH, frame_offset=rank * SPP)
+    npix = WIDTH * HEIGHT
+    stream = torch.cuda.Stream(device=dev)
+    out = torch.empty(npix * 3, dtype=torch.float32, device=dev)
+    accum = torch.zeros(npix * 3, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step(stats: RenderStats | None):
+        scene.render_device(cam, params, out.data_ptr(), accum.data_ptr(), stream.cuda_stream, stats)
+        if world > 1:
+            with torch.cuda.stream(stream):
+                dist.reduce(accum, dst=0)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step(RenderStats())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    sampler = ClockSampler(uuid) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    tot = {"ext": 0, "sh": 0, "paths": 0, "launches": 0, "ext_ms": 0.0, "sh_ms": 0.0, "ext_launch": 0,
+           "sh_launch": 0}
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            st = RenderStats()
+            ev[k][0].record(stream)
+            step(st)
+            ev[k][1].record(stream)
+            tot["ext"] += st.extension_rays
+            tot["sh"] += st.shadow_rays
+            tot["paths"] += st.paths
+            tot["launches"] += st.kernel_launches
+            tot["ext_ms"] += st.extend_ms
+            tot["sh_ms"] += st.shadow_ms
+            tot["ext_launch"] += st.extend_launches
+            tot["sh_launch"] += st.shadow_launches
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop() if sampler else None
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    rays = torch.tensor([tot["ext"] + tot["sh"], tot["paths"]], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(rays, op=dist.ReduceOp.SUM)
+    total_ms = float(t.item())
+    all_rays, all_paths = float(rays[0].item()), float(rays[1].item())
+    value = all_rays / (total_ms / 1e3) / 1e6
+
+    # end to end through the C ABI with host buffers (image copied back every step)
+    e2e_s = []
+    e2e_rays = 0
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        img, st = scene.render(cam, params)
+        e2e_s.append(time.perf_counter() - t0)
+        e2e_rays += st.extension_rays + st.shadow_rays
+    e2e_t = torch.tensor([sum(e2e_s)], dtype=torch.float64, device=dev)
+    e2e_r = torch.tensor([float(e2e_rays)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(e2e_r, op=dist.ReduceOp.SUM)
+    e2e_value = float(e2e_r.item()) / float(e2e_t.item()) / 1e6
+
+    if rank == 0:
+        with open(os.path.join(ROOT, "tests", "golden", "algorithmic_bytes.json")) as f:
+            ab = json.load(f)
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peaks = json.load(f)
+        except Exception:
+            pass
+        hbm = peaks.get("hbm_gbs")
+        peak_src = "measured" if hbm else "fallback"
+        hbm = hbm or 6650.0
+        kernels = {
+            "extend (closest hit)": (tot["ext_ms"], tot["ext_launch"], tot["ext"] * ab["extension"]["bytes_per_query"]),
+            "shadow (any hit)": (tot["sh_ms"], tot["sh_launch"], tot["sh"] * ab["shadow"]["bytes_per_query"]),
+        }
+        dom = max(kernels, key=lambda k: kernels[k][0])
+        ms, nl, byts = kernels[dom]
+        per_launch_bytes = byts / max(nl, 1)
+        per_launch_s = ms / 1e3 / max(nl, 1)
+        achieved = per_launch_bytes / per_launch_s / 1e9 if per_launch_s > 0 else None
+        l2 = measure_l2(torch, dev)
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                tj = json.load(f)
+            tk = "extend" if dom.startswith("extend") else "shadow"
+            if tk in tj and "dram_bytes_per_query" in tj[tk]:
+                traffic = tj[tk]["dram_bytes_per_query"] * (tot["ext"] if tk == "extend" else tot["sh"]) / max(nl, 1)
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+            "config": config_block(world),
+            "samples_per_s": round(all_paths / (total_ms / 1e3), 1),
+            "rays": {"extension": tot["ext"], "shadow": tot["sh"], "per_path": round((tot["ext"] + tot["sh"]) / max(tot["paths"], 1), 4)},
+            "kernel_ms": {"extend": round(tot["ext_ms"], 3), "shadow": round(tot["sh_ms"], 3), "total": round(total_ms, 3)},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1) if achieved else None,
+                         "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4) if achieved else None,
+                         "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback",
+                         "traffic": traffic,
+                         "algorithmic_bytes_per_query": ab["extension" if dom.startswith("extend") else "shadow"]["bytes_per_query"],
+                         "l2_copy_gbs_measured": round(l2, 1),
+                         "frac_of_l2_copy": round(achieved / l2, 4) if achieved and l2 else None},
+            "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s",
+                    "h2d_bytes_per_step": ctypes.sizeof(Camera) + ctypes.sizeof(RenderParams),
+                    "d2h_bytes_per_step": npix * 3 * 4},
+            "gpu_launches": int(tot["launches"]),
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu:
+            cs = cpu_sample(objs, cam, params, args.cpu_seconds, cpu_threads())
+            line["cpu_baseline"] = {"value": round(cs["value"], 4), "unit": "Mrays/s", "cores": cpu_threads(),
+                                    "kind": cs["kind"],
+                                    "sample": f"every {cs['step']}th pixel of the image ({cs['pixels']} pixels) at 1 spp, "
+                                              f"{cs['ext'] + cs['shadow']} queries in {cs['seconds']:.1f} s"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def measure_l2(torch, dev) -> float:
+    """Copy bandwidth of an L2-resident 32 MiB buffer (read + write bytes)."""
+    a = torch.empty(8 << 20, dtype=torch.float32, device=dev)
+    b = torch.empty_like(a)
+    for _ in range(5):
+        b.copy_(a)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record()
+    for _ in range(200):
+        b.copy_(a)
+    e.record()
+    torch.cuda.synchronize()
+    return 2 * a.numel() * 4 * 200 / (s.elapsed_time(e) / 1e3) / 1e9
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    objs = scenes.spheres_scene()
+    cam = scenes.spheres_camera(WIDTH, HEIGHT)
+    params = make_params(spp=SPP, max_depth=DEPTH)
+    threads = cpu_threads()
+    osc = None
+    vals, secs, qs = [], [], 0
+    sample = None
+    for k in range(args.warmup + args.steps):
+        cs = cpu_sample(objs, cam, params, args.cpu_seconds, threads, osc=osc)
+        osc = cs["osc"]
+        if k >= args.warmup:
+            vals.append(cs["value"])
+            secs.append(cs["seconds"])
+            qs += cs["ext"] + cs["shadow"]
+            sample = cs
+    value = qs / sum(secs) / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * sum(secs) / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+        "config": config_block(world), "impl": "reference",
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": threads, "kind": sample["kind"],
+                         "sample": f"per step every {sample['step']}th pixel ({sample['pixels']} pixels) at 1 spp "
+                                   f"on {threads} host threads (OpenMP)"},
+        "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU sample length per measurement")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -122,13 +122,20 @@ typedef struct ar_scene_info {
     int32_t camera_inside; /* reserved */
 } ar_scene_info;
 
+/* Counters of one ar_render call.  Passing a stats pointer also times every
+ * closest-hit and any-hit traversal launch with CUDA events on the caller's
+ * stream (a few microseconds of overhead per launch). */
 typedef struct ar_render_stats {
-    int64_t paths;         /* camera paths traced                                     */
-    int64_t extension_rays;/* closest-hit BVH queries                                 */
-    int64_t shadow_rays;   /* any-hit BVH queries                                     */
-    int64_t kernel_launches;
-    float   trace_ms;      /* device time of the traversal kernels (CUDA events)      */
-    float   total_ms;      /* device time of the whole render call                    */
+    int64_t paths;           /* camera paths traced                                  */
+    int64_t extension_rays;  /* closest-hit BVH queries                              */
+    int64_t shadow_rays;     /* any-hit BVH queries actually traversed               */
+    int64_t kernel_launches; /* kernels this call launched                           */
+    int64_t extend_launches; /* closest-hit traversal launches                       */
+    int64_t shadow_launches; /* any-hit traversal launches                           */
+    float   extend_ms;       /* summed device time of the closest-hit launches       */
+    float   shadow_ms;       /* summed device time of the any-hit launches           */
+    float   total_ms;        /* device time of the whole render call                 */
+    int32_t reserved;
 } ar_render_stats;
 
 typedef struct ar_scene ar_scene;

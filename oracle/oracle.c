@@ -1244,7 +1244,19 @@ static V3 sky_lighting(V3 d, int sky)
 /* ------------------------------------------------------------------------ */
 /* Path loop                                                                  */
 /* ------------------------------------------------------------------------ */
-typedef struct { int64_t ext_rays, shadow_rays; } Counters;
+typedef struct {
+    int64_t ext_rays, shadow_rays;
+    /* optional recorders of every query (8 floats per ray) */
+    float* ext_out; int64_t ext_cap;
+    float* sh_out; int64_t sh_cap;
+} Counters;
+
+static void record_ray(float* out, int64_t cap, int64_t k, V3 o, float tmin, V3 d, float tmax)
+{
+    if (!out || k >= cap) return;
+    float* r = out + 8 * k;
+    r[0] = o.x; r[1] = o.y; r[2] = o.z; r[3] = tmin; r[4] = d.x; r[5] = d.y; r[6] = d.z; r[7] = tmax;
+}
 
 static int path_mode(const or_scene* s)
 {
@@ -1274,6 +1286,7 @@ static int segment_occluded(const or_scene* s, float eps_d, V3 src, V3 dst, Coun
     const float eps = eps_d * fmaxf(1.0f, fmaxf(len3(src), len3(dst)));
     const float tMax = fmaxf(0.0f, dist - eps);
     if (tMax <= 0.0f) return 0;
+    record_ray(cnt->sh_out, cnt->sh_cap, cnt->shadow_rays, src, 0.0f, dir, tMax);
     cnt->shadow_rays++;
     const TraceResult r = traverse(s, src, dir, 0.0f, tMax, 1, path_mode(s));
     return r.obj >= 0;
@@ -1306,6 +1319,7 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
         memset(&ic, 0, sizeof(ic));
         ic.obj = -1; ic.light = -1;
         int hit;
+        record_ray(cnt->ext_out, cnt->ext_cap, cnt->ext_rays, cro, eps, crd, INFINITY);
         cnt->ext_rays++;
         if (media.inside && media.obj >= 0 &&
             (s->o[media.obj].type != AR_OBJ_TRIANGLE || (s->flags & OR_TRIANGLE_SOLO_MEDIA))) {
@@ -1485,7 +1499,8 @@ int64_t or_render_paths(const or_scene* s, const ar_camera* cam, const ar_render
         float ray[8];
         or_camera_ray(cam, i, j, jx, jy, ray);
         PathOut po;
-        Counters cnt = {0, 0};
+        Counters cnt;
+        memset(&cnt, 0, sizeof(cnt));
         calculate_radiance(s, p, inside, &g, v3(ray[0], ray[1], ray[2]), v3(ray[4], ray[5], ray[6]), &po, &cnt);
         ar_path_record* r = &rec[k];
         memset(r, 0, sizeof(*r));
@@ -1500,19 +1515,23 @@ int64_t or_render_paths(const or_scene* s, const ar_camera* cam, const ar_render
 }
 
 void or_render_image(const or_scene* s, const ar_camera* cam, const ar_render_params* p,
-                     int64_t pb, int64_t pe, double* accum, int64_t* ext, int64_t* shadow, int threads)
+                     int64_t pb, int64_t pe, int64_t step, double* accum, int64_t* ext, int64_t* shadow, int threads)
 {
     const int64_t W = cam->width;
     const int inside = camera_overlap(s, from_ar(cam->position));
     int64_t e = 0, sh = 0;
+    if (step < 1) step = 1;
+    const int64_t count = (pe - pb + step - 1) / step;
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
-#pragma omp parallel for schedule(dynamic, 64) reduction(+ : e, sh)
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : e, sh)
 #endif
-    for (int64_t pix = pb; pix < pe; ++pix) {
+    for (int64_t k = 0; k < count; ++k) {
+        const int64_t pix = pb + k * step;
         const int i = (int)(pix % W), j = (int)(pix / W);
         double acc[3] = {0.0, 0.0, 0.0};
-        Counters cnt = {0, 0};
+        Counters cnt;
+        memset(&cnt, 0, sizeof(cnt));
         for (int smp = 0; smp < p->spp; ++smp) {
             Rng g;
             g.tape = NULL; g.limit = 0; g.pos = 0; g.overflow = 0;
@@ -1536,3 +1555,29 @@ float or_cosf(float x) { return om_cosf(x); }
 float or_expf(float x) { return om_expf(x); }
 float or_logf(float x) { return om_logf(x); }
 float or_powf(float x, float y) { return om_powf(x, y); }
+
+int64_t or_collect_rays(const or_scene* s, const ar_camera* cam, const ar_render_params* p, int64_t pb, int64_t pe,
+                        float* ext, int64_t ext_cap, int64_t* n_ext, float* sh, int64_t sh_cap, int64_t* n_sh)
+{
+    const int64_t W = cam->width;
+    const int inside = camera_overlap(s, from_ar(cam->position));
+    Counters cnt;
+    memset(&cnt, 0, sizeof(cnt));
+    cnt.ext_out = ext; cnt.ext_cap = ext_cap; cnt.sh_out = sh; cnt.sh_cap = sh_cap;
+    for (int64_t pix = pb; pix < pe; ++pix) {
+        const int i = (int)(pix % W), j = (int)(pix / W);
+        for (int smp = 0; smp < p->spp; ++smp) {
+            Rng g;
+            g.tape = NULL; g.limit = 0; g.pos = 0; g.overflow = 0;
+            g.state = p->seed ^ ((uint64_t)pix * 0x9e3779b97f4a7c15ull) ^ ((uint64_t)(smp + p->frame_offset) << 40);
+            const float jx = rng1(&g), jy = rng1(&g);
+            float ray[8];
+            or_camera_ray(cam, i, j, jx, jy, ray);
+            PathOut po;
+            calculate_radiance(s, p, inside, &g, v3(ray[0], ray[1], ray[2]), v3(ray[4], ray[5], ray[6]), &po, &cnt);
+        }
+    }
+    *n_ext = cnt.ext_rays < ext_cap ? cnt.ext_rays : ext_cap;
+    *n_sh = cnt.shadow_rays < sh_cap ? cnt.shadow_rays : sh_cap;
+    return cnt.ext_rays + cnt.shadow_rays;
+}

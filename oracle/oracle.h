@@ -86,11 +86,18 @@ int64_t or_render_paths(const or_scene* s, const ar_camera* cam, const ar_render
                         const float* tape, int per_path, ar_path_record* records,
                         int threads);
 
-/* CPU baseline: render with an own per-path random generator (not curand), FP64
- * sums added into accum (w*h*3).  Counts closest-hit and shadow queries. */
+/* CPU baseline: render pixels pixel_begin, pixel_begin + step, ... < pixel_end
+ * with an own per-path random generator (not curand), FP64 sums added into
+ * accum (w*h*3).  Counts closest-hit and shadow queries. */
 void or_render_image(const or_scene* s, const ar_camera* cam, const ar_render_params* p,
-                     int64_t pixel_begin, int64_t pixel_end, double* accum,
+                     int64_t pixel_begin, int64_t pixel_end, int64_t step, double* accum,
                      int64_t* extension_rays, int64_t* shadow_rays, int threads);
+
+/* Run the CPU baseline path loop over pixels [pb, pe) single-threaded and
+ * record every closest-hit query (ext) and any-hit segment (sh) as 8-float rays,
+ * up to the given capacities.  Returns the number of queries. */
+int64_t or_collect_rays(const or_scene* s, const ar_camera* cam, const ar_render_params* p, int64_t pb, int64_t pe,
+                        float* ext, int64_t ext_cap, int64_t* n_ext, float* sh, int64_t sh_cap, int64_t* n_sh);
 
 /* Deterministic transcendental functions (exported for their own tests). */
 float or_sinf(float x);

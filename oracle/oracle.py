@@ -52,11 +52,14 @@ def load():
     lib.or_camera_ray.argtypes = [c_void_p, c_int, c_int, c_float, c_float, c_void_p]
     lib.or_render_paths.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int]
     lib.or_render_paths.restype = c_int64
-    lib.or_render_image.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, POINTER(c_int64),
-                                    POINTER(c_int64), c_int]
+    lib.or_render_image.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_void_p,
+                                    POINTER(c_int64), POINTER(c_int64), c_int]
     for f in ("or_sinf", "or_cosf", "or_expf", "or_logf"):
         getattr(lib, f).argtypes = [c_float]
         getattr(lib, f).restype = c_float
+    lib.or_collect_rays.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_void_p, c_int64,
+                                    POINTER(c_int64), c_void_p, c_int64, POINTER(c_int64)]
+    lib.or_collect_rays.restype = c_int64
     lib.or_powf.argtypes = [c_float, c_float]
     lib.or_powf.restype = c_float
     _lib = lib
@@ -133,15 +136,26 @@ class OracleScene:
                                     _p(rec), threads)
         return rec, over
 
-    def render_image(self, camera, params, pixel_begin=0, pixel_end=None, threads=0):
+    def render_image(self, camera, params, pixel_begin=0, pixel_end=None, step=1, threads=0):
+        """FP64 sums of pixels pixel_begin, +step, ... (others stay zero), query counts."""
         npix = camera.width * camera.height
         if pixel_end is None:
             pixel_end = npix
         acc = np.zeros((npix, 3), np.float64)
         e, s = c_int64(0), c_int64(0)
-        _lib.or_render_image(self._h, ctypes.byref(camera), ctypes.byref(params), pixel_begin, pixel_end, _p(acc),
-                             ctypes.byref(e), ctypes.byref(s), threads)
+        _lib.or_render_image(self._h, ctypes.byref(camera), ctypes.byref(params), pixel_begin, pixel_end, step,
+                             _p(acc), ctypes.byref(e), ctypes.byref(s), threads)
         return acc, e.value, s.value
+
+
+def collect_rays(scene: "OracleScene", camera, params, pixel_begin, pixel_end, cap=2_000_000):
+    """Extension and shadow queries of the CPU path loop over a pixel range."""
+    ext = np.zeros((cap, 8), np.float32)
+    sh = np.zeros((cap, 8), np.float32)
+    ne, ns = c_int64(0), c_int64(0)
+    _lib.or_collect_rays(scene._h, ctypes.byref(camera), ctypes.byref(params), pixel_begin, pixel_end, _p(ext), cap,
+                         ctypes.byref(ne), _p(sh), cap, ctypes.byref(ns))
+    return ext[:ne.value].copy(), sh[:ns.value].copy()
 
 
 def camera_ray(camera, i, j, jx, jy) -> np.ndarray:
