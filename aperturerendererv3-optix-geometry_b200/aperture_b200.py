@@ -60,7 +60,7 @@ class RenderParams(ctypes.Structure):
 
 class PathRecord(ctypes.Structure):
     _fields_ = [("radiance", c_float * 3), ("segments", c_int32), ("uniforms", c_int32), ("nee_rays", c_int32),
-                ("reserved", c_int32 * 2), ("hit_object", c_int32 * DEBUG_MAX_HITS)]
+                ("nee_depth_mask", c_int32), ("reserved", c_int32), ("hit_object", c_int32 * DEBUG_MAX_HITS)]
 
 
 class SceneInfo(ctypes.Structure):
@@ -71,6 +71,8 @@ class SceneInfo(ctypes.Structure):
 class RenderStats(ctypes.Structure):
     _fields_ = [("paths", c_int64), ("extension_rays", c_int64), ("shadow_rays", c_int64),
                 ("kernel_launches", c_int64), ("extend_launches", c_int64), ("shadow_launches", c_int64),
+                ("extend_node_visits", c_int64), ("extend_prim_tests", c_int64), ("shadow_node_visits", c_int64),
+                ("shadow_prim_tests", c_int64),
                 ("extend_ms", c_float), ("shadow_ms", c_float), ("total_ms", c_float), ("reserved", c_int32)]
 
 

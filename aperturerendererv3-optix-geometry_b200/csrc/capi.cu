@@ -76,7 +76,7 @@ private:
     bool changed_ = false;
 };
 
-constexpr int64_t kMaxWave = int64_t(1) << 22;
+constexpr int64_t kMaxPool = int64_t(1) << 21;  // paths in flight
 
 }  // namespace
 
@@ -84,7 +84,7 @@ struct ar_scene {
     int device = 0;
     int sm_count = 148;
     ar::SceneView view{};
-    int stack_depth = 32;
+    int grid_trace = 0;
     int64_t objects = 0, triangles = 0, lights = 0, nodes = 0, prims = 0;
     int64_t device_bytes = 0;
     std::vector<void*> owned;
@@ -101,11 +101,12 @@ struct ar_scene {
     uint2* base1 = nullptr;
     double* accum = nullptr;
     float* fout = nullptr;
-    int32_t* counts = nullptr;
+    ar::PoolCtl* ctl = nullptr;
     unsigned long long* stats = nullptr;
     int* err = nullptr;
+    uint32_t* ovf = nullptr;  // traversal stack overflow slabs, one per persistent thread
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::vector<cudaEvent_t> timer_events;  // 2 kinds x 2 events x launches
+    std::vector<cudaEvent_t> timer_ext, timer_sh;  // event pairs around traversal launches
 
     ~ar_scene()
     {
@@ -114,7 +115,8 @@ struct ar_scene {
         if (ws) cudaFree(ws);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
-        for (cudaEvent_t e : timer_events) cudaEventDestroy(e);
+        for (cudaEvent_t e : timer_ext) cudaEventDestroy(e);
+        for (cudaEvent_t e : timer_sh) cudaEventDestroy(e);
     }
 };
 
@@ -134,8 +136,10 @@ void ensure_workspace(ar_scene* s, int64_t wave, int64_t npix, bool debug)
     const size_t o_r0 = take(16 * W), o_r1 = take(8 * W), o_info = take(16 * W), o_prev = take(16 * W);
     const size_t o_media = take(16 * W), o_hit = take(16 * W), o_nee = take(16 * W), o_s0 = take(16 * W);
     const size_t o_s1 = take(16 * W), o_q0 = take(4 * W), o_q1 = take(4 * W), o_qs = take(4 * W), o_uc = take(4 * W);
+    const size_t o_qr = take(4 * W), o_free = take(4 * W);
     const size_t o_b0 = take(16 * N), o_b1 = take(8 * N), o_acc = take(24 * N), o_fout = take(12 * N);
-    const size_t o_cnt = take(64), o_stats = take(64), o_err = take(64);
+    const size_t o_cnt = take(sizeof(ar::PoolCtl)), o_stats = take(64), o_err = take(64);
+    const size_t o_ovf = take(static_cast<size_t>(s->grid_trace) * ar::kTraceBlock * ar::kStackOverflow * 4);
     s->ws = dalloc<char>(off, "render workspace");
     s->ws_bytes = off;
     s->ws_wave = wave;
@@ -152,13 +156,16 @@ void ensure_workspace(ar_scene* s, int64_t wave, int64_t npix, bool debug)
     P.q[0] = reinterpret_cast<int32_t*>(b + o_q0); P.q[1] = reinterpret_cast<int32_t*>(b + o_q1);
     P.qs = reinterpret_cast<int32_t*>(b + o_qs);
     P.ucount = reinterpret_cast<int32_t*>(b + o_uc);
+    P.qr = reinterpret_cast<int32_t*>(b + o_qr);
+    P.freeq = reinterpret_cast<int32_t*>(b + o_free);
     s->base0 = reinterpret_cast<uint4*>(b + o_b0);
     s->base1 = reinterpret_cast<uint2*>(b + o_b1);
     s->accum = reinterpret_cast<double*>(b + o_acc);
     s->fout = reinterpret_cast<float*>(b + o_fout);
-    s->counts = reinterpret_cast<int32_t*>(b + o_cnt);
+    s->ctl = reinterpret_cast<ar::PoolCtl*>(b + o_cnt);
     s->stats = reinterpret_cast<unsigned long long*>(b + o_stats);
     s->err = reinterpret_cast<int*>(b + o_err);
+    s->ovf = reinterpret_cast<uint32_t*>(b + o_ovf);
 }
 
 // intersection::Overlap (intersection.cuh:399-414) at the camera position; the
@@ -246,9 +253,11 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
     using namespace ar;
     ar::FrameParams fp = make_frame(s, cam, p);
     const int64_t npix = fp.npix;
-    int64_t wave = p->wave_paths > 0 ? std::min<int64_t>(p->wave_paths, kMaxWave) : kMaxWave;
-    wave = std::min<int64_t>(wave, npix);
-    ensure_workspace(s, wave, npix, rec_dev != nullptr);
+    const int64_t total = npix * p->spp;
+    int64_t pool = p->wave_paths > 0 ? std::min<int64_t>(p->wave_paths, kMaxPool) : kMaxPool;
+    pool = std::max<int64_t>(1, std::min<int64_t>(pool, total));
+    fp.pool = static_cast<int32_t>(pool);
+    ensure_workspace(s, pool, npix, rec_dev != nullptr);
     PathSoA P = s->paths;
     if (!rec_dev) P.ucount = nullptr;
     ck(cudaMemsetAsync(s->accum, 0, sizeof(double) * 3 * npix, st), "memset accum");
@@ -257,51 +266,61 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
     if (!s->ev0) { ck(cudaEventCreate(&s->ev0), "event"); ck(cudaEventCreate(&s->ev1), "event"); }
     ck(cudaEventRecord(s->ev0, st), "event record");
     ck(launch_rng_init(fp, s->base0, s->base1, st), "rng init");
-    int64_t launches = 1;
-    const int grid_trace = s->sm_count * 8;
-    const int grid_shade = s->sm_count * 4;
-    const int64_t waves = static_cast<int64_t>(p->spp) * ((npix + wave - 1) / wave);
+    ck(launch_pool_init(P, s->ctl, static_cast<int>(pool), total, st), "pool init");
+    int64_t launches = 2;
+    const int grid_trace = s->grid_trace;
+    const int grid_other = s->sm_count * 4;
     LaunchTimers tm;
-    LaunchTimers* tmp = nullptr;
-    if (stats) {
-        const size_t pairs = static_cast<size_t>(waves * p->max_depth);
-        if (pairs <= (size_t(1) << 16)) {
-            while (s->timer_events.size() < 4 * pairs) {
-                cudaEvent_t e;
-                ck(cudaEventCreate(&e), "event create");
-                s->timer_events.push_back(e);
+    LaunchTimers* tmp = stats ? &tm : nullptr;
+    constexpr int kBatch = 16;
+    // every iteration retires or advances each path by one segment: a hard bound
+    const int64_t max_iter = (total / pool + 2) * (static_cast<int64_t>(p->max_depth) + 2) + kBatch;
+    int cur = 0;
+    int64_t iters = 0;
+    int64_t retired = 0;
+    for (;;) {
+        if (tmp) {
+            const size_t need = static_cast<size_t>(2 * (iters + kBatch));
+            for (auto* v : {&s->timer_ext, &s->timer_sh}) {
+                while (v->size() < need) {
+                    cudaEvent_t e;
+                    ck(cudaEventCreate(&e), "event create");
+                    v->push_back(e);
+                }
             }
-            tm.extend_ev = s->timer_events.data();
-            tm.shadow_ev = s->timer_events.data() + 2 * pairs;
-            tm.cap = static_cast<int>(pairs);
-            tmp = &tm;
+            // the vectors may have grown: re-point; recorded pairs keep their handles
+            tm.extend_ev = s->timer_ext.data();
+            tm.shadow_ev = s->timer_sh.data();
+            tm.cap = static_cast<int>(need / 2);
         }
-    }
-    for (int sidx = 0; sidx < p->spp; ++sidx) {
-        for (int64_t first = 0; first < npix; first += wave) {
-            fp.spp_index = sidx;
-            fp.first_pixel = static_cast<int32_t>(first);
-            fp.wave = static_cast<int32_t>(std::min<int64_t>(wave, npix - first));
-            ck(launch_wave(s->view, s->stack_depth, fp, P, s->base0, s->base1, s->counts, s->stats, s->err, s->accum,
-                           rec_dev, grid_trace, grid_shade, st, &launches, tmp),
-               "render launch");
-        }
+        ck(launch_iterations(s->view, fp, P, s->ctl, s->base0, s->base1, s->stats, s->ovf, s->err, s->accum, rec_dev,
+                             kBatch, &cur, grid_trace, grid_other, st, &launches, tmp),
+           "render launch");
+        iters += kBatch;
+        ck(cudaMemcpyAsync(&retired, &s->ctl->retired, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "poll");
+        ck(cudaStreamSynchronize(st), "sync");
+        if (retired >= total) break;
+        if (iters > max_iter) return fail(AR_ERR_DEVICE_FAULT, "path pool did not drain");
     }
     ck(cudaEventRecord(s->ev1, st), "event record");
     if (stats) {
-        unsigned long long h[2];
+        unsigned long long h[6];
         ck(cudaMemcpyAsync(h, s->stats, sizeof(h), cudaMemcpyDeviceToHost, st), "stats copy");
         ck(cudaStreamSynchronize(st), "sync");
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, s->ev0, s->ev1);
         std::memset(stats, 0, sizeof(*stats));
-        stats->paths = npix * p->spp;
+        stats->paths = total;
         stats->extension_rays = static_cast<int64_t>(h[0]);
         stats->shadow_rays = static_cast<int64_t>(h[1]);
         stats->kernel_launches = launches;
         stats->total_ms = ms;
-        stats->extend_launches = waves * p->max_depth;
-        stats->shadow_launches = waves * p->max_depth;
+        stats->extend_launches = iters;
+        stats->shadow_launches = iters;
+        stats->extend_node_visits = static_cast<int64_t>(h[2]);
+        stats->extend_prim_tests = static_cast<int64_t>(h[3]);
+        stats->shadow_node_visits = static_cast<int64_t>(h[4]);
+        stats->shadow_prim_tests = static_cast<int64_t>(h[5]);
         float e_ms = 0.0f, s_ms = 0.0f;
         for (int k = 0; k < tm.n_extend; ++k) {
             float t = 0.0f;
@@ -313,8 +332,8 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
             cudaEventElapsedTime(&t, tm.shadow_ev[2 * k], tm.shadow_ev[2 * k + 1]);
             s_ms += t;
         }
-        stats->extend_ms = tmp ? e_ms : -1.0f;
-        stats->shadow_ms = tmp ? s_ms : -1.0f;
+        stats->extend_ms = e_ms;
+        stats->shadow_ms = s_ms;
     }
     return AR_OK;
 }
@@ -380,8 +399,15 @@ ar_status ar_scene_create(const ar_object_desc* objects, size_t count, int32_t d
         v.num_nodes = static_cast<int32_t>(hs.prims.empty() ? 0 : hs.nodes.size());
         v.num_objects = static_cast<int32_t>(hs.objects.size());
         v.num_lights = static_cast<int32_t>(hs.light_object.size());
-        s->stack_depth = hs.stack_bound <= 32 ? 32 : (hs.stack_bound <= 64 ? 64 : 128);
-        if (hs.stack_bound > 128) throw std::domain_error("BVH too deep for the traversal stack");
+        if (hs.stack_bound > ar::kStackMax) throw std::domain_error("BVH too deep for the traversal stack");
+        s->grid_trace = ar::trace_grid(s->sm_count);
+        {
+            ar_camera c0{};
+            c0.width = c0.height = 1;
+            c0.fov_y_deg = 60.0f;
+            const ar::FrameParams f0 = make_frame(s, &c0, nullptr);
+            ck(ar::set_intersect_eps(f0.eps_tab), "upload INTERSECT_EPS");
+        }
         s->objects = static_cast<int64_t>(count);
         s->triangles = hs.triangles;
         s->lights = static_cast<int64_t>(hs.light_object.size());
@@ -484,9 +510,15 @@ ar_status ar_trace_rays(ar_scene* s, const float* rays, size_t n, int32_t any_hi
         dobj = hit_object;
         dt = hit_t;
     }
-    const int grid = s->sm_count * 8;
-    cudaError_t e = ar::launch_trace_rays(s->view, s->stack_depth, drays, static_cast<int64_t>(n), any_hit ? 1 : 0, dobj, dt,
-                                          s->err, grid, st);
+    cudaError_t e = cudaSuccess;
+    const size_t chunk = size_t(1) << 30;
+    for (size_t first = 0; first < n && e == cudaSuccess; first += chunk) {
+        const int cnt = static_cast<int>(std::min(chunk, n - first));
+        e = cudaMemsetAsync(&s->ctl->fetch_rays, 0, sizeof(int32_t), st);
+        if (e == cudaSuccess)
+            e = ar::launch_trace_rays(s->view, drays + 2 * first, cnt, any_hit ? 1 : 0, dobj + first,
+                                      dt ? dt + first : nullptr, s->ctl, s->ovf, s->err, s->grid_trace, st);
+    }
     if (e == cudaSuccess && mem_kind == AR_MEM_HOST) {
         e = cudaMemcpyAsync(hit_object, dobj, n * 4, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess && hit_t) e = cudaMemcpyAsync(hit_t, dt, n * 4, cudaMemcpyDeviceToHost, st);

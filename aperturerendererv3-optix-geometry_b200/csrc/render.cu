@@ -70,22 +70,39 @@ __device__ __forceinline__ unsigned long long ref_pixel_index(int i, int j, int 
 }
 
 // ------------------------------------------------------------------ ray queries
-template <int kDepth>
-__global__ void __launch_bounds__(kTraceBlock) k_trace_rays(SceneView s, const float4* __restrict__ rays, int64_t n,
-                                                            int any_hit, int32_t* __restrict__ out_obj,
-                                                            float* __restrict__ out_t, int* err)
+
+__device__ __forceinline__ uint32_t* lane_stack(uint32_t* smem)
+{
+    return smem + (threadIdx.x >> 5) * (kStackShared * 32) + lane_id();
+}
+__device__ __forceinline__ uint32_t* thread_overflow(uint32_t* base)
+{
+    return base + (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) * kStackOverflow;
+}
+
+struct RaysIO {
+    const float4* rays;
+    int32_t* out_obj;
+    float* out_t;
+    __device__ __forceinline__ int load(const SceneView&, int k, RayState& r)
+    {
+        const float4 a = rays[2 * static_cast<int64_t>(k)], b = rays[2 * static_cast<int64_t>(k) + 1];
+        ray_begin(r, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w);
+        return k;
+    }
+    __device__ __forceinline__ void store(const SceneView&, int k, const RayState& r)
+    {
+        out_obj[k] = r.best.obj;
+        if (out_t) out_t[k] = r.best.t;
+    }
+};
+
+template <bool kAny>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_rays(SceneView s, RaysIO io, int n, PoolCtl* ctl,
+                                                            uint32_t* ovf, int* err)
 {
     extern __shared__ uint32_t smem[];
-    uint32_t* stack = smem + (threadIdx.x >> 5) * (kDepth * 32) + lane_id();
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const float4 a = rays[2 * i], b = rays[2 * i + 1];
-        const f3 o = mk(a.x, a.y, a.z), d = mk(b.x, b.y, b.z);
-        const Hit h = any_hit ? trace_ray<true, kDepth>(s, o, d, a.w, b.w, stack, err)
-                              : trace_ray<false, kDepth>(s, o, d, a.w, b.w, stack, err);
-        out_obj[i] = h.obj;
-        if (out_t) out_t[i] = h.t;
-    }
+    traverse_queue<kAny>(s, io, n, &ctl->fetch_rays, lane_stack(smem), thread_overflow(ovf), err, nullptr);
 }
 
 // ------------------------------------------------------------------ RNG
@@ -115,91 +132,161 @@ __global__ void k_rng_tape(FrameParams fp, int spp, int per_path, float* out)
     }
 }
 
-// ------------------------------------------------------------------ raygen
-// RenderCamera (scene.cu:213-230) + CalculateRadiance prologue (render.cuh:520-539)
-__global__ void k_raygen(FrameParams fp, PathSoA P, uint4* base0, uint2* base1, int32_t* counts, ar_path_record* rec)
+// ------------------------------------------------------------------ path pool
+__global__ void k_pool_init(PathSoA P, PoolCtl* ctl, int pool, int64_t total)
 {
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot == 0) { counts[0] = fp.wave; }
-    if (slot >= fp.wave) return;
-    const int p = fp.first_pixel + slot;
-    const int i = p % fp.width, j = p / fp.width;
-    Rng r;
-    {
-        const uint4 a = base0[p];
-        const uint2 b = base1[p];
-        r.st.d = a.x; r.st.v[0] = a.y; r.st.v[1] = a.z; r.st.v[2] = a.w; r.st.v[3] = b.x; r.st.v[4] = b.y;
-        r.st.boxmuller_flag = 0; r.st.boxmuller_flag_double = 0;
-        r.st.boxmuller_extra = 0.0f; r.st.boxmuller_extra_double = 0.0;
-        r.used = 0;
-        // advance the per-pixel base state to the next frame: offset + 2^32
-        curandStateXORWOW_t nx = r.st;
-        skipahead(1ull << 32, &nx);
-        base0[p] = make_uint4(nx.d, nx.v[0], nx.v[1], nx.v[2]);
-        base1[p] = make_uint2(nx.v[3], nx.v[4]);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < pool) P.freeq[i] = i;
+    if (i == 0) {
+        ctl->qcount[0] = 0;
+        ctl->qcount[1] = 0;
+        ctl->shadow_count = 0;
+        ctl->retire_count = 0;
+        ctl->fetch_ext = 0;
+        ctl->fetch_shadow = 0;
+        ctl->fetch_rays = 0;
+        ctl->free_count = pool;
+        ctl->plan_new = 0;
+        ctl->plan_src = 0;
+        ctl->gen_next = 0;
+        ctl->plan_first = 0;
+        ctl->retired = 0;
+        ctl->total = total;
     }
-    const float jx = r.next();
-    const float jy = r.next();
-    const float u = (static_cast<float>(i) + jx) / static_cast<float>(fp.width);
-    const float v = (static_cast<float>(j) + jy) / static_cast<float>(fp.height);
-    const float ndcx = u * 2.0f - 1.0f;
-    const float ndcy = static_cast<float>((1.0 - static_cast<double>(v)) * 2.0 - 1.0);
-    const float sx = ndcx * fp.tan_half_x;
-    const float sy = ndcy * fp.tan_half_y;
-    const f3 cd = mk(fp.cam_d[0], fp.cam_d[1], fp.cam_d[2]);
-    const f3 right = mk(fp.right[0], fp.right[1], fp.right[2]);
-    const f3 up = mk(fp.up[0], fp.up[1], fp.up[2]);
-    const f3 dir0 = normalize(cd + right * sx + up * sy);
-    const f3 dir = normalize(dir0);  // CalculateRadiance: rayDirection = normalize(rayDirection)
-    const f3 o = mk(fp.cam_o[0], fp.cam_o[1], fp.cam_o[2]);
-    P.o[slot] = f4(o, 0.0f);
-    P.d[slot] = f4(dir, 0.0f);
-    P.mask[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    P.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const int ri = fp.spp_index * fp.npix + p;
-    if (rec) {
+}
+
+// Start of an iteration: decide how many new samples enter the pool (at most
+// one per pixel per iteration, so the per-pixel random state is advanced in
+// sample order), and reset the queues this iteration fills.
+__global__ void k_plan(PoolCtl* ctl, int cur, int npix)
+{
+    const int64_t remaining = ctl->total - ctl->gen_next;
+    int n = min(ctl->free_count, npix);
+    if (static_cast<int64_t>(n) > remaining) n = static_cast<int>(remaining);
+    ctl->plan_new = n;
+    ctl->plan_src = ctl->free_count - n;
+    ctl->free_count -= n;
+    ctl->plan_first = ctl->gen_next;
+    ctl->gen_next += n;
+    ctl->qcount[1 - cur] = 0;
+    ctl->shadow_count = 0;
+    ctl->retire_count = 0;
+    ctl->fetch_ext = 0;
+    ctl->fetch_shadow = 0;
+}
+
+// RenderCamera (scene.cu:213-230) + CalculateRadiance prologue (render.cuh:520-539)
+// for sample g = s * npix + p, in a free slot; appended to the extension queue.
+__global__ void k_regen(FrameParams fp, PathSoA P, PoolCtl* ctl, int cur, uint4* base0, uint2* base1,
+                        ar_path_record* rec)
+{
+    const int n = ctl->plan_new;
+    const int src = ctl->plan_src;
+    const int64_t first = ctl->plan_first;
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        const bool act = i < n;
+        int slot = 0;
+        if (act) {
+            slot = P.freeq[src + i];
+            const int64_t g = first + i;
+            const int sidx = static_cast<int>(g / fp.npix);
+            const int p = static_cast<int>(g - static_cast<int64_t>(sidx) * fp.npix);
+            const int px = p % fp.width, py = p / fp.width;
+            Rng r;
+            {
+                const uint4 a = base0[p];
+                const uint2 b = base1[p];
+                r.st.d = a.x; r.st.v[0] = a.y; r.st.v[1] = a.z; r.st.v[2] = a.w; r.st.v[3] = b.x; r.st.v[4] = b.y;
+                r.st.boxmuller_flag = 0; r.st.boxmuller_flag_double = 0;
+                r.st.boxmuller_extra = 0.0f; r.st.boxmuller_extra_double = 0.0;
+                r.used = 0;
+                // advance the per-pixel state to the next frame: offset + 2^32
+                curandStateXORWOW_t nx = r.st;
+                skipahead(1ull << 32, &nx);
+                base0[p] = make_uint4(nx.d, nx.v[0], nx.v[1], nx.v[2]);
+                base1[p] = make_uint2(nx.v[3], nx.v[4]);
+            }
+            const float jx = r.next();
+            const float jy = r.next();
+            const float u = (static_cast<float>(px) + jx) / static_cast<float>(fp.width);
+            const float v = (static_cast<float>(py) + jy) / static_cast<float>(fp.height);
+            const float ndcx = u * 2.0f - 1.0f;
+            const float ndcy = static_cast<float>((1.0 - static_cast<double>(v)) * 2.0 - 1.0);
+            const float sx = ndcx * fp.tan_half_x;
+            const float sy = ndcy * fp.tan_half_y;
+            const f3 cd = mk(fp.cam_d[0], fp.cam_d[1], fp.cam_d[2]);
+            const f3 right = mk(fp.right[0], fp.right[1], fp.right[2]);
+            const f3 up = mk(fp.up[0], fp.up[1], fp.up[2]);
+            const f3 dir0 = normalize(cd + right * sx + up * sy);
+            const f3 dir = normalize(dir0);  // CalculateRadiance: rayDirection = normalize(rayDirection)
+            const f3 o = mk(fp.cam_o[0], fp.cam_o[1], fp.cam_o[2]);
+            P.o[slot] = f4(o, 0.0f);
+            P.d[slot] = f4(dir, 0.0f);
+            P.mask[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            P.rad[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (rec) {
 #pragma unroll
-        for (int k = 0; k < AR_DEBUG_MAX_HITS; ++k) rec[ri].hit_object[k] = -1;
+                for (int k = 0; k < AR_DEBUG_MAX_HITS; ++k) rec[g].hit_object[k] = -1;
+            }
+            P.info[slot] = make_int4(p, 0, sidx, fp.camera_inside ? kFlagInside : 0);
+            P.prev[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            P.media[slot] = make_float4(o.x, o.y, o.z, __int_as_float(-1));
+            P.rng0[slot] = make_uint4(r.st.d, r.st.v[0], r.st.v[1], r.st.v[2]);
+            P.rng1[slot] = make_uint2(r.st.v[3], r.st.v[4]);
+            if (P.ucount) P.ucount[slot] = r.used;
+        }
+        warp_append(&ctl->qcount[cur], P.q[cur], act, slot);
     }
-    P.info[slot] = make_int4(ri, 0, 0, fp.camera_inside ? kFlagInside : 0);
-    P.prev[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    P.media[slot] = make_float4(o.x, o.y, o.z, __int_as_float(-1));
-    if (P.ucount) P.ucount[slot] = 0;
-    P.q[0][slot] = slot;
-    P.rng0[slot] = make_uint4(r.st.d, r.st.v[0], r.st.v[1], r.st.v[2]);
-    P.rng1[slot] = make_uint2(r.st.v[3], r.st.v[4]);
-    if (P.ucount) P.ucount[slot] = r.used;
 }
 
 // ------------------------------------------------------------------ extend
-template <int kDepth>
-__global__ void __launch_bounds__(kTraceBlock) k_extend(SceneView s, FrameParams fp, PathSoA P, int cur,
-                                                        int32_t* counts, unsigned long long* stats, int* err)
+// INTERSECT_EPS(d) for d = 0..8 (config.cuh:3), computed on the host with the
+// fixed exp of detmath.h and uploaded once (set_intersect_eps).
+__constant__ float c_eps_tab[9];
+
+cudaError_t set_intersect_eps(const float* tab9)
 {
-    extern __shared__ uint32_t smem[];
-    uint32_t* stack = smem + (threadIdx.x >> 5) * (kDepth * 32) + lane_id();
-    if (blockIdx.x == 0 && threadIdx.x == 0) { counts[1 - cur] = 0; counts[2] = 0; }
-    const int n = counts[cur];
-    const int32_t* q = P.q[cur];
-    for (int qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n; qi += gridDim.x * blockDim.x) {
-        const int slot = q[qi];
-        const float4 o4 = P.o[slot], d4 = P.d[slot];
+    return cudaMemcpyToSymbol(c_eps_tab, tab9, 9 * sizeof(float));
+}
+
+struct ExtendIO {
+    PathSoA P;
+    const int32_t* q;
+    __device__ __forceinline__ int load(const SceneView& s, int k, RayState& r)
+    {
+        const int slot = q[k];
+        const f3 o = xyz(P.o[slot]), d = xyz(P.d[slot]);
         const int4 info = P.info[slot];
-        const f3 o = xyz(o4), d = xyz(d4);
-        const float eps = fp.eps_tab[min(info.z, 8)];
-        int4 hr = make_int4(-1, -1, 0, 0);
+        const float e = c_eps_tab[min(info.y >> 16, 8)];
         const int mobj = __float_as_int(P.media[slot].w);
         if ((info.w & kFlagInside) && mobj >= 0 && s.objects[mobj].type != AR_OBJ_TRIANGLE) {
             // solo trace of the medium's object (render.cuh:91-94, intersection.cuh:185-193)
             const float t = isect_analytic_t(s, mobj, o, d);
-            if (t >= 0.0f && !(t < eps)) hr = make_int4(mobj, -1, __float_as_int(t), 0);
-        } else {
-            const Hit h = trace_ray<false, kDepth>(s, o, d, eps, INFINITY, stack, err);
-            if (h.obj >= 0) hr = make_int4(h.obj, h.prim, __float_as_int(h.t), 0);
+            P.hit[slot] = (t >= 0.0f && !(t < e)) ? make_int4(mobj, -1, __float_as_int(t), 0) : make_int4(-1, -1, 0, 0);
+            return -1;
         }
-        P.hit[slot] = hr;
-        warp_count(&stats[0], true);
+        ray_begin(r, o, d, e, INFINITY);
+        return slot;
     }
+    __device__ __forceinline__ void store(const SceneView&, int slot, const RayState& r)
+    {
+        P.hit[slot] = r.best.obj >= 0 ? make_int4(r.best.obj, r.best.prim, __float_as_int(r.best.t), 0)
+                                      : make_int4(-1, -1, 0, 0);
+    }
+};
+
+// Trace's closest-hit query (render.cuh:86-99) for every queued path.
+__global__ void __launch_bounds__(kTraceBlock) k_extend(SceneView s, PathSoA P, int cur, PoolCtl* ctl,
+                                                        unsigned long long* stats, uint32_t* ovf, int* err)
+{
+    extern __shared__ uint32_t smem[];
+    const int n = ctl->qcount[cur];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&stats[0], static_cast<unsigned long long>(n));
+    ExtendIO io;
+    io.P = P;
+    io.q = P.q[cur];
+    traverse_queue<false>(s, io, n, &ctl->fetch_ext, lane_stack(smem), thread_overflow(ovf), err, &stats[2]);
 }
 
 // ------------------------------------------------------------------ shading helpers
@@ -599,10 +686,10 @@ __device__ __forceinline__ f3 sky_lighting(f3 d, int sky)
 // One iteration of the CalculateRadiance loop body (render.cuh:541-908) up to
 // the shadow query: Trace's material evaluation and hit offset, emission with
 // MIS, light sampling for NEE, throughput and Russian roulette.
-__global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams fp, PathSoA P, int cur, int32_t* counts,
+__global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams fp, PathSoA P, int cur, PoolCtl* ctl,
                                                        ar_path_record* rec)
 {
-    const int n = counts[cur];
+    const int n = ctl->qcount[cur];
     const int32_t* q = P.q[cur];
     for (int qi0 = blockIdx.x * blockDim.x; qi0 < n; qi0 += gridDim.x * blockDim.x) {
         const int qi = qi0 + threadIdx.x;
@@ -612,8 +699,9 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         if (active) {
             slot = q[qi];
             int4 info = P.info[slot];
-            const int depth = info.y;
-            int nonDelta = info.z;
+            const int depth = info.y & 0xFFFF;
+            int nonDelta = info.y >> 16;
+            const int64_t ri = static_cast<int64_t>(info.z) * fp.npix + info.x;
             int flags = info.w & 0xFF;
             int mdepth = info.w >> 8;
             const float4 o4 = P.o[slot], d4 = P.d[slot];
@@ -627,11 +715,11 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             const int mobj = __float_as_int(md.w);
             const int4 hr = P.hit[slot];
             const bool hit = hr.x >= 0;
-            const float eps = fp.eps_tab[min(nonDelta, 8)];
+            const float eps = c_eps_tab[min(nonDelta, 8)];
             Rng g;
             rng_load(P, slot, g);
-            if (rec && depth < AR_DEBUG_MAX_HITS) rec[info.x].hit_object[depth] = hit ? hr.x : -1;
-            if (rec) rec[info.x].segments = depth + 1;
+            if (rec && depth < AR_DEBUG_MAX_HITS) rec[ri].hit_object[depth] = hit ? hr.x : -1;
+            if (rec) rec[ri].segments = depth + 1;
             // ---- intersection details (re-run of the accepted test)
             f3 pos = mk(0.0f, 0.0f, 0.0f), nrm = mk(0.0f, 0.0f, 0.0f);
             GB gb;
@@ -798,9 +886,12 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                                 pending = mask * (contrib * power_heuristic(pL, pB));
                             }
                             shadow = true;
-                            P.sseg0[slot] = f4(pos, fp.eps_tab[min(depth, 8)]);
+                            P.sseg0[slot] = f4(pos, c_eps_tab[min(depth, 8)]);
                             P.sseg1[slot] = f4(ls.p, 0.0f);
-                            if (rec) rec[info.x].nee_rays += 1;
+                            if (rec) {
+                                rec[ri].nee_rays += 1;
+                                if (depth < 32) rec[ri].nee_depth_mask |= static_cast<int32_t>(1u << depth);
+                            }
                         }
                     }
                     flags = (flags & ~kFlagPrevNEE) | (newPrev ? kFlagPrevNEE : 0);
@@ -832,53 +923,69 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             P.rad[slot] = f4(radiance, 0.0f);
             P.nee[slot] = f4(pending, 0.0f);
             P.media[slot] = make_float4(nvloc.x, nvloc.y, nvloc.z, __int_as_float(nmobj));
-            P.info[slot] = make_int4(info.x, depth + 1, nonDelta, flags | (nmdepth << 8));
+            P.info[slot] = make_int4(info.x, (depth + 1) | (nonDelta << 16), info.z, flags | (nmdepth << 8));
             rng_store(P, slot, g);
         }
-        warp_append(&counts[1 - cur], P.q[1 - cur], cont, slot);
-        warp_append(&counts[2], P.qs, shadow, slot);
+        warp_append(&ctl->qcount[1 - cur], P.q[1 - cur], cont, slot);
+        warp_append(&ctl->shadow_count, P.qs, shadow, slot);
+        warp_append(&ctl->retire_count, P.qr, active && !cont, slot);
     }
 }
 
 // ------------------------------------------------------------------ shadow
 // SegmentTrace -> AnyHitSegmentBVH (render.cuh:167-183, intersection.cuh:372-397)
-// and the remainder of NEE (render.cuh:242-343).
-template <int kDepth>
-__global__ void __launch_bounds__(kTraceBlock) k_shadow(SceneView s, PathSoA P, int32_t* counts,
-                                                        unsigned long long* stats, int* err)
-{
-    extern __shared__ uint32_t smem[];
-    uint32_t* stack = smem + (threadIdx.x >> 5) * (kDepth * 32) + lane_id();
-    const int n = counts[2];
-    for (int qi = blockIdx.x * blockDim.x + threadIdx.x; qi < n; qi += gridDim.x * blockDim.x) {
-        const int slot = P.qs[qi];
-        const float4 a = P.sseg0[slot], b = P.sseg1[slot];
-        const f3 src = xyz(a), dst = xyz(b);
-        bool occ = false;
-        f3 dir = dst - src;
-        const float dist = length(dir);
-        bool traced = false;
-        if (dist > 0.0f) {
-            dir = dir / dist;
-            const float eps = a.w * fmaxf(1.0f, fmaxf(length(src), length(dst)));
-            const float tMax = fmaxf(0.0f, dist - eps);
-            if (tMax > 0.0f) {
-                traced = true;
-                const Hit h = trace_ray<true, kDepth>(s, src, dir, 0.0f, tMax, stack, err);
-                occ = h.obj >= 0;
-            }
-        }
-        warp_count(&stats[1], traced);
+// and the remainder of NEE (render.cuh:242-343): the pending term is added when
+// the segment is unoccluded, and previousDidNEE_ becomes "occluded or cos > 0".
+struct ShadowIO {
+    PathSoA P;
+    unsigned long long traced;
+    __device__ __forceinline__ void finish(int slot, bool occ)
+    {
         int4 info = P.info[slot];
         const bool cosOK = (info.w & kFlagNeeCosOK) != 0;
         if (!occ && cosOK) {
             const float4 r = P.rad[slot], pn = P.nee[slot];
             P.rad[slot] = make_float4(r.x + pn.x, r.y + pn.y, r.z + pn.z, 0.0f);
         }
-        const bool valid = occ || cosOK;
-        info.w = (info.w & ~kFlagPrevNEE) | (valid ? kFlagPrevNEE : 0);
+        info.w = (info.w & ~kFlagPrevNEE) | ((occ || cosOK) ? kFlagPrevNEE : 0);
         P.info[slot] = info;
     }
+    __device__ __forceinline__ int load(const SceneView&, int k, RayState& r)
+    {
+        const int slot = P.qs[k];
+        const float4 a = P.sseg0[slot], b = P.sseg1[slot];
+        const f3 src = xyz(a), dst = xyz(b);
+        f3 dir = dst - src;
+        const float dist = length(dir);
+        if (dist > 0.0f) {
+            dir = dir / dist;
+            const float eps = a.w * fmaxf(1.0f, fmaxf(length(src), length(dst)));
+            const float tMax = fmaxf(0.0f, dist - eps);
+            if (tMax > 0.0f) {
+                ray_begin(r, src, dir, 0.0f, tMax);
+                ++traced;
+                return slot;
+            }
+        }
+        finish(slot, false);
+        return -1;
+    }
+    __device__ __forceinline__ void store(const SceneView&, int slot, const RayState& r) { finish(slot, r.best.obj >= 0); }
+};
+
+__global__ void __launch_bounds__(kTraceBlock) k_shadow(SceneView s, PathSoA P, PoolCtl* ctl,
+                                                        unsigned long long* stats, uint32_t* ovf, int* err)
+{
+    extern __shared__ uint32_t smem[];
+    const int n = ctl->shadow_count;
+    ShadowIO io;
+    io.P = P;
+    io.traced = 0;
+    traverse_queue<true>(s, io, n, &ctl->fetch_shadow, lane_stack(smem), thread_overflow(ovf), err, &stats[4]);
+    unsigned long long c = io.traced;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    if (lane_id() == 0 && c) atomicAdd(&stats[1], c);
 }
 
 // ------------------------------------------------------------------ finish
@@ -889,23 +996,34 @@ __device__ __forceinline__ float fix_nan_inf(float x)
     if (isinf_(x)) return x > 0.0f ? 0.0f : -0.0f;
     return x;
 }
-__global__ void k_finish(FrameParams fp, PathSoA P, double* accum, ar_path_record* rec)
+// Paths that ended this iteration (after their last shadow query): FP64 sum
+// into the pixel, slot back onto the free stack.
+__global__ void k_retire(FrameParams fp, PathSoA P, PoolCtl* ctl, double* accum, ar_path_record* rec)
 {
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= fp.wave) return;
-    const float4 r = P.rad[slot];
-    const float x = fmaxf(clampf(fix_nan_inf(r.x), 0.0f, 1.0e3f), 0.0f);
-    const float y = fmaxf(clampf(fix_nan_inf(r.y), 0.0f, 1.0e3f), 0.0f);
-    const float z = fmaxf(clampf(fix_nan_inf(r.z), 0.0f, 1.0e3f), 0.0f);
-    const int p = fp.first_pixel + slot;
-    double* a = accum + 3 * static_cast<int64_t>(p);
-    a[0] += static_cast<double>(x);
-    a[1] += static_cast<double>(y);
-    a[2] += static_cast<double>(z);
-    if (rec) {
-        const int ri = P.info[slot].x;
-        rec[ri].radiance[0] = x; rec[ri].radiance[1] = y; rec[ri].radiance[2] = z;
-        rec[ri].uniforms = P.ucount ? P.ucount[slot] : 0;
+    const int n = ctl->retire_count;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->retired += n;
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        const bool act = i < n;
+        int slot = 0;
+        if (act) {
+            slot = P.qr[i];
+            const float4 r = P.rad[slot];
+            const float x = fmaxf(clampf(fix_nan_inf(r.x), 0.0f, 1.0e3f), 0.0f);
+            const float y = fmaxf(clampf(fix_nan_inf(r.y), 0.0f, 1.0e3f), 0.0f);
+            const float z = fmaxf(clampf(fix_nan_inf(r.z), 0.0f, 1.0e3f), 0.0f);
+            const int4 info = P.info[slot];
+            double* a = accum + 3 * static_cast<int64_t>(info.x);
+            atomicAdd(a + 0, static_cast<double>(x));
+            atomicAdd(a + 1, static_cast<double>(y));
+            atomicAdd(a + 2, static_cast<double>(z));
+            if (rec) {
+                const int64_t ri = static_cast<int64_t>(info.z) * fp.npix + info.x;
+                rec[ri].radiance[0] = x; rec[ri].radiance[1] = y; rec[ri].radiance[2] = z;
+                rec[ri].uniforms = P.ucount ? P.ucount[slot] : 0;
+            }
+        }
+        warp_append(&ctl->free_count, P.freeq, act, slot);
     }
 }
 
@@ -922,22 +1040,33 @@ __global__ void k_add(const double* src, int64_t n, double* dst)
 }
 
 // ------------------------------------------------------------------ launchers
-template <int kDepth>
-static cudaError_t launch_trace_rays_t(const SceneView& s, const float4* rays, int64_t n, int any, int32_t* obj, float* t,
-                                       int* err, int grid, cudaStream_t st)
+constexpr size_t kTraceSmem = static_cast<size_t>(kStackShared) * kTraceBlock * 4;
+
+int trace_grid(int sm_count)
 {
-    const size_t smem = static_cast<size_t>(kDepth) * kTraceBlock * 4;
-    cudaFuncSetAttribute(k_trace_rays<kDepth>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    k_trace_rays<kDepth><<<grid, kTraceBlock, smem, st>>>(s, rays, n, any, obj, t, err);
-    return cudaGetLastError();
+    static int blocks = 0;
+    if (blocks == 0) {
+        int b0 = 1, b1 = 1, b2 = 1, b3 = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend, kTraceBlock, kTraceSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow, kTraceBlock, kTraceSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_trace_rays<false>, kTraceBlock, kTraceSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_trace_rays<true>, kTraceBlock, kTraceSmem);
+        cudaGetLastError();
+        blocks = max(1, max(max(b0, b1), max(b2, b3)));
+    }
+    return blocks * sm_count;
 }
 
-cudaError_t launch_trace_rays(const SceneView& s, int stack_depth, const float4* rays, int64_t n, int any, int32_t* obj,
-                              float* t, int* err, int grid, cudaStream_t st)
+cudaError_t launch_trace_rays(const SceneView& s, const float4* rays, int n, int any, int32_t* obj, float* t,
+                              PoolCtl* ctl, uint32_t* ovf, int* err, int grid, cudaStream_t st)
 {
-    if (stack_depth <= 32) return launch_trace_rays_t<32>(s, rays, n, any, obj, t, err, grid, st);
-    if (stack_depth <= 64) return launch_trace_rays_t<64>(s, rays, n, any, obj, t, err, grid, st);
-    return launch_trace_rays_t<128>(s, rays, n, any, obj, t, err, grid, st);
+    RaysIO io;
+    io.rays = rays;
+    io.out_obj = obj;
+    io.out_t = t;
+    if (any) k_trace_rays<true><<<grid, kTraceBlock, kTraceSmem, st>>>(s, io, n, ctl, ovf, err);
+    else k_trace_rays<false><<<grid, kTraceBlock, kTraceSmem, st>>>(s, io, n, ctl, ovf, err);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_rng_init(const FrameParams& fp, uint4* b0, uint2* b1, cudaStream_t st)
@@ -952,44 +1081,34 @@ cudaError_t launch_rng_tape(const FrameParams& fp, int spp, int per_path, float*
     return cudaGetLastError();
 }
 
-template <int kDepth>
-static cudaError_t launch_depth_loop_t(const SceneView& s, const FrameParams& fp, const PathSoA& P, int32_t* counts,
-                                       unsigned long long* stats, int* err, ar_path_record* rec, int grid_trace,
-                                       int grid_shade, cudaStream_t st, int64_t* launches, LaunchTimers* tm)
+cudaError_t launch_pool_init(const PathSoA& P, PoolCtl* ctl, int pool, int64_t total, cudaStream_t st)
 {
-    const size_t smem = static_cast<size_t>(kDepth) * kTraceBlock * 4;
-    cudaFuncSetAttribute(k_extend<kDepth>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    cudaFuncSetAttribute(k_shadow<kDepth>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    int cur = 0;
-    for (int depth = 0; depth < fp.max_depth; ++depth) {
-        const bool te = tm && tm->n_extend < tm->cap;
-        if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend], st);
-        k_extend<kDepth><<<grid_trace, kTraceBlock, smem, st>>>(s, fp, P, cur, counts, stats, err);
-        if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend++ + 1], st);
-        k_shade<<<grid_shade, kShadeBlock, 0, st>>>(s, fp, P, cur, counts, rec);
-        const bool ts = tm && tm->n_shadow < tm->cap;
-        if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow], st);
-        k_shadow<kDepth><<<grid_trace, kTraceBlock, smem, st>>>(s, P, counts, stats, err);
-        if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow++ + 1], st);
-        *launches += 3;
-        cur = 1 - cur;
-    }
+    k_pool_init<<<(pool + 255) / 256, 256, 0, st>>>(P, ctl, pool, total);
     return cudaGetLastError();
 }
 
-cudaError_t launch_wave(const SceneView& s, int stack_depth, const FrameParams& fp, const PathSoA& P, uint4* b0, uint2* b1,
-                        int32_t* counts, unsigned long long* stats, int* err, double* accum, ar_path_record* rec,
-                        int grid_trace, int grid_shade, cudaStream_t st, int64_t* launches, LaunchTimers* tm)
+cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const PathSoA& P, PoolCtl* ctl, uint4* b0,
+                              uint2* b1, unsigned long long* stats, uint32_t* ovf, int* err, double* accum,
+                              ar_path_record* rec, int iterations, int* cur, int grid_trace, int grid_other,
+                              cudaStream_t st, int64_t* launches, LaunchTimers* tm)
 {
-    k_raygen<<<(fp.wave + 255) / 256, 256, 0, st>>>(fp, P, b0, b1, counts, rec);
-    *launches += 1;
-    cudaError_t e;
-    if (stack_depth <= 32) e = launch_depth_loop_t<32>(s, fp, P, counts, stats, err, rec, grid_trace, grid_shade, st, launches, tm);
-    else if (stack_depth <= 64) e = launch_depth_loop_t<64>(s, fp, P, counts, stats, err, rec, grid_trace, grid_shade, st, launches, tm);
-    else e = launch_depth_loop_t<128>(s, fp, P, counts, stats, err, rec, grid_trace, grid_shade, st, launches, tm);
-    if (e != cudaSuccess) return e;
-    k_finish<<<(fp.wave + 255) / 256, 256, 0, st>>>(fp, P, accum, rec);
-    *launches += 1;
+    for (int it = 0; it < iterations; ++it) {
+        const int c = *cur;
+        k_plan<<<1, 1, 0, st>>>(ctl, c, fp.npix);
+        k_regen<<<grid_other, kShadeBlock, 0, st>>>(fp, P, ctl, c, b0, b1, rec);
+        const bool te = tm && tm->n_extend < tm->cap;
+        if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend], st);
+        k_extend<<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, P, c, ctl, stats, ovf, err);
+        if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend++ + 1], st);
+        k_shade<<<grid_other, kShadeBlock, 0, st>>>(s, fp, P, c, ctl, rec);
+        const bool ts = tm && tm->n_shadow < tm->cap;
+        if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow], st);
+        k_shadow<<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, P, ctl, stats, ovf, err);
+        if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow++ + 1], st);
+        k_retire<<<grid_other, kShadeBlock, 0, st>>>(fp, P, ctl, accum, rec);
+        *launches += 6;
+        *cur = 1 - c;
+    }
     return cudaGetLastError();
 }
 

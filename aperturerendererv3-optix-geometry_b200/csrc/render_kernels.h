@@ -12,10 +12,15 @@ namespace ar {
 constexpr int kTraceBlock = 128;  // threads per traversal block (4 warps)
 constexpr int kShadeBlock = 256;
 
-cudaError_t launch_trace_rays(const SceneView& s, int stack_depth, const float4* rays, int64_t n, int any, int32_t* obj,
-                              float* t, int* err, int grid, cudaStream_t st);
+// Upload INTERSECT_EPS(0..8) to the current device.
+cudaError_t set_intersect_eps(const float* tab9);
+// Blocks of the persistent traversal kernels: occupancy limit x SM count.
+int trace_grid(int sm_count);
+cudaError_t launch_trace_rays(const SceneView& s, const float4* rays, int n, int any, int32_t* obj, float* t,
+                              PoolCtl* ctl, uint32_t* ovf, int* err, int grid, cudaStream_t st);
 cudaError_t launch_rng_init(const FrameParams& fp, uint4* b0, uint2* b1, cudaStream_t st);
 cudaError_t launch_rng_tape(const FrameParams& fp, int spp, int per_path, float* out, cudaStream_t st);
+
 // Optional event pairs around every traversal launch: ev[2k], ev[2k+1].
 struct LaunchTimers {
     cudaEvent_t* extend_ev = nullptr;
@@ -25,9 +30,12 @@ struct LaunchTimers {
     int n_shadow = 0;
 };
 
-cudaError_t launch_wave(const SceneView& s, int stack_depth, const FrameParams& fp, const PathSoA& P, uint4* b0, uint2* b1,
-                        int32_t* counts, unsigned long long* stats, int* err, double* accum, ar_path_record* rec,
-                        int grid_trace, int grid_shade, cudaStream_t st, int64_t* launches, LaunchTimers* timers);
+cudaError_t launch_pool_init(const PathSoA& P, PoolCtl* ctl, int pool, int64_t total, cudaStream_t st);
+// `iterations` rounds of plan -> regen -> extend -> shade -> shadow -> retire.
+cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const PathSoA& P, PoolCtl* ctl, uint4* b0,
+                              uint2* b1, unsigned long long* stats, uint32_t* ovf, int* err, double* accum,
+                              ar_path_record* rec, int iterations, int* cur, int grid_trace, int grid_other,
+                              cudaStream_t st, int64_t* launches, LaunchTimers* tm);
 cudaError_t launch_mean(const double* accum, int64_t n, double inv, float* out, cudaStream_t st);
 cudaError_t launch_add(const double* src, int64_t n, double* dst, cudaStream_t st);
 

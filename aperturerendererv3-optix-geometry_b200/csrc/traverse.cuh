@@ -146,7 +146,63 @@ struct Hit {
     int32_t prim;  // leaf-order primitive slot, -1 = none
 };
 
+// Traversal stack: kStackShared entries per lane in shared memory, the rest in
+// a per-thread slab of global memory (only deep BVH paths reach it).
+constexpr int kStackShared = 32;
+constexpr int kStackOverflow = 96;
+constexpr int kStackMax = kStackShared + kStackOverflow;
+
+struct RayState {
+    f3 o, d;
+    float ix, iy, iz;  // reciprocal direction, |d| clamped to 2^-64
+    float tmin;
+    Hit best;
+    uint32_t node;
+    int sp;
+    uint32_t visits;  // nodes visited
+    uint32_t tests;   // primitives tested
+};
+
+__device__ __forceinline__ void ray_begin(RayState& r, f3 o, f3 d, float tmin, float tmax)
+{
+    r.o = o;
+    r.d = d;
+    const float dx = fabsf(d.x) < kMinDir ? copysignf(kMinDir, d.x) : d.x;
+    const float dy = fabsf(d.y) < kMinDir ? copysignf(kMinDir, d.y) : d.y;
+    const float dz = fabsf(d.z) < kMinDir ? copysignf(kMinDir, d.z) : d.z;
+    r.ix = __frcp_rn(dx);
+    r.iy = __frcp_rn(dy);
+    r.iz = __frcp_rn(dz);
+    r.tmin = tmin;
+    r.best.t = tmax;
+    r.best.obj = -1;
+    r.best.prim = -1;
+    r.node = 0;
+    r.sp = 0;
+    r.visits = 0;
+    r.tests = 0;
+}
+
 __device__ __forceinline__ uint32_t byte_of(uint32_t w, int k) { return (w >> (8 * k)) & 0xFFu; }
+
+// byte k of w as a float without a conversion instruction: 0x4B0000qq is 2^23 + qq
+__device__ __forceinline__ float byte_float(uint32_t w, int k)
+{
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u + static_cast<uint32_t>(k))) - 8388608.0f;
+}
+
+__device__ __forceinline__ float max3f(float a, float b, float c)
+{
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c)
+{
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
 
 __device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b)
 {
@@ -154,123 +210,170 @@ __device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b)
     a = lo; b = hi;
 }
 
-// Closest hit (kAny = false) or any hit (kAny = true) on [tmin, tmax).
-// stack: this lane's first stack entry in shared memory; entries are 32 apart.
-template <bool kAny, int kDepth>
-__device__ __forceinline__ Hit trace_ray(const SceneView& s, f3 o, f3 d, float tmin, float tmax,
-                                         uint32_t* stack, int* err)
+// Visit node r.node: test its 8 child boxes, intersect the primitives of hit
+// leaf children nearest first, push hit internal children far to near, pop the
+// next node.  Returns true when the ray is finished (stack empty, any-hit
+// found, or stack overflow reported through *err).
+template <bool kAny>
+__device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32_t* stack, uint32_t* ovf, int* err)
 {
-    Hit best;
-    best.t = tmax; best.obj = -1; best.prim = -1;
-    if (s.num_nodes == 0) return best;
-    const float dx = fabsf(d.x) < kMinDir ? copysignf(kMinDir, d.x) : d.x;
-    const float dy = fabsf(d.y) < kMinDir ? copysignf(kMinDir, d.y) : d.y;
-    const float dz = fabsf(d.z) < kMinDir ? copysignf(kMinDir, d.z) : d.z;
-    const float idx = __frcp_rn(dx), idy = __frcp_rn(dy), idz = __frcp_rn(dz);
-    const bool nx = idx < 0.0f, ny = idy < 0.0f, nz = idz < 0.0f;
-    int sp = 0;
-    uint32_t node = 0;
-    for (;;) {
-        const WideNode* np = s.nodes + node;
-        const float4 w0 = ldg4(reinterpret_cast<const char*>(np));
-        const uint4 w1 = ldgu4(reinterpret_cast<const char*>(np) + 16);
-        const uint4 w2 = ldgu4(reinterpret_cast<const char*>(np) + 32);
-        const uint4 w3 = ldgu4(reinterpret_cast<const char*>(np) + 48);
-        const uint4 w4 = ldgu4(reinterpret_cast<const char*>(np) + 64);
-        const uint32_t exps = __float_as_uint(w0.w);
-        const float sx = __uint_as_float((exps & 0xFFu) << 23);
-        const float sy = __uint_as_float(((exps >> 8) & 0xFFu) << 23);
-        const float sz = __uint_as_float(((exps >> 16) & 0xFFu) << 23);
-        const float ax = sx * idx, ay = sy * idy, az = sz * idz;
-        const float bx = (w0.x - o.x) * idx, by = (w0.y - o.y) * idy, bz = (w0.z - o.z) * idz;
-        // quantised planes: w2 = qlo_x[8] | qlo_y[8]; w3 = qlo_z[8] | qhi_x[8]; w4 = qhi_y[8] | qhi_z[8]
-        const uint32_t lox0 = w2.x, lox1 = w2.y, loy0 = w2.z, loy1 = w2.w;
-        const uint32_t loz0 = w3.x, loz1 = w3.y, hix0 = w3.z, hix1 = w3.w;
-        const uint32_t hiy0 = w4.x, hiy1 = w4.y, hiz0 = w4.z, hiz1 = w4.w;
-        const uint32_t nx0 = nx ? hix0 : lox0, nx1 = nx ? hix1 : lox1, fx0 = nx ? lox0 : hix0, fx1 = nx ? lox1 : hix1;
-        const uint32_t ny0 = ny ? hiy0 : loy0, ny1 = ny ? hiy1 : loy1, fy0 = ny ? loy0 : hiy0, fy1 = ny ? loy1 : hiy1;
-        const uint32_t nz0 = nz ? hiz0 : loz0, nz1 = nz ? hiz1 : loz1, fz0 = nz ? loz0 : hiz0, fz1 = nz ? loz1 : hiz1;
-        const uint32_t meta0 = w1.z, meta1 = w1.w;
-        const float limit = fminf(best.t, FLT_MAX);
-        uint32_t key[8];
+    const WideNode* np = s.nodes + r.node;
+    ++r.visits;
+    const float4 w0 = ldg4(reinterpret_cast<const char*>(np));
+    const uint4 w1 = ldgu4(reinterpret_cast<const char*>(np) + 16);
+    const uint4 w2 = ldgu4(reinterpret_cast<const char*>(np) + 32);
+    const uint4 w3 = ldgu4(reinterpret_cast<const char*>(np) + 48);
+    const uint4 w4 = ldgu4(reinterpret_cast<const char*>(np) + 64);
+    const uint32_t exps = __float_as_uint(w0.w);
+    const float sx = __uint_as_float((exps & 0xFFu) << 23);
+    const float sy = __uint_as_float(((exps >> 8) & 0xFFu) << 23);
+    const float sz = __uint_as_float(((exps >> 16) & 0xFFu) << 23);
+    const float ax = sx * r.ix, ay = sy * r.iy, az = sz * r.iz;
+    const float bx = (w0.x - r.o.x) * r.ix, by = (w0.y - r.o.y) * r.iy, bz = (w0.z - r.o.z) * r.iz;
+    // w2 = qlo_x | qlo_y, w3 = qlo_z | qhi_x, w4 = qhi_y | qhi_z (8 bytes each)
+    const bool nx = r.ix < 0.0f, ny = r.iy < 0.0f, nz = r.iz < 0.0f;
+    const uint32_t nx0 = nx ? w3.z : w2.x, nx1 = nx ? w3.w : w2.y, fx0 = nx ? w2.x : w3.z, fx1 = nx ? w2.y : w3.w;
+    const uint32_t ny0 = ny ? w4.x : w2.z, ny1 = ny ? w4.y : w2.w, fy0 = ny ? w2.z : w4.x, fy1 = ny ? w2.w : w4.y;
+    const uint32_t nz0 = nz ? w4.z : w3.x, nz1 = nz ? w4.w : w3.y, fz0 = nz ? w3.x : w4.z, fz1 = nz ? w3.y : w4.w;
+    const uint32_t meta0 = w1.z, meta1 = w1.w;
+    const float limit = fminf(r.best.t, FLT_MAX);
+    uint32_t key[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const uint32_t wnx = k < 4 ? nx0 : nx1, wfx = k < 4 ? fx0 : fx1;
-            const uint32_t wny = k < 4 ? ny0 : ny1, wfy = k < 4 ? fy0 : fy1;
-            const uint32_t wnz = k < 4 ? nz0 : nz1, wfz = k < 4 ? fz0 : fz1;
-            const int b = k & 3;
-            const float tnx = fmaf(static_cast<float>(byte_of(wnx, b)), ax, bx);
-            const float tfx = fmaf(static_cast<float>(byte_of(wfx, b)), ax, bx);
-            const float tny = fmaf(static_cast<float>(byte_of(wny, b)), ay, by);
-            const float tfy = fmaf(static_cast<float>(byte_of(wfy, b)), ay, by);
-            const float tnz = fmaf(static_cast<float>(byte_of(wnz, b)), az, bz);
-            const float tfz = fmaf(static_cast<float>(byte_of(wfz, b)), az, bz);
-            const float tnear = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-            const float tfar = fminf(fminf(fminf(tfx, tfy), tfz), limit) * kSlabWiden;
-            const uint32_t meta = byte_of(k < 4 ? meta0 : meta1, b);
-            const bool hit = (tnear <= tfar) && (meta != kMetaEmpty);
-            // tnear >= tmin >= 0, so its bit pattern orders like the value
-            key[k] = hit ? ((__float_as_uint(fmaxf(tnear, 0.0f)) & ~7u) | static_cast<uint32_t>(k)) : 0xFFFFFFFFu;
+    for (int k = 0; k < 8; ++k) {
+        const int b = k & 3;
+        const float tnx = fmaf(byte_float(k < 4 ? nx0 : nx1, b), ax, bx);
+        const float tfx = fmaf(byte_float(k < 4 ? fx0 : fx1, b), ax, bx);
+        const float tny = fmaf(byte_float(k < 4 ? ny0 : ny1, b), ay, by);
+        const float tfy = fmaf(byte_float(k < 4 ? fy0 : fy1, b), ay, by);
+        const float tnz = fmaf(byte_float(k < 4 ? nz0 : nz1, b), az, bz);
+        const float tfz = fmaf(byte_float(k < 4 ? fz0 : fz1, b), az, bz);
+        const float tnear = max3f(tnx, tny, fmaxf(tnz, r.tmin));
+        const float tfar = min3f(tfx, tfy, fminf(tfz, limit)) * kSlabWiden;
+        const uint32_t meta = byte_of(k < 4 ? meta0 : meta1, b);
+        const bool hit = (tnear <= tfar) && (meta != kMetaEmpty);
+        // tnear >= tmin >= 0, so its bit pattern orders like the value
+        key[k] = hit ? ((__float_as_uint(fmaxf(tnear, 0.0f)) & ~7u) | static_cast<uint32_t>(k)) : 0xFFFFFFFFu;
+    }
+    // sort the 8 keys (Batcher odd-even merge network, 19 comparators)
+    cswap(key[0], key[1]); cswap(key[2], key[3]); cswap(key[4], key[5]); cswap(key[6], key[7]);
+    cswap(key[0], key[2]); cswap(key[1], key[3]); cswap(key[4], key[6]); cswap(key[5], key[7]);
+    cswap(key[1], key[2]); cswap(key[5], key[6]);
+    cswap(key[0], key[4]); cswap(key[1], key[5]); cswap(key[2], key[6]); cswap(key[3], key[7]);
+    cswap(key[2], key[4]); cswap(key[3], key[5]);
+    cswap(key[1], key[2]); cswap(key[3], key[4]); cswap(key[5], key[6]);
+    // leaves, nearest first
+    const uint32_t prim_base = w1.y;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t kk = key[k];
+        if (kk == 0xFFFFFFFFu) break;
+        const int slot = static_cast<int>(kk & 7u);
+        const uint32_t meta = byte_of(slot < 4 ? meta0 : meta1, slot & 3);
+        if (meta & kMetaInternal) continue;
+        const float tn = __uint_as_float(kk & ~7u);
+        if (!(tn <= fminf(r.best.t, FLT_MAX) * kSlabWiden)) continue;
+        const int count = static_cast<int>(meta >> 5) + 1;
+        const uint32_t first = prim_base + (meta & 31u);
+        for (int p = 0; p < count; ++p) {
+            const PrimRec* pr = s.prims + first + p;
+            ++r.tests;
+            const float4 a = ldg4(&pr->v0[0]);
+            const float4 e1 = ldg4(&pr->e1[0]);
+            const int obj = __float_as_int(a.w);
+            float t;
+            if (__float_as_int(e1.w) == kPrimTriangle) {
+                const float4 e2 = ldg4(&pr->e2[0]);
+                t = mt_triangle(r.o, r.d, mk(a.x, a.y, a.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z));
+            } else {
+                t = isect_analytic_t(s, obj, r.o, r.d);
+            }
+            if (t < 0.0f || t < r.tmin) continue;
+            if (t < r.best.t || (r.best.obj >= 0 && t == r.best.t && obj < r.best.obj)) {
+                r.best.t = t;
+                r.best.obj = obj;
+                r.best.prim = static_cast<int>(first) + p;
+                if (kAny) return true;
+            }
         }
-        // sort the 8 keys (Batcher odd-even merge network, 19 comparators)
-        cswap(key[0], key[1]); cswap(key[2], key[3]); cswap(key[4], key[5]); cswap(key[6], key[7]);
-        cswap(key[0], key[2]); cswap(key[1], key[3]); cswap(key[4], key[6]); cswap(key[5], key[7]);
-        cswap(key[1], key[2]); cswap(key[5], key[6]);
-        cswap(key[0], key[4]); cswap(key[1], key[5]); cswap(key[2], key[6]); cswap(key[3], key[7]);
-        cswap(key[2], key[4]); cswap(key[3], key[5]);
-        cswap(key[1], key[2]); cswap(key[3], key[4]); cswap(key[5], key[6]);
-        // leaves, nearest first
-        const uint32_t prim_base = w1.y;
+    }
+    // internal children, pushed far to near
+    const uint32_t child_base = w1.x;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const uint32_t kk = key[k];
-            if (kk == 0xFFFFFFFFu) break;
-            const int slot = static_cast<int>(kk & 7u);
-            const uint32_t meta = byte_of(slot < 4 ? meta0 : meta1, slot & 3);
-            if (meta & kMetaInternal) continue;
-            const float tn = __uint_as_float(kk & ~7u);
-            if (!(tn <= fminf(best.t, FLT_MAX) * kSlabWiden)) continue;
-            const int count = static_cast<int>(meta >> 5) + 1;
-            const uint32_t first = prim_base + (meta & 31u);
-            for (int p = 0; p < count; ++p) {
-                const PrimRec* pr = s.prims + first + p;
-                const float4 a = ldg4(&pr->v0[0]);
-                const float4 e1 = ldg4(&pr->e1[0]);
-                const int obj = __float_as_int(a.w);
-                float t;
-                if (__float_as_int(e1.w) == kPrimTriangle) {
-                    const float4 e2 = ldg4(&pr->e2[0]);
-                    t = mt_triangle(o, d, mk(a.x, a.y, a.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z));
-                } else {
-                    t = isect_analytic_t(s, obj, o, d);
-                }
-                if (t < 0.0f || t < tmin) continue;
-                if (t < best.t || (best.obj >= 0 && t == best.t && obj < best.obj)) {
-                    best.t = t; best.obj = obj; best.prim = static_cast<int>(first) + p;
-                    if (kAny) return best;
+    for (int k = 7; k >= 0; --k) {
+        const uint32_t kk = key[k];
+        if (kk == 0xFFFFFFFFu) continue;
+        const int slot = static_cast<int>(kk & 7u);
+        const uint32_t meta = byte_of(slot < 4 ? meta0 : meta1, slot & 3);
+        if (!(meta & kMetaInternal)) continue;
+        const float tn = __uint_as_float(kk & ~7u);
+        if (!(tn <= fminf(r.best.t, FLT_MAX) * kSlabWiden)) continue;
+        const uint32_t child = child_base + (meta & 7u);
+        if (r.sp < kStackShared) stack[r.sp * 32] = child;
+        else if (r.sp < kStackMax) ovf[r.sp - kStackShared] = child;
+        else { atomicOr(err, 1); return true; }
+        ++r.sp;
+    }
+    if (r.sp == 0) return true;
+    --r.sp;
+    r.node = (r.sp < kStackShared) ? stack[r.sp * 32] : ovf[r.sp - kStackShared];
+    return false;
+}
+
+// Persistent traversal loop shared by every ray-query kernel.  Each warp keeps
+// 32 rays in flight; a lane whose ray finishes takes the next queue entry right
+// away (one atomic per warp per refill), so lanes do not idle until the
+// slowest ray of the warp is done.  IO supplies count(), load() -> item id or
+// -1 when the entry finished without traversal, and store().
+template <bool kAny, class IO>
+__device__ __forceinline__ void traverse_queue(const SceneView& s, IO& io, int n, int* fetch, uint32_t* stack,
+                                               uint32_t* ovf, int* err, unsigned long long* work)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    RayState r;
+    int item = -1;
+    unsigned long long visits = 0, tests = 0;
+    bool exhausted = (s.num_nodes == 0 && false);
+    for (;;) {
+        if (!exhausted) {
+            const unsigned idle = __ballot_sync(0xFFFFFFFFu, item < 0);
+            if (idle) {
+                const int leader = __ffs(idle) - 1;
+                int base = 0;
+                if (static_cast<int>(lane) == leader) base = atomicAdd(fetch, __popc(idle));
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (base + __popc(idle) >= n) exhausted = true;
+                if (item < 0) {
+                    const int k = base + __popc(idle & ((1u << lane) - 1u));
+                    if (k < n) item = io.load(s, k, r);
                 }
             }
         }
-        // internal children, pushed far to near
-        const uint32_t child_base = w1.x;
-#pragma unroll
-        for (int k = 7; k >= 0; --k) {
-            const uint32_t kk = key[k];
-            if (kk == 0xFFFFFFFFu) continue;
-            const int slot = static_cast<int>(kk & 7u);
-            const uint32_t meta = byte_of(slot < 4 ? meta0 : meta1, slot & 3);
-            if (!(meta & kMetaInternal)) continue;
-            const float tn = __uint_as_float(kk & ~7u);
-            if (!(tn <= fminf(best.t, FLT_MAX) * kSlabWiden)) continue;
-            if (sp >= kDepth) { atomicOr(err, 1); return best; }
-            stack[sp * 32] = child_base + (meta & 7u);
-            ++sp;
+        const unsigned busy = __ballot_sync(0xFFFFFFFFu, item >= 0);
+        if (busy == 0) {
+            if (exhausted) break;
+            continue;
         }
-        if (sp == 0) break;
-        --sp;
-        node = stack[sp * 32];
+        if (item >= 0) {
+            const bool done = (s.num_nodes == 0) || ray_step<kAny>(s, r, stack, ovf, err);
+            if (done) {
+                io.store(s, item, r);
+                visits += r.visits;
+                tests += r.tests;
+                item = -1;
+            }
+        }
     }
-    return best;
+    if (work) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            visits += __shfl_xor_sync(0xFFFFFFFFu, visits, o);
+            tests += __shfl_xor_sync(0xFFFFFFFFu, tests, o);
+        }
+        if (lane == 0) {
+            atomicAdd(&work[0], visits);
+            atomicAdd(&work[1], tests);
+        }
+    }
 }
 
 }  // namespace ar

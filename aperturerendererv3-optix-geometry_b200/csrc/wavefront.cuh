@@ -28,6 +28,24 @@ enum : int32_t {
     kFlagMissThin = 8      // last segment was a thin-surface miss inside media
 };
 
+// Control block of the path pool (device memory).  Paths live in `pool` slots;
+// retired slots go onto a free stack and are refilled with the next samples
+// (sample-major order g = s * npix + p) until `total` samples have been traced.
+struct PoolCtl {
+    int32_t qcount[2];     // extension queue lengths (ping-pong)
+    int32_t shadow_count;  // shadow queue length
+    int32_t retire_count;  // paths that ended this iteration
+    int32_t fetch_ext, fetch_shadow, fetch_rays;  // persistent-kernel work counters
+    int32_t free_count;    // free slots on the stack
+    int32_t plan_new;      // samples started this iteration
+    int32_t plan_src;      // first free-stack entry they use
+    int32_t pad[2];
+    int64_t gen_next;      // next sample index to start
+    int64_t plan_first;    // sample index of the first path started this iteration
+    int64_t retired;       // paths finished so far
+    int64_t total;         // samples of this render (spp * npix)
+};
+
 struct PathSoA {
     float4* o;       // ray origin xyz
     float4* d;       // ray direction xyz
@@ -35,7 +53,7 @@ struct PathSoA {
     float4* rad;     // radiance rgb
     uint4* rng0;     // xorwow d, v0, v1, v2
     uint2* rng1;     // xorwow v3, v4
-    int4* info;      // x record index, y depth, z nonDeltaDepth, w flags | media depth << 8
+    int4* info;      // x pixel, y depth | nonDeltaDepth << 16, z sample index, w flags | media depth << 8
     float4* prev;    // previous vertex xyz, w previous BSDF pdf
     float4* media;   // media vertex location xyz, w media object (int bits)
     int4* hit;       // object, prim slot, t bits
@@ -44,6 +62,8 @@ struct PathSoA {
     float4* sseg1;   // shadow segment target xyz
     int32_t* q[2];   // extension queues (ping-pong)
     int32_t* qs;     // shadow queue
+    int32_t* qr;     // paths that ended this iteration
+    int32_t* freeq;  // free-slot stack
     int32_t* ucount; // uniforms consumed per slot (debug only)
 };
 
@@ -59,9 +79,7 @@ struct FrameParams {
     int32_t camera_inside;   // intersection::Overlap at the camera
     int32_t max_depth, rr_depth, use_nee, sky;
     int32_t npix;            // width * height
-    int32_t spp_index;       // sample index within this call
-    int32_t first_pixel;     // first pixel of this wave
-    int32_t wave;            // paths in this wave
+    int32_t pool;            // path slots
     uint64_t seed;
     uint64_t frame0;         // TOTAL_FRAME_INDEX of the first sample
     float eps_tab[9];        // INTERSECT_EPS(0..8)

@@ -123,23 +123,26 @@ def cpu_sample(objs, cam: Camera, params: RenderParams, target_s: float, threads
     oracle, kind = reference_cpu_impl()
     if osc is None:
         osc = oracle.OracleScene(objs)
-    p1 = make_params(spp=1, max_depth=params.max_depth, rr_depth=params.rr_depth, use_nee=params.use_nee,
-                     sky=params.sky, seed=params.seed)
     npix = cam.width * cam.height
 
-    def run(step: int, offset: int):
+    def run(step: int, spp: int):
+        q = make_params(spp=spp, max_depth=params.max_depth, rr_depth=params.rr_depth, use_nee=params.use_nee,
+                        sky=params.sky, seed=params.seed)
         t0 = time.perf_counter()
-        _, e, s = osc.render_image(cam, p1, offset, npix, step=step, threads=threads)
+        _, e, s = osc.render_image(cam, q, 0, npix, step=step, threads=threads)
         return time.perf_counter() - t0, e, s
 
-    step = 4096                              # start with ~506 pixels spread over the image
+    step, spp = 4096, 1                      # start with ~506 pixels spread over the image
     while True:
-        dt, e, s = run(step, 0)
-        if dt >= 0.5 * target_s or step == 1:
+        dt, e, s = run(step, spp)
+        if dt >= 0.5 * target_s:
             break
-        step = max(1, int(step * max(dt, 1e-3) / target_s))
+        if step > 1:
+            step = max(1, int(step * max(dt, 1e-3) / target_s))
+        else:
+            spp = max(spp + 1, int(spp * target_s / max(dt, 1e-3)))
     return {"osc": osc, "value": (e + s) / dt / 1e6, "seconds": dt, "pixels": (npix + step - 1) // step,
-            "ext": e, "shadow": s, "kind": kind, "step": step}
+            "ext": e, "shadow": s, "kind": kind, "step": step, "spp": spp}
 
 
 # ----------------------------------------------------------------------------- ours
@@ -207,6 +210,10 @@ def run_ours(args) -> None:
             tot["sh_ms"] += st.shadow_ms
             tot["ext_launch"] += st.extend_launches
             tot["sh_launch"] += st.shadow_launches
+            tot["ev"] = tot.get("ev", 0) + st.extend_node_visits
+            tot["et"] = tot.get("et", 0) + st.extend_prim_tests
+            tot["sv"] = tot.get("sv", 0) + st.shadow_node_visits
+            tot["stt"] = tot.get("stt", 0) + st.shadow_prim_tests
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -275,6 +282,10 @@ def run_ours(args) -> None:
             "samples_per_s": round(all_paths / (total_ms / 1e3), 1),
             "rays": {"extension": tot["ext"], "shadow": tot["sh"], "per_path": round((tot["ext"] + tot["sh"]) / max(tot["paths"], 1), 4)},
             "kernel_ms": {"extend": round(tot["ext_ms"], 3), "shadow": round(tot["sh_ms"], 3), "total": round(total_ms, 3)},
+            "work_per_query": {"extend_nodes": round(tot["ev"] / max(tot["ext"], 1), 3),
+                               "extend_prims": round(tot["et"] / max(tot["ext"], 1), 3),
+                               "shadow_nodes": round(tot["sv"] / max(tot["sh"], 1), 3),
+                               "shadow_prims": round(tot["stt"] / max(tot["sh"], 1), 3)},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1) if achieved else None,
                          "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4) if achieved else None,
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback",
@@ -292,7 +303,7 @@ def run_ours(args) -> None:
             cs = cpu_sample(objs, cam, params, args.cpu_seconds, cpu_threads())
             line["cpu_baseline"] = {"value": round(cs["value"], 4), "unit": "Mrays/s", "cores": cpu_threads(),
                                     "kind": cs["kind"],
-                                    "sample": f"every {cs['step']}th pixel of the image ({cs['pixels']} pixels) at 1 spp, "
+                                    "sample": f"every {cs['step']}th pixel of the image ({cs['pixels']} pixels) at {cs['spp']} spp, "
                                               f"{cs['ext'] + cs['shadow']} queries in {cs['seconds']:.1f} s"}
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -344,11 +355,26 @@ def run_reference(args) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
         "config": config_block(world), "impl": "reference",
         "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": threads, "kind": sample["kind"],
-                         "sample": f"per step every {sample['step']}th pixel ({sample['pixels']} pixels) at 1 spp "
+                         "sample": f"per step every {sample['step']}th pixel ({sample['pixels']} pixels) at {sample['spp']} spp "
                                    f"on {threads} host threads (OpenMP)"},
         "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def profile_queues() -> None:
+    """One 8-spp render of the benchmark scene for ncu captures (-k/-s/-c select
+    a launch of the steady state, where the path pool is full), then the mean
+    extension and shadow queries per traversal launch of that render."""
+    objs = scenes.spheres_scene()
+    scene = Scene(objs)
+    cam = scenes.spheres_camera(WIDTH, HEIGHT)
+    params = make_params(spp=8, max_depth=DEPTH)
+    img, st = scene.render(cam, params)
+    print(json.dumps({"profile": "config2 at 8 spp", "iterations": st.extend_launches,
+                      "extension_rays": st.extension_rays, "shadow_rays": st.shadow_rays,
+                      "extension_per_launch": st.extension_rays / max(st.extend_launches, 1),
+                      "shadow_per_launch": st.shadow_rays / max(st.shadow_launches, 1)}), flush=True)
 
 
 def main():
@@ -359,7 +385,12 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU sample length per measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--profile-queues", action="store_true",
+                    help="render the workload once at 1 spp (for ncu captures) and print the per-depth queue sizes")
     args = ap.parse_args()
+    if args.profile_queues:
+        profile_queues()
+        return
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
     if args.impl == "reference":
         run_reference(args)

@@ -107,7 +107,8 @@ typedef struct ar_path_record {
     int32_t segments;      /* loop iterations executed (Trace calls)                 */
     int32_t uniforms;      /* curand_uniform values this path consumed               */
     int32_t nee_rays;      /* shadow rays cast                                        */
-    int32_t reserved[2];
+    int32_t nee_depth_mask;/* bit d set: a shadow ray was cast at loop depth d (< 32) */
+    int32_t reserved;
     int32_t hit_object[AR_DEBUG_MAX_HITS]; /* closest-hit object per segment, -1 = miss */
 } ar_path_record;          /* 96 bytes */
 
@@ -132,6 +133,10 @@ typedef struct ar_render_stats {
     int64_t kernel_launches; /* kernels this call launched                           */
     int64_t extend_launches; /* closest-hit traversal launches                       */
     int64_t shadow_launches; /* any-hit traversal launches                           */
+    int64_t extend_node_visits; /* 8-wide nodes visited by closest-hit queries       */
+    int64_t extend_prim_tests;  /* primitives tested by closest-hit queries          */
+    int64_t shadow_node_visits; /* 8-wide nodes visited by any-hit queries           */
+    int64_t shadow_prim_tests;  /* primitives tested by any-hit queries              */
     float   extend_ms;       /* summed device time of the closest-hit launches       */
     float   shadow_ms;       /* summed device time of the any-hit launches           */
     float   total_ms;        /* device time of the whole render call                 */

@@ -1292,7 +1292,7 @@ static int segment_occluded(const or_scene* s, float eps_d, V3 src, V3 dst, Coun
     return r.obj >= 0;
 }
 
-typedef struct { V3 radiance; int segments, nee_rays; int hits[AR_DEBUG_MAX_HITS]; } PathOut;
+typedef struct { V3 radiance; int segments, nee_rays, nee_mask; int hits[AR_DEBUG_MAX_HITS]; } PathOut;
 
 /* CalculateRadiance<bUseBVH=true, bUseNEE, bUsePathGuiding=false>, RGB
  * (render.cuh:460-999), with camera_inside = intersection::Overlap at the
@@ -1310,7 +1310,7 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
     int prevDidNEE = 0;
     float prevPdf = 0.0f;
     V3 prevPos = v3(0.0f, 0.0f, 0.0f);
-    po->segments = 0; po->nee_rays = 0;
+    po->segments = 0; po->nee_rays = 0; po->nee_mask = 0;
     for (int k = 0; k < AR_DEBUG_MAX_HITS; ++k) po->hits[k] = -1;
     for (int depth = 0; depth < p->max_depth; depth++) {
         /* ---- Trace (render.cuh:75-163), depth argument = nonDeltaDepth ---- */
@@ -1392,6 +1392,7 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
                     const float d2 = fmaxf(dot3(lu, lu), 1.0e-12f);
                     const V3 ld = vscale(lu, om_rsqrtf(d2));
                     po->nee_rays++;
+                    if (depth < 32) po->nee_mask |= (int)(1u << depth);
                     const int occ = segment_occluded(s, s->eps_tab[depth < 8 ? depth : 8], ic.pos, ls.p, cnt);
                     if (occ) {
                         neeValid = 1;
@@ -1508,6 +1509,7 @@ int64_t or_render_paths(const or_scene* s, const ar_camera* cam, const ar_render
         r->segments = po.segments;
         r->uniforms = g.pos;
         r->nee_rays = po.nee_rays;
+        r->nee_depth_mask = po.nee_mask;
         for (int h = 0; h < AR_DEBUG_MAX_HITS; ++h) r->hit_object[h] = po.hits[h];
         if (g.overflow) overflow++;
     }

@@ -22,7 +22,7 @@ def compare(objects, cam, params, per_path=512):
     tape = rng_tape(cam, params, per_path)
     o, overflow = oracle.OracleScene(objects).render_paths(cam, params, tape)
     assert overflow == 0, "tape too short"
-    for f in ("segments", "uniforms", "nee_rays"):
+    for f in ("segments", "uniforms", "nee_rays", "nee_depth_mask"):
         bad = np.nonzero(g[f] != o[f])[0]
         assert bad.size == 0, f"{f}: {bad.size} paths differ, first {bad[:5]} gpu {g[f][bad[:5]]} cpu {o[f][bad[:5]]}"
     assert np.array_equal(g["hit_object"], o["hit_object"]), "closest-hit ids differ"
