@@ -16,6 +16,7 @@
 #include "../../include/aperture_b200.h"
 #include "render_kernels.h"
 #include "scene_build.h"
+#include "xorwow_jump.h"
 
 namespace {
 
@@ -85,6 +86,7 @@ struct ar_scene {
     int sm_count = 148;
     ar::SceneView view{};
     int grid_trace = 0;
+    const uint32_t* jump_table = nullptr;  // A^(2^32) lookup table of the XORWOW register
     int64_t objects = 0, triangles = 0, lights = 0, nodes = 0, prims = 0;
     int64_t device_bytes = 0;
     std::vector<void*> owned;
@@ -96,7 +98,7 @@ struct ar_scene {
     size_t ws_bytes = 0;
     int64_t ws_wave = 0;
     int64_t ws_pix = 0;
-    ar::PathSoA paths{};
+    ar::PathBuffers bufs{};
     uint4* base0 = nullptr;
     uint2* base1 = nullptr;
     double* accum = nullptr;
@@ -122,42 +124,36 @@ struct ar_scene {
 
 namespace {
 
-// Carve the per-path SoA arrays, queues and per-pixel buffers from one allocation.
-void ensure_workspace(ar_scene* s, int64_t wave, int64_t npix, bool debug)
+// Carve the two path pools, side arrays, queues and per-pixel buffers from one
+// allocation (re-used across calls; grown when a larger pool or image comes).
+void ensure_workspace(ar_scene* s, int64_t pool, int64_t npix)
 {
-    if (s->ws && s->ws_wave >= wave && s->ws_pix >= npix && (!debug || s->paths.ucount)) return;
+    if (s->ws && s->ws_wave >= pool && s->ws_pix >= npix) return;
     if (s->ws) { cudaFree(s->ws); s->ws = nullptr; }
-    wave = std::max(wave, s->ws_wave);
+    pool = std::max(pool, s->ws_wave);
     npix = std::max(npix, s->ws_pix);
     size_t off = 0;
     auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
-    const size_t W = static_cast<size_t>(wave), N = static_cast<size_t>(npix);
-    const size_t o_o = take(16 * W), o_d = take(16 * W), o_mask = take(16 * W), o_rad = take(16 * W);
-    const size_t o_r0 = take(16 * W), o_r1 = take(8 * W), o_info = take(16 * W), o_prev = take(16 * W);
-    const size_t o_media = take(16 * W), o_hit = take(16 * W), o_nee = take(16 * W), o_s0 = take(16 * W);
-    const size_t o_s1 = take(16 * W), o_q0 = take(4 * W), o_q1 = take(4 * W), o_qs = take(4 * W), o_uc = take(4 * W);
-    const size_t o_qr = take(4 * W), o_free = take(4 * W);
+    const size_t W = static_cast<size_t>(pool), N = static_cast<size_t>(npix);
+    const size_t o_p0 = take(sizeof(ar::PathRec) * W), o_p1 = take(sizeof(ar::PathRec) * W);
+    const size_t o_hit = take(16 * W), o_qsh = take(4 * W * ar::kShadeBuckets);
+    const size_t o_sh = take(sizeof(ar::ShadowRec) * W), o_rt = take(sizeof(ar::RetireRec) * W);
     const size_t o_b0 = take(16 * N), o_b1 = take(8 * N), o_acc = take(24 * N), o_fout = take(12 * N);
     const size_t o_cnt = take(sizeof(ar::PoolCtl)), o_stats = take(64), o_err = take(64);
     const size_t o_ovf = take(static_cast<size_t>(s->grid_trace) * ar::kTraceBlock * ar::kStackOverflow * 4);
     s->ws = dalloc<char>(off, "render workspace");
     s->ws_bytes = off;
-    s->ws_wave = wave;
+    s->ws_wave = pool;
     s->ws_pix = npix;
     char* b = s->ws;
-    ar::PathSoA& P = s->paths;
-    P.o = reinterpret_cast<float4*>(b + o_o); P.d = reinterpret_cast<float4*>(b + o_d);
-    P.mask = reinterpret_cast<float4*>(b + o_mask); P.rad = reinterpret_cast<float4*>(b + o_rad);
-    P.rng0 = reinterpret_cast<uint4*>(b + o_r0); P.rng1 = reinterpret_cast<uint2*>(b + o_r1);
-    P.info = reinterpret_cast<int4*>(b + o_info); P.prev = reinterpret_cast<float4*>(b + o_prev);
-    P.media = reinterpret_cast<float4*>(b + o_media); P.hit = reinterpret_cast<int4*>(b + o_hit);
-    P.nee = reinterpret_cast<float4*>(b + o_nee); P.sseg0 = reinterpret_cast<float4*>(b + o_s0);
-    P.sseg1 = reinterpret_cast<float4*>(b + o_s1);
-    P.q[0] = reinterpret_cast<int32_t*>(b + o_q0); P.q[1] = reinterpret_cast<int32_t*>(b + o_q1);
-    P.qs = reinterpret_cast<int32_t*>(b + o_qs);
-    P.ucount = reinterpret_cast<int32_t*>(b + o_uc);
-    P.qr = reinterpret_cast<int32_t*>(b + o_qr);
-    P.freeq = reinterpret_cast<int32_t*>(b + o_free);
+    ar::PathBuffers& B = s->bufs;
+    B.pool[0] = reinterpret_cast<ar::PathRec*>(b + o_p0);
+    B.pool[1] = reinterpret_cast<ar::PathRec*>(b + o_p1);
+    B.hit = reinterpret_cast<int4*>(b + o_hit);
+    B.qsh = reinterpret_cast<int32_t*>(b + o_qsh);
+    B.shadow = reinterpret_cast<ar::ShadowRec*>(b + o_sh);
+    B.retire = reinterpret_cast<ar::RetireRec*>(b + o_rt);
+    B.capacity = static_cast<int32_t>(pool);
     s->base0 = reinterpret_cast<uint4*>(b + o_b0);
     s->base1 = reinterpret_cast<uint2*>(b + o_b1);
     s->accum = reinterpret_cast<double*>(b + o_acc);
@@ -257,16 +253,16 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
     int64_t pool = p->wave_paths > 0 ? std::min<int64_t>(p->wave_paths, kMaxPool) : kMaxPool;
     pool = std::max<int64_t>(1, std::min<int64_t>(pool, total));
     fp.pool = static_cast<int32_t>(pool);
-    ensure_workspace(s, pool, npix, rec_dev != nullptr);
-    PathSoA P = s->paths;
-    if (!rec_dev) P.ucount = nullptr;
+    ensure_workspace(s, pool, npix);
+    PathBuffers B = s->bufs;
+    B.capacity = static_cast<int32_t>(pool);
     ck(cudaMemsetAsync(s->accum, 0, sizeof(double) * 3 * npix, st), "memset accum");
     ck(cudaMemsetAsync(s->stats, 0, 64, st), "memset stats");
     ck(cudaMemsetAsync(s->err, 0, 64, st), "memset err");
     if (!s->ev0) { ck(cudaEventCreate(&s->ev0), "event"); ck(cudaEventCreate(&s->ev1), "event"); }
     ck(cudaEventRecord(s->ev0, st), "event record");
     ck(launch_rng_init(fp, s->base0, s->base1, st), "rng init");
-    ck(launch_pool_init(P, s->ctl, static_cast<int>(pool), total, st), "pool init");
+    ck(launch_pool_init(s->ctl, total, st), "pool init");
     int64_t launches = 2;
     const int grid_trace = s->grid_trace;
     const int grid_other = s->sm_count * 4;
@@ -293,7 +289,8 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
             tm.shadow_ev = s->timer_sh.data();
             tm.cap = static_cast<int>(need / 2);
         }
-        ck(launch_iterations(s->view, fp, P, s->ctl, s->base0, s->base1, s->stats, s->ovf, s->err, s->accum, rec_dev,
+        ck(launch_iterations(s->view, fp, B, s->ctl, s->base0, s->base1, s->jump_table, s->stats, s->ovf, s->err,
+                             s->accum, rec_dev,
                              kBatch, &cur, grid_trace, grid_other, st, &launches, tmp),
            "render launch");
         iters += kBatch;
@@ -396,6 +393,10 @@ ar_status ar_scene_create(const ar_object_desc* objects, size_t count, int32_t d
         v.materials = static_cast<const ar::MaterialRec*>(own(upload(hs.materials, "materials"), hs.materials.size() * sizeof(ar::MaterialRec)));
         v.light_object = static_cast<const int32_t*>(own(upload(hs.light_object, "lights"), hs.light_object.size() * 4));
         v.light_prob = static_cast<const float*>(own(upload(hs.light_prob, "lights"), hs.light_prob.size() * 4));
+        {
+            static const std::vector<uint32_t> jt = ar::xorwow_jump_table_2p32();
+            s->jump_table = static_cast<const uint32_t*>(own(upload(jt, "rng jump table"), jt.size() * 4));
+        }
         v.num_nodes = static_cast<int32_t>(hs.prims.empty() ? 0 : hs.nodes.size());
         v.num_objects = static_cast<int32_t>(hs.objects.size());
         v.num_lights = static_cast<int32_t>(hs.light_object.size());
@@ -491,7 +492,7 @@ ar_status ar_trace_rays(ar_scene* s, const float* rays, size_t n, int32_t any_hi
     AR_GUARD_BEGIN
     DeviceGuard g(s->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (!s->err) ensure_workspace(s, 1, 1, false);
+    if (!s->err) ensure_workspace(s, 1, 1);
     ck(cudaMemsetAsync(s->err, 0, 64, st), "memset err");
     const float4* drays;
     int32_t* dobj;

@@ -30,12 +30,12 @@ struct LaunchTimers {
     int n_shadow = 0;
 };
 
-cudaError_t launch_pool_init(const PathSoA& P, PoolCtl* ctl, int pool, int64_t total, cudaStream_t st);
-// `iterations` rounds of plan -> regen -> extend -> shade -> shadow -> retire.
-cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const PathSoA& P, PoolCtl* ctl, uint4* b0,
-                              uint2* b1, unsigned long long* stats, uint32_t* ovf, int* err, double* accum,
-                              ar_path_record* rec, int iterations, int* cur, int grid_trace, int grid_other,
-                              cudaStream_t st, int64_t* launches, LaunchTimers* tm);
+cudaError_t launch_pool_init(PoolCtl* ctl, int64_t total, cudaStream_t st);
+// `iterations` rounds of plan -> regen -> extend -> shade (per material) -> shadow -> retire.
+cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const PathBuffers& B, PoolCtl* ctl,
+                              uint4* b0, uint2* b1, const uint32_t* jump_table, unsigned long long* stats,
+                              uint32_t* ovf, int* err, double* accum, ar_path_record* rec, int iterations, int* cur,
+                              int grid_trace, int grid_other, cudaStream_t st, int64_t* launches, LaunchTimers* tm);
 cudaError_t launch_mean(const double* accum, int64_t n, double inv, float* out, cudaStream_t st);
 cudaError_t launch_add(const double* src, int64_t n, double* dst, cudaStream_t st);
 
