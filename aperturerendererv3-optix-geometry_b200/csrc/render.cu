@@ -88,7 +88,7 @@ struct RaysIO {
 };
 
 template <bool kAny>
-__global__ void __launch_bounds__(kTraceBlock) k_trace_rays(SceneView s, RaysIO io, int n, PoolCtl* ctl,
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_trace_rays(SceneView s, RaysIO io, int n, PoolCtl* ctl,
                                                             uint32_t* ovf, int* err)
 {
     extern __shared__ uint32_t smem[];
@@ -270,7 +270,7 @@ struct ExtendIO {
 };
 
 // Trace's closest-hit query (render.cuh:86-99) for every path of the pool.
-__global__ void __launch_bounds__(kTraceBlock) k_extend(SceneView s, PathBuffers B, int cur, PoolCtl* ctl,
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(SceneView s, PathBuffers B, int cur, PoolCtl* ctl,
                                                         unsigned long long* stats, uint32_t* ovf, int* err)
 {
     extern __shared__ uint32_t smem[];
@@ -602,7 +602,7 @@ struct ShadowIO {
     __device__ __forceinline__ void store(const SceneView&, int m, const RayState& r) { finish(m, r.best.obj >= 0); }
 };
 
-__global__ void __launch_bounds__(kTraceBlock) k_shadow(SceneView s, PathBuffers B, int cur, PoolCtl* ctl,
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks - 1) k_shadow(SceneView s, PathBuffers B, int cur, PoolCtl* ctl,
                                                         unsigned long long* stats, uint32_t* ovf, int* err)
 {
     extern __shared__ uint32_t smem[];

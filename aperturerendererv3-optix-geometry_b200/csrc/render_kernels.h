@@ -10,6 +10,7 @@
 namespace ar {
 
 constexpr int kTraceBlock = 128;  // threads per traversal block (4 warps)
+constexpr int kTraceMinBlocks = 8;  // resident blocks per SM the traversal kernels are built for (<= 64 registers)
 constexpr int kShadeBlock = 256;
 
 // Upload INTERSECT_EPS(0..8) to the current device.

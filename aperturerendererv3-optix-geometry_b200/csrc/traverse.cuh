@@ -214,11 +214,11 @@ __device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b)
 // leaf children nearest first, push hit internal children far to near, pop the
 // next node.  Returns true when the ray is finished (stack empty, any-hit
 // found, or stack overflow reported through *err).
-template <bool kAny>
+template <bool kAny, bool kCount>
 __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32_t* stack, uint32_t* ovf, int* err)
 {
     const WideNode* np = s.nodes + r.node;
-    ++r.visits;
+    if (kCount) ++r.visits;
     const float4 w0 = ldg4(reinterpret_cast<const char*>(np));
     const uint4 w1 = ldgu4(reinterpret_cast<const char*>(np) + 16);
     const uint4 w2 = ldgu4(reinterpret_cast<const char*>(np) + 32);
@@ -254,7 +254,9 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
         // tnear >= tmin >= 0, so its bit pattern orders like the value
         key[k] = hit ? ((__float_as_uint(fmaxf(tnear, 0.0f)) & ~7u) | static_cast<uint32_t>(k)) : 0xFFFFFFFFu;
     }
-    // sort the 8 keys (Batcher odd-even merge network, 19 comparators)
+    // visit children nearest first -- sort the 8 keys (Batcher odd-even merge
+    // network, 19 comparators).  Any-hit queries profit too: the occluder of a
+    // shadow segment is usually close to its start.
     cswap(key[0], key[1]); cswap(key[2], key[3]); cswap(key[4], key[5]); cswap(key[6], key[7]);
     cswap(key[0], key[2]); cswap(key[1], key[3]); cswap(key[4], key[6]); cswap(key[5], key[7]);
     cswap(key[1], key[2]); cswap(key[5], key[6]);
@@ -276,7 +278,7 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
         const uint32_t first = prim_base + (meta & 31u);
         for (int p = 0; p < count; ++p) {
             const PrimRec* pr = s.prims + first + p;
-            ++r.tests;
+            if (kCount) ++r.tests;
             const float4 a = ldg4(&pr->v0[0]);
             const float4 e1 = ldg4(&pr->e1[0]);
             const int obj = __float_as_int(a.w);
@@ -324,7 +326,7 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
 // away (one atomic per warp per refill), so lanes do not idle until the
 // slowest ray of the warp is done.  IO supplies count(), load() -> item id or
 // -1 when the entry finished without traversal, and store().
-template <bool kAny, class IO>
+template <bool kAny, class IO, bool kCount = false>
 __device__ __forceinline__ void traverse_queue(const SceneView& s, IO& io, int n, int* fetch, uint32_t* stack,
                                                uint32_t* ovf, int* err, unsigned long long* work)
 {
@@ -354,16 +356,18 @@ __device__ __forceinline__ void traverse_queue(const SceneView& s, IO& io, int n
             continue;
         }
         if (item >= 0) {
-            const bool done = (s.num_nodes == 0) || ray_step<kAny>(s, r, stack, ovf, err);
+            const bool done = (s.num_nodes == 0) || ray_step<kAny, kCount>(s, r, stack, ovf, err);
             if (done) {
                 io.store(s, item, r);
-                visits += r.visits;
-                tests += r.tests;
+                if (kCount) {
+                    visits += r.visits;
+                    tests += r.tests;
+                }
                 item = -1;
             }
         }
     }
-    if (work) {
+    if (kCount && work) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             visits += __shfl_xor_sync(0xFFFFFFFFu, visits, o);

@@ -282,10 +282,6 @@ def run_ours(args) -> None:
             "samples_per_s": round(all_paths / (total_ms / 1e3), 1),
             "rays": {"extension": tot["ext"], "shadow": tot["sh"], "per_path": round((tot["ext"] + tot["sh"]) / max(tot["paths"], 1), 4)},
             "kernel_ms": {"extend": round(tot["ext_ms"], 3), "shadow": round(tot["sh_ms"], 3), "total": round(total_ms, 3)},
-            "work_per_query": {"extend_nodes": round(tot["ev"] / max(tot["ext"], 1), 3),
-                               "extend_prims": round(tot["et"] / max(tot["ext"], 1), 3),
-                               "shadow_nodes": round(tot["sv"] / max(tot["sh"], 1), 3),
-                               "shadow_prims": round(tot["stt"] / max(tot["sh"], 1), 3)},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1) if achieved else None,
                          "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4) if achieved else None,
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured" else "fallback",

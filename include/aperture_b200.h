@@ -133,10 +133,10 @@ typedef struct ar_render_stats {
     int64_t kernel_launches; /* kernels this call launched                           */
     int64_t extend_launches; /* closest-hit traversal launches                       */
     int64_t shadow_launches; /* any-hit traversal launches                           */
-    int64_t extend_node_visits; /* 8-wide nodes visited by closest-hit queries       */
-    int64_t extend_prim_tests;  /* primitives tested by closest-hit queries          */
-    int64_t shadow_node_visits; /* 8-wide nodes visited by any-hit queries           */
-    int64_t shadow_prim_tests;  /* primitives tested by any-hit queries              */
+    int64_t extend_node_visits; /* reserved (0): node visits of closest-hit queries  */
+    int64_t extend_prim_tests;  /* reserved (0)                                       */
+    int64_t shadow_node_visits; /* reserved (0)                                       */
+    int64_t shadow_prim_tests;  /* reserved (0)                                       */
     float   extend_ms;       /* summed device time of the closest-hit launches       */
     float   shadow_ms;       /* summed device time of the any-hit launches           */
     float   total_ms;        /* device time of the whole render call                 */
