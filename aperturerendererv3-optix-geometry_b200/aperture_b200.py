@@ -82,7 +82,8 @@ OBJECT_DTYPE = np.dtype(ObjectDesc)
 RECORD_DTYPE = np.dtype(PathRecord)
 
 EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create", "ar_scene_destroy",
-                    "ar_scene_get_info", "ar_render", "ar_trace_rays", "ar_render_debug_paths", "ar_rng_tape")
+                    "ar_scene_get_info", "ar_render", "ar_trace_rays", "ar_trace_rays_static",
+                    "ar_render_debug_paths", "ar_rng_tape")
 
 
 class ArError(RuntimeError):
@@ -115,6 +116,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_render.restype = c_int32
     lib.ar_trace_rays.argtypes = [c_void_p, c_void_p, c_size_t, c_int32, c_void_p, c_void_p, c_int32, c_void_p]
     lib.ar_trace_rays.restype = c_int32
+    lib.ar_trace_rays_static.argtypes = [c_void_p, c_void_p, c_size_t, c_int32, c_void_p, c_void_p, c_void_p]
+    lib.ar_trace_rays_static.restype = c_int32
     lib.ar_render_debug_paths.argtypes = [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_int32,
                                           c_void_p]
     lib.ar_render_debug_paths.restype = c_int32
@@ -216,6 +219,12 @@ class Scene:
                           stream: int = 0) -> None:
         _check(_lib.ar_trace_rays(self._h, c_void_p(rays_ptr), n, int(any_hit), c_void_p(obj_ptr),
                                   c_void_p(t_ptr) if t_ptr else None, MEM_DEVICE, c_void_p(stream)))
+
+    def trace_rays_static(self, rays_ptr: int, n: int, any_hit: bool, obj_ptr: int, t_ptr: int | None,
+                          stream: int = 0) -> None:
+        """ar_trace_rays_static: device buffers, no allocation by the library."""
+        _check(_lib.ar_trace_rays_static(self._h, c_void_p(rays_ptr), n, int(any_hit), c_void_p(obj_ptr),
+                                         c_void_p(t_ptr) if t_ptr else None, c_void_p(stream)))
 
     def debug_paths(self, camera: Camera, params: RenderParams) -> np.ndarray:
         n = camera.width * camera.height * params.spp

@@ -358,6 +358,19 @@ ar_status check_err(ar_scene* s, cudaStream_t st)
 
 }  // namespace
 
+namespace ar {
+// Internal accessors for entry points defined in other translation units.
+bool scene_view_of(const ar_scene* s, SceneView* v, int* device, int* sm_count)
+{
+    if (!s) return false;
+    *v = s->view;
+    *device = s->device;
+    *sm_count = s->sm_count;
+    return true;
+}
+ar_status set_error(ar_status st, const std::string& msg) { return fail(st, msg); }
+}  // namespace ar
+
 extern "C" {
 
 int32_t ar_version(void) { return AR_ABI_VERSION; }

@@ -1,0 +1,154 @@
+// trace_static.cu -- ar_trace_rays_static: ray queries that allocate nothing.
+//
+// Some callers cannot call cudaMalloc at the moment they need a ray query: a
+// host that hands the library a fixed memory budget and forbids further device
+// allocation, a real-time thread that must not take the allocator's locks, or
+// code that runs while another part of the process is capturing a CUDA graph
+// (cudaMalloc is not allowed then).  ar_trace_rays allocates a workspace on
+// first use; this entry point instead keeps its scratch -- two counters and the
+// traversal-stack overflow slabs of its persistent threads -- in one file-scope
+// __device__ array of kStaticScratchBytes (16 MiB), which every GPU that loads
+// the library holds until the process exits.
+//
+// Set-up: the first call on a device looks up the array's device address with
+// cudaGetSymbolAddress (with that device current) and caches it; make that
+// first call before any stream capture.  Every call shares the array, so calls
+// whose work overlaps on the GPU race with each other; issue them on one
+// stream or otherwise serialise them.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <mutex>
+#include <string>
+
+#include "../../include/aperture_b200.h"
+#include "render_kernels.h"
+#include "traverse.cuh"
+
+namespace ar {
+
+// internal accessors of the scene handle and the error string (capi.cu)
+bool scene_view_of(const ar_scene* s, SceneView* v, int* device, int* sm_count);
+ar_status set_error(ar_status st, const std::string& msg);
+
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;
+constexpr size_t kStaticHeaderBytes = 256;  // [0] work counter, [1] error word
+constexpr size_t kSlabBytes = static_cast<size_t>(kStackOverflow) * 4;
+constexpr int kStaticMaxBlocks =
+    static_cast<int>((kStaticScratchBytes - kStaticHeaderBytes) / (kSlabBytes * kTraceBlock));
+
+static __device__ __align__(256) unsigned char g_trace_scratch[kStaticScratchBytes];
+
+struct StaticRaysIO {
+    const float4* rays;
+    int32_t* out_obj;
+    float* out_t;
+    __device__ __forceinline__ int load(const SceneView&, int k, RayState& r)
+    {
+        const float4 a = rays[2 * static_cast<int64_t>(k)], b = rays[2 * static_cast<int64_t>(k) + 1];
+        ray_begin(r, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w);
+        return k;
+    }
+    __device__ __forceinline__ void store(const SceneView&, int k, const RayState& r)
+    {
+        out_obj[k] = r.best.obj;
+        if (out_t) out_t[k] = r.best.t;
+    }
+};
+
+template <bool kAny>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_rays_static(SceneView s, StaticRaysIO io, int n,
+                                                                   unsigned char* scratch)
+{
+    extern __shared__ uint32_t smem[];
+    int* fetch = reinterpret_cast<int*>(scratch);
+    int* err = fetch + 1;
+    uint32_t* ovf = reinterpret_cast<uint32_t*>(scratch + kStaticHeaderBytes) +
+                    (static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) * kStackOverflow;
+    uint32_t* stack = smem + (threadIdx.x >> 5) * (kStackShared * 32) + (threadIdx.x & 31u);
+    traverse_queue<kAny>(s, io, n, fetch, stack, ovf, err, nullptr);
+}
+
+std::mutex g_setup_mutex;
+unsigned char* g_scratch_of_device[256] = {};
+int g_blocks_of_device[256] = {};
+
+}  // namespace
+}  // namespace ar
+
+extern "C" ar_status ar_trace_rays_static(const ar_scene* scene, const float* rays, size_t n, int32_t any_hit,
+                                          int32_t* hit_object, float* hit_t, void* stream)
+{
+    using namespace ar;
+    SceneView view;
+    int device = 0, sms = 0;
+    if (!scene_view_of(scene, &view, &device, &sms)) return set_error(AR_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (n == 0) return AR_OK;
+    if (!rays || !hit_object) return set_error(AR_ERR_INVALID_ARGUMENT, "rays/hit_object is NULL");
+    if (reinterpret_cast<uintptr_t>(rays) & 15u)
+        return set_error(AR_ERR_INVALID_ARGUMENT, "ray buffer must be 16-byte aligned device memory");
+    if (n > static_cast<size_t>(INT_MAX))
+        return set_error(AR_ERR_INVALID_ARGUMENT,
+                         "ar_trace_rays_static takes at most 2147483647 rays per call; split the batch");
+    if (device < 0 || device >= 256) return set_error(AR_ERR_UNSUPPORTED, "device index above 255");
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(AR_ERR_CUDA, "cudaGetDevice failed");
+    }
+    if (prev != device && cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(AR_ERR_CUDA, "cudaSetDevice failed");
+    }
+    struct Restore {
+        int prev, dev;
+        ~Restore() { if (prev != dev) cudaSetDevice(prev); }
+    } restore{prev, device};
+    unsigned char* scratch;
+    int blocks;
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        if (!g_scratch_of_device[device]) {
+            void* p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_trace_scratch);
+            if (e != cudaSuccess || !p) {
+                cudaGetLastError();
+                return set_error(AR_ERR_CUDA, std::string("cudaGetSymbolAddress of the static scratch failed: ") +
+                                                  cudaGetErrorString(e));
+            }
+            const size_t smem = static_cast<size_t>(kStackShared) * kTraceBlock * 4;
+            int b0 = 1, b1 = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_trace_rays_static<false>, kTraceBlock, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_trace_rays_static<true>, kTraceBlock, smem);
+            cudaGetLastError();
+            g_blocks_of_device[device] = std::max(1, std::min(std::min(b0, b1) * sms, kStaticMaxBlocks));
+            g_scratch_of_device[device] = static_cast<unsigned char*>(p);
+        }
+        scratch = g_scratch_of_device[device];
+        blocks = g_blocks_of_device[device];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, kStaticHeaderBytes, st);  // work counter and error word
+    if (e == cudaSuccess) {
+        StaticRaysIO io;
+        io.rays = reinterpret_cast<const float4*>(rays);
+        io.out_obj = hit_object;
+        io.out_t = hit_t;
+        const size_t smem = static_cast<size_t>(kStackShared) * kTraceBlock * 4;
+        if (any_hit) k_trace_rays_static<true><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
+        else k_trace_rays_static<false><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
+        e = cudaGetLastError();
+    }
+    int err_word = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&err_word, scratch + 4, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(AR_ERR_CUDA, std::string("ar_trace_rays_static: ") + cudaGetErrorString(e));
+    }
+    if (err_word != 0) return set_error(AR_ERR_DEVICE_FAULT, "traversal stack overflow reported by a kernel");
+    return AR_OK;
+}

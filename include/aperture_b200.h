@@ -186,6 +186,23 @@ ar_status ar_render(ar_scene* scene, const ar_camera* camera, const ar_render_pa
 ar_status ar_trace_rays(ar_scene* scene, const float* rays, size_t n, int32_t any_hit,
                         int32_t* hit_object, float* hit_t, int32_t mem_kind, void* stream);
 
+/* Closest-hit / any-hit ray queries like ar_trace_rays, for callers that
+ * cannot allocate device memory when they query: hosts that give the library
+ * a fixed memory budget, real-time threads that must not take allocator
+ * locks, processes where another thread may be capturing a CUDA graph.  It
+ * calls no cudaMalloc/cudaFree: its scratch (a work counter, an error word and
+ * the traversal-stack overflow of its persistent threads) is one file-scope
+ * __device__ array of 16 MiB that each GPU loading the library holds until the
+ * process exits.  rays, hit_object and hit_t (may be NULL) are device
+ * pointers; rays 16-byte aligned; at most 2147483647 rays per call (larger
+ * batches are rejected with AR_ERR_INVALID_ARGUMENT: split them).  The first
+ * call on a device looks up the array's address (cudaGetSymbolAddress); make
+ * it before any stream capture.  All calls share the array: calls whose work
+ * overlaps on the GPU race -- serialise them (one stream).  Returns after the
+ * queries finished (synchronises `stream`).  No counterpart in the reference. */
+ar_status ar_trace_rays_static(const ar_scene* scene, const float* rays, size_t n, int32_t any_hit,
+                               int32_t* hit_object, float* hit_t, void* stream);
+
 /* Render spp samples and record every path (width*height*spp records, sample
  * major: record[(s*height + j)*width + i]).  Debug/parity entry; same kernels
  * as ar_render. */
