@@ -51,8 +51,8 @@ inline Bits160 mat_apply(const Mat160& m, const Bits160& v)
     return r;
 }
 
-// Table of A^(2^32) for the device apply (layout [chunk][word][nibble]).
-inline std::vector<uint32_t> xorwow_jump_table_2p32()
+// Table of A^(2^p) for the device apply (layout [chunk][word][nibble]).
+inline std::vector<uint32_t> xorwow_jump_table_pow2(int p)
 {
     Mat160 m;
     for (int i = 0; i < 160; ++i) {
@@ -60,7 +60,7 @@ inline std::vector<uint32_t> xorwow_jump_table_2p32()
         e.w[i >> 5] = 1u << (i & 31);
         m.col[i] = xorwow_register_step(e);
     }
-    for (int sq = 0; sq < 32; ++sq) {  // A^(2^(k+1)) = A^(2^k) * A^(2^k)
+    for (int sq = 0; sq < p; ++sq) {  // A^(2^(k+1)) = A^(2^k) * A^(2^k)
         Mat160 n;
         for (int i = 0; i < 160; ++i) n.col[i] = mat_apply(m, m.col[i]);
         m = n;
@@ -76,6 +76,20 @@ inline std::vector<uint32_t> xorwow_jump_table_2p32()
         }
     return t;
 }
+
+// Host apply of a table built by xorwow_jump_table_pow2.
+inline Bits160 xorwow_jump_apply(const std::vector<uint32_t>& table, const Bits160& v)
+{
+    Bits160 r = {{0, 0, 0, 0, 0}};
+    for (int c = 0; c < kJumpChunks; ++c) {
+        const uint32_t nib = (v.w[c >> 3] >> (4 * (c & 7))) & 15u;
+        for (int k = 0; k < 5; ++k) r.w[k] ^= table[(c * 5 + k) * 16 + nib];
+    }
+    return r;
+}
+
+// The frame jump: 2^32 draws.
+inline std::vector<uint32_t> xorwow_jump_table_2p32() { return xorwow_jump_table_pow2(32); }
 
 #ifdef __CUDACC__
 // v (the five register words, curand order v[0..4]) <- A^(2^32) v, with the

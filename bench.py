@@ -37,6 +37,7 @@ sys.path.insert(0, PKG)
 
 import scenes  # noqa: E402
 from aperture_b200 import Camera, RenderParams, RenderStats, Scene, make_params  # noqa: E402
+from sharding import job_totals, rank_frame_offset, reduce_accumulators  # noqa: E402
 
 METRIC = "Mrays/s"
 WIDTH, HEIGHT, SPP, DEPTH = 1920, 1080, 64, 12
@@ -166,7 +167,7 @@ def run_ours(args) -> None:
     objs = scenes.spheres_scene()
     scene = Scene(objs, device=local)
     cam = scenes.spheres_camera(WIDTH, HEIGHT)
-    params = make_params(spp=SPP, max_depth=DEPTH, frame_offset=rank * SPP)
+    params = make_params(spp=SPP, max_depth=DEPTH, frame_offset=rank_frame_offset(rank, SPP))
     npix = WIDTH * HEIGHT
     stream = torch.cuda.Stream(device=dev)
     out = torch.empty(npix * 3, dtype=torch.float32, device=dev)
@@ -177,7 +178,7 @@ def run_ours(args) -> None:
         scene.render_device(cam, params, out.data_ptr(), accum.data_ptr(), stream.cuda_stream, stats)
         if world > 1:
             with torch.cuda.stream(stream):
-                dist.reduce(accum, dst=0)
+                reduce_accumulators(accum, dist)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -220,13 +221,8 @@ def run_ours(args) -> None:
     clocks = sampler.stop() if sampler else None
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = float(sum(step_ms))
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    rays = torch.tensor([tot["ext"] + tot["sh"], tot["paths"]], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(rays, op=dist.ReduceOp.SUM)
-    total_ms = float(t.item())
-    all_rays, all_paths = float(rays[0].item()), float(rays[1].item())
+    total_ms, (all_rays, all_paths) = job_totals(total_ms, [tot["ext"] + tot["sh"], tot["paths"]],
+                                                 dist if world > 1 else None, dev)
     value = all_rays / (total_ms / 1e3) / 1e6
 
     # end to end through the C ABI with host buffers (image copied back every step)
@@ -237,12 +233,8 @@ def run_ours(args) -> None:
         img, st = scene.render(cam, params)
         e2e_s.append(time.perf_counter() - t0)
         e2e_rays += st.extension_rays + st.shadow_rays
-    e2e_t = torch.tensor([sum(e2e_s)], dtype=torch.float64, device=dev)
-    e2e_r = torch.tensor([float(e2e_rays)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(e2e_r, op=dist.ReduceOp.SUM)
-    e2e_value = float(e2e_r.item()) / float(e2e_t.item()) / 1e6
+    e2e_t, (e2e_r,) = job_totals(sum(e2e_s), [e2e_rays], dist if world > 1 else None, dev)
+    e2e_value = e2e_r / e2e_t / 1e6
 
     if rank == 0:
         with open(os.path.join(ROOT, "tests", "golden", "algorithmic_bytes.json")) as f:

@@ -687,8 +687,8 @@ void or_trace_rays(const or_scene* s, const float* rays, int64_t n, int any_hit,
                    int32_t* hit_object, float* hit_t, int32_t* node_visits, int32_t* prim_tests, int threads)
 {
 #ifdef _OPENMP
-    if (threads > 0) omp_set_num_threads(threads);
-#pragma omp parallel for schedule(dynamic, 256)
+    const int nthreads = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
 #endif
     for (int64_t i = 0; i < n; ++i) {
         const float* q = rays + 8 * i;
@@ -704,8 +704,8 @@ void or_trace_rays_brute(const or_scene* s, const float* rays, int64_t n, int an
                          int32_t* hit_object, float* hit_t, int threads)
 {
 #ifdef _OPENMP
-    if (threads > 0) omp_set_num_threads(threads);
-#pragma omp parallel for schedule(dynamic, 64)
+    const int nthreads = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
 #endif
     for (int64_t i = 0; i < n; ++i) {
         const float* q = rays + 8 * i;
@@ -1489,8 +1489,8 @@ int64_t or_render_paths(const or_scene* s, const ar_camera* cam, const ar_render
     const int inside = camera_overlap(s, from_ar(cam->position));
     int64_t overflow = 0;
 #ifdef _OPENMP
-    if (threads > 0) omp_set_num_threads(threads);
-#pragma omp parallel for schedule(dynamic, 16) reduction(+ : overflow)
+    const int nthreads = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : overflow) num_threads(nthreads)
 #endif
     for (int64_t k = 0; k < W * H * S; ++k) {
         const int i = (int)(k % W), j = (int)((k / W) % H);
@@ -1525,8 +1525,8 @@ void or_render_image(const or_scene* s, const ar_camera* cam, const ar_render_pa
     if (step < 1) step = 1;
     const int64_t count = (pe - pb + step - 1) / step;
 #ifdef _OPENMP
-    if (threads > 0) omp_set_num_threads(threads);
-#pragma omp parallel for schedule(dynamic, 4) reduction(+ : e, sh)
+    const int nthreads = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : e, sh) num_threads(nthreads)
 #endif
     for (int64_t k = 0; k < count; ++k) {
         const int64_t pix = pb + k * step;
