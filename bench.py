@@ -291,7 +291,7 @@ def run_ours(args) -> None:
             cs = cpu_sample(objs, cam, params, args.cpu_seconds, cpu_threads())
             line["cpu_baseline"] = {"value": round(cs["value"], 4), "unit": "Mrays/s", "cores": cpu_threads(),
                                     "kind": cs["kind"],
-                                    "sample": f"every {cs['step']}th pixel of the image ({cs['pixels']} pixels) at {cs['spp']} spp, "
+                                    "sample": f"{cs['pixels']} pixels spread over the image (every {cs['step']}. pixel) at {cs['spp']} spp, "
                                               f"{cs['ext'] + cs['shadow']} queries in {cs['seconds']:.1f} s"}
         print(json.dumps(line), flush=True)
     if world > 1:

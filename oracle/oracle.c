@@ -715,6 +715,10 @@ void or_trace_rays_brute(const or_scene* s, const float* rays, int64_t n, int an
     }
 }
 
+/* Forward declarations of the per-query exports below (defined after the
+ * shading helpers they use). */
+static int overlap_index(const or_scene* s, V3 p);
+
 /* ------------------------------------------------------------------------ */
 /* Random numbers: a tape of curand uniforms, or an own generator             */
 /* ------------------------------------------------------------------------ */
@@ -1443,23 +1447,27 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
     po->radiance = vmaxs(out, 0.0f);
 }
 
-/* intersection::Overlap (intersection.cuh:399-414) at the camera position */
-static int camera_overlap(const or_scene* s, V3 p)
+/* intersection::Overlap (intersection.cuh:399-414): the first object that
+ * contains p, or -1 */
+static int overlap_index(const or_scene* s, V3 p)
 {
     for (int i = 0; i < s->n; ++i) {
         const OObj* o = &s->o[i];
         if (o->type == AR_OBJ_CUBE) {
             const V3 l = mmul(&o->w2o, vsub(p, o->center));
             const V3 mn = vneg(o->extent), mx = o->extent;
-            if (mn.x < l.x && mn.y < l.y && mn.z < l.z && mx.x > l.x && mx.y > l.y && mx.z > l.z) return 1;
+            if (mn.x < l.x && mn.y < l.y && mn.z < l.z && mx.x > l.x && mx.y > l.y && mx.z > l.z) return i;
         } else if (o->type == AR_OBJ_SPHERE) {
             const V3 l = mmul(&o->w2o, vsub(p, o->center));
             const float r = max3f(o->extent);
-            if (dot3(l, l) < r * r) return 1;
+            if (dot3(l, l) < r * r) return i;
         }
     }
-    return 0;
+    return -1;
 }
+
+/* at the camera position */
+static int camera_overlap(const or_scene* s, V3 p) { return overlap_index(s, p) >= 0; }
 
 /* RenderCamera ray generation (scene.cu:213-230), field of view as parameter */
 void or_camera_ray(const ar_camera* cam, int i, int j, float jx, float jy, float* ray8)
@@ -1583,3 +1591,66 @@ int64_t or_collect_rays(const or_scene* s, const ar_camera* cam, const ar_render
     *n_sh = cnt.shadow_rays < sh_cap ? cnt.shadow_rays : sh_cap;
     return cnt.ext_rays + cnt.shadow_rays;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Per-query exports used to pin the restatement against the reference       */
+/* ------------------------------------------------------------------------ */
+void or_trace_detail(const or_scene* s, const float* rays, int64_t n, int mode, int32_t* hit_object, float* hit_t,
+                     float* pos, float* nrm, int32_t* inside, int threads)
+{
+#ifdef _OPENMP
+    const int nthreads = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
+#endif
+    for (int64_t i = 0; i < n; ++i) {
+        const float* q = rays + 8 * i;
+        const V3 ro = v3(q[0], q[1], q[2]), rd = v3(q[4], q[5], q[6]);
+        const TraceResult r = traverse(s, ro, rd, q[3], q[7], 0, mode);
+        hit_object[i] = r.obj;
+        hit_t[i] = r.obj >= 0 ? r.t : q[7];
+        Isect c;
+        memset(&c, 0, sizeof(c));
+        if (r.obj >= 0) isect_object(s, r.obj, ro, rd, &c);
+        pos[3 * i + 0] = c.pos.x; pos[3 * i + 1] = c.pos.y; pos[3 * i + 2] = c.pos.z;
+        nrm[3 * i + 0] = c.nrm.x; nrm[3 * i + 1] = c.nrm.y; nrm[3 * i + 2] = c.nrm.z;
+        inside[i] = r.obj >= 0 ? c.inside : 0;
+    }
+}
+
+void or_segments_occluded(const or_scene* s, const float* seg6, const int32_t* depth, int64_t n, int mode,
+                          int32_t* occluded, int threads)
+{
+#ifdef _OPENMP
+    const int nthreads = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
+#endif
+    for (int64_t i = 0; i < n; ++i) {
+        const float* q = seg6 + 6 * i;
+        const V3 src = v3(q[0], q[1], q[2]), dst = v3(q[3], q[4], q[5]);
+        const int d = depth[i] < 8 ? (depth[i] < 0 ? 0 : depth[i]) : 8;
+        V3 dir = vsub(dst, src);
+        const float dist = len3(dir);
+        occluded[i] = 0;
+        if (dist <= 0.0f) continue;
+        dir = vdivs(dir, dist);
+        const float eps = s->eps_tab[d] * fmaxf(1.0f, fmaxf(len3(src), len3(dst)));
+        const float tMax = fmaxf(0.0f, dist - eps);
+        if (tMax <= 0.0f) continue;
+        occluded[i] = traverse(s, src, dir, 0.0f, tMax, 1, mode).obj >= 0;
+    }
+}
+
+void or_overlap(const or_scene* s, const float* p3, int64_t n, int32_t* object_index)
+{
+    for (int64_t i = 0; i < n; ++i) object_index[i] = overlap_index(s, v3(p3[3 * i], p3[3 * i + 1], p3[3 * i + 2]));
+}
+
+float or_bsdf_pdf(int model, const ar_material* m, const float* N, const float* ray_dir, const float* L)
+{
+    Isect c;
+    memset(&c, 0, sizeof(c));
+    gbuffer_material(&c, m);
+    return bsdf_pdf(model, &c, v3(N[0], N[1], N[2]), v3(ray_dir[0], ray_dir[1], ray_dir[2]), v3(L[0], L[1], L[2]));
+}
+
+float or_power_heuristic(float a, float b) { return power_heuristic(a, b); }

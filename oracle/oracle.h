@@ -100,6 +100,21 @@ int64_t or_collect_rays(const or_scene* s, const ar_camera* cam, const ar_render
                         float* ext, int64_t ext_cap, int64_t* n_ext, float* sh, int64_t sh_cap, int64_t* n_sh);
 
 /* Deterministic transcendental functions (exported for their own tests). */
+/* Closest hit plus the hit's world position, normal and inside flag
+ * (IntersectionContext fields), per ray; misses leave zeros. */
+void or_trace_detail(const or_scene* s, const float* rays, int64_t n, int mode, int32_t* hit_object,
+                     float* hit_t, float* pos, float* nrm, int32_t* inside, int threads);
+/* AnyHitSegmentBVH (intersection.cuh:372-397): segments as src.xyz, dst.xyz,
+ * eps of the given loop depth; occluded[i] = 1 when something blocks it. */
+void or_segments_occluded(const or_scene* s, const float* seg6, const int32_t* depth, int64_t n, int mode,
+                          int32_t* occluded, int threads);
+/* intersection::Overlap: first object containing each point, or -1. */
+void or_overlap(const or_scene* s, const float* p3, int64_t n, int32_t* object_index);
+/* BSDF_PDF (RGB) for one material, normal, ray direction and light direction. */
+float or_bsdf_pdf(int model, const ar_material* m, const float* N, const float* ray_dir, const float* L);
+/* PowerHeuristic (render.cuh:185-196). */
+float or_power_heuristic(float a, float b);
+
 float or_sinf(float x);
 float or_cosf(float x);
 float or_expf(float x);

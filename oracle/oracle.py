@@ -62,6 +62,13 @@ def load():
     lib.or_collect_rays.restype = c_int64
     lib.or_powf.argtypes = [c_float, c_float]
     lib.or_powf.restype = c_float
+    lib.or_trace_detail.argtypes = [c_void_p, c_void_p, c_int64, c_int] + [c_void_p] * 5 + [c_int]
+    lib.or_segments_occluded.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p, c_int]
+    lib.or_overlap.argtypes = [c_void_p, c_void_p, c_int64, c_void_p]
+    lib.or_bsdf_pdf.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.or_bsdf_pdf.restype = c_float
+    lib.or_power_heuristic.argtypes = [c_float, c_float]
+    lib.or_power_heuristic.restype = c_float
     _lib = lib
     return lib
 
@@ -118,6 +125,33 @@ class OracleScene:
             return obj, t, nv, pt
         return obj, t
 
+    def trace_detail(self, rays, mode=TIE_LOWEST_INDEX | SLAB_STANDARD, threads=0):
+        """Closest hit with position, normal and inside flag:
+        (hit_object, t, position[n,3], normal[n,3], inside)."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        obj = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        pos = np.empty((n, 3), np.float32)
+        nrm = np.empty((n, 3), np.float32)
+        ins = np.empty(n, np.int32)
+        _lib.or_trace_detail(self._h, _p(rays), n, mode, _p(obj), _p(t), _p(pos), _p(nrm), _p(ins), threads)
+        return obj, t, pos, nrm, ins
+
+    def segments_occluded(self, seg6, depth, mode=TIE_LOWEST_INDEX | SLAB_STANDARD, threads=0):
+        """AnyHitSegmentBVH of src.xyz -> dst.xyz segments at the given loop depths."""
+        seg6 = np.ascontiguousarray(seg6, np.float32).reshape(-1, 6)
+        depth = np.ascontiguousarray(depth, np.int32)
+        out = np.empty(len(seg6), np.int32)
+        _lib.or_segments_occluded(self._h, _p(seg6), _p(depth), len(seg6), mode, _p(out), threads)
+        return out
+
+    def overlap(self, points):
+        p = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.empty(len(p), np.int32)
+        _lib.or_overlap(self._h, _p(p), len(p), _p(out))
+        return out
+
     def trace_brute(self, rays, any_hit=False, threads=0):
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
         n = rays.shape[0]
@@ -163,3 +197,15 @@ def camera_ray(camera, i, j, jx, jy) -> np.ndarray:
     r = np.zeros(8, np.float32)
     lib.or_camera_ray(ctypes.byref(camera), i, j, jx, jy, _p(r))
     return r
+
+
+def bsdf_pdf(model: int, material, N, ray_dir, L) -> float:
+    """BSDF_PDF (RGB) of the restatement for one ar_material (ctypes struct)."""
+    lib = load()
+    f = lambda v: np.ascontiguousarray(v, np.float32)  # noqa: E731
+    n, r, l = f(N), f(ray_dir), f(L)
+    return lib.or_bsdf_pdf(model, ctypes.addressof(material), _p(n), _p(r), _p(l))
+
+
+def power_heuristic(a: float, b: float) -> float:
+    return load().or_power_heuristic(a, b)

@@ -1,0 +1,223 @@
+// ref_harness.cu -- drives the reference renderer's own host-callable code, to
+// pin the C restatement (oracle.c).  TEST INFRASTRUCTURE ONLY: built by
+// `make -C oracle ref` into oracle/_ref/libref.so from the reference's headers
+// where they lie (include path REF_CORE), never shipped, loaded only by the
+// fixture generator under tests/golden/ and by pinning tests.
+//
+// Everything called here is the reference's code, unchanged:
+//   SceneObject(center, extent, material, rotation, type, info)
+//       core/render/object.cuh:344-364 (world transform, BVH proxy)
+//   SceneObject::GetArea / GetEmissivePower   core/render/object.cuh:270-306
+//   BuildBVH                                  core/bvh/bvh.cuh:142-422
+//   intersection::TraverseBVH<bAnyHit>        core/render/intersection.cuh:235-370
+//   intersection::AnyHitSegmentBVH            core/render/intersection.cuh:372-397
+//   intersection::Intersect (linear scan)     core/render/intersection.cuh:175-205
+//   intersection::Overlap                     core/render/intersection.cuh:399-414
+//   BSDF_PDF (RGB)                            core/render/material.cuh:332-387
+//   PowerHeuristic                            core/render/render.cuh:185-196 (restated
+//       below: render.cuh does not compile in the RGB configuration)
+// The light table follows UpdateSceneToDeviceIfDirty (core/scene.cu:1046-1080):
+// this file repeats its loop because scene.cu itself needs OptiX and the GUI.
+#include <cstdint>
+#include <vector>
+
+#include "bvh/bvh.cuh"
+#include "render/intersection.cuh"
+#include "render/material.cuh"
+
+#include "../include/aperture_b200.h"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+// The SDF cache pointers the reference declares extern (object/sdf/sdf_master.cuh:12-13);
+// scene.cu defines them in the reference build.  No SDF object is used here.
+namespace sdf {
+__device__ SDFVolumeInfo* cachedSDFInfoPtrs = nullptr;
+__device__ uint32_t cachedSDFInfoPtrsCount = 0;
+}  // namespace sdf
+
+namespace {
+
+float3 f3(const ar_vec3& v) { return make_float3(v.x, v.y, v.z); }
+
+Material material_of(const ar_material& m)
+{
+    Material r = {};
+    r.shadingModel_ = static_cast<EShadingModel>(m.shading_model);
+    r.texture_.textureType_ = ETextureType::TEX_PURE_COLOR;
+    GBuffer& g = r.texture_.baseTexture_;
+    g.albedo_ = f3(m.albedo);
+    g.emissive_ = f3(m.emissive);
+    g.specular_ = m.specular;
+    g.metallic_ = m.metallic;
+    g.roughness_ = m.roughness;
+    g.IOR_ = m.ior;
+    g.sigmaA_ = m.sigma_a;
+    g.abbeNumber_ = m.abbe_number;
+    g.tiltNumber_ = m.tilt_number;
+    return r;
+}
+
+SceneObject object_of(const ar_object_desc& d)
+{
+    AdditionalObjectInfo info = {};
+    if (d.type == AR_OBJ_TRIANGLE) {
+        Vertex* v[3] = {&info.triangleInfo_.v0_, &info.triangleInfo_.v1_, &info.triangleInfo_.v2_};
+        for (int k = 0; k < 3; ++k) {
+            v[k]->position_ = f3(d.tri[k].position);
+            v[k]->normal_ = f3(d.tri[k].normal);
+            v[k]->uv_ = make_float2(d.tri[k].u, d.tri[k].v);
+        }
+    }
+    SceneObject o(f3(d.center), f3(d.extent), material_of(d.material), f3(d.rotation_deg),
+                  static_cast<EObjectType>(d.type), info);
+    o.bVisible_ = d.visible != 0;
+    return o;
+}
+
+int thread_count(int threads)
+{
+#ifdef _OPENMP
+    return threads > 0 ? threads : omp_get_max_threads();
+#else
+    (void)threads;
+    return 1;
+#endif
+}
+
+}  // namespace
+
+struct ref_scene {
+    std::vector<SceneObject> objects;
+    BVHHost bvh;
+    std::vector<AdditionalLightInfo> lights;
+};
+
+extern "C" {
+
+ref_scene* ref_scene_create(const ar_object_desc* objects, size_t count, int leaf_size, int bin_count)
+{
+    ref_scene* s = new ref_scene;
+    s->objects.reserve(count);
+    for (size_t i = 0; i < count; ++i) s->objects.push_back(object_of(objects[i]));
+    std::vector<PrimitiveProxy> proxies;
+    proxies.reserve(count);
+    for (const SceneObject& o : s->objects) proxies.push_back(o.proxy_);
+    s->bvh = BuildBVH(proxies, leaf_size, bin_count);
+    float total = 0.0f;
+    for (size_t i = 0; i < s->objects.size(); ++i) {
+        SceneObject& o = s->objects[i];
+        o.objectIndex_ = static_cast<int>(i);
+        if (o.material_.shadingModel_ == EShadingModel::MAT_LIGHT) {
+            o.lightIndex_ = static_cast<int>(s->lights.size());
+            AdditionalLightInfo li;
+            li.objectIndex_ = static_cast<int>(i);
+            li.importanceWeight_ = fmaxf(o.GetArea() * o.GetEmissivePower(), 1.0e-20f);
+            total += li.importanceWeight_;
+            s->lights.push_back(li);
+        } else {
+            o.lightIndex_ = -1;
+        }
+    }
+    for (AdditionalLightInfo& li : s->lights) li.selectProb_ = li.importanceWeight_ / total;
+    return s;
+}
+
+void ref_scene_destroy(ref_scene* s) { delete s; }
+
+int64_t ref_scene_node_count(const ref_scene* s) { return static_cast<int64_t>(s->bvh.nodes_.size()); }
+
+void ref_scene_nodes(const ref_scene* s, float* b6, int32_t* l4)
+{
+    for (size_t i = 0; i < s->bvh.nodes_.size(); ++i) {
+        const BVHNode& n = s->bvh.nodes_[i];
+        b6[6 * i + 0] = n.boundMin_.x; b6[6 * i + 1] = n.boundMin_.y; b6[6 * i + 2] = n.boundMin_.z;
+        b6[6 * i + 3] = n.boundMax_.x; b6[6 * i + 4] = n.boundMax_.y; b6[6 * i + 5] = n.boundMax_.z;
+        l4[4 * i + 0] = n.left_; l4[4 * i + 1] = n.right_; l4[4 * i + 2] = n.first_; l4[4 * i + 3] = n.count_;
+    }
+}
+
+void ref_scene_indices(const ref_scene* s, int32_t* idx)
+{
+    for (size_t i = 0; i < s->bvh.objectIndices_.size(); ++i) idx[i] = s->bvh.objectIndices_[i];
+}
+
+int64_t ref_scene_light_count(const ref_scene* s) { return static_cast<int64_t>(s->lights.size()); }
+
+void ref_scene_lights(const ref_scene* s, int32_t* object_index, float* select_prob)
+{
+    for (size_t i = 0; i < s->lights.size(); ++i) {
+        object_index[i] = s->lights[i].objectIndex_;
+        select_prob[i] = s->lights[i].selectProb_;
+    }
+}
+
+// Rays as 8 floats (origin, tmin, direction, tmax).  mode 0: TraverseBVH over
+// the reference BVH; mode 1: the linear Intersect scan.  Closest hits also
+// return the hit position, normal and inside flag.
+void ref_trace_rays(const ref_scene* s, const float* rays, int64_t n, int any_hit, int mode, int32_t* hit_object,
+                    float* hit_t, float* pos, float* nrm, int32_t* inside, int threads)
+{
+    const intersection::SceneObjectsIntersector isect{s->objects.data(), static_cast<int>(s->objects.size())};
+    const BVHNode* nodes = s->bvh.nodes_.data();
+    const int node_count = static_cast<int>(s->bvh.nodes_.size());
+    const int* indices = s->bvh.objectIndices_.data();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(thread_count(threads))
+    for (int64_t i = 0; i < n; ++i) {
+        const float* q = rays + 8 * i;
+        const float3 o = make_float3(q[0], q[1], q[2]);
+        const float3 d = make_float3(q[4], q[5], q[6]);
+        IntersectionContext c;
+        if (mode == 1)
+            c = intersection::Intersect(0, o, d, isect, -1, q[3], q[7]);
+        else if (any_hit)
+            c = intersection::TraverseBVH<true>(0, o, d, isect, nodes, node_count, indices, q[3], q[7]);
+        else
+            c = intersection::TraverseBVH<false>(0, o, d, isect, nodes, node_count, indices, q[3], q[7]);
+        hit_object[i] = c.bHit_ ? c.objectIndex_ : -1;
+        if (hit_t) hit_t[i] = c.bHit_ ? c.distance_ : q[7];
+        if (pos) { pos[3 * i] = c.bHit_ ? c.hitPosition_.x : 0.0f; pos[3 * i + 1] = c.bHit_ ? c.hitPosition_.y : 0.0f; pos[3 * i + 2] = c.bHit_ ? c.hitPosition_.z : 0.0f; }
+        if (nrm) { nrm[3 * i] = c.bHit_ ? c.hitNormal_.x : 0.0f; nrm[3 * i + 1] = c.bHit_ ? c.hitNormal_.y : 0.0f; nrm[3 * i + 2] = c.bHit_ ? c.hitNormal_.z : 0.0f; }
+        if (inside) inside[i] = c.bHit_ ? static_cast<int32_t>(c.isInside_) : 0;
+    }
+}
+
+// AnyHitSegmentBVH for segments src.xyz, dst.xyz at the given loop depth.
+void ref_segments_occluded(const ref_scene* s, const float* seg6, const int32_t* depth, int64_t n,
+                           int32_t* occluded, int threads)
+{
+    const intersection::SceneObjectsIntersector isect{s->objects.data(), static_cast<int>(s->objects.size())};
+    const BVHNode* nodes = s->bvh.nodes_.data();
+    const int node_count = static_cast<int>(s->bvh.nodes_.size());
+    const int* indices = s->bvh.objectIndices_.data();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(thread_count(threads))
+    for (int64_t i = 0; i < n; ++i) {
+        const float* q = seg6 + 6 * i;
+        const IntersectionContext c = intersection::AnyHitSegmentBVH(
+            depth[i], make_float3(q[0], q[1], q[2]), make_float3(q[3], q[4], q[5]), isect, nodes, node_count, indices);
+        occluded[i] = c.bHit_ ? 1 : 0;
+    }
+}
+
+void ref_overlap(const ref_scene* s, const float* p3, int64_t n, int32_t* object_index)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        const OverlapContext c = intersection::Overlap(make_float3(p3[3 * i], p3[3 * i + 1], p3[3 * i + 2]),
+                                                       s->objects.data(), static_cast<int>(s->objects.size()));
+        object_index[i] = c.bOverlap_ ? c.objectIndex_ : -1;
+    }
+}
+
+float ref_bsdf_pdf(int model, const ar_material* m, const float* N, const float* ray_dir, const float* L)
+{
+    const GBuffer g = material_of(*m).texture_.baseTexture_;
+    return BSDF_PDF(static_cast<EShadingModel>(model), g, make_float3(0.0f, 0.0f, 0.0f), make_float3(N[0], N[1], N[2]),
+                    make_float3(ray_dir[0], ray_dir[1], ray_dir[2]), make_float3(L[0], L[1], L[2]));
+}
+
+// INTERSECT_EPS (config.cuh:3) as the reference's host pass evaluates it.
+float ref_intersect_eps(int depth) { return INTERSECT_EPS(depth); }
+
+}  // extern "C"

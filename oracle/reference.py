@@ -1,0 +1,129 @@
+"""ctypes wrapper of oracle/_ref/libref.so: the reference renderer's own
+BuildBVH, TraverseBVH, AnyHitSegmentBVH, Intersect, Overlap and BSDF_PDF,
+compiled from the reference's headers by `make -C oracle ref`.
+
+TEST INFRASTRUCTURE ONLY: used to generate the golden fixtures under
+tests/golden/ and, where the library has been built, to check the oracle
+against the reference directly.  Absent on machines without the reference
+source; callers test `available()` first.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import c_float, c_int, c_int64, c_size_t, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_ref", "libref.so")
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB)
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    lib = ctypes.CDLL(LIB)
+    lib.ref_scene_create.argtypes = [c_void_p, c_size_t, c_int, c_int]
+    lib.ref_scene_create.restype = c_void_p
+    lib.ref_scene_destroy.argtypes = [c_void_p]
+    lib.ref_scene_node_count.argtypes = [c_void_p]
+    lib.ref_scene_node_count.restype = c_int64
+    lib.ref_scene_nodes.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.ref_scene_indices.argtypes = [c_void_p, c_void_p]
+    lib.ref_scene_light_count.argtypes = [c_void_p]
+    lib.ref_scene_light_count.restype = c_int64
+    lib.ref_scene_lights.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.ref_trace_rays.argtypes = [c_void_p, c_void_p, c_int64, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                   c_void_p, c_int]
+    lib.ref_segments_occluded.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int]
+    lib.ref_overlap.argtypes = [c_void_p, c_void_p, c_int64, c_void_p]
+    lib.ref_bsdf_pdf.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.ref_bsdf_pdf.restype = c_float
+    lib.ref_intersect_eps.argtypes = [c_int]
+    lib.ref_intersect_eps.restype = c_float
+    _lib = lib
+    return lib
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class RefScene:
+    """The reference's SceneObject array, BVH (BuildBVH) and light table."""
+
+    def __init__(self, objects: np.ndarray, leaf_size: int = 8, bin_count: int = 12):
+        lib = load()
+        from aperture_b200 import OBJECT_DTYPE
+        self._objs = np.ascontiguousarray(objects, dtype=OBJECT_DTYPE)
+        self._h = lib.ref_scene_create(_p(self._objs), len(self._objs), leaf_size, bin_count)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib.ref_scene_destroy(self._h)
+            self._h = None
+
+    def nodes(self):
+        n = _lib.ref_scene_node_count(self._h)
+        b = np.zeros((n, 6), np.float32)
+        l = np.zeros((n, 4), np.int32)
+        if n:
+            _lib.ref_scene_nodes(self._h, _p(b), _p(l))
+        return b, l
+
+    def indices(self):
+        idx = np.zeros(len(self._objs), np.int32)
+        _lib.ref_scene_indices(self._h, _p(idx))
+        return idx
+
+    def lights(self):
+        n = _lib.ref_scene_light_count(self._h)
+        o = np.zeros(n, np.int32)
+        p = np.zeros(n, np.float32)
+        if n:
+            _lib.ref_scene_lights(self._h, _p(o), _p(p))
+        return o, p
+
+    def trace(self, rays, any_hit=False, linear=False, threads=0):
+        """(hit_object, t, position[n,3], normal[n,3], inside) per ray."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        obj = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        pos = np.empty((n, 3), np.float32)
+        nrm = np.empty((n, 3), np.float32)
+        ins = np.empty(n, np.int32)
+        _lib.ref_trace_rays(self._h, _p(rays), n, int(any_hit), 1 if linear else 0, _p(obj), _p(t), _p(pos), _p(nrm),
+                            _p(ins), threads)
+        return obj, t, pos, nrm, ins
+
+    def segments_occluded(self, seg6, depth, threads=0):
+        seg6 = np.ascontiguousarray(seg6, np.float32).reshape(-1, 6)
+        depth = np.ascontiguousarray(depth, np.int32)
+        out = np.empty(len(seg6), np.int32)
+        _lib.ref_segments_occluded(self._h, _p(seg6), _p(depth), len(seg6), _p(out), threads)
+        return out
+
+    def overlap(self, points):
+        p = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.empty(len(p), np.int32)
+        _lib.ref_overlap(self._h, _p(p), len(p), _p(out))
+        return out
+
+
+def bsdf_pdf(model: int, material, N, ray_dir, L) -> float:
+    lib = load()
+    f = lambda v: np.ascontiguousarray(v, np.float32)  # noqa: E731
+    n, r, l = f(N), f(ray_dir), f(L)
+    return lib.ref_bsdf_pdf(model, ctypes.addressof(material), _p(n), _p(r), _p(l))
+
+
+def intersect_eps(depth: int) -> float:
+    return load().ref_intersect_eps(depth)
