@@ -83,7 +83,7 @@ RECORD_DTYPE = np.dtype(PathRecord)
 
 EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create", "ar_scene_destroy",
                     "ar_scene_get_info", "ar_render", "ar_trace_rays", "ar_trace_rays_static",
-                    "ar_render_debug_paths", "ar_rng_tape")
+                    "ar_render_debug_paths", "ar_rng_tape", "ar_tonemap")
 
 
 class ArError(RuntimeError):
@@ -123,6 +123,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_render_debug_paths.restype = c_int32
     lib.ar_rng_tape.argtypes = [POINTER(Camera), POINTER(RenderParams), c_int32, c_void_p, c_int32, c_void_p]
     lib.ar_rng_tape.restype = c_int32
+    lib.ar_tonemap.argtypes = [c_void_p, c_size_t, c_int32, c_float, c_int32, c_void_p, c_int32, c_void_p]
+    lib.ar_tonemap.restype = c_int32
     _lib = lib
     return lib
 
@@ -239,4 +241,16 @@ def rng_tape(camera: Camera, params: RenderParams, per_path: int) -> np.ndarray:
     n = camera.width * camera.height * params.spp
     out = np.empty((n, per_path), np.float32)
     _check(_lib.ar_rng_tape(ctypes.byref(camera), ctypes.byref(params), int(per_path), _ptr(out), MEM_HOST, None))
+    return out
+
+
+TONE_NONE, TONE_GAMMA, TONE_ACES = 0, 1, 2
+
+
+def tonemap(rgb: np.ndarray, tone: int = TONE_ACES, exposure: float = 1.0, xyz_input: bool = False) -> np.ndarray:
+    """Linear rgb[n, 3] (host) -> 0xAARRGGBB per pixel, the reference's LDR format."""
+    lib = load_library()
+    rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)
+    out = np.empty(len(rgb), np.uint32)
+    _check(lib.ar_tonemap(_ptr(rgb), len(rgb), tone, exposure, int(xyz_input), _ptr(out), MEM_HOST, None))
     return out

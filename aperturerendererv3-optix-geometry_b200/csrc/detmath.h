@@ -40,6 +40,7 @@ AR_HD f3 operator-(f3 a) { return mk(-a.x, -a.y, -a.z); }
 AR_HD f3 operator*(f3 a, f3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
 AR_HD f3 operator*(f3 a, float b) { return mk(a.x * b, a.y * b, a.z * b); }
 AR_HD f3 operator/(f3 a, float b) { return mk(a.x / b, a.y / b, a.z / b); }
+AR_HD f3 operator/(f3 a, f3 b) { return mk(a.x / b.x, a.y / b.y, a.z / b.z); }
 AR_HD float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 AR_HD f3 cross(f3 a, f3 b) { return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
 AR_HD float length(f3 a) { return sqrtf(dot(a, a)); }

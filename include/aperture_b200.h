@@ -218,6 +218,17 @@ ar_status ar_render_debug_paths(ar_scene* scene, const ar_camera* camera,
 ar_status ar_rng_tape(const ar_camera* camera, const ar_render_params* params, int32_t per_path,
                       float* out, int32_t mem_kind, void* stream);
 
+/* Output epilogue of the reference's Tonemap kernel (core/scene.cu:180-199,
+ * curves of core/tonemap.cuh): for each of n pixels, linear RGB (or CIE XYZ
+ * when xyz_input != 0, converted by XYZ2SRGBLinearD65) times exposure, then
+ * tone_type 0 = none, 1 = gamma 1/2.2, 2 = ACES; saturated and packed as
+ * 0xAARRGGBB (alpha 0xff) -- the reference's ldrTarget format.  rgb holds 3*n
+ * floats; mem_kind says where both buffers live.  The offline path
+ * (Camera::RenderToFile, core/camera.cu:64-89) applies the same curves on the
+ * host before SaveBMP. */
+ar_status ar_tonemap(const float* rgb, size_t n, int32_t tone_type, float exposure, int32_t xyz_input,
+                     uint32_t* bgra, int32_t mem_kind, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1654,3 +1654,80 @@ float or_bsdf_pdf(int model, const ar_material* m, const float* N, const float* 
 }
 
 float or_power_heuristic(float a, float b) { return power_heuristic(a, b); }
+
+/* ------------------------------------------------------------------------ */
+/* Output epilogue: Tonemap kernel (scene.cu:180-199), curves of tonemap.cuh  */
+/* ------------------------------------------------------------------------ */
+static M3 rows3(V3 a, V3 b, V3 c) { M3 m; m.x = a; m.y = b; m.z = c; return m; }
+static V3 vmax0(V3 a) { return v3(fmaxf(0.0f, a.x), fmaxf(0.0f, a.y), fmaxf(0.0f, a.z)); }
+
+/* Gamma (tonemap.cuh:6-9) */
+static V3 tone_gamma(V3 c)
+{
+    const float e = 1.0f / 2.2f;
+    return v3(om_powf(c.x, e), om_powf(c.y, e), om_powf(c.z, e));
+}
+
+/* XYZ2SRGBLinearD65 (tonemap.cuh:119-130) */
+static V3 xyz_to_srgb(V3 xyz)
+{
+    const M3 m = rows3(v3(3.2406f, -1.5372f, -0.4986f), v3(-0.9689f, 1.8758f, 0.0415f), v3(0.0557f, -0.204f, 1.057f));
+    return vmax0(mmul(&m, xyz));
+}
+
+/* ACES (tonemap.cuh:11-117) */
+static V3 tone_aces(V3 col)
+{
+    const M3 ap1_xyz = rows3(v3(0.6624541811f, 0.1340042065f, 0.1561876870f), v3(0.2722287168f, 0.6740817658f, 0.0536895174f),
+                             v3(-0.0055746495f, 0.0040607335f, 1.0103391003f));
+    const M3 srgb_ap0 = rows3(v3(0.4397010f, 0.3829780f, 0.1773350f), v3(0.0897923f, 0.8134230f, 0.0967616f),
+                              v3(0.0175440f, 0.1115440f, 0.8707040f));
+    const M3 ap0_ap1 = rows3(v3(1.4514393161f, -0.2365107469f, -0.2149285693f), v3(-0.0765537734f, 1.1762296998f, -0.0996759264f),
+                             v3(0.0083161484f, -0.0060324498f, 0.9977163014f));
+    const M3 xyz_ap1 = rows3(v3(1.6410233797f, -0.3248032942f, -0.2364246952f), v3(-0.6636628587f, 1.6153315917f, 0.0167563477f),
+                             v3(0.0117218943f, -0.0082844420f, 0.9883948585f));
+    const M3 d60_d65 = rows3(v3(0.98722400f, -0.00611327f, 0.0159533f), v3(-0.00759836f, 1.00186000f, 0.0053302f),
+                             v3(0.00307257f, -0.00509595f, 1.0816800f));
+    const M3 xyz_709 = rows3(v3(3.2409699419f, -1.5373831776f, -0.4986107603f), v3(-0.9692436363f, 1.8759675015f, 0.0415550574f),
+                             v3(0.0556300797f, -0.2039769589f, 1.0569715142f));
+    const V3 y_of = v3(0.272229f, 0.674082f, 0.0536895f);
+    const V3 ap0 = mmul(&srgb_ap0, col);
+    V3 cg = mmul(&ap0_ap1, ap0);
+    float y = dot3(cg, y_of);
+    cg = vlerp(v3(y, y, y), cg, 0.96f);
+    const float a = 278.5085f, b = 10.7772f, c = 293.6045f, d = 88.7122f, e = 80.6889f;
+    V3 post;
+    post.x = (cg.x * (cg.x * a + b)) / (cg.x * (cg.x * c + d) + e);
+    post.y = (cg.y * (cg.y * a + b)) / (cg.y * (cg.y * c + d) + e);
+    post.z = (cg.z * (cg.z * a + b)) / (cg.z * (cg.z * c + d) + e);
+    V3 xyz = mmul(&ap1_xyz, post);
+    const float dv = fmaxf(dot3(xyz, v3(1.0f, 1.0f, 1.0f)), 1.0e-4f);
+    V3 xyY = v3(xyz.x / dv, xyz.y / dv, xyz.y);
+    xyY.z = fminf(fmaxf(xyY.z, 0.0f), 65504.0f);
+    xyY.z = om_powf(xyY.z, 0.9811f);
+    const float m = xyY.z / fmaxf(xyY.y, 1e-4f);
+    xyz = v3(xyY.x, xyY.z, (1.0f - xyY.x - xyY.y));
+    xyz.x *= m;
+    xyz.z *= m;
+    V3 cv = mmul(&xyz_ap1, xyz);
+    y = dot3(cv, y_of);
+    cv = vlerp(v3(y, y, y), cv, 0.93f);
+    const V3 x1 = mmul(&ap1_xyz, cv);
+    const V3 x2 = mmul(&d60_d65, x1);
+    return tone_gamma(vmax0(mmul(&xyz_709, x2)));
+}
+
+static float sat_(float v) { return (v != v) ? 0.0f : fminf(fmaxf(v, 0.0f), 1.0f); }
+
+void or_tonemap(const float* rgb, int64_t n, int tone, float exposure, int xyz_input, uint32_t* out)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        V3 v = v3(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2]);
+        if (xyz_input) v = xyz_to_srgb(v);
+        v = vscale(v, exposure);
+        if (tone == 1) v = tone_gamma(v);
+        else if (tone == 2) v = tone_aces(v);
+        const uint32_t r = (uint32_t)(255.0f * sat_(v.x)), g = (uint32_t)(255.0f * sat_(v.y)), b = (uint32_t)(255.0f * sat_(v.z));
+        out[i] = 0xff000000u | (r << 16) | (g << 8) | b;
+    }
+}

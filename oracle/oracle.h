@@ -115,6 +115,9 @@ float or_bsdf_pdf(int model, const ar_material* m, const float* N, const float* 
 /* PowerHeuristic (render.cuh:185-196). */
 float or_power_heuristic(float a, float b);
 
+/* Tonemap kernel (scene.cu:180-199): n pixels of RGB (or XYZ) -> 0xAARRGGBB. */
+void or_tonemap(const float* rgb, int64_t n, int tone, float exposure, int xyz_input, uint32_t* out);
+
 float or_sinf(float x);
 float or_cosf(float x);
 float or_expf(float x);

@@ -62,6 +62,7 @@ def load():
     lib.or_collect_rays.restype = c_int64
     lib.or_powf.argtypes = [c_float, c_float]
     lib.or_powf.restype = c_float
+    lib.or_tonemap.argtypes = [c_void_p, c_int64, c_int, c_float, c_int, c_void_p]
     lib.or_trace_detail.argtypes = [c_void_p, c_void_p, c_int64, c_int] + [c_void_p] * 5 + [c_int]
     lib.or_segments_occluded.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p, c_int]
     lib.or_overlap.argtypes = [c_void_p, c_void_p, c_int64, c_void_p]
@@ -209,3 +210,11 @@ def bsdf_pdf(model: int, material, N, ray_dir, L) -> float:
 
 def power_heuristic(a: float, b: float) -> float:
     return load().or_power_heuristic(a, b)
+
+
+def tonemap(rgb: np.ndarray, tone: int, exposure: float = 1.0, xyz_input: bool = False) -> np.ndarray:
+    """The Tonemap kernel's output (0xAARRGGBB per pixel) for linear rgb[n, 3]."""
+    rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)
+    out = np.empty(len(rgb), np.uint32)
+    load().or_tonemap(_p(rgb), len(rgb), tone, exposure, int(xyz_input), _p(out))
+    return out

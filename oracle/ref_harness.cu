@@ -14,8 +14,9 @@
 //   intersection::Intersect (linear scan)     core/render/intersection.cuh:175-205
 //   intersection::Overlap                     core/render/intersection.cuh:399-414
 //   BSDF_PDF (RGB)                            core/render/material.cuh:332-387
-//   PowerHeuristic                            core/render/render.cuh:185-196 (restated
-//       below: render.cuh does not compile in the RGB configuration)
+//   Gamma, ACES, XYZ2SRGBLinearD65            core/tonemap.cuh (the per-pixel steps of
+//       the Tonemap kernel around them, core/scene.cu:180-199, are repeated below:
+//       scene.cu itself needs OptiX and the GUI)
 // The light table follows UpdateSceneToDeviceIfDirty (core/scene.cu:1046-1080):
 // this file repeats its loop because scene.cu itself needs OptiX and the GUI.
 #include <cstdint>
@@ -24,6 +25,7 @@
 #include "bvh/bvh.cuh"
 #include "render/intersection.cuh"
 #include "render/material.cuh"
+#include "tonemap.cuh"
 
 #include "../include/aperture_b200.h"
 
@@ -215,6 +217,23 @@ float ref_bsdf_pdf(int model, const ar_material* m, const float* N, const float*
     const GBuffer g = material_of(*m).texture_.baseTexture_;
     return BSDF_PDF(static_cast<EShadingModel>(model), g, make_float3(0.0f, 0.0f, 0.0f), make_float3(N[0], N[1], N[2]),
                     make_float3(ray_dir[0], ray_dir[1], ray_dir[2]), make_float3(L[0], L[1], L[2]));
+}
+
+// The default branch of the Tonemap kernel (core/scene.cu:180-199) per pixel;
+// exposure is the kernel's __device__ `exposure` (SetExposure).
+void ref_tonemap(const float* rgb, int64_t n, int tone, float exposure, int xyz_input, uint32_t* out)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        const float3 in = make_float3(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2]);
+        const float3 result = xyz_input ? XYZ2SRGBLinearD65(in) : in;
+        float3 value = result * exposure;
+        if (tone == 1) value = Gamma(value);
+        else if (tone == 2) value = ACES(value);
+        const unsigned int red = static_cast<unsigned int>(255.0f * saturate_(value.x));
+        const unsigned int green = static_cast<unsigned int>(255.0f * saturate_(value.y));
+        const unsigned int blue = static_cast<unsigned int>(255.0f * saturate_(value.z));
+        out[i] = 0xff000000u | (red << 16) | (green << 8) | blue;
+    }
 }
 
 // INTERSECT_EPS (config.cuh:3) as the reference's host pass evaluates it.

@@ -46,6 +46,7 @@ def load():
     lib.ref_overlap.argtypes = [c_void_p, c_void_p, c_int64, c_void_p]
     lib.ref_bsdf_pdf.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p]
     lib.ref_bsdf_pdf.restype = c_float
+    lib.ref_tonemap.argtypes = [c_void_p, c_int64, c_int, c_float, c_int, c_void_p]
     lib.ref_intersect_eps.argtypes = [c_int]
     lib.ref_intersect_eps.restype = c_float
     _lib = lib
@@ -127,3 +128,10 @@ def bsdf_pdf(model: int, material, N, ray_dir, L) -> float:
 
 def intersect_eps(depth: int) -> float:
     return load().ref_intersect_eps(depth)
+
+
+def tonemap(rgb: np.ndarray, tone: int, exposure: float = 1.0, xyz_input: bool = False) -> np.ndarray:
+    rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)
+    out = np.empty(len(rgb), np.uint32)
+    load().ref_tonemap(_p(rgb), len(rgb), tone, exposure, int(xyz_input), _p(out))
+    return out

@@ -7,7 +7,8 @@ on the host here: SceneObject construction and BuildBVH (core/bvh/bvh.cuh),
 the light table of UpdateSceneToDeviceIfDirty (core/scene.cu:1046-1080),
 TraverseBVH closest and any hit (core/render/intersection.cuh:235-370),
 AnyHitSegmentBVH (372-397), Overlap (399-414), BSDF_PDF (RGB,
-core/render/material.cuh:332-387) and INTERSECT_EPS (core/config.cuh:3).
+core/render/material.cuh:332-387), INTERSECT_EPS (core/config.cuh:3) and the
+Tonemap kernel's curves (core/tonemap.cuh) at exposure 1.7.
 
 Scenes: config 1 (scenes.box_scene()) and a small sphere field
 (scenes.spheres_scene(n_spheres=24, n_lights=4, box=20, subdivisions=1):
@@ -109,6 +110,14 @@ def main():
         m.ior, m.sigma_a = 1.5, 1.0
         pdf[i] = reference.bsdf_pdf(int(model[i]), m, dirs[i, 0], dirs[i, 1], dirs[i, 2])
     out.update({"bsdf_model": model, "bsdf_albedo": albedo, "bsdf_smr": spec, "bsdf_dirs": dirs, "bsdf_pdf": pdf})
+
+    # Tonemap kernel (core/scene.cu:180-199) with Gamma / ACES / XYZ2SRGBLinearD65
+    hdr = np.exp(rng.normal(-1.0, 2.0, (4000, 3))).astype(np.float32)
+    hdr[:100] = 0.0
+    out["tonemap_hdr"] = hdr
+    for tone in (0, 1, 2):
+        for xyz in (0, 1):
+            out[f"tonemap_t{tone}_x{xyz}"] = reference.tonemap(hdr, tone, 1.7, bool(xyz))
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT} ({os.path.getsize(OUT)} bytes)")
 

@@ -2,7 +2,7 @@
 
 tests/golden/reference_queries.npz holds outputs of the reference's
 BuildBVH, light table, TraverseBVH (closest and any hit), AnyHitSegmentBVH,
-Overlap, BSDF_PDF and INTERSECT_EPS, compiled from the reference's headers and
+Overlap, BSDF_PDF, INTERSECT_EPS and tone curves, compiled from the reference's headers and
 run on the host (tests/golden/make_reference_fixtures.py).  The oracle must
 reproduce them:
 
@@ -166,3 +166,18 @@ def test_live_against_reference_build(scene_objs):
     seg = rng.uniform(-23, 23, (20_000, 6)).astype(np.float32)
     dep = rng.integers(0, 12, len(seg)).astype(np.int32)
     assert np.array_equal(rs.segments_occluded(seg, dep), osc.segments_occluded(seg, dep, mode=REF_MODE))
+
+
+@pytest.mark.parametrize("tone", [0, 1, 2])
+@pytest.mark.parametrize("xyz", [0, 1])
+def test_tonemap_matches_reference(fx, tone, xyz):
+    """The Tonemap kernel's packed 0xAARRGGBB output: identical except where
+    the fixed powf and the host powf round differently across a 1/255 step
+    (at most 1 LSB, on a few pixels in 10^4)."""
+    got = oracle.tonemap(fx["tonemap_hdr"], tone, 1.7, bool(xyz))
+    ref = fx[f"tonemap_t{tone}_x{xyz}"]
+    diff = got != ref
+    assert diff.mean() <= 5e-4
+    for shift in (24, 16, 8, 0):
+        d = ((got >> shift) & 255).astype(np.int32) - ((ref >> shift) & 255).astype(np.int32)
+        assert np.abs(d).max() <= 1
