@@ -83,7 +83,7 @@ RECORD_DTYPE = np.dtype(PathRecord)
 
 EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create", "ar_scene_destroy",
                     "ar_scene_get_info", "ar_render", "ar_trace_rays", "ar_trace_rays_static",
-                    "ar_render_debug_paths", "ar_rng_tape", "ar_tonemap")
+                    "ar_render_debug_paths", "ar_rng_tape", "ar_tonemap", "ar_accum_resolve", "ar_tone_curve")
 
 
 class ArError(RuntimeError):
@@ -125,6 +125,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_rng_tape.restype = c_int32
     lib.ar_tonemap.argtypes = [c_void_p, c_size_t, c_int32, c_float, c_int32, c_void_p, c_int32, c_void_p]
     lib.ar_tonemap.restype = c_int32
+    lib.ar_accum_resolve.argtypes = [c_void_p, c_size_t, c_double, c_void_p, c_int32, c_void_p]
+    lib.ar_accum_resolve.restype = c_int32
+    lib.ar_tone_curve.argtypes = [c_void_p, c_int32, c_void_p]
+    lib.ar_tone_curve.restype = c_int32
     _lib = lib
     return lib
 

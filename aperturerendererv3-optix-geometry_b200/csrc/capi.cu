@@ -492,6 +492,27 @@ ar_status ar_render(ar_scene* s, const ar_camera* cam, const ar_render_params* p
     AR_GUARD_END
 }
 
+ar_status ar_accum_resolve(const double* accum, size_t n, double scale, float* out, int32_t mem_kind, void* stream)
+{
+    g_last_error.clear();
+    if (n == 0) return AR_OK;
+    if (!accum || !out) return fail(AR_ERR_INVALID_ARGUMENT, "accum/out is NULL");
+    if (mem_kind == AR_MEM_HOST) {
+        for (size_t i = 0; i < n; ++i) out[i] = static_cast<float>(accum[i] * scale);
+        return AR_OK;
+    }
+    if (mem_kind != AR_MEM_DEVICE) return fail(AR_ERR_INVALID_ARGUMENT, "bad mem_kind");
+    AR_GUARD_BEGIN
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(AR_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    ck(ar::launch_mean(accum, static_cast<int64_t>(n), scale, out, static_cast<cudaStream_t>(stream)), "resolve");
+    return AR_OK;
+    AR_GUARD_END
+}
+
 ar_status ar_trace_rays(ar_scene* s, const float* rays, size_t n, int32_t any_hit, int32_t* hit_object, float* hit_t,
                         int32_t mem_kind, void* stream)
 {

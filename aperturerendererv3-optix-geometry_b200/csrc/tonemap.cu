@@ -86,3 +86,17 @@ extern "C" ar_status ar_tonemap(const float* rgb, size_t n, int32_t tone_type, f
     }
     return AR_OK;
 }
+
+extern "C" ar_status ar_tone_curve(const float* rgb3, int32_t tone_type, float* out3)
+{
+    using namespace ar;
+    if (!rgb3 || !out3) return set_error(AR_ERR_INVALID_ARGUMENT, "rgb3/out3 is NULL");
+    if (tone_type < 0 || tone_type > 2) return set_error(AR_ERR_INVALID_ARGUMENT, "tone_type must be 0, 1 or 2");
+    f3 v = mk(rgb3[0], rgb3[1], rgb3[2]);
+    if (tone_type == 1) v = tone_gamma(v);
+    else if (tone_type == 2) v = tone_aces(v);
+    out3[0] = v.x;
+    out3[1] = v.y;
+    out3[2] = v.z;
+    return AR_OK;
+}

@@ -218,6 +218,14 @@ ar_status ar_render_debug_paths(ar_scene* scene, const ar_camera* camera,
 ar_status ar_rng_tape(const ar_camera* camera, const ar_render_params* params, int32_t per_path,
                       float* out, int32_t mem_kind, void* stream);
 
+/* Running-mean resolve for progressive rendering: out[i] = (float)(accum[i] *
+ * scale) for n values (scale = 1 / samples so far).  With ar_render's FP64
+ * accum this replaces the reference's per-frame FP32 running mean of the
+ * interactive SceneRenderer::Render (target = lerp(target, result,
+ * 1/(1+frameIndex)), core/scene.cu:241-242).  mem_kind: where both live. */
+ar_status ar_accum_resolve(const double* accum, size_t n, double scale, float* out, int32_t mem_kind,
+                           void* stream);
+
 /* Output epilogue of the reference's Tonemap kernel (core/scene.cu:180-199,
  * curves of core/tonemap.cuh): for each of n pixels, linear RGB (or CIE XYZ
  * when xyz_input != 0, converted by XYZ2SRGBLinearD65) times exposure, then
@@ -228,6 +236,12 @@ ar_status ar_rng_tape(const ar_camera* camera, const ar_render_params* params, i
  * host before SaveBMP. */
 ar_status ar_tonemap(const float* rgb, size_t n, int32_t tone_type, float exposure, int32_t xyz_input,
                      uint32_t* bgra, int32_t mem_kind, void* stream);
+
+/* The tone curve of ar_tonemap for one pixel, on the host, before
+ * quantisation: out3 = Gamma(rgb3) (tone_type 1), ACES(rgb3) (2) or rgb3 (0)
+ * (core/tonemap.cuh:6-117).  No device is needed.  Used by the C++ shim's
+ * Gamma / ACES functions (include/aperture_b200_renderer.hpp). */
+ar_status ar_tone_curve(const float* rgb3, int32_t tone_type, float* out3);
 
 #ifdef __cplusplus
 }
