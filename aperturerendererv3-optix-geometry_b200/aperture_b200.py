@@ -42,9 +42,39 @@ class Vertex(ctypes.Structure):
     _fields_ = [("position", Vec3), ("normal", Vec3), ("u", c_float), ("v", c_float)]
 
 
+class SdfParams(ctypes.Structure):
+    _fields_ = [("info", c_float * 4), ("kind", c_int32), ("volume", c_int32)]
+
+
 class ObjectDesc(ctypes.Structure):
+    """ar_object_desc; `tri` (triangles) and `sdf` (SDF objects) share storage."""
     _fields_ = [("type", c_int32), ("center", Vec3), ("extent", Vec3), ("rotation_deg", Vec3),
                 ("material", Material), ("tri", Vertex * 3), ("visible", c_int32), ("reserved", c_int32 * 3)]
+
+
+class SdfVolume(ctypes.Structure):
+    _fields_ = [("dims", c_int32 * 3), ("precision", c_int32), ("data", c_void_p), ("fill_kind", c_int32),
+                ("fill_info", c_float * 4), ("reserved", c_int32)]
+
+
+SDF_TORUS, SDF_VOLUME = 0, 1
+SDF_OFFSET = ObjectDesc.tri.offset   # ar_object_desc.sdf overlays tri[0]
+
+
+def set_sdf(obj, kind: int, info=(0.0, 0.0, 0.0, 0.0), volume: int = 0) -> None:
+    """Fill the sdf member of one ar_object_desc record (numpy structured scalar
+    or array element view) -- it shares storage with tri[0]."""
+    raw = obj.view(np.uint8) if isinstance(obj, np.ndarray) else None
+    assert raw is not None, "pass a 1-element OBJECT_DTYPE array view"
+    p = SdfParams()
+    p.info[:] = [float(x) for x in info]
+    p.kind, p.volume = kind, volume
+    raw[SDF_OFFSET:SDF_OFFSET + ctypes.sizeof(SdfParams)] = np.frombuffer(bytes(p), np.uint8)
+
+
+def get_sdf(obj) -> SdfParams:
+    raw = obj.view(np.uint8)
+    return SdfParams.from_buffer_copy(raw[SDF_OFFSET:SDF_OFFSET + ctypes.sizeof(SdfParams)].tobytes())
 
 
 class Camera(ctypes.Structure):
@@ -81,7 +111,8 @@ assert ctypes.sizeof(PathRecord) == 96
 OBJECT_DTYPE = np.dtype(ObjectDesc)
 RECORD_DTYPE = np.dtype(PathRecord)
 
-EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create", "ar_scene_destroy",
+EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create", "ar_scene_create_ex",
+                    "ar_scene_destroy",
                     "ar_scene_get_info", "ar_render", "ar_trace_rays", "ar_trace_rays_static",
                     "ar_render_debug_paths", "ar_rng_tape", "ar_tonemap", "ar_accum_resolve", "ar_tone_curve")
 
@@ -107,6 +138,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_get_last_error_string.restype = c_char_p
     lib.ar_scene_create.argtypes = [c_void_p, c_size_t, c_int32, POINTER(c_void_p)]
     lib.ar_scene_create.restype = c_int32
+    lib.ar_scene_create_ex.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int32, POINTER(c_void_p)]
+    lib.ar_scene_create_ex.restype = c_int32
     lib.ar_scene_destroy.argtypes = [c_void_p]
     lib.ar_scene_destroy.restype = None
     lib.ar_scene_get_info.argtypes = [c_void_p, POINTER(SceneInfo)]
@@ -157,12 +190,19 @@ def make_params(spp=1, max_depth=8, rr_depth=3, use_nee=1, sky=1, frame_offset=0
 class Scene:
     """Owns one ar_scene handle (the SceneRenderer of the reference)."""
 
-    def __init__(self, objects: np.ndarray, device: int = 0):
+    def __init__(self, objects: np.ndarray, device: int = 0, volumes=None):
+        """volumes: list of (SdfVolume, keep-alive array or None) from make_volume()."""
         lib = load_library()
         objects = np.ascontiguousarray(objects, dtype=OBJECT_DTYPE)
         self._objects_keepalive = objects
         h = c_void_p()
-        _check(lib.ar_scene_create(_ptr(objects) if len(objects) else None, len(objects), device, ctypes.byref(h)))
+        if volumes:
+            arr = (SdfVolume * len(volumes))(*[v for v, _ in volumes])
+            _check(lib.ar_scene_create_ex(_ptr(objects) if len(objects) else None, len(objects), arr, len(volumes),
+                                          device, ctypes.byref(h)))
+        else:
+            _check(lib.ar_scene_create(_ptr(objects) if len(objects) else None, len(objects), device,
+                                       ctypes.byref(h)))
         self._h = h
         self.num_objects = len(objects)
 
@@ -258,3 +298,20 @@ def tonemap(rgb: np.ndarray, tone: int = TONE_ACES, exposure: float = 1.0, xyz_i
     out = np.empty(len(rgb), np.uint32)
     _check(lib.ar_tonemap(_ptr(rgb), len(rgb), tone, exposure, int(xyz_input), _ptr(out), MEM_HOST, None))
     return out
+
+
+def make_volume(dims, data: np.ndarray | None = None, precision: int = 32, fill_kind: int = SDF_TORUS,
+                fill_info=(0.375, 0.125, 0.0, 0.0)):
+    """An ar_sdf_volume: host data (float32 or float16 array of dims[2]*dims[1]*dims[0]
+    values, x fastest) or, without data, filled on the device from fill_kind."""
+    v = SdfVolume()
+    v.dims[:] = [int(d) for d in dims]
+    v.precision = precision
+    keep = None
+    if data is not None:
+        keep = np.ascontiguousarray(data, np.float16 if precision == 16 else np.float32).reshape(-1)
+        assert keep.size == int(np.prod(dims))
+        v.data = keep.ctypes.data
+    v.fill_kind = fill_kind
+    v.fill_info[:] = [float(x) for x in fill_info]
+    return v, keep

@@ -16,6 +16,7 @@
 #include "../../include/aperture_b200.h"
 #include "render_kernels.h"
 #include "scene_build.h"
+#include "sdf.cuh"
 #include "xorwow_jump.h"
 
 namespace {
@@ -93,6 +94,8 @@ struct ar_scene {
     // host copy for the camera overlap test (intersection::Overlap)
     std::vector<ar::ObjInfo> h_objects;
     std::vector<ar::Analytic> h_analytic;
+    std::vector<ar::SdfRec> h_sdf;              // data pointers into h_volumes
+    std::vector<ar::HostVolume> h_volumes;
     // render workspace
     char* ws = nullptr;
     size_t ws_bytes = 0;
@@ -171,6 +174,11 @@ bool camera_inside(const ar_scene* s, ar::f3 p)
     using namespace ar;
     for (size_t i = 0; i < s->h_objects.size(); ++i) {
         const ObjInfo& oi = s->h_objects[i];
+        if (oi.type == AR_OBJ_SDF) {
+            const SdfRec& g = s->h_sdf[oi.aux];
+            if (sdf_contains(g, s->h_analytic[g.analytic], p)) return true;
+            continue;
+        }
         if (oi.type != AR_OBJ_CUBE && oi.type != AR_OBJ_SPHERE) continue;
         const Analytic& an = s->h_analytic[oi.aux];
         m3 w2o;
@@ -379,6 +387,12 @@ const char* ar_get_last_error_string(void) { return g_last_error.c_str(); }
 
 ar_status ar_scene_create(const ar_object_desc* objects, size_t count, int32_t device, ar_scene** out_scene)
 {
+    return ar_scene_create_ex(objects, count, nullptr, 0, device, out_scene);
+}
+
+ar_status ar_scene_create_ex(const ar_object_desc* objects, size_t count, const ar_sdf_volume* volumes,
+                             size_t volume_count, int32_t device, ar_scene** out_scene)
+{
     g_last_error.clear();
     if (!out_scene) return fail(AR_ERR_INVALID_ARGUMENT, "out_scene is NULL");
     *out_scene = nullptr;
@@ -390,7 +404,8 @@ ar_status ar_scene_create(const ar_object_desc* objects, size_t count, int32_t d
         return fail(AR_ERR_NO_DEVICE, "no CUDA device available");
     }
     if (device < 0 || device >= ndev) return fail(AR_ERR_INVALID_ARGUMENT, "device index out of range");
-    ar::HostScene hs = ar::build_scene(objects, count);
+    if (volume_count > 0 && !volumes) return fail(AR_ERR_INVALID_ARGUMENT, "volumes is NULL");
+    ar::HostScene hs = ar::build_scene(objects, count, volumes, volume_count);
     DeviceGuard g(device);
     ar_scene* s = new ar_scene();
     s->device = device;
@@ -409,6 +424,25 @@ ar_status ar_scene_create(const ar_object_desc* objects, size_t count, int32_t d
         {
             static const std::vector<uint32_t> jt = ar::xorwow_jump_table_2p32();
             s->jump_table = static_cast<const uint32_t*>(own(upload(jt, "rng jump table"), jt.size() * 4));
+        }
+        {
+            // SDF volumes, then the SDF records pointing at them (device and host copies)
+            std::vector<const void*> vdev(hs.volumes.size());
+            for (size_t k = 0; k < hs.volumes.size(); ++k) {
+                const std::vector<unsigned char>& b = hs.volumes[k].bytes;
+                vdev[k] = own(upload(b, "sdf volume"), b.size());
+            }
+            std::vector<ar::SdfRec> dsdf = hs.sdf;
+            s->h_volumes = std::move(hs.volumes);
+            s->h_sdf = hs.sdf;
+            for (size_t k = 0; k < dsdf.size(); ++k) {
+                if (dsdf[k].kind != ar::kSdfVolume) continue;
+                const size_t vi = static_cast<size_t>(dsdf[k].pad[0]);
+                dsdf[k].data = vdev[vi];
+                s->h_sdf[k].data = s->h_volumes[vi].bytes.data();
+            }
+            v.sdf = static_cast<const ar::SdfRec*>(own(upload(dsdf, "sdf"), dsdf.size() * sizeof(ar::SdfRec)));
+            v.num_sdf = static_cast<int32_t>(dsdf.size());
         }
         v.num_nodes = static_cast<int32_t>(hs.prims.empty() ? 0 : hs.nodes.size());
         v.num_objects = static_cast<int32_t>(hs.objects.size());

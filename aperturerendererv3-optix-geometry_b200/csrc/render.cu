@@ -70,25 +70,33 @@ __device__ __forceinline__ PathRec* pool_of(const PathBuffers& B, int c) { retur
 __device__ __forceinline__ float fbits(int i) { return __int_as_float(i); }
 
 // ------------------------------------------------------------------ ray queries
+template <bool kSdf>
 struct RaysIO {
     const float4* rays;
     int32_t* out_obj;
     float* out_t;
+    int any;
     __device__ __forceinline__ int load(const SceneView&, int k, RayState& r)
     {
         const float4 a = rays[2 * static_cast<int64_t>(k)], b = rays[2 * static_cast<int64_t>(k) + 1];
         ray_begin(r, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w);
         return k;
     }
-    __device__ __forceinline__ void store(const SceneView&, int k, const RayState& r)
+    __device__ __forceinline__ void store(const SceneView& s, int k, const RayState& r)
     {
-        out_obj[k] = r.best.obj;
-        if (out_t) out_t[k] = r.best.t;
+        int32_t obj = r.best.obj;
+        float t = r.best.t;
+        if (kSdf && s.num_sdf > 0) {  // standalone queries use the depth-0 tolerance
+            if (!any) sdf_closest(s, r.o, r.d, r.tmin, kEpsDepth0, &t, &obj);
+            else if (obj < 0) obj = sdf_any(s, r.o, r.d, r.tmin, t, kEpsDepth0);
+        }
+        out_obj[k] = obj;
+        if (out_t) out_t[k] = t;
     }
 };
 
-template <bool kAny>
-__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_trace_rays(SceneView s, RaysIO io, int n, PoolCtl* ctl,
+template <bool kAny, bool kSdf>
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_trace_rays(SceneView s, RaysIO<kSdf> io, int n, PoolCtl* ctl,
                                                             uint32_t* ovf, int* err)
 {
     extern __shared__ uint32_t smem[];
@@ -231,6 +239,7 @@ __global__ void k_regen(FrameParams fp, PathBuffers B, PoolCtl* ctl, int cur, ui
 }
 
 // ------------------------------------------------------------------ extend
+template <bool kSdf>
 struct ExtendIO {
     const PathRec* pool;
     int4* hit;
@@ -252,7 +261,8 @@ struct ExtendIO {
             const int mobj = static_cast<int>(pool[k].rng1.z);
             if (mobj >= 0 && s.objects[mobj].type != AR_OBJ_TRIANGLE) {
                 // solo trace of the medium's object (render.cuh:91-94, intersection.cuh:185-193)
-                const float t = isect_analytic_t(s, mobj, o, d);
+                const float t = (kSdf && s.objects[mobj].type == AR_OBJ_SDF) ? sdf_solo_t(s, mobj, o, d, e)
+                                                                             : isect_analytic_t(s, mobj, o, d);
                 const bool h = t >= 0.0f && !(t < e);
                 hit[k] = h ? make_int4(mobj, -1, ibits(t), 0) : make_int4(-1, -1, 0, 0);
                 to_shade(s, k, h ? mobj : -1);
@@ -264,17 +274,25 @@ struct ExtendIO {
     }
     __device__ __forceinline__ void store(const SceneView& s, int k, const RayState& r)
     {
-        hit[k] = r.best.obj >= 0 ? make_int4(r.best.obj, r.best.prim, ibits(r.best.t), 0) : make_int4(-1, -1, 0, 0);
-        to_shade(s, k, r.best.obj);
+        int32_t obj = r.best.obj, prim = r.best.prim;
+        float t = r.best.t;
+        if (kSdf && s.num_sdf > 0) {
+            const int32_t before = obj;
+            sdf_closest(s, r.o, r.d, r.tmin, c_eps_tab[min(ibits(pool[k].o.w) >> 16, 8)], &t, &obj);
+            if (obj != before) prim = -1;
+        }
+        hit[k] = obj >= 0 ? make_int4(obj, prim, ibits(t), 0) : make_int4(-1, -1, 0, 0);
+        to_shade(s, k, obj);
     }
 };
 
 // Trace's closest-hit query (render.cuh:86-99) for every path of the pool.
+template <bool kSdf>
 __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(SceneView s, PathBuffers B, int cur, PoolCtl* ctl,
                                                         unsigned long long* stats, uint32_t* ovf, int* err)
 {
     extern __shared__ uint32_t smem[];
-    ExtendIO io;
+    ExtendIO<kSdf> io;
     io.pool = pool_of(B, cur);
     io.hit = B.hit;
     io.shade_count = ctl->shade_count;
@@ -290,7 +308,7 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(SceneVi
 // the shadow query: Trace's material evaluation and hit offset, emission with
 // MIS, light sampling for NEE, throughput and Russian roulette.  kModel is the
 // shading model of every path of this launch's bucket, -1 = miss.
-template <int kModel>
+template <int kModel, bool kSdf>
 __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams fp, PathBuffers B, int cur,
                                                        PoolCtl* ctl, ar_path_record* rec)
 {
@@ -353,6 +371,8 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                 nrm = dot(crd, ni) > 0.0f ? -ni : ni;
             } else if (oi.type == AR_OBJ_CUBE) {
                 isect_cube<true>(s.analytic[oi.aux], cro, crd, &pos, &nrm);
+            } else if (kSdf && oi.type == AR_OBJ_SDF) {
+                sdf_surface_of(s, oi.aux, cro, crd, fbits(hr.z), eps, &pos, &nrm);
             } else {
                 isect_sphere<true>(s.analytic[oi.aux], cro, crd, &pos, &nrm);
             }
@@ -552,6 +572,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
 // SegmentTrace -> AnyHitSegmentBVH (render.cuh:167-183, intersection.cuh:372-397)
 // and the remainder of NEE (render.cuh:242-343): the pending term is added when
 // the segment is unoccluded, and previousDidNEE_ becomes "occluded or cos > 0".
+template <bool kSdf>
 struct ShadowIO {
     const ShadowRec* rec;
     PathRec* next_pool;
@@ -599,15 +620,21 @@ struct ShadowIO {
         finish(m, false);
         return -1;
     }
-    __device__ __forceinline__ void store(const SceneView&, int m, const RayState& r) { finish(m, r.best.obj >= 0); }
+    __device__ __forceinline__ void store(const SceneView& s, int m, const RayState& r)
+    {
+        bool occ = r.best.obj >= 0;
+        if (kSdf && !occ && s.num_sdf > 0) occ = sdf_any(s, r.o, r.d, 0.0f, r.best.t, rec[m].src.w) >= 0;
+        finish(m, occ);
+    }
 };
 
+template <bool kSdf>
 __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks - 1) k_shadow(SceneView s, PathBuffers B, int cur, PoolCtl* ctl,
                                                         unsigned long long* stats, uint32_t* ovf, int* err)
 {
     extern __shared__ uint32_t smem[];
     const int n = ctl->shadow_count;
-    ShadowIO io;
+    ShadowIO<kSdf> io;
     io.rec = B.shadow;
     io.next_pool = pool_of(B, 1 - cur);
     io.retire = B.retire;
@@ -670,10 +697,10 @@ int trace_grid(int sm_count)
     static int blocks = 0;
     if (blocks == 0) {
         int b0 = 1, b1 = 1, b2 = 1, b3 = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend, kTraceBlock, kTraceSmem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow, kTraceBlock, kTraceSmem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_trace_rays<false>, kTraceBlock, kTraceSmem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_trace_rays<true>, kTraceBlock, kTraceSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend<false>, kTraceBlock, kTraceSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow<false>, kTraceBlock, kTraceSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_trace_rays<false, false>, kTraceBlock, kTraceSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_trace_rays<true, false>, kTraceBlock, kTraceSmem);
         cudaGetLastError();
         blocks = max(1, max(max(b0, b1), max(b2, b3)));
     }
@@ -683,12 +710,23 @@ int trace_grid(int sm_count)
 cudaError_t launch_trace_rays(const SceneView& s, const float4* rays, int n, int any, int32_t* obj, float* t,
                               PoolCtl* ctl, uint32_t* ovf, int* err, int grid, cudaStream_t st)
 {
-    RaysIO io;
-    io.rays = rays;
-    io.out_obj = obj;
-    io.out_t = t;
-    if (any) k_trace_rays<true><<<grid, kTraceBlock, kTraceSmem, st>>>(s, io, n, ctl, ovf, err);
-    else k_trace_rays<false><<<grid, kTraceBlock, kTraceSmem, st>>>(s, io, n, ctl, ovf, err);
+    if (s.num_sdf > 0) {
+        RaysIO<true> io;
+        io.rays = rays;
+        io.out_obj = obj;
+        io.out_t = t;
+        io.any = any ? 1 : 0;
+        if (any) k_trace_rays<true, true><<<grid, kTraceBlock, kTraceSmem, st>>>(s, io, n, ctl, ovf, err);
+        else k_trace_rays<false, true><<<grid, kTraceBlock, kTraceSmem, st>>>(s, io, n, ctl, ovf, err);
+    } else {
+        RaysIO<false> io;
+        io.rays = rays;
+        io.out_obj = obj;
+        io.out_t = t;
+        io.any = any ? 1 : 0;
+        if (any) k_trace_rays<true, false><<<grid, kTraceBlock, kTraceSmem, st>>>(s, io, n, ctl, ovf, err);
+        else k_trace_rays<false, false><<<grid, kTraceBlock, kTraceSmem, st>>>(s, io, n, ctl, ovf, err);
+    }
     return cudaGetLastError();
 }
 
@@ -721,16 +759,26 @@ cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const P
         k_regen<<<grid_other, kShadeBlock, 0, st>>>(fp, B, ctl, c, b0, b1, jump_table, rec);
         const bool te = tm && tm->n_extend < tm->cap;
         if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend], st);
-        k_extend<<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
+        if (s.num_sdf > 0) k_extend<true><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
+        else k_extend<false><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
         if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend++ + 1], st);
-        k_shade<-1><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-        k_shade<AR_MAT_DIFFUSE><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-        k_shade<AR_MAT_LIGHT><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-        k_shade<AR_MAT_GLASS><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-        k_shade<AR_MAT_GGX><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+        if (s.num_sdf > 0) {
+            k_shade<-1, true><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+            k_shade<AR_MAT_DIFFUSE, true><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+            k_shade<AR_MAT_LIGHT, true><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+            k_shade<AR_MAT_GLASS, true><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+            k_shade<AR_MAT_GGX, true><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+        } else {
+            k_shade<-1, false><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+            k_shade<AR_MAT_DIFFUSE, false><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+            k_shade<AR_MAT_LIGHT, false><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+            k_shade<AR_MAT_GLASS, false><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+            k_shade<AR_MAT_GGX, false><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+        }
         const bool ts = tm && tm->n_shadow < tm->cap;
         if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow], st);
-        k_shadow<<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
+        if (s.num_sdf > 0) k_shadow<true><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
+        else k_shadow<false><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
         if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow++ + 1], st);
         k_retire<<<grid_other, kShadeBlock, 0, st>>>(fp, B, ctl, accum, rec);
         *launches += 10;

@@ -14,6 +14,8 @@
 // one grid step so the decoded box always contains the exact one.
 #include "scene_build.h"
 
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -21,6 +23,8 @@
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
+
+#include "sdf.cuh"
 
 namespace ar {
 
@@ -206,11 +210,51 @@ void euler_matrices(f3 deg, m3* o2w, m3* w2o)
     w2o->z = mk(o2w->x.z, o2w->y.z, o2w->z.z);
 }
 
-HostScene build_scene(const ar_object_desc* objs, size_t n)
+// Volumes as they will be uploaded: the caller's values (float or half), or
+// the torus fill of FillSDFVolume computed here, on the host, so that the
+// camera-inside test can read the same grid.
+void ingest_volumes(HostScene& hs, const ar_sdf_volume* vols, size_t nv)
+{
+    if (nv > 0 && vols == nullptr) throw std::invalid_argument("volumes is NULL");
+    for (size_t v = 0; v < nv; ++v) {
+        const ar_sdf_volume& sv = vols[v];
+        const std::string tag = "volume " + std::to_string(v) + ": ";
+        if (sv.dims[0] < 1 || sv.dims[1] < 1 || sv.dims[2] < 1 || sv.dims[0] > 4096 || sv.dims[1] > 4096 ||
+            sv.dims[2] > 4096)
+            throw std::invalid_argument(tag + "dims must be in 1..4096");
+        if (sv.precision != 32 && sv.precision != 16) throw std::invalid_argument(tag + "precision must be 32 or 16");
+        const size_t count = static_cast<size_t>(sv.dims[0]) * sv.dims[1] * sv.dims[2];
+        if (count > (size_t(1) << 31)) throw std::invalid_argument(tag + "more than 2^31 values");
+        HostVolume hv;
+        for (int k = 0; k < 3; ++k) hv.dims[k] = sv.dims[k];
+        hv.fp16 = sv.precision == 16;
+        hv.voxel_size_max = voxel_size_max(hv.dims);
+        hv.bytes.resize(count * (hv.fp16 ? 2 : 4));
+        if (sv.data) {
+            std::memcpy(hv.bytes.data(), sv.data, hv.bytes.size());
+        } else {
+            if (sv.fill_kind != AR_SDF_TORUS) throw std::invalid_argument(tag + "unknown fill_kind");
+            float* f = reinterpret_cast<float*>(hv.bytes.data());
+            __half* h = reinterpret_cast<__half*>(hv.bytes.data());
+            size_t i = 0;
+            for (int z = 0; z < hv.dims[2]; ++z)
+                for (int y = 0; y < hv.dims[1]; ++y)
+                    for (int x = 0; x < hv.dims[0]; ++x, ++i) {
+                        const float d = torus_fill_value(x, y, z, hv.dims, sv.fill_info[0], sv.fill_info[1]);
+                        if (hv.fp16) h[i] = __float2half_rn(d);
+                        else f[i] = d;
+                    }
+        }
+        hs.volumes.push_back(std::move(hv));
+    }
+}
+
+HostScene build_scene(const ar_object_desc* objs, size_t n, const ar_sdf_volume* vols, size_t nv)
 {
     if (n > 0 && objs == nullptr) throw std::invalid_argument("objects is NULL");
     if (n >= (1u << 30)) throw std::invalid_argument("too many objects");
     HostScene hs;
+    ingest_volumes(hs, vols, nv);
     hs.objects.resize(n);
     std::unordered_map<std::string, int32_t> matIndex;
     std::vector<Bounds> pbounds;
@@ -224,8 +268,14 @@ HostScene build_scene(const ar_object_desc* objs, size_t n)
         const ar_object_desc& d = objs[i];
         if (d.type < AR_OBJ_CUBE || d.type > AR_OBJ_TRIANGLE)
             throw std::invalid_argument("object " + std::to_string(i) + ": invalid type");
-        if (d.type == AR_OBJ_SDF)
-            throw std::domain_error("object " + std::to_string(i) + ": SDF objects are not supported");
+        if (d.type == AR_OBJ_SDF) {
+            if (d.sdf.kind != AR_SDF_TORUS && d.sdf.kind != AR_SDF_VOLUME)
+                throw std::invalid_argument("object " + std::to_string(i) + ": invalid sdf.kind");
+            if (d.sdf.kind == AR_SDF_VOLUME && (d.sdf.volume < 0 || static_cast<size_t>(d.sdf.volume) >= nv))
+                throw std::invalid_argument("object " + std::to_string(i) + ": sdf.volume out of range");
+            if (!(d.extent.x != 0.0f && d.extent.y != 0.0f && d.extent.z != 0.0f))
+                throw std::invalid_argument("object " + std::to_string(i) + ": SDF box extent must be non-zero");
+        }
         if (d.material.shading_model < AR_MAT_DIFFUSE || d.material.shading_model > AR_MAT_GGX)
             throw std::invalid_argument("object " + std::to_string(i) + ": invalid shading model");
         if (!finite3(d.center) || !finite3(d.extent) || !finite3(d.rotation_deg))
@@ -305,7 +355,25 @@ HostScene build_scene(const ar_object_desc* objs, size_t n)
             for (int k = 0; k < 9; ++k) { an.o2w[k] = mo[k]; an.w2o[k] = mw[k]; }
             oi.aux = static_cast<int32_t>(hs.analytic.size());
             hs.analytic.push_back(an);
-            if (d.type == AR_OBJ_CUBE) {
+            if (d.type == AR_OBJ_SDF) {
+                SdfRec sr;
+                std::memset(&sr, 0, sizeof(sr));
+                sr.object = static_cast<int32_t>(i);
+                sr.analytic = oi.aux;
+                sr.kind = d.sdf.kind == AR_SDF_TORUS ? kSdfTorus : kSdfVolume;
+                for (int k = 0; k < 4; ++k) sr.info[k] = d.sdf.info[k];
+                if (sr.kind == kSdfVolume) {
+                    const HostVolume& hv = hs.volumes[static_cast<size_t>(d.sdf.volume)];
+                    for (int k = 0; k < 3; ++k) sr.dims[k] = hv.dims[k];
+                    sr.fp16 = hv.fp16 ? 1 : 0;
+                    sr.voxel_size_max = hv.voxel_size_max;
+                    sr.pad[0] = d.sdf.volume;   // resolved to a device pointer at upload
+                }
+                oi.aux = static_cast<int32_t>(hs.sdf.size());
+                hs.sdf.push_back(sr);
+                // SceneObject::GetArea of OBJ_SDF is the box's (object.cuh:278-285); not a BVH primitive
+                area = 8.0f * (extent.x * extent.y + extent.x * extent.z + extent.y * extent.z);
+            } else if (d.type == AR_OBJ_CUBE) {
                 // UpdateProxy (object.cuh:312-323) then a relative pad for rounding
                 const f3 axx = mul(o2w, mk(1, 0, 0)), ayy = mul(o2w, mk(0, 1, 0)), azz = mul(o2w, mk(0, 0, 1));
                 f3 h;
@@ -322,16 +390,18 @@ HostScene build_scene(const ar_object_desc* objs, size_t n)
                 const float rr = std::fabs(extent.x);
                 area = 4.0f * kPi * rr * rr;
             }
-            const float pad = 1e-5f * (max3(vabs(center)) + max3(extent)) + 1e-30f;
-            bb.lo = bb.lo - mk(pad, pad, pad);
-            bb.hi = bb.hi + mk(pad, pad, pad);
-            PrimRec pr;
-            std::memset(&pr, 0, sizeof(pr));
-            pr.object = static_cast<int32_t>(i);
-            pr.kind = kPrimAnalytic;
-            pbounds.push_back(bb);
-            pcent.push_back(center);
-            precs.push_back(pr);
+            if (d.type != AR_OBJ_SDF) {  // SDF objects are tested after the BVH, not in it
+                const float pad = 1e-5f * (max3(vabs(center)) + max3(extent)) + 1e-30f;
+                bb.lo = bb.lo - mk(pad, pad, pad);
+                bb.hi = bb.hi + mk(pad, pad, pad);
+                PrimRec pr;
+                std::memset(&pr, 0, sizeof(pr));
+                pr.object = static_cast<int32_t>(i);
+                pr.kind = kPrimAnalytic;
+                pbounds.push_back(bb);
+                pcent.push_back(center);
+                precs.push_back(pr);
+            }
         }
         if (d.material.shading_model == AR_MAT_LIGHT) {
             // scene.cu:1060-1076

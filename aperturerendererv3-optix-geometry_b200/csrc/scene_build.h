@@ -11,6 +11,14 @@
 
 namespace ar {
 
+// A signed-distance volume as uploaded: float or half values, x fastest.
+struct HostVolume {
+    int dims[3] = {0, 0, 0};
+    bool fp16 = false;
+    std::vector<unsigned char> bytes;
+    float voxel_size_max = 0.0f;
+};
+
 struct HostScene {
     std::vector<ObjInfo> objects;
     std::vector<TriShade> trishade;
@@ -18,6 +26,8 @@ struct HostScene {
     std::vector<MaterialRec> materials;
     std::vector<PrimRec> prims;
     std::vector<WideNode> nodes;
+    std::vector<SdfRec> sdf;           // data pointers index `volumes` until upload
+    std::vector<HostVolume> volumes;
     std::vector<int32_t> light_object;
     std::vector<float> light_prob;
     int64_t triangles = 0;
@@ -30,7 +40,8 @@ struct HostScene {
 // scene: world-space triangles, light table (scene.cu:1056-1080), SAH BVH
 // collapsed to 8-wide quantised nodes.  Throws std::runtime_error on invalid
 // input.
-HostScene build_scene(const ar_object_desc* objects, size_t count);
+HostScene build_scene(const ar_object_desc* objects, size_t count, const ar_sdf_volume* volumes = nullptr,
+                      size_t volume_count = 0);
 
 // objectToWorld = Rz * (Ry * Rx) from Euler degrees with host libm, exactly as
 // the SceneObject constructor (object.cuh:344-364, vector.cuh:378-416).

@@ -8,7 +8,8 @@
 //                               analytic object
 //   ObjInfo   objects[]   16 B  per reference SceneObject: type, material, light, aux
 //   TriShade  trishade[]  48 B  world vertex normals of triangle objects (shading)
-//   Analytic  analytic[] 112 B  cube / sphere transform records
+//   Analytic  analytic[] 112 B  cube / sphere / SDF transform records
+//   SdfRec    sdf[]       64 B  SDF objects (tested after the BVH), volume grids
 //   MaterialRec materials[] 48 B  de-duplicated materials
 //   lights: object index + selection probability, in object order
 #pragma once
@@ -63,6 +64,24 @@ struct alignas(16) Analytic {
     float pad1[2];
 };
 static_assert(sizeof(Analytic) == 112, "Analytic must be 112 bytes");
+
+// Signed-distance object (SDF torus or sampled volume).  SDF objects are not
+// BVH primitives: every query tests them after its BVH traversal (there are a
+// few per scene, each behind its own box test).
+enum : int32_t { kSdfTorus = 0, kSdfVolume = 1 };
+
+struct alignas(16) SdfRec {
+    int32_t object;         // scene object index
+    int32_t analytic;       // centre, extent and matrices in analytic[]
+    int32_t kind;           // kSdfTorus / kSdfVolume
+    int32_t fp16;           // volume values stored as half floats
+    float info[4];          // SDFInfo::sdfInfo0_
+    int32_t dims[3];        // volume grid
+    float voxel_size_max;   // SDFVolumeInfo::voxelSizeMax_
+    const void* data;       // volume values (device), x fastest
+    int32_t pad[2];
+};
+static_assert(sizeof(SdfRec) == 64, "SdfRec must be 64 bytes");
 
 struct alignas(16) MaterialRec {
     int32_t model;

@@ -42,25 +42,33 @@ constexpr int kStaticMaxBlocks =
 
 static __device__ __align__(256) unsigned char g_trace_scratch[kStaticScratchBytes];
 
+template <bool kSdf>
 struct StaticRaysIO {
     const float4* rays;
     int32_t* out_obj;
     float* out_t;
+    int any;
     __device__ __forceinline__ int load(const SceneView&, int k, RayState& r)
     {
         const float4 a = rays[2 * static_cast<int64_t>(k)], b = rays[2 * static_cast<int64_t>(k) + 1];
         ray_begin(r, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w);
         return k;
     }
-    __device__ __forceinline__ void store(const SceneView&, int k, const RayState& r)
+    __device__ __forceinline__ void store(const SceneView& s, int k, const RayState& r)
     {
-        out_obj[k] = r.best.obj;
-        if (out_t) out_t[k] = r.best.t;
+        int32_t obj = r.best.obj;
+        float t = r.best.t;
+        if (kSdf && s.num_sdf > 0) {
+            if (!any) sdf_closest(s, r.o, r.d, r.tmin, kEpsDepth0, &t, &obj);
+            else if (obj < 0) obj = sdf_any(s, r.o, r.d, r.tmin, t, kEpsDepth0);
+        }
+        out_obj[k] = obj;
+        if (out_t) out_t[k] = t;
     }
 };
 
-template <bool kAny>
-__global__ void __launch_bounds__(kTraceBlock) k_trace_rays_static(SceneView s, StaticRaysIO io, int n,
+template <bool kAny, bool kSdf>
+__global__ void __launch_bounds__(kTraceBlock) k_trace_rays_static(SceneView s, StaticRaysIO<kSdf> io, int n,
                                                                    unsigned char* scratch)
 {
     extern __shared__ uint32_t smem[];
@@ -121,8 +129,8 @@ extern "C" ar_status ar_trace_rays_static(const ar_scene* scene, const float* ra
             }
             const size_t smem = static_cast<size_t>(kStackShared) * kTraceBlock * 4;
             int b0 = 1, b1 = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_trace_rays_static<false>, kTraceBlock, smem);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_trace_rays_static<true>, kTraceBlock, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_trace_rays_static<false, false>, kTraceBlock, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_trace_rays_static<true, false>, kTraceBlock, smem);
             cudaGetLastError();
             g_blocks_of_device[device] = std::max(1, std::min(std::min(b0, b1) * sms, kStaticMaxBlocks));
             g_scratch_of_device[device] = static_cast<unsigned char*>(p);
@@ -133,13 +141,24 @@ extern "C" ar_status ar_trace_rays_static(const ar_scene* scene, const float* ra
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaMemsetAsync(scratch, 0, kStaticHeaderBytes, st);  // work counter and error word
     if (e == cudaSuccess) {
-        StaticRaysIO io;
-        io.rays = reinterpret_cast<const float4*>(rays);
-        io.out_obj = hit_object;
-        io.out_t = hit_t;
         const size_t smem = static_cast<size_t>(kStackShared) * kTraceBlock * 4;
-        if (any_hit) k_trace_rays_static<true><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
-        else k_trace_rays_static<false><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
+        if (view.num_sdf > 0) {
+            StaticRaysIO<true> io;
+            io.rays = reinterpret_cast<const float4*>(rays);
+            io.out_obj = hit_object;
+            io.out_t = hit_t;
+            io.any = any_hit ? 1 : 0;
+            if (any_hit) k_trace_rays_static<true, true><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
+            else k_trace_rays_static<false, true><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
+        } else {
+            StaticRaysIO<false> io;
+            io.rays = reinterpret_cast<const float4*>(rays);
+            io.out_obj = hit_object;
+            io.out_t = hit_t;
+            io.any = any_hit ? 1 : 0;
+            if (any_hit) k_trace_rays_static<true, false><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
+            else k_trace_rays_static<false, false><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
+        }
         e = cudaGetLastError();
     }
     int err_word = 0;

@@ -16,7 +16,9 @@
 #include <cstdint>
 
 #include "detmath.h"
+#include "../../include/aperture_b200.h"
 #include "scene_types.h"
+#include "sdf.cuh"
 
 namespace ar {
 
@@ -29,10 +31,11 @@ struct SceneView {
     const MaterialRec* materials;
     const int32_t* light_object;
     const float* light_prob;
+    const SdfRec* sdf;       // SDF objects, tested after the BVH
     int32_t num_nodes;
     int32_t num_objects;
     int32_t num_lights;
-    int32_t pad;
+    int32_t num_sdf;
 };
 
 constexpr float kSlabWiden = 1.000001f;
@@ -138,6 +141,54 @@ __device__ __forceinline__ float isect_analytic_t(const SceneView& s, int obj, f
     if (oi.type == 0) return isect_cube<false>(an, ro, rd, &p, &n);
     if (oi.type == 1) return isect_sphere<false>(an, ro, rd, &p, &n);
     return -1.0f;
+}
+
+// INTERSECT_EPS(0) = 1e-3 * exp(0) (config.cuh:3): the tolerance of standalone ray queries.
+constexpr float kEpsDepth0 = 1.0e-3f;
+
+// SDF objects are not in the BVH: each query tests them after its traversal
+// with the same acceptance rule as a leaf (tmin <= t < best; an equal
+// distance goes to the lower object index).  eps is INTERSECT_EPS(depth) of
+// the query, which sets the sphere-tracing tolerance.  Out of line: the
+// marching loop stays out of the traversal kernels' register budget.
+static __device__ __noinline__ void sdf_closest(const SceneView& s, f3 o, f3 d, float tmin, float eps, float* best_t,
+                                         int32_t* best_obj)
+{
+    for (int k = 0; k < s.num_sdf; ++k) {
+        const SdfRec g = s.sdf[k];
+        const float t = sdf_march(g, s.analytic[g.analytic], o, d, eps);
+        if (t < 0.0f || t < tmin) continue;
+        if (t < *best_t || (t == *best_t && *best_obj >= 0 && g.object < *best_obj)) {
+            *best_t = t;
+            *best_obj = g.object;
+        }
+    }
+}
+
+// Any SDF object hit in [tmin, tmax): its object index, else -1.
+static __device__ __noinline__ int32_t sdf_any(const SceneView& s, f3 o, f3 d, float tmin, float tmax, float eps)
+{
+    for (int k = 0; k < s.num_sdf; ++k) {
+        const SdfRec g = s.sdf[k];
+        const float t = sdf_march(g, s.analytic[g.analytic], o, d, eps);
+        if (t >= 0.0f && !(t < tmin) && t < tmax) return g.object;
+    }
+    return -1;
+}
+
+// Hit position and normal on an SDF object (out of line, for the shading kernels).
+static __device__ __noinline__ void sdf_surface_of(const SceneView& s, int aux, f3 ro, f3 rd, float t, float eps,
+                                                   f3* pos, f3* nrm)
+{
+    const SdfRec g = s.sdf[aux];
+    sdf_surface(g, s.analytic[g.analytic], ro, rd, t, eps, pos, nrm);
+}
+
+// Solo trace of an SDF object (the medium a path is inside).
+static __device__ __noinline__ float sdf_solo_t(const SceneView& s, int obj, f3 ro, f3 rd, float eps)
+{
+    const SdfRec g = s.sdf[s.objects[obj].aux];
+    return sdf_march(g, s.analytic[g.analytic], ro, rd, eps);
 }
 
 struct Hit {

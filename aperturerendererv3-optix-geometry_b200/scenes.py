@@ -10,13 +10,15 @@ Generators use numpy's PCG64 with seed 0xA11CE + config number.
   box_scene     -- config 1: unit box, 2 seeded cubes, ceiling light, 256^2.
   spheres_scene -- config 2: 800 icospheres x 1280 triangles (+ ground quad,
                    16 emissive spheres), 1920x1080.
+  sdf_box_scene -- config 1 plus two signed-distance tori (object/sdf): an
+                   analytic one and one sampled on a grid (float or half).
 """
 from __future__ import annotations
 
 import numpy as np
 
-from aperture_b200 import (MAT_DIFFUSE, MAT_GGX, MAT_GLASS, MAT_LIGHT, OBJ_CUBE, OBJ_SPHERE, OBJ_TRIANGLE,
-                           OBJECT_DTYPE, make_camera)
+from aperture_b200 import (MAT_DIFFUSE, MAT_GGX, MAT_GLASS, MAT_LIGHT, OBJ_CUBE, OBJ_SDF, OBJ_SPHERE, OBJ_TRIANGLE,
+                           OBJECT_DTYPE, SDF_TORUS, SDF_VOLUME, make_camera, make_volume, set_sdf)
 
 SEED_BASE = 0xA11CE
 THICK = 0.01  # SceneHelper::THICK (scene_helper.h:14)
@@ -251,3 +253,32 @@ def spheres_scene(seed: int = SEED_BASE + 2, n_spheres: int = 800, subdivisions:
 def spheres_camera(width=1920, height=1080, fov=60.0):
     d = np.array([0.0, -40.0, 150.0])
     return make_camera((0.0, 30.0, -150.0), d / np.linalg.norm(d), fov, width, height)
+
+
+def sdf_object(center, extent, rotation=(0.0, 0.0, 0.0), kind: int = SDF_TORUS, info=(0.375, 0.125, 0.0, 0.0),
+               volume: int = 0) -> np.ndarray:
+    """One OBJ_SDF object: the box [-extent, extent] around centre holds the
+    unit-box signed distance (AdditionalObjectInfo / SDFInfo of the reference)."""
+    a = _empty(1)
+    a["type"] = OBJ_SDF
+    _set3(a["center"], np.asarray([center], np.float32))
+    _set3(a["extent"], np.asarray([extent], np.float32))
+    _set3(a["rotation_deg"], np.asarray([rotation], np.float32))
+    set_sdf(a[0:1], kind, info, volume)
+    return a
+
+
+def sdf_box_scene(seed: int = SEED_BASE + 3, precision: int = 32, grid: int = 64):
+    """The config-1 box with a glass analytic torus and a GGX torus sampled on
+    a grid^3 volume (FillSDFVolume of the torus functor), both rotated.
+    Returns (objects, volumes) for Scene(objects, volumes=volumes)."""
+    rng = np.random.default_rng(seed)
+    base = box_scene()
+    tor = sdf_object((0.18, -0.3, 0.12), (0.16, 0.16, 0.16), (20.0, float(rng.uniform(-40, 40)), 0.0), SDF_TORUS,
+                     (0.3, 0.12, 0.0, 0.0))
+    glass(tor, (0.95, 0.95, 0.95), 1.5, 0.5)
+    vol = sdf_object((-0.2, -0.25, -0.05), (0.2, 0.15, 0.2), (0.0, float(rng.uniform(-40, 40)), -15.0), SDF_VOLUME,
+                     (0.0, 0.0, 0.0, 0.0), 0)
+    ggx(vol, (0.9, 0.6, 0.3), 0.3, 1.0, 0.5)
+    volumes = [make_volume((grid, grid, grid), None, precision, SDF_TORUS, (0.32, 0.14, 0.0, 0.0))]
+    return np.concatenate([base, tor, vol]), volumes

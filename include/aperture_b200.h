@@ -59,6 +59,9 @@ typedef struct ar_material {
     float tilt_number;
 } ar_material;             /* 56 bytes */
 
+/* ESDFType (core/render/object.cuh:37-43) of an AR_OBJ_SDF object. */
+enum { AR_SDF_TORUS = 0, AR_SDF_VOLUME = 1 };
+
 /* Vertex (core/render/object.cuh:233-238), object space. */
 typedef struct ar_vertex { ar_vec3 position; ar_vec3 normal; float u, v; } ar_vertex; /* 32 B */
 
@@ -69,13 +72,38 @@ typedef struct ar_vertex { ar_vec3 position; ar_vec3 normal; float u, v; } ar_ve
 typedef struct ar_object_desc {
     int32_t type;          /* AR_OBJ_*                                              */
     ar_vec3 center;
-    ar_vec3 extent;        /* cube half-size; sphere radius = max component         */
+    ar_vec3 extent;        /* cube / SDF box half-size; sphere radius = max component */
     ar_vec3 rotation_deg;  /* Euler (x, y, z) in degrees                            */
     ar_material material;
-    ar_vertex tri[3];      /* AR_OBJ_TRIANGLE only, object space                    */
+    union {
+        ar_vertex tri[3];  /* AR_OBJ_TRIANGLE: object-space vertices                */
+        struct {           /* AR_OBJ_SDF (AdditionalObjectInfo, object.cuh:219-229) */
+            float info[4]; /* SDFInfo::sdfInfo0_: torus (R, r) in the unit box      */
+            int32_t kind;  /* AR_SDF_TORUS or AR_SDF_VOLUME                         */
+            int32_t volume;/* AR_SDF_VOLUME: index into the scene's volume list     */
+        } sdf;
+    };
     int32_t visible;       /* 0 = skipped by intersection (SceneObject::bVisible_)  */
     int32_t reserved[3];
 } ar_object_desc;          /* 208 bytes */
+
+/* A sampled signed-distance volume (SDFVolumeInfo, object/sdf/sdf_volume.cuh:14-45),
+ * the grid of an AR_SDF_VOLUME object: dims[0]*dims[1]*dims[2] distances in
+ * the unit box [0,1]^3 of the object (x fastest, Index3D), in the object's
+ * unit-box distance units.  Either `data` (host memory, precision 32 = float,
+ * 16 = IEEE half) or, when data is NULL, filled on the device from an analytic
+ * function like SDFCacheManager::AddVolume / FillSDFVolume
+ * (object/sdf/sdf_cache_manager.cuh:16-104): fill_kind AR_SDF_TORUS with
+ * fill_info (R, r).  Samples are nearest or trilinear as SampleSDFAdaptive01.
+ * precision 16 stores the grid as half floats (half the bytes per tap). */
+typedef struct ar_sdf_volume {
+    int32_t dims[3];
+    int32_t precision;     /* 32 or 16                                              */
+    const void* data;      /* host values, or NULL to fill from fill_kind           */
+    int32_t fill_kind;     /* AR_SDF_TORUS                                          */
+    float fill_info[4];
+    int32_t reserved;
+} ar_sdf_volume;           /* 48 bytes */
 
 /* Pinhole camera of RenderCamera (core/scene.cu:201-230) with the field of view
  * as a parameter instead of the hard-coded 60 degrees. */
@@ -158,6 +186,11 @@ const char* ar_get_last_error_string(void);
  * defers to the first Render, UpdateSceneToDeviceIfDirty (core/scene.cu:1025-1118). */
 ar_status ar_scene_create(const ar_object_desc* objects, size_t count, int32_t device,
                           ar_scene** out_scene);
+
+/* ar_scene_create with the signed-distance volumes its AR_SDF_VOLUME objects
+ * refer to (the reference's SDFCacheManager entries, indexed in order). */
+ar_status ar_scene_create_ex(const ar_object_desc* objects, size_t count, const ar_sdf_volume* volumes,
+                             size_t volume_count, int32_t device, ar_scene** out_scene);
 
 /* Release every device allocation of the scene (SceneRenderer::~SceneRenderer,
  * core/scene.cu:1158-1163).  NULL is accepted. */

@@ -120,6 +120,11 @@ typedef struct {
     V3 p0, p1, p2;        /* world-space triangle vertices */
     V3 n0, n1, n2;        /* objectToWorld * vertex normal */
     V3 bmin, bmax, pc;    /* PrimitiveProxy */
+    int sdf_kind;         /* AR_SDF_* of AR_OBJ_SDF objects */
+    float sdf_info[4];    /* SDFInfo::sdfInfo0_ */
+    const float* vol;     /* AR_SDF_VOLUME: grid values (x fastest) */
+    int dims[3];
+    float vmax;           /* SDFVolumeInfo::voxelSizeMax_ */
 } OObj;
 
 typedef struct { V3 bmin, bmax; int left, right, first, count; } ONode;
@@ -127,6 +132,8 @@ typedef struct { V3 bmin, bmax; int left, right, first, count; } ONode;
 struct or_scene {
     int n;
     OObj* o;
+    float** vols;          /* SDF volume grids (float copies) */
+    int nvol;
     ONode* nodes;
     int nn, cap;
     int* idx;
@@ -365,9 +372,94 @@ static int build_rec(BuildCtx* c, int start, int end)
     return ni;
 }
 
+static float sdf_torus(V3 u, float R, float r);
+
+/* float -> IEEE half, round to nearest even */
+static uint16_t float_to_half_rn(float f)
+{
+    uint32_t x;
+    memcpy(&x, &f, 4);
+    const uint16_t sign = (uint16_t)((x >> 16) & 0x8000u);
+    const uint32_t ax = x & 0x7FFFFFFFu;
+    if (ax >= 0x7F800000u) return (uint16_t)(sign | (ax > 0x7F800000u ? 0x7E00u : 0x7C00u));
+    if (ax >= 0x477FF000u) return (uint16_t)(sign | 0x7C00u);          /* rounds to infinity */
+    if (ax < 0x38800000u) {                                            /* half subnormal or zero */
+        if (ax < 0x33000000u) return sign;
+        const uint32_t e = ax >> 23;
+        const uint32_t m = (ax & 0x7FFFFFu) | 0x800000u;
+        const uint32_t shift = 126u - e;
+        uint32_t r = m >> shift;
+        const uint32_t rem = m & ((1u << shift) - 1u), half = 1u << (shift - 1u);
+        if (rem > half || (rem == half && (r & 1u))) ++r;
+        return (uint16_t)(sign | r);
+    }
+    uint32_t h = (ax >> 13) - (112u << 10);
+    const uint32_t rem = ax & 0x1FFFu;
+    if (rem > 0x1000u || (rem == 0x1000u && (h & 1u))) ++h;
+    return (uint16_t)(sign | h);
+}
+
+/* IEEE half -> float (exact) */
+static float half_to_float(uint16_t h)
+{
+    const uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+    const uint32_t ex = (h >> 10) & 0x1Fu, man = h & 0x3FFu;
+    uint32_t bits;
+    if (ex == 0) {
+        if (man == 0) bits = sign;
+        else {                       /* subnormal: renormalise */
+            int e = -1;
+            uint32_t m = man;
+            do { m <<= 1; ++e; } while (!(m & 0x400u));
+            bits = sign | ((uint32_t)(112 - e) << 23) | ((m & 0x3FFu) << 13);
+        }
+    } else if (ex == 31) {
+        bits = sign | 0x7F800000u | (man << 13);
+    } else {
+        bits = sign | ((ex + 112u) << 23) | (man << 13);
+    }
+    float f;
+    memcpy(&f, &bits, 4);
+    return f;
+}
+
+/* SDF volumes as float grids: the caller's values, or the torus fill of
+ * FillSDFVolume (object/sdf/sdf_cache_manager.cuh:16-38).  Half-precision
+ * volumes keep their half values (rounded once, as the device stores them). */
+static float* make_volume(const ar_sdf_volume* v)
+{
+    const size_t n = (size_t)v->dims[0] * v->dims[1] * v->dims[2];
+    float* g = (float*)malloc((n ? n : 1) * sizeof(float));
+    if (v->data) {
+        for (size_t i = 0; i < n; ++i)
+            g[i] = v->precision == 16 ? half_to_float(((const uint16_t*)v->data)[i]) : ((const float*)v->data)[i];
+        return g;
+    }
+    size_t i = 0;
+    for (int z = 0; z < v->dims[2]; ++z)
+        for (int y = 0; y < v->dims[1]; ++y)
+            for (int x = 0; x < v->dims[0]; ++x, ++i) {
+                const float nx = v->dims[0] > 1 ? (float)x / (float)(v->dims[0] - 1) : 0.0f;
+                const float ny = v->dims[1] > 1 ? (float)y / (float)(v->dims[1] - 1) : 0.0f;
+                const float nz = v->dims[2] > 1 ? (float)z / (float)(v->dims[2] - 1) : 0.0f;
+                const float d = sdf_torus(v3(nx - 0.5f, ny - 0.5f, nz - 0.5f), v->fill_info[0], v->fill_info[1]);
+                g[i] = v->precision == 16 ? half_to_float(float_to_half_rn(d)) : d;
+            }
+    return g;
+}
+
 or_scene* or_scene_create(const ar_object_desc* objects, size_t count, int flags, int leaf_size, int bin_count)
 {
+    return or_scene_create_ex(objects, count, NULL, 0, flags, leaf_size, bin_count);
+}
+
+or_scene* or_scene_create_ex(const ar_object_desc* objects, size_t count, const ar_sdf_volume* volumes, size_t nvol,
+                             int flags, int leaf_size, int bin_count)
+{
     or_scene* s = (or_scene*)calloc(1, sizeof(or_scene));
+    s->nvol = (int)nvol;
+    s->vols = (float**)calloc(nvol ? nvol : 1, sizeof(float*));
+    for (size_t v = 0; v < nvol; ++v) s->vols[v] = make_volume(&volumes[v]);
     s->n = (int)count;
     s->flags = flags;
     s->o = (OObj*)calloc(count ? count : 1, sizeof(OObj));
@@ -382,6 +474,19 @@ or_scene* or_scene_create(const ar_object_desc* objects, size_t count, int flags
         o->extent = vabs(from_ar(d->extent));
         o->mat = d->material;
         euler_to_matrix(from_ar(d->rotation_deg), &o->o2w, &o->w2o);
+        if (o->type == AR_OBJ_SDF) {
+            o->sdf_kind = d->sdf.kind;
+            for (int k = 0; k < 4; ++k) o->sdf_info[k] = d->sdf.info[k];
+            if (o->sdf_kind == AR_SDF_VOLUME && d->sdf.volume >= 0 && d->sdf.volume < s->nvol) {
+                const ar_sdf_volume* v = &volumes[d->sdf.volume];
+                o->vol = s->vols[d->sdf.volume];
+                for (int k = 0; k < 3; ++k) o->dims[k] = v->dims[k];
+                /* SDFVolumeInfo::ComputeVoxelSize (sdf_volume.cuh:24-44) */
+                const V3 inv = v3(1.0f / fmaxf((float)v->dims[0], 1.0f), 1.0f / fmaxf((float)v->dims[1], 1.0f),
+                                  1.0f / fmaxf((float)v->dims[2], 1.0f));
+                o->vmax = len3(inv) * 2.5f;
+            }
+        }
         if (o->type == AR_OBJ_TRIANGLE) {
             /* intersection.cuh:27-29 and 75-77 */
             o->p0 = vadd(mmul(&o->o2w, from_ar(d->tri[0].position)), o->center);
@@ -427,6 +532,8 @@ or_scene* or_scene_create(const ar_object_desc* objects, size_t count, int flags
 void or_scene_destroy(or_scene* s)
 {
     if (!s) return;
+    for (int v = 0; v < s->nvol; ++v) free(s->vols[v]);
+    free(s->vols);
     free(s->o); free(s->nodes); free(s->idx); free(s->lobj); free(s->lprob); free(s);
 }
 
@@ -568,25 +675,145 @@ static int isect_sphere(const OObj* o, V3 ro, V3 rd, Isect* out)
     return 1;
 }
 
+/* ------------------------------------------------------------------------ */
+/* SDF objects (object/sdf/ of the reference)                                 */
+/* ------------------------------------------------------------------------ */
+/* SdfTorus (sdf_torus.cuh:14-18) */
+static float sdf_torus(V3 u, float R, float r)
+{
+    const float qx = sqrtf(u.x * u.x + u.z * u.z) - R;
+    return sqrtf(qx * qx + u.y * u.y) - r;
+}
+static int clampi_(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+static size_t grid_index(const OObj* o, int x, int y, int z)
+{
+    return (size_t)z * o->dims[0] * o->dims[1] + (size_t)y * o->dims[0] + x;
+}
+/* SampleSDFNearest01 (sdf_volume.cuh:69-83) */
+static float grid_nearest(const OObj* o, V3 p)
+{
+    const V3 q = v3(p.x * (float)(o->dims[0] - 1), p.y * (float)(o->dims[1] - 1), p.z * (float)(o->dims[2] - 1));
+    const int x = clampi_((int)floorf(q.x + 0.5f), 0, o->dims[0] - 1);
+    const int y = clampi_((int)floorf(q.y + 0.5f), 0, o->dims[1] - 1);
+    const int z = clampi_((int)floorf(q.z + 0.5f), 0, o->dims[2] - 1);
+    return o->vol[grid_index(o, x, y, z)];
+}
+/* SampleSDFTrilinear01 (sdf_volume.cuh:85-124) */
+static float grid_trilinear(const OObj* o, V3 p)
+{
+    const V3 q = v3(p.x * (float)(o->dims[0] - 1), p.y * (float)(o->dims[1] - 1), p.z * (float)(o->dims[2] - 1));
+    int x0 = (int)floorf(q.x), y0 = (int)floorf(q.y), z0 = (int)floorf(q.z);
+    const int x1 = clampi_(x0 + 1, 0, o->dims[0] - 1);
+    const int y1 = clampi_(y0 + 1, 0, o->dims[1] - 1);
+    const int z1 = clampi_(z0 + 1, 0, o->dims[2] - 1);
+    x0 = clampi_(x0, 0, o->dims[0] - 1);
+    y0 = clampi_(y0, 0, o->dims[1] - 1);
+    z0 = clampi_(z0, 0, o->dims[2] - 1);
+    const float fx = fminf(fmaxf(q.x - (float)x0, 0.0f), 1.0f);
+    const float fy = fminf(fmaxf(q.y - (float)y0, 0.0f), 1.0f);
+    const float fz = fminf(fmaxf(q.z - (float)z0, 0.0f), 1.0f);
+    const float* v = o->vol;
+    const float c000 = v[grid_index(o, x0, y0, z0)], c100 = v[grid_index(o, x1, y0, z0)];
+    const float c010 = v[grid_index(o, x0, y1, z0)], c110 = v[grid_index(o, x1, y1, z0)];
+    const float c001 = v[grid_index(o, x0, y0, z1)], c101 = v[grid_index(o, x1, y0, z1)];
+    const float c011 = v[grid_index(o, x0, y1, z1)], c111 = v[grid_index(o, x1, y1, z1)];
+    const float c00 = c000 * (1.0f - fx) + c100 * fx;
+    const float c10 = c010 * (1.0f - fx) + c110 * fx;
+    const float c01 = c001 * (1.0f - fx) + c101 * fx;
+    const float c11 = c011 * (1.0f - fx) + c111 * fx;
+    const float c0 = c00 * (1.0f - fy) + c10 * fy;
+    const float c1 = c01 * (1.0f - fy) + c11 * fy;
+    return c0 * (1.0f - fz) + c1 * fz;
+}
+/* SDFTorusFunctor / SDFVolumeFunctor + SampleSDFAdaptive01 (sdf_volume.cuh:143-171) */
+static float sdf_eval(const OObj* o, V3 u)
+{
+    if (o->sdf_kind == AR_SDF_TORUS) return sdf_torus(u, o->sdf_info[0], o->sdf_info[1]);
+    if (!o->vol || o->dims[0] * o->dims[1] * o->dims[2] == 0) return 1.0e20f;
+    const V3 p = v3(u.x + 0.5f, u.y + 0.5f, u.z + 0.5f);
+    const float dn = grid_nearest(o, p);
+    return fabsf(dn) > o->vmax ? dn : grid_trilinear(o, p);
+}
+/* ToUnitSpace (sdf_base.cuh:12-21) */
+static V3 to_unit(V3 pl, V3 e)
+{
+    const float ex = fmaxf(e.x, 1e-8f), ey = fmaxf(e.y, 1e-8f), ez = fmaxf(e.z, 1e-8f);
+    return v3(pl.x / (2.0f * ex), pl.y / (2.0f * ey), pl.z / (2.0f * ez));
+}
+/* IntersectSDFObject + RaymarchLocal + sdfNormalUnit (sdf_base.cuh:40-163);
+ * eps_d = INTERSECT_EPS(depth), SDF_EPS = eps_d / 2 (config.cuh:73). */
+static int isect_sdf(const OObj* o, V3 ro, V3 rd, float eps_d, Isect* out)
+{
+    const V3 lo = mmul(&o->w2o, vsub(ro, o->center));
+    const V3 ld = vnormalize(mmul(&o->w2o, rd));
+    const V3 e = o->extent;
+    const V3 dv = v3(inv_safe(ld.x), inv_safe(ld.y), inv_safe(ld.z));
+    const V3 t1 = vmul(vsub(vneg(e), lo), dv);
+    const V3 t2 = vmul(vsub(e, lo), dv);
+    const V3 tmn = vmin3(t1, t2), tmx = vmax3(t1, t2);
+    const float tEnter = fmaxf(fmaxf(tmn.x, tmn.y), tmn.z);
+    const float tExit = fminf(fminf(tmx.x, tmx.y), tmx.z);
+    if (tEnter > tExit || tExit <= 0.0f) return 0;
+    const float eps = eps_d * 0.5f;
+    const float minStep = eps * 0.5f;
+    const int inside = sdf_eval(o, to_unit(lo, e)) <= 0.0f;
+    const float sMin = 2.0f * fminf(e.x, fminf(e.y, e.z));
+    float t = fmaxf(0.0f, tEnter);
+    float tHit = -1.0f;
+    V3 pHit = v3(0.0f, 0.0f, 0.0f);
+    for (int i = 0; i < 512; ++i) {
+        const float tLast = t;
+        const V3 pl = vadd(lo, vscale(ld, t));
+        const float dLocal = sdf_eval(o, to_unit(pl, e)) * sMin;
+        if (inside ? (dLocal > 0.0f && dLocal < eps) : (dLocal < 0.0f && -dLocal < eps)) {
+            tHit = tLast;
+            pHit = pl;
+            break;
+        }
+        const float adv = o->sdf_kind == AR_SDF_VOLUME ? fmaxf(fabsf(dLocal) * 0.9f, minStep) : fmaxf(fabsf(dLocal), minStep);
+        t += adv;
+        if (t > tExit) break;
+    }
+    if (tHit < 0.0f) return 0;
+    out->hit = 1;
+    out->dist = tHit;
+    if (out->obj != -2) {
+        const float h = eps / fmaxf(sMin, 1e-8f);
+        const V3 u = to_unit(pHit, e);
+        const float dx = sdf_eval(o, vadd(u, v3(h, 0.0f, 0.0f))) - sdf_eval(o, vsub(u, v3(h, 0.0f, 0.0f)));
+        const float dy = sdf_eval(o, vadd(u, v3(0.0f, h, 0.0f))) - sdf_eval(o, vsub(u, v3(0.0f, h, 0.0f)));
+        const float dz = sdf_eval(o, vadd(u, v3(0.0f, 0.0f, h))) - sdf_eval(o, vsub(u, v3(0.0f, 0.0f, h)));
+        const V3 nu = vnormalize(v3(dx, dy, dz));
+        const float ex = fmaxf(e.x, 1e-8f), ey = fmaxf(e.y, 1e-8f), ez = fmaxf(e.z, 1e-8f);
+        const V3 nl = vnormalize(v3(nu.x / (2.0f * ex), nu.y / (2.0f * ey), nu.z / (2.0f * ez)));
+        out->pos = vadd(mmul(&o->o2w, pHit), o->center);
+        out->nrm = vnormalize(mmul(&o->o2w, nl));
+        out->inside = 0;
+        gbuffer_material(out, &o->mat);
+    }
+    return 1;
+}
+
 /* IntersectBase (intersection.cuh:93-113).  SDF objects are not part of this
  * restatement; they never hit. */
-static int isect_object(const or_scene* s, int i, V3 ro, V3 rd, Isect* out)
+static int isect_object(const or_scene* s, int i, V3 ro, V3 rd, float eps_d, Isect* out)
 {
     const OObj* o = &s->o[i];
     switch (o->type) {
     case AR_OBJ_CUBE: return isect_cube(o, ro, rd, out);
     case AR_OBJ_SPHERE: return isect_sphere(o, ro, rd, out);
+    case AR_OBJ_SDF: return isect_sdf(o, ro, rd, eps_d, out);
     case AR_OBJ_TRIANGLE: return isect_triangle(s, o, ro, rd, out);
     default: return 0;
     }
 }
 
 /* distance of a hit only (same arithmetic) */
-static int isect_t(const or_scene* s, int i, V3 ro, V3 rd, float* t)
+static int isect_t(const or_scene* s, int i, V3 ro, V3 rd, float eps_d, float* t)
 {
     Isect c;
     c.hit = 0; c.obj = -2;
-    if (!isect_object(s, i, ro, rd, &c)) return 0;
+    if (!isect_object(s, i, ro, rd, eps_d, &c)) return 0;
     *t = c.dist;
     return 1;
 }
@@ -621,7 +848,7 @@ static inline int slab_std(V3 ro, V3 inv, V3 mn, V3 mx, float tMin, float tMax, 
 
 typedef struct { int obj; float t; int visits, tests; } TraceResult;
 
-static TraceResult traverse(const or_scene* s, V3 ro, V3 rd, float tMin, float tMax, int any, int mode)
+static TraceResult traverse(const or_scene* s, V3 ro, V3 rd, float tMin, float tMax, int any, int mode, float eps_d)
 {
     TraceResult r;
     r.obj = -1; r.t = tMax; r.visits = 0; r.tests = 0;
@@ -644,7 +871,7 @@ static TraceResult traverse(const or_scene* s, V3 ro, V3 rd, float tMin, float t
                 const int oi = s->idx[n->first + i];
                 float t;
                 r.tests++;
-                if (!isect_t(s, oi, ro, rd, &t)) continue;
+                if (!isect_t(s, oi, ro, rd, eps_d, &t)) continue;
                 if (t < tMin) continue;
                 if (t < r.t || (tie_lowest && r.obj >= 0 && t == r.t && oi < r.obj)) {
                     r.t = t; r.obj = oi;
@@ -669,13 +896,13 @@ static TraceResult traverse(const or_scene* s, V3 ro, V3 rd, float tMin, float t
     return r;
 }
 
-static TraceResult brute(const or_scene* s, V3 ro, V3 rd, float tMin, float tMax, int any)
+static TraceResult brute(const or_scene* s, V3 ro, V3 rd, float tMin, float tMax, int any, float eps_d)
 {
     TraceResult r;
     r.obj = -1; r.t = tMax; r.visits = 0; r.tests = 0;
     for (int i = 0; i < s->n; ++i) {
         float t;
-        if (!isect_t(s, i, ro, rd, &t)) continue;
+        if (!isect_t(s, i, ro, rd, eps_d, &t)) continue;
         if (t < tMin || t >= r.t) continue;
         r.t = t; r.obj = i;
         if (any) return r;
@@ -692,7 +919,8 @@ void or_trace_rays(const or_scene* s, const float* rays, int64_t n, int any_hit,
 #endif
     for (int64_t i = 0; i < n; ++i) {
         const float* q = rays + 8 * i;
-        const TraceResult r = traverse(s, v3(q[0], q[1], q[2]), v3(q[4], q[5], q[6]), q[3], q[7], any_hit, mode);
+        const TraceResult r = traverse(s, v3(q[0], q[1], q[2]), v3(q[4], q[5], q[6]), q[3], q[7], any_hit, mode,
+                                       s->eps_tab[0]);
         hit_object[i] = r.obj;
         if (hit_t) hit_t[i] = r.obj >= 0 ? r.t : q[7];
         if (node_visits) node_visits[i] = r.visits;
@@ -709,7 +937,7 @@ void or_trace_rays_brute(const or_scene* s, const float* rays, int64_t n, int an
 #endif
     for (int64_t i = 0; i < n; ++i) {
         const float* q = rays + 8 * i;
-        const TraceResult r = brute(s, v3(q[0], q[1], q[2]), v3(q[4], q[5], q[6]), q[3], q[7], any_hit);
+        const TraceResult r = brute(s, v3(q[0], q[1], q[2]), v3(q[4], q[5], q[6]), q[3], q[7], any_hit, s->eps_tab[0]);
         hit_object[i] = r.obj;
         if (hit_t) hit_t[i] = r.obj >= 0 ? r.t : q[7];
     }
@@ -1270,11 +1498,12 @@ static int path_mode(const or_scene* s)
 
 static int closest(const or_scene* s, V3 ro, V3 rd, float tMin, Isect* out)
 {
-    const TraceResult r = traverse(s, ro, rd, tMin, INFINITY, 0, path_mode(s));
+    /* Trace's closest hit: tMin is INTERSECT_EPS(depth), also the SDF tolerance */
+    const TraceResult r = traverse(s, ro, rd, tMin, INFINITY, 0, path_mode(s), tMin);
     if (r.obj < 0) return 0;
     memset(out, 0, sizeof(*out));
     out->obj = r.obj;
-    isect_object(s, r.obj, ro, rd, out);
+    isect_object(s, r.obj, ro, rd, tMin, out);
     out->obj = r.obj;
     out->light = s->o[r.obj].light_index;
     return 1;
@@ -1292,7 +1521,7 @@ static int segment_occluded(const or_scene* s, float eps_d, V3 src, V3 dst, Coun
     if (tMax <= 0.0f) return 0;
     record_ray(cnt->sh_out, cnt->sh_cap, cnt->shadow_rays, src, 0.0f, dir, tMax);
     cnt->shadow_rays++;
-    const TraceResult r = traverse(s, src, dir, 0.0f, tMax, 1, path_mode(s));
+    const TraceResult r = traverse(s, src, dir, 0.0f, tMax, 1, path_mode(s), eps_d);
     return r.obj >= 0;
 }
 
@@ -1331,7 +1560,7 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
             Isect t;
             memset(&t, 0, sizeof(t));
             t.obj = -1;
-            hit = isect_object(s, media.obj, cro, crd, &t) && !(t.dist < eps);
+            hit = isect_object(s, media.obj, cro, crd, eps, &t) && !(t.dist < eps);
             if (hit) { ic = t; ic.obj = media.obj; ic.light = s->o[media.obj].light_index; }
             else { memset(&ic, 0, sizeof(ic)); ic.obj = -1; ic.light = -1; }
         } else {
@@ -1461,6 +1690,9 @@ static int overlap_index(const or_scene* s, V3 p)
             const V3 l = mmul(&o->w2o, vsub(p, o->center));
             const float r = max3f(o->extent);
             if (dot3(l, l) < r * r) return i;
+        } else if (o->type == AR_OBJ_SDF) {
+            /* OverlapSDFObject (sdf_base.cuh:166-177) */
+            if (sdf_eval(o, to_unit(mmul(&o->w2o, vsub(p, o->center)), o->extent)) <= 0.0f) return i;
         }
     }
     return -1;
@@ -1605,12 +1837,12 @@ void or_trace_detail(const or_scene* s, const float* rays, int64_t n, int mode, 
     for (int64_t i = 0; i < n; ++i) {
         const float* q = rays + 8 * i;
         const V3 ro = v3(q[0], q[1], q[2]), rd = v3(q[4], q[5], q[6]);
-        const TraceResult r = traverse(s, ro, rd, q[3], q[7], 0, mode);
+        const TraceResult r = traverse(s, ro, rd, q[3], q[7], 0, mode, s->eps_tab[0]);
         hit_object[i] = r.obj;
         hit_t[i] = r.obj >= 0 ? r.t : q[7];
         Isect c;
         memset(&c, 0, sizeof(c));
-        if (r.obj >= 0) isect_object(s, r.obj, ro, rd, &c);
+        if (r.obj >= 0) isect_object(s, r.obj, ro, rd, s->eps_tab[0], &c);
         pos[3 * i + 0] = c.pos.x; pos[3 * i + 1] = c.pos.y; pos[3 * i + 2] = c.pos.z;
         nrm[3 * i + 0] = c.nrm.x; nrm[3 * i + 1] = c.nrm.y; nrm[3 * i + 2] = c.nrm.z;
         inside[i] = r.obj >= 0 ? c.inside : 0;
@@ -1636,7 +1868,7 @@ void or_segments_occluded(const or_scene* s, const float* seg6, const int32_t* d
         const float eps = s->eps_tab[d] * fmaxf(1.0f, fmaxf(len3(src), len3(dst)));
         const float tMax = fmaxf(0.0f, dist - eps);
         if (tMax <= 0.0f) continue;
-        occluded[i] = traverse(s, src, dir, 0.0f, tMax, 1, mode).obj >= 0;
+        occluded[i] = traverse(s, src, dir, 0.0f, tMax, 1, mode, s->eps_tab[d]).obj >= 0;
     }
 }
 
@@ -1730,4 +1962,31 @@ void or_tonemap(const float* rgb, int64_t n, int tone, float exposure, int xyz_i
         const uint32_t r = (uint32_t)(255.0f * sat_(v.x)), g = (uint32_t)(255.0f * sat_(v.y)), b = (uint32_t)(255.0f * sat_(v.z));
         out[i] = 0xff000000u | (r << 16) | (g << 8) | b;
     }
+}
+
+void or_object_isect(const or_scene* s, int32_t obj, const float* rays, int64_t n, int32_t depth, float* t, float* pos,
+                     float* nrm)
+{
+    const float eps_d = s->eps_tab[depth < 8 ? (depth < 0 ? 0 : depth) : 8];
+    for (int64_t i = 0; i < n; ++i) {
+        const float* q = rays + 8 * i;
+        Isect c;
+        memset(&c, 0, sizeof(c));
+        c.obj = obj;
+        const int h = isect_object(s, obj, v3(q[0], q[1], q[2]), v3(q[4], q[5], q[6]), eps_d, &c);
+        t[i] = h ? c.dist : -1.0f;
+        pos[3 * i] = h ? c.pos.x : 0.0f; pos[3 * i + 1] = h ? c.pos.y : 0.0f; pos[3 * i + 2] = h ? c.pos.z : 0.0f;
+        nrm[3 * i] = h ? c.nrm.x : 0.0f; nrm[3 * i + 1] = h ? c.nrm.y : 0.0f; nrm[3 * i + 2] = h ? c.nrm.z : 0.0f;
+    }
+}
+
+void or_volume_grid(const or_scene* s, int32_t v, float* out)
+{
+    if (v < 0 || v >= s->nvol) return;
+    for (int i = 0; i < s->n; ++i)
+        if (s->o[i].vol == s->vols[v]) {
+            const size_t n = (size_t)s->o[i].dims[0] * s->o[i].dims[1] * s->o[i].dims[2];
+            memcpy(out, s->vols[v], n * sizeof(float));
+            return;
+        }
 }

@@ -57,6 +57,9 @@ typedef struct or_scene or_scene;
 
 or_scene* or_scene_create(const ar_object_desc* objects, size_t count, int flags,
                           int leaf_size, int bin_count);
+/* With the SDF volumes that AR_SDF_VOLUME objects refer to. */
+or_scene* or_scene_create_ex(const ar_object_desc* objects, size_t count, const ar_sdf_volume* volumes,
+                             size_t volume_count, int flags, int leaf_size, int bin_count);
 void or_scene_destroy(or_scene* s);
 
 /* BVH export: per node bmin[3], bmax[3] floats and left, right, first, count. */
@@ -117,6 +120,13 @@ float or_power_heuristic(float a, float b);
 
 /* Tonemap kernel (scene.cu:180-199): n pixels of RGB (or XYZ) -> 0xAARRGGBB. */
 void or_tonemap(const float* rgb, int64_t n, int tone, float exposure, int xyz_input, uint32_t* out);
+
+/* One object's hit at loop depth `depth` (SDF tolerance INTERSECT_EPS(depth)/2):
+ * t = -1 on a miss, with world position and normal. */
+void or_object_isect(const or_scene* s, int32_t obj, const float* rays, int64_t n, int32_t depth, float* t,
+                     float* pos, float* nrm);
+/* The float grid of SDF volume v as an object of the scene uses it. */
+void or_volume_grid(const or_scene* s, int32_t v, float* out);
 
 float or_sinf(float x);
 float or_cosf(float x);

@@ -38,6 +38,8 @@ def load():
     lib = ctypes.CDLL(LIB)
     lib.or_scene_create.argtypes = [c_void_p, c_size_t, c_int, c_int, c_int]
     lib.or_scene_create.restype = c_void_p
+    lib.or_scene_create_ex.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, c_int, c_int]
+    lib.or_scene_create_ex.restype = c_void_p
     lib.or_scene_destroy.argtypes = [c_void_p]
     lib.or_scene_node_count.argtypes = [c_void_p]
     lib.or_scene_node_count.restype = c_int64
@@ -62,6 +64,8 @@ def load():
     lib.or_collect_rays.restype = c_int64
     lib.or_powf.argtypes = [c_float, c_float]
     lib.or_powf.restype = c_float
+    lib.or_object_isect.argtypes = [c_void_p, c_int32, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]
+    lib.or_volume_grid.argtypes = [c_void_p, c_int32, c_void_p]
     lib.or_tonemap.argtypes = [c_void_p, c_int64, c_int, c_float, c_int, c_void_p]
     lib.or_trace_detail.argtypes = [c_void_p, c_void_p, c_int64, c_int] + [c_void_p] * 5 + [c_int]
     lib.or_segments_occluded.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p, c_int]
@@ -79,12 +83,15 @@ def _p(a: np.ndarray) -> int:
 
 
 class OracleScene:
-    def __init__(self, objects: np.ndarray, flags: int = 0, leaf_size: int = 8, bin_count: int = 12):
+    def __init__(self, objects: np.ndarray, flags: int = 0, leaf_size: int = 8, bin_count: int = 12, volumes=None):
+        """volumes: list of (SdfVolume, keep-alive) from aperture_b200.make_volume()."""
         lib = load()
-        from aperture_b200 import OBJECT_DTYPE
+        from aperture_b200 import OBJECT_DTYPE, SdfVolume
         self._objs = np.ascontiguousarray(objects, dtype=OBJECT_DTYPE)
-        self._h = lib.or_scene_create(_p(self._objs) if len(self._objs) else None, len(self._objs), flags,
-                                      leaf_size, bin_count)
+        self._vols = volumes
+        arr = (SdfVolume * len(volumes))(*[v for v, _ in volumes]) if volumes else None
+        self._h = lib.or_scene_create_ex(_p(self._objs) if len(self._objs) else None, len(self._objs), arr,
+                                         len(volumes) if volumes else 0, flags, leaf_size, bin_count)
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -151,6 +158,21 @@ class OracleScene:
         p = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
         out = np.empty(len(p), np.int32)
         _lib.or_overlap(self._h, _p(p), len(p), _p(out))
+        return out
+
+    def object_isect(self, obj: int, rays, depth: int = 0):
+        """(t or -1, position[n,3], normal[n,3]) of one object for each ray at loop depth `depth`."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        t = np.empty(n, np.float32)
+        pos = np.empty((n, 3), np.float32)
+        nrm = np.empty((n, 3), np.float32)
+        _lib.or_object_isect(self._h, obj, _p(rays), n, depth, _p(t), _p(pos), _p(nrm))
+        return t, pos, nrm
+
+    def volume_grid(self, v: int, dims) -> np.ndarray:
+        out = np.zeros(int(np.prod(dims)), np.float32)
+        _lib.or_volume_grid(self._h, v, _p(out))
         return out
 
     def trace_brute(self, rays, any_hit=False, threads=0):

@@ -12,6 +12,8 @@
 //   intersection::TraverseBVH<bAnyHit>        core/render/intersection.cuh:235-370
 //   intersection::AnyHitSegmentBVH            core/render/intersection.cuh:372-397
 //   intersection::Intersect (linear scan)     core/render/intersection.cuh:175-205
+//   IntersectBase, sdf::IntersectSDFObject    core/render/intersection.cuh:93-113,
+//       core/object/sdf/sdf_base.cuh:54-163 (torus and volume functors)
 //   intersection::Overlap                     core/render/intersection.cuh:399-414
 //   BSDF_PDF (RGB)                            core/render/material.cuh:332-387
 //   Gamma, ACES, XYZ2SRGBLinearD65            core/tonemap.cuh (the per-pixel steps of
@@ -65,6 +67,11 @@ Material material_of(const ar_material& m)
 SceneObject object_of(const ar_object_desc& d)
 {
     AdditionalObjectInfo info = {};
+    if (d.type == AR_OBJ_SDF) {
+        info.sdfType_ = d.sdf.kind == AR_SDF_TORUS ? ESDFType::SDF_TORUS : ESDFType::SDF_VOLUME;
+        info.sdfInfo_.sdfInfo0_ = make_float4(d.sdf.info[0], d.sdf.info[1], d.sdf.info[2], d.sdf.info[3]);
+        info.sdfInfo_.cachedVolumeIndex_ = d.sdf.volume;
+    }
     if (d.type == AR_OBJ_TRIANGLE) {
         Vertex* v[3] = {&info.triangleInfo_.v0_, &info.triangleInfo_.v1_, &info.triangleInfo_.v2_};
         for (int k = 0; k < 3; ++k) {
@@ -234,6 +241,51 @@ void ref_tonemap(const float* rgb, int64_t n, int tone, float exposure, int xyz_
         const unsigned int blue = static_cast<unsigned int>(255.0f * saturate_(value.z));
         out[i] = 0xff000000u | (red << 16) | (green << 8) | blue;
     }
+}
+
+// One object's intersection at loop depth `depth` (IntersectBase, with the
+// volume functor of sdf_volume.cuh built on a host grid for SDF volumes: the
+// reference reads its volumes through a device-only pointer table).  Rays as
+// for ref_trace_rays (tmin/tmax ignored); t = -1 on a miss.
+void ref_object_isect(const ref_scene* s, int32_t obj, const float* grid, const int32_t* dims, const float* rays,
+                      int64_t n, int32_t depth, float* t, float* pos, float* nrm)
+{
+    const SceneObject& o = s->objects[static_cast<size_t>(obj)];
+    sdf::SDFVolumeInfo vi{};
+    const bool volume = o.type_ == EObjectType::OBJ_SDF && o.additionalObjectInfo_.sdfType_ == ESDFType::SDF_VOLUME;
+    if (volume) {
+        vi.volumePtr_ = const_cast<float*>(grid);
+        vi.dim_ = make_int3(dims[0], dims[1], dims[2]);
+        vi.ComputeVoxelSize();
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        const float* q = rays + 8 * i;
+        const float3 ro = make_float3(q[0], q[1], q[2]), rd = make_float3(q[4], q[5], q[6]);
+        const IntersectionContext c =
+            volume ? sdf::IntersectSDFObject<sdf::SDFVolumeFunctor, true>(depth, ro, rd, o, sdf::SDFVolumeFunctor(vi))
+                   : intersection::IntersectBase(depth, ro, rd, o);
+        t[i] = c.bHit_ ? c.distance_ : -1.0f;
+        pos[3 * i] = c.hitPosition_.x; pos[3 * i + 1] = c.hitPosition_.y; pos[3 * i + 2] = c.hitPosition_.z;
+        nrm[3 * i] = c.hitNormal_.x; nrm[3 * i + 1] = c.hitNormal_.y; nrm[3 * i + 2] = c.hitNormal_.z;
+        if (!c.bHit_) for (int k = 0; k < 3; ++k) pos[3 * i + k] = nrm[3 * i + k] = 0.0f;
+    }
+}
+
+// The grid FillSDFVolume (object/sdf/sdf_cache_manager.cuh:16-38) writes for
+// the torus functor, evaluated on the host with the reference's functor.
+void ref_fill_torus(const int32_t* dims, float R, float r, float* out)
+{
+    const SDFInfo info{make_float4(R, r, 0.0f, 0.0f)};
+    const sdf::SDFTorusFunctor f{};
+    size_t i = 0;
+    for (int z = 0; z < dims[2]; ++z)
+        for (int y = 0; y < dims[1]; ++y)
+            for (int x = 0; x < dims[0]; ++x, ++i) {
+                const float nx = (dims[0] > 1) ? static_cast<float>(x) / static_cast<float>(dims[0] - 1) : 0.0f;
+                const float ny = (dims[1] > 1) ? static_cast<float>(y) / static_cast<float>(dims[1] - 1) : 0.0f;
+                const float nz = (dims[2] > 1) ? static_cast<float>(z) / static_cast<float>(dims[2] - 1) : 0.0f;
+                out[i] = f(make_float3(nx, ny, nz) - 0.5f, info);
+            }
 }
 
 // INTERSECT_EPS (config.cuh:3) as the reference's host pass evaluates it.

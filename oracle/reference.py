@@ -46,6 +46,9 @@ def load():
     lib.ref_overlap.argtypes = [c_void_p, c_void_p, c_int64, c_void_p]
     lib.ref_bsdf_pdf.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p]
     lib.ref_bsdf_pdf.restype = c_float
+    lib.ref_object_isect.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p,
+                                     c_void_p, c_void_p]
+    lib.ref_fill_torus.argtypes = [c_void_p, c_float, c_float, c_void_p]
     lib.ref_tonemap.argtypes = [c_void_p, c_int64, c_int, c_float, c_int, c_void_p]
     lib.ref_intersect_eps.argtypes = [c_int]
     lib.ref_intersect_eps.restype = c_float
@@ -105,6 +108,18 @@ class RefScene:
                             _p(ins), threads)
         return obj, t, pos, nrm, ins
 
+    def object_isect(self, obj: int, rays, depth: int = 0, grid=None, dims=(0, 0, 0)):
+        """IntersectBase of one object (SDF volumes read `grid`): (t or -1, position, normal)."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        t = np.empty(n, np.float32)
+        pos = np.empty((n, 3), np.float32)
+        nrm = np.empty((n, 3), np.float32)
+        g = np.ascontiguousarray(grid, np.float32) if grid is not None else np.zeros(1, np.float32)
+        d = np.asarray(dims, np.int32)
+        _lib.ref_object_isect(self._h, obj, _p(g), _p(d), _p(rays), n, depth, _p(t), _p(pos), _p(nrm))
+        return t, pos, nrm
+
     def segments_occluded(self, seg6, depth, threads=0):
         seg6 = np.ascontiguousarray(seg6, np.float32).reshape(-1, 6)
         depth = np.ascontiguousarray(depth, np.int32)
@@ -134,4 +149,11 @@ def tonemap(rgb: np.ndarray, tone: int, exposure: float = 1.0, xyz_input: bool =
     rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)
     out = np.empty(len(rgb), np.uint32)
     load().ref_tonemap(_p(rgb), len(rgb), tone, exposure, int(xyz_input), _p(out))
+    return out
+
+
+def fill_torus(dims, R: float, r: float) -> np.ndarray:
+    d = np.asarray(dims, np.int32)
+    out = np.empty(int(np.prod(dims)), np.float32)
+    load().ref_fill_torus(_p(d), R, r, _p(out))
     return out

@@ -8,7 +8,9 @@ the light table of UpdateSceneToDeviceIfDirty (core/scene.cu:1046-1080),
 TraverseBVH closest and any hit (core/render/intersection.cuh:235-370),
 AnyHitSegmentBVH (372-397), Overlap (399-414), BSDF_PDF (RGB,
 core/render/material.cuh:332-387), INTERSECT_EPS (core/config.cuh:3) and the
-Tonemap kernel's curves (core/tonemap.cuh) at exposure 1.7.
+Tonemap kernel's curves (core/tonemap.cuh) at exposure 1.7, and the SDF
+intersector (IntersectBase / sdf::IntersectSDFObject with the torus and
+volume functors, core/object/sdf/) with the grid FillSDFVolume writes.
 
 Scenes: config 1 (scenes.box_scene()) and a small sphere field
 (scenes.spheres_scene(n_spheres=24, n_lights=4, box=20, subdivisions=1):
@@ -118,6 +120,30 @@ def main():
     for tone in (0, 1, 2):
         for xyz in (0, 1):
             out[f"tonemap_t{tone}_x{xyz}"] = reference.tonemap(hdr, tone, 1.7, bool(xyz))
+    # SDF objects (IntersectBase -> sdf::IntersectSDFObject): an analytic torus and
+    # a torus sampled on a 64^3 grid (FillSDFVolume), at loop depths 0 and 5
+    objs, vols = scenes.sdf_box_scene()
+    rs = reference.RefScene(objs)
+    dims = tuple(vols[0][0].dims)
+    grid = reference.fill_torus(dims, vols[0][0].fill_info[0], vols[0][0].fill_info[1])
+    out["sdf_sha256"] = np.frombuffer(hashlib.sha256(objs.tobytes()).digest(), np.uint8)
+    out["sdf_grid_sha256"] = np.frombuffer(hashlib.sha256(grid.tobytes()).digest(), np.uint8)
+    rays = []
+    for obj in (len(objs) - 2, len(objs) - 1):     # aimed at points inside each object's box
+        c = np.array([objs["center"][obj][f] for f in "xyz"])
+        e = np.array([objs["extent"][obj][f] for f in "xyz"])
+        o = rng.uniform(-0.55, 0.55, (500, 3))
+        d = c + rng.uniform(-1, 1, (500, 3)) * e - o
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        r = np.zeros((500, 8), np.float32)
+        r[:, :3], r[:, 4:7], r[:, 3], r[:, 7] = o, d, 1e-4, np.inf
+        rays.append(r)
+    rays = np.concatenate(rays)
+    out["sdf_rays"] = rays
+    for obj in (len(objs) - 2, len(objs) - 1):
+        for depth in (0, 5):
+            t, pos, nrm = rs.object_isect(obj, rays, depth, grid, dims)
+            out[f"sdf_o{obj}_d{depth}"] = np.concatenate([t[:, None], pos, nrm], 1).astype(np.float32)
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT} ({os.path.getsize(OUT)} bytes)")
 
