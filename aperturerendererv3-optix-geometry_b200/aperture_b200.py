@@ -85,7 +85,7 @@ class Camera(ctypes.Structure):
 class RenderParams(ctypes.Structure):
     _fields_ = [("spp", c_int32), ("max_depth", c_int32), ("rr_depth", c_int32), ("use_nee", c_int32),
                 ("sky", c_int32), ("frame_offset", c_int32), ("seed", c_uint64), ("sort_rays", c_int32),
-                ("wave_paths", c_int32)]
+                ("wave_paths", c_int32), ("spectral", c_int32), ("reserved", c_int32)]
 
 
 class PathRecord(ctypes.Structure):
@@ -114,7 +114,8 @@ RECORD_DTYPE = np.dtype(PathRecord)
 EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create", "ar_scene_create_ex",
                     "ar_scene_destroy",
                     "ar_scene_get_info", "ar_render", "ar_trace_rays", "ar_trace_rays_static",
-                    "ar_render_debug_paths", "ar_rng_tape", "ar_tonemap", "ar_accum_resolve", "ar_tone_curve")
+                    "ar_render_debug_paths", "ar_rng_tape", "ar_tonemap", "ar_accum_resolve", "ar_tone_curve",
+                    "ar_scene_set_spectral", "ar_scene_get_spectral_luts")
 
 
 class ArError(RuntimeError):
@@ -162,6 +163,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_accum_resolve.restype = c_int32
     lib.ar_tone_curve.argtypes = [c_void_p, c_int32, c_void_p]
     lib.ar_tone_curve.restype = c_int32
+    lib.ar_scene_set_spectral.argtypes = [c_void_p, c_void_p, c_size_t, c_int32]
+    lib.ar_scene_set_spectral.restype = c_int32
+    lib.ar_scene_get_spectral_luts.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.ar_scene_get_spectral_luts.restype = c_int32
     _lib = lib
     return lib
 
@@ -182,9 +187,9 @@ def make_camera(position, direction, fov_y_deg, width, height) -> Camera:
 
 
 def make_params(spp=1, max_depth=8, rr_depth=3, use_nee=1, sky=1, frame_offset=0, seed=REFERENCE_SEED,
-                sort_rays=0, wave_paths=0) -> RenderParams:
+                sort_rays=0, wave_paths=0, spectral=0) -> RenderParams:
     return RenderParams(int(spp), int(max_depth), int(rr_depth), int(use_nee), int(sky), int(frame_offset),
-                        int(seed) & 0xFFFFFFFFFFFFFFFF, int(sort_rays), int(wave_paths))
+                        int(seed) & 0xFFFFFFFFFFFFFFFF, int(sort_rays), int(wave_paths), int(spectral), 0)
 
 
 class Scene:
@@ -205,6 +210,23 @@ class Scene:
                                        ctypes.byref(h)))
         self._h = h
         self.num_objects = len(objects)
+
+    def set_spectral(self, lut_res: int = 64, tables: np.ndarray | None = None) -> None:
+        """Enable spectral rendering: the reference's tables (spectral_tables.load()
+        unless given) and an lut_res^3 RGB lookup table built on the device."""
+        if tables is None:
+            import spectral_tables
+            tables = spectral_tables.load()[0]
+        t = np.ascontiguousarray(tables, np.float32)
+        _check(_lib.ar_scene_set_spectral(self._h, _ptr(t), t.size, lut_res))
+        self.lut_res = lut_res
+
+    def spectral_luts(self):
+        """(lambda table [840, 4], rgb table [res^3, 4]) as built on the device."""
+        lam = np.zeros((840, 4), np.float32)
+        rgb = np.zeros((self.lut_res ** 3, 4), np.float32)
+        _check(_lib.ar_scene_get_spectral_luts(self._h, _ptr(lam), _ptr(rgb)))
+        return lam, rgb
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:

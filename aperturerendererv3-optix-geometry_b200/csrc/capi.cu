@@ -94,6 +94,11 @@ struct ar_scene {
     // host copy for the camera overlap test (intersection::Overlap)
     std::vector<ar::ObjInfo> h_objects;
     std::vector<ar::Analytic> h_analytic;
+    // spectral mode (ar_scene_set_spectral): reference tables and lookup tables
+    float* spec_tables = nullptr;
+    float4* spec_lut_lam = nullptr;
+    float4* spec_lut_rgb = nullptr;
+    int spec_res = 0;
     std::vector<ar::SdfRec> h_sdf;              // data pointers into h_volumes
     std::vector<ar::HostVolume> h_volumes;
     // render workspace
@@ -213,6 +218,7 @@ ar_status check_params(const ar_render_params* p)
     if (p->max_depth <= 0 || p->max_depth > 4096) return fail(AR_ERR_INVALID_ARGUMENT, "max_depth must be in [1, 4096]");
     if (p->rr_depth < 0) return fail(AR_ERR_INVALID_ARGUMENT, "rr_depth must be >= 0");
     if (p->frame_offset < 0) return fail(AR_ERR_INVALID_ARGUMENT, "frame_offset must be >= 0");
+    if (p->spectral != 0 && p->spectral != 1) return fail(AR_ERR_INVALID_ARGUMENT, "spectral must be 0 or 1");
     return AR_OK;
 }
 
@@ -246,6 +252,13 @@ ar::FrameParams make_frame(const ar_scene* s, const ar_camera* c, const ar_rende
         fp.sky = p->sky;
         fp.seed = p->seed;
         fp.frame0 = static_cast<uint64_t>(p->frame_offset);
+        if (p->spectral) {
+            fp.spectral = 1;
+            fp.spec.tables = s->spec_tables;
+            fp.spec.lut_lam = s->spec_lut_lam;
+            fp.spec.lut_rgb = s->spec_lut_rgb;
+            fp.spec.res = s->spec_res;
+        }
     }
     for (int d = 0; d <= 8; ++d) fp.eps_tab[d] = 1.0e-3f * exp_det(fminf(static_cast<float>(d) * 0.5f, 4.0f));
     return fp;
@@ -255,6 +268,8 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
                      cudaStream_t st, ar_render_stats* stats)
 {
     using namespace ar;
+    if (p->spectral && !s->spec_tables)
+        return fail(AR_ERR_UNSUPPORTED, "spectral rendering needs ar_scene_set_spectral first");
     ar::FrameParams fp = make_frame(s, cam, p);
     const int64_t npix = fp.npix;
     const int64_t total = npix * p->spp;
@@ -523,6 +538,59 @@ ar_status ar_render(ar_scene* s, const ar_camera* cam, const ar_render_params* p
         }
     }
     return check_err(s, st);
+    AR_GUARD_END
+}
+
+ar_status ar_scene_set_spectral(ar_scene* s, const float* tables, size_t count, int32_t lut_res)
+{
+    g_last_error.clear();
+    if (!s) return fail(AR_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (!tables) return fail(AR_ERR_INVALID_ARGUMENT, "tables is NULL");
+    if (count != static_cast<size_t>(ar::kTabFloats))
+        return fail(AR_ERR_INVALID_ARGUMENT, "tables must hold " + std::to_string(ar::kTabFloats) + " floats");
+    if (lut_res < 2 || lut_res > 512) return fail(AR_ERR_INVALID_ARGUMENT, "lut_res must be in [2, 512]");
+    AR_GUARD_BEGIN
+    DeviceGuard g(s->device);
+    auto drop = [&](void* p) {
+        if (!p) return;
+        for (auto it = s->owned.begin(); it != s->owned.end(); ++it)
+            if (*it == p) { s->owned.erase(it); break; }
+        cudaFree(p);
+    };
+    drop(s->spec_tables); drop(s->spec_lut_lam); drop(s->spec_lut_rgb);
+    s->spec_tables = nullptr; s->spec_lut_lam = nullptr; s->spec_lut_rgb = nullptr; s->spec_res = 0;
+    const size_t nrgb = static_cast<size_t>(lut_res) * lut_res * lut_res;
+    float* tab = dalloc<float>(count, "spectral tables");
+    s->owned.push_back(tab);
+    float4* lam = dalloc<float4>(ar::kLambdaLutRes, "spectral lambda table");
+    s->owned.push_back(lam);
+    float4* rgb = dalloc<float4>(nrgb, "spectral rgb table");
+    s->owned.push_back(rgb);
+    ck(cudaMemcpy(tab, tables, count * sizeof(float), cudaMemcpyHostToDevice), "copy spectral tables");
+    ck(ar::launch_spectral_luts(tab, lut_res, lam, rgb, s->sm_count, nullptr), "spectral tables");
+    ck(cudaDeviceSynchronize(), "spectral tables");
+    s->spec_tables = tab;
+    s->spec_lut_lam = lam;
+    s->spec_lut_rgb = rgb;
+    s->spec_res = lut_res;
+    return AR_OK;
+    AR_GUARD_END
+}
+
+ar_status ar_scene_get_spectral_luts(const ar_scene* s, float* lambda_lut, float* rgb_lut)
+{
+    g_last_error.clear();
+    if (!s) return fail(AR_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (!s->spec_tables) return fail(AR_ERR_UNSUPPORTED, "no spectral tables set");
+    AR_GUARD_BEGIN
+    DeviceGuard g(s->device);
+    if (lambda_lut)
+        ck(cudaMemcpy(lambda_lut, s->spec_lut_lam, sizeof(float4) * ar::kLambdaLutRes, cudaMemcpyDeviceToHost),
+           "copy lambda table");
+    if (rgb_lut)
+        ck(cudaMemcpy(rgb_lut, s->spec_lut_rgb, sizeof(float4) * static_cast<size_t>(s->spec_res) * s->spec_res * s->spec_res,
+                      cudaMemcpyDeviceToHost), "copy rgb table");
+    return AR_OK;
     AR_GUARD_END
 }
 

@@ -229,6 +229,11 @@ __global__ void k_regen(FrameParams fp, PathBuffers B, PoolCtl* ctl, int cur, ui
         pr.o = f4(o, fbits(0));
         pr.d = f4(dir, fbits(fp.camera_inside ? kFlagInside : 0));
         pr.mask = make_float4(1.0f, 1.0f, 1.0f, fbits(p));
+        if (fp.spectral) {  // CalculateRadiance starts with SampleCIE1931(Rand3(seed)) (render.cuh:467)
+            const float r0 = r.next(), r1 = r.next(), r2 = r.next();
+            const LambdaSample ls = sample_cie1931(r0, r1, r2);
+            pr.mask = make_float4(1.0f, ls.lambda, ls.pdf, fbits(p));
+        }
         pr.rad = make_float4(0.0f, 0.0f, 0.0f, fbits(sidx));
         pr.rng0 = make_uint4(r.st.d, r.st.v[0], r.st.v[1], r.st.v[2]);
         pr.rng1 = make_uint4(r.st.v[3], r.st.v[4], static_cast<uint32_t>(-1), static_cast<uint32_t>(r.used));
@@ -308,7 +313,7 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(SceneVi
 // the shadow query: Trace's material evaluation and hit offset, emission with
 // MIS, light sampling for NEE, throughput and Russian roulette.  kModel is the
 // shading model of every path of this launch's bucket, -1 = miss.
-template <int kModel, bool kSdf>
+template <int kModel, bool kSdf, bool kSpec>
 __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams fp, PathBuffers B, int cur,
                                                        PoolCtl* ctl, ar_path_record* rec)
 {
@@ -331,6 +336,18 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         const f3 cro = xyz(pr.o);
         f3 mask = xyz(pr.mask);
         f3 radiance = xyz(pr.rad);
+        // spectral: scalar throughput and radiance broadcast to the three lanes
+        // of the RGB arithmetic, the wavelength's basis and D65 weight
+        float lambda = 0.0f, lpdf = 0.0f, d65 = 1.0f;
+        float4 lk = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (kSpec) {
+            lambda = pr.mask.y;
+            lpdf = pr.mask.z;
+            mask = mk(pr.mask.x, pr.mask.x, pr.mask.x);
+            radiance = mk(pr.rad.x, pr.rad.x, pr.rad.x);
+            lk = query_lambda(fp.spec.lut_lam, lambda);
+            d65 = d65_norm(fp.spec.tables, lambda);
+        }
         const bool inside = (flags & kFlagInside) != 0;
         const f3 vloc = xyz(pr.vloc);
         const int4 hr = B.hit[k];
@@ -347,6 +364,15 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         if (hit) {
             const ObjInfo oi = s.objects[hr.x];
             gb = load_gb(s.materials[oi.material]);
+            if (kSpec) {  // EvaluateMaterial / SampleBSDF at the path's wavelength (material.cuh)
+                const float a = interact(fp.spec.lut_rgb, fp.spec.res, lk, gb.albedo);
+                const float e = interact(fp.spec.lut_rgb, fp.spec.res, lk, gb.emissive);
+                gb.albedo = mk(a, a, a);
+                gb.emissive = mk(e, e, e);
+                gb.ior = ior_abbe(lambda, gb.ior, gb.abbe);
+                gb.sigma_a = sigma_tilt(gb.sigma_a, lambda, gb.tilt);
+                gb.spectral = true;
+            }
             light = oi.light;
             if (oi.type == AR_OBJ_TRIANGLE) {
                 const PrimRec& prim = s.prims[hr.y];
@@ -425,7 +451,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                     float alpha, kD;
                     f3 F0;
                     ggx_params(gb, alpha, kD, F0);
-                    const float pSpec = clampf(luminance(F0), 0.1f, 0.9f);
+                    const float pSpec = ggx_pspec(gb, F0);
                     const float uu = g.next();
                     const float e0 = g.next(), e1 = g.next(), e2 = g.next();
                     if (uu < pSpec) {
@@ -455,6 +481,10 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             next = crd;
             pdf = 1.0f;
             emis = sky_lighting(crd, fp.sky);
+            if (kSpec) {
+                const float e = interact(fp.spec.lut_rgb, fp.spec.res, lk, emis);
+                emis = mk(e, e, e);
+            }
             nInside = false;
         }
         {   // hit offset, always one uniform (render.cuh:156-160)
@@ -466,7 +496,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         const bool mInside = nInside;  // media state after this segment
         // ---- emission (render.cuh:648-723)
         if (!hit) {
-            if (!missThin) radiance = radiance + mask * emis;
+            if (!missThin) radiance = radiance + (mask * emis) * d65;
         } else if (light >= 0) {
             float misW = 1.0f;
             if (fp.use_nee && depth > 0 && (flags & kFlagPrevNEE)) {
@@ -474,7 +504,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                 const float pL = pdf_light_from_hit(s, hr.x, xyz(pr.prev), pos, nrm);
                 if (pL >= 0.0f && pB > 0.0f) misW = power_heuristic(pB, pL);
             }
-            radiance = radiance + (mask * emis) * misW;
+            radiance = radiance + ((mask * emis) * d65) * misW;
         }
         const bool brk = (!hit && !missThin) || terminate;
         bool cont = false, shadow = false, cosOK = false;
@@ -483,10 +513,14 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         if (!brk) {
             // ---- NEE (render.cuh:766-827)
             if (!missThin) {
-                const float lum = luminance(mask);
+                const float lum = kSpec ? mask.x : luminance(mask);
                 const float rate = sqrtf(saturate(lum));
                 if (fp.use_nee && nonDelta < 10 && !delta && !mInside && g.next() < rate) {
-                    const LightSample ls = sample_light(s, pos, g);
+                    LightSample ls = sample_light(s, pos, g);
+                    if (kSpec) {
+                        const float e = interact(fp.spec.lut_rgb, fp.spec.res, lk, ls.emis);
+                        ls.emis = mk(e, e, e);
+                    }
                     if (ls.valid) {
                         const float pATotal = fmaxf(1e-20f, ls.pA * ls.pFacet);
                         const f3 lu = ls.p - pos;
@@ -501,7 +535,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                             const f3 contrib = (fcos * ls.emis) * (G / pATotal);
                             const float pL = area_to_solid_angle(pos, ls.p, ls.n, ls.pFacet * ls.pA);
                             const float pB = fmaxf(bsdf_pdf(kModel, gb, nrm, crd, ld), 0.0f);
-                            pending = mask * (contrib * power_heuristic(pL, pB));
+                            pending = (mask * (contrib * power_heuristic(pL, pB))) * d65;
                         }
                         shadow = true;
                         lightP = ls.p;
@@ -520,8 +554,8 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             float qrr = 1.0f;
             bool survived = true;
             if (nonDelta >= fp.rr_depth) {
-                const float lum = luminance(mask);
-                const float mx = max3(mask);
+                const float lum = kSpec ? mask.x : luminance(mask);
+                const float mx = kSpec ? mask.x : max3(mask);
                 const float basic = clampf(lum * 0.5f + mx * 0.5f, 0.05f, 0.95f);
                 qrr = lerpf(basic, 1.0f, mInside ? 0.99f : 0.0f);
                 if (g.next() > qrr) survived = false;
@@ -542,8 +576,8 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             PathRec out;
             out.o = f4(pos, fbits((depth + 1) | (nonDelta << 16)));
             out.d = f4(next, fbits(flags | (nmdepth << 8)));
-            out.mask = f4(mask, fbits(pixel));
-            out.rad = f4(radiance, fbits(sidx));
+            out.mask = kSpec ? make_float4(mask.x, lambda, lpdf, fbits(pixel)) : f4(mask, fbits(pixel));
+            out.rad = kSpec ? make_float4(radiance.x, 0.0f, 0.0f, fbits(sidx)) : f4(radiance, fbits(sidx));
             out.rng0 = make_uint4(g.st.d, g.st.v[0], g.st.v[1], g.st.v[2]);
             out.rng1 = make_uint4(g.st.v[3], g.st.v[4], static_cast<uint32_t>(nmobj), used);
             out.prev = prevOut;
@@ -553,7 +587,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         } else {
             RetireRec out;
             out.rad = f4(radiance, fbits(pixel));
-            out.meta = make_int4(sidx, static_cast<int>(used), 0, 0);
+            out.meta = make_int4(sidx, static_cast<int>(used), ibits(lambda), ibits(lpdf));
             B.retire[r] = out;
             target = ~r;
         }
@@ -661,9 +695,18 @@ __global__ void k_retire(FrameParams fp, PathBuffers B, PoolCtl* ctl, double* ac
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->retired += n;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const RetireRec rr = B.retire[i];
-        const float x = fmaxf(clampf(fix_nan_inf(rr.rad.x), 0.0f, 1.0e3f), 0.0f);
-        const float y = fmaxf(clampf(fix_nan_inf(rr.rad.y), 0.0f, 1.0e3f), 0.0f);
-        const float z = fmaxf(clampf(fix_nan_inf(rr.rad.z), 0.0f, 1.0e3f), 0.0f);
+        f3 v = xyz(rr.rad);
+        if (fp.spectral) {  // lambdaXYZ * radiance / pdf (render.cuh:966), linear CIE XYZ
+            const float lam = fbits(rr.meta.z), lpdf = fbits(rr.meta.w);
+            const float r = fix_nan_inf(rr.rad.x);
+            const f3 c = cmf_xyz(fp.spec.tables, lam);
+            v = mk((c.x * r) / lpdf, (c.y * r) / lpdf, (c.z * r) / lpdf);
+        } else {
+            v = mk(fix_nan_inf(v.x), fix_nan_inf(v.y), fix_nan_inf(v.z));
+        }
+        const float x = fmaxf(clampf(v.x, 0.0f, 1.0e3f), 0.0f);
+        const float y = fmaxf(clampf(v.y, 0.0f, 1.0e3f), 0.0f);
+        const float z = fmaxf(clampf(v.z, 0.0f, 1.0e3f), 0.0f);
         const int pixel = ibits(rr.rad.w);
         double* a = accum + 3 * static_cast<int64_t>(pixel);
         atomicAdd(a + 0, static_cast<double>(x));
@@ -748,6 +791,18 @@ cudaError_t launch_pool_init(PoolCtl* ctl, int64_t total, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// The five per-material shading launches of one iteration.
+template <bool kSdf, bool kSpec>
+void launch_shade(const SceneView& s, const FrameParams& fp, const PathBuffers& B, int c, PoolCtl* ctl,
+                  ar_path_record* rec, int grid, cudaStream_t st)
+{
+    k_shade<-1, kSdf, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_DIFFUSE, kSdf, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_LIGHT, kSdf, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_GLASS, kSdf, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_GGX, kSdf, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+}
+
 cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const PathBuffers& B, PoolCtl* ctl,
                               uint4* b0, uint2* b1, const uint32_t* jump_table, unsigned long long* stats,
                               uint32_t* ovf, int* err, double* accum, ar_path_record* rec, int iterations, int* cur,
@@ -762,18 +817,12 @@ cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const P
         if (s.num_sdf > 0) k_extend<true><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
         else k_extend<false><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
         if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend++ + 1], st);
-        if (s.num_sdf > 0) {
-            k_shade<-1, true><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-            k_shade<AR_MAT_DIFFUSE, true><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-            k_shade<AR_MAT_LIGHT, true><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-            k_shade<AR_MAT_GLASS, true><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-            k_shade<AR_MAT_GGX, true><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+        if (fp.spectral) {
+            if (s.num_sdf > 0) launch_shade<true, true>(s, fp, B, c, ctl, rec, grid_other, st);
+            else launch_shade<false, true>(s, fp, B, c, ctl, rec, grid_other, st);
         } else {
-            k_shade<-1, false><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-            k_shade<AR_MAT_DIFFUSE, false><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-            k_shade<AR_MAT_LIGHT, false><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-            k_shade<AR_MAT_GLASS, false><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-            k_shade<AR_MAT_GGX, false><<<grid_other, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+            if (s.num_sdf > 0) launch_shade<true, false>(s, fp, B, c, ctl, rec, grid_other, st);
+            else launch_shade<false, false>(s, fp, B, c, ctl, rec, grid_other, st);
         }
         const bool ts = tm && tm->n_shadow < tm->cap;
         if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow], st);

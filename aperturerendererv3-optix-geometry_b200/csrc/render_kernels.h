@@ -37,6 +37,9 @@ cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const P
                               uint4* b0, uint2* b1, const uint32_t* jump_table, unsigned long long* stats,
                               uint32_t* ovf, int* err, double* accum, ar_path_record* rec, int iterations, int* cur,
                               int grid_trace, int grid_other, cudaStream_t st, int64_t* launches, LaunchTimers* tm);
+// Spectral lookup tables from the network weights in `tab` (device memory).
+cudaError_t launch_spectral_luts(const float* tab, int res, float4* lut_lam, float4* lut_rgb, int sm_count,
+                                 cudaStream_t st);
 cudaError_t launch_mean(const double* accum, int64_t n, double inv, float* out, cudaStream_t st);
 cudaError_t launch_add(const double* src, int64_t n, double* dst, cudaStream_t st);
 

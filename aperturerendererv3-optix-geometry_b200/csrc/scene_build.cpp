@@ -288,6 +288,7 @@ HostScene build_scene(const ar_object_desc* objs, size_t n, const ar_sdf_volume*
         mr.emissive[0] = d.material.emissive.x; mr.emissive[1] = d.material.emissive.y; mr.emissive[2] = d.material.emissive.z;
         mr.specular = d.material.specular; mr.metallic = d.material.metallic; mr.roughness = d.material.roughness;
         mr.ior = d.material.ior; mr.sigma_a = d.material.sigma_a;
+        mr.abbe = d.material.abbe_number; mr.tilt = d.material.tilt_number;
         std::string key(reinterpret_cast<const char*>(&mr), sizeof(mr));
         auto it = matIndex.find(key);
         int32_t mi;

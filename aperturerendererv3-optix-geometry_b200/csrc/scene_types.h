@@ -10,7 +10,7 @@
 //   TriShade  trishade[]  48 B  world vertex normals of triangle objects (shading)
 //   Analytic  analytic[] 112 B  cube / sphere / SDF transform records
 //   SdfRec    sdf[]       64 B  SDF objects (tested after the BVH), volume grids
-//   MaterialRec materials[] 48 B  de-duplicated materials
+//   MaterialRec materials[] 64 B  de-duplicated materials
 //   lights: object index + selection probability, in object order
 #pragma once
 
@@ -89,7 +89,9 @@ struct alignas(16) MaterialRec {
     float emissive[3];
     float specular;
     float metallic, roughness, ior, sigma_a;
+    float abbe, tilt;        // glass dispersion / absorption tilt (spectral mode)
+    float pad[2];
 };
-static_assert(sizeof(MaterialRec) == 48, "MaterialRec must be 48 bytes");
+static_assert(sizeof(MaterialRec) == 64, "MaterialRec must be 64 bytes");
 
 }  // namespace ar

@@ -30,9 +30,15 @@ __device__ __forceinline__ float4 f4(f3 a, float w) { return make_float4(a.x, a.
 __constant__ float c_eps_tab[9];
 
 // ------------------------------------------------------------------ shading helpers
+// Shading inputs of a hit.  In spectral mode albedo and emissive hold the
+// colour's response at the path's wavelength in all three components, ior and
+// sigma_a their values at that wavelength, and `spectral` selects the scalar
+// forms of the few expressions that mix channels (GGX lobe probability).
 struct GB {
     f3 albedo, emissive;
     float specular, metallic, roughness, ior, sigma_a;
+    float abbe, tilt;
+    bool spectral;
 };
 
 __device__ __forceinline__ GB load_gb(const MaterialRec& m)
@@ -41,7 +47,16 @@ __device__ __forceinline__ GB load_gb(const MaterialRec& m)
     g.albedo = mk(m.albedo[0], m.albedo[1], m.albedo[2]);
     g.emissive = mk(m.emissive[0], m.emissive[1], m.emissive[2]);
     g.specular = m.specular; g.metallic = m.metallic; g.roughness = m.roughness; g.ior = m.ior; g.sigma_a = m.sigma_a;
+    g.abbe = m.abbe; g.tilt = m.tilt;
+    g.spectral = false;
     return g;
+}
+
+// GGX lobe-selection probability: clamp(luminance(F0)) in RGB, clamp(F0) at one
+// wavelength (material.cuh:283-289, 372-378).
+__device__ __forceinline__ float ggx_pspec(const GB& g, f3 F0)
+{
+    return clampf(g.spectral ? F0.x : luminance(F0), 0.1f, 0.9f);
 }
 
 // BuildTangentBasis / BuildTangentBasisRandom (vector.cuh:264-283)
@@ -225,7 +240,7 @@ __device__ __forceinline__ float bsdf_pdf(int model, const GB& g, f3 N, f3 rayDi
         float alpha, kD;
         f3 F0;
         ggx_params(g, alpha, kD, F0);
-        const float pSpec = clampf(luminance(F0), 0.1f, 0.9f);
+        const float pSpec = ggx_pspec(g, F0);
         const float pdfSpec = ggx_vndf_pdf(V, N, L, alpha);
         const float pdfDiff = NoL * (1.0f / kPi);
         return fmaxf(0.0f, pSpec * pdfSpec + (1.0f - pSpec) * pdfDiff);

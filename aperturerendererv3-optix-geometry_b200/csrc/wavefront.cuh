@@ -23,6 +23,7 @@
 #include <cstdint>
 
 #include "../../include/aperture_b200.h"
+#include "spectral.cuh"
 #include "traverse.cuh"
 
 namespace ar {
@@ -37,8 +38,8 @@ constexpr int kShadeBuckets = 5;  // miss, then shading model + 1
 struct alignas(16) PathRec {
     float4 o;     // ray origin xyz; w: depth | nonDeltaDepth << 16 (int bits)
     float4 d;     // ray direction xyz; w: flags | media depth << 8 (int bits)
-    float4 mask;  // throughput rgb; w: pixel (int bits)
-    float4 rad;   // radiance rgb; w: sample index (int bits)
+    float4 mask;  // throughput rgb (spectral: x throughput, y wavelength, z its pdf); w: pixel (int bits)
+    float4 rad;   // radiance rgb (spectral: x); w: sample index (int bits)
     uint4 rng0;   // xorwow d, v0, v1, v2
     uint4 rng1;   // xorwow v3, v4; z media object; w uniforms consumed
     float4 prev;  // previous NEE vertex xyz; w previous BSDF pdf
@@ -54,7 +55,7 @@ struct alignas(16) ShadowRec {
 
 struct alignas(16) RetireRec {
     float4 rad;   // radiance rgb; w pixel (int bits)
-    int4 meta;    // x sample index, y uniforms consumed
+    int4 meta;    // x sample index, y uniforms consumed, z/w wavelength and pdf bits (spectral)
 };
 
 // Control block of the path pool (device memory).
@@ -99,6 +100,8 @@ struct FrameParams {
     uint64_t seed;
     uint64_t frame0;         // TOTAL_FRAME_INDEX of the first sample
     float eps_tab[9];        // INTERSECT_EPS(0..8)
+    int32_t spectral;        // 1: one hero wavelength per path, XYZ output
+    SpectralView spec;       // tables and lookup tables of the spectral mode
 };
 
 }  // namespace ar

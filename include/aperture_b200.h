@@ -126,6 +126,10 @@ typedef struct ar_render_params {
     uint64_t seed;         /* GLOBAL_SEED (reference: 0x9e3779b97f4a7c15)            */
     int32_t sort_rays;     /* 1 = sort extension rays by material/direction octant  */
     int32_t wave_paths;    /* paths in flight per wave; 0 = automatic                */
+    int32_t spectral;      /* 1 = USE_SPECTRUM_RENDERING: one hero wavelength per path
+                              (SampleCIE1931), output linear CIE XYZ; needs
+                              ar_scene_set_spectral.  0 = RGB                        */
+    int32_t reserved;
 } ar_render_params;
 
 /* Per-path record of ar_render_debug_paths (one per pixel and sample). */
@@ -250,6 +254,20 @@ ar_status ar_render_debug_paths(ar_scene* scene, const ar_camera* camera,
  * major.  Lets a CPU replay consume exactly the GPU's sample sequence. */
 ar_status ar_rng_tape(const ar_camera* camera, const ar_render_params* params, int32_t per_path,
                       float* out, int32_t mem_kind, void* stream);
+
+/* Spectral mode set-up for a scene (SceneRenderer::SetupSpectrumLUT,
+ * core/scene.cu; spectrum_lut.cuh:12-79): `tables` holds, as float32, the
+ * reference's CIE 1931 colour matching functions (421 x 3, 360..780 nm), its
+ * D65 spectrum (421) and the weights of its two spectrum-basis networks
+ * (spectrum_basis.cuh: RGB_IN_W/B, RGB_BLK0..6_W/B, RGB_OUT_W, LAM_BLK0..6_W/B,
+ * LAM_OUT_W), 17780 values in that order.  The wavelength lookup table (840
+ * entries) and the RGB lookup table (lut_res^3 entries; the reference's
+ * SPECTRUM_RGB_LUT_RES is 512) are then built on the scene's device. */
+ar_status ar_scene_set_spectral(ar_scene* scene, const float* tables, size_t count, int32_t lut_res);
+
+/* Copies of the spectral lookup tables (840 x 4 and lut_res^3 x 4 floats, x
+ * fastest); either pointer may be NULL. */
+ar_status ar_scene_get_spectral_luts(const ar_scene* scene, float* lambda_lut, float* rgb_lut);
 
 /* Running-mean resolve for progressive rendering: out[i] = (float)(accum[i] *
  * scale) for n values (scale = 1 / samples so far).  With ar_render's FP64

@@ -134,6 +134,10 @@ struct or_scene {
     OObj* o;
     float** vols;          /* SDF volume grids (float copies) */
     int nvol;
+    float* spec_tab;       /* spectral tables (or_scene_set_spectral) */
+    float* lut_lam;        /* 840 x 4 */
+    float* lut_rgb;        /* res^3 x 4 */
+    int spec_res;
     ONode* nodes;
     int nn, cap;
     int* idx;
@@ -534,6 +538,7 @@ void or_scene_destroy(or_scene* s)
     if (!s) return;
     for (int v = 0; v < s->nvol; ++v) free(s->vols[v]);
     free(s->vols);
+    free(s->spec_tab); free(s->lut_lam); free(s->lut_rgb);
     free(s->o); free(s->nodes); free(s->idx); free(s->lobj); free(s->lprob); free(s);
 }
 
@@ -562,9 +567,11 @@ typedef struct {
     float dist;
     V3 pos, nrm;
     int inside;
-    /* GBuffer fields used by shading */
+    /* GBuffer fields used by shading (spectral: responses at the path's
+     * wavelength in all three components) */
     V3 albedo, emissive;
     float specular, metallic, roughness, ior, sigma_a;
+    int spectral;
 } Isect;
 
 static void gbuffer_default(Isect* c)
@@ -1224,7 +1231,7 @@ static SCtx sample_bsdf(Rng* g, int model, V3 rayDir, const Isect* ic, const Med
         if (NoV <= 0.0f) { r.terminate = 1; return r; }
         float alpha, kD; V3 F0;
         bsdf_ggx_params(ic, &alpha, &kD, &F0);
-        const float pSpec = clampf_(luminance3(F0), 0.1f, 0.9f);
+        const float pSpec = clampf_(ic->spectral ? F0.x : luminance3(F0), 0.1f, 0.9f);
         const float u = rng1(g);
         if (u < pSpec) {
             const float e0 = rng1(g), e1 = rng1(g), e2 = rng1(g);
@@ -1260,7 +1267,7 @@ static float bsdf_pdf(int model, const Isect* ic, V3 N, V3 rayDir, V3 L)
         if (NoV <= 0.0f || NoL <= 0.0f) return 0.0f;
         float alpha, kD; V3 F0;
         bsdf_ggx_params(ic, &alpha, &kD, &F0);
-        const float pSpec = clampf_(luminance3(F0), 0.1f, 0.9f);
+        const float pSpec = clampf_(ic->spectral ? F0.x : luminance3(F0), 0.1f, 0.9f);
         const float pdfSpec = ggx_vndf_pdf(V, N, L, alpha);
         const float pdfDiff = NoL * (1.0f / OR_PI);
         return fmaxf(0.0f, pSpec * pdfSpec + (1.0f - pSpec) * pdfDiff);
@@ -1525,6 +1532,328 @@ static int segment_occluded(const or_scene* s, float eps_d, V3 src, V3 dst, Coun
     return r.obj >= 0;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Spectral mode (core/spectrum/ of the reference, USE_SPECTRUM_RENDERING)    */
+/* ------------------------------------------------------------------------ */
+/* offsets of the table block (ar_scene_set_spectral layout) */
+enum { SP_CMF = 0, SP_D65 = 1263, SP_RGB_IN_W = 1684, SP_RGB_IN_B = 2708, SP_RGB_BLK_W = 2740,
+       SP_RGB_BLK_B = 9908, SP_RGB_OUT_W = 10132, SP_LAM_BLK_W = 10260, SP_LAM_BLK_B = 17428,
+       SP_LAM_OUT_W = 17652, SP_FLOATS = 17780, SP_LAMBDA_RES = 840 };
+#define SP_PI 3.141592654f /* CUDART_PI_F */
+
+/* D65Norm (ciexyz.cuh:67-82) */
+static float sp_d65(const float* tab, float l)
+{
+    const float* d = tab + SP_D65;
+    const float k = 1.0f / 10567.065f;
+    if (l <= 360.0f) return d[0] * k;
+    if (l >= 780.0f) return d[420] * k;
+    const float x = l - 360.0f;
+    const int i = (int)floorf(x);
+    const float t = x - (float)i;
+    return (d[i] + (d[i + 1] - d[i]) * t) * k;
+}
+/* LambdaToCIE1931_XYZ (ciexyz.cuh:522-541) */
+static V3 sp_cmf(const float* tab, float l)
+{
+    const float* c = tab + SP_CMF;
+    if (l <= 360.0f) return v3(c[0], c[1], c[2]);
+    if (l >= 780.0f) return v3(c[1260], c[1261], c[1262]);
+    const float u = (l - 360.0f) * (1.0f / 1.0f);
+    const int i = (int)u;
+    const float t = u - (float)i;
+    const float* a = c + 3 * i;
+    const float* b = a + 3;
+    return v3(a[0] + (b[0] - a[0]) * t, a[1] + (b[1] - a[1]) * t, a[2] + (b[2] - a[2]) * t);
+}
+/* erfc: Numerical Recipes 6.2 rational approximation (fractional error < 1.2e-7) */
+static float sp_erfc(float x)
+{
+    const float z = fabsf(x);
+    const float t = 1.0f / (1.0f + 0.5f * z);
+    const float p = -z * z - 1.26551223f +
+                    t * (1.00002368f + t * (0.37409196f + t * (0.09678418f + t * (-0.18628806f +
+                    t * (0.27886807f + t * (-1.13520398f + t * (1.48851587f + t * (-0.82215223f + t * 0.17087277f))))))));
+    const float r = t * om_expf(p);
+    return x >= 0.0f ? r : 2.0f - r;
+}
+/* ndtrif (sample_ciexyz.cuh:28-156): Acklam's inverse normal CDF + one Newton step */
+static float sp_ndtri(float u)
+{
+    const float uu = fminf(fmaxf(u, 0.0f), 1.0f);
+    const float pLow = 0.02425f, pHigh = 1.0f - 0.02425f;
+    float x;
+    if (uu < pLow || uu > pHigh) {
+        const float q = uu < pLow ? sqrtf(-2.0f * om_logf(uu)) : sqrtf(-2.0f * om_logf(1.0f - uu));
+        float num = fmaf(-7.784894002430293e-03f, q, -3.223964580411365e-01f);
+        num = fmaf(num, q, -2.400758277161838e+00f);
+        num = fmaf(num, q, -2.549732539343734e+00f);
+        num = fmaf(num, q, 4.374664141464968e+00f);
+        num = fmaf(num, q, 2.938163982698783e+00f);
+        float den = fmaf(7.784695709041462e-03f, q, 3.224671290700398e-01f);
+        den = fmaf(den, q, 2.445134137142996e+00f);
+        den = fmaf(den, q, 3.754408661907416e+00f);
+        den = fmaf(den, q, 1.0f);
+        x = uu < pLow ? num / den : -num / den;
+    } else {
+        const float q = uu - 0.5f;
+        const float r = q * q;
+        float num = fmaf(-3.969683028665376e+01f, r, 2.209460984245205e+02f);
+        num = fmaf(num, r, -2.759285104469687e+02f);
+        num = fmaf(num, r, 1.383577518672690e+02f);
+        num = fmaf(num, r, -3.066479806614716e+01f);
+        num = fmaf(num, r, 2.506628277459239e+00f);
+        num *= q;
+        float den = fmaf(-5.447609879822406e+01f, r, 1.615858368580409e+02f);
+        den = fmaf(den, r, -1.556989798598866e+02f);
+        den = fmaf(den, r, 6.680131188771972e+01f);
+        den = fmaf(den, r, -1.328068155288572e+01f);
+        den = fmaf(den, r, 1.0f);
+        x = num / den;
+    }
+    const float pdf = om_expf(fmaf(-0.5f, x * x, 0.0f)) * 0.3989422804014327f;
+    const float cdf = 0.5f * sp_erfc(-x * 0.7071067811865476f);
+    x -= (cdf - uu) / pdf;
+    return x;
+}
+static float sp_clamp_l(float h) { return h < 360.0f ? 360.0f : (h > 780.0f ? 780.0f : h); }
+/* single-lobe CMF fits (Wyman, Sloan, Shirley 2013; sample_ciexyz.cuh:243-279) */
+static float sp_fx(float l)
+{
+    const float k1 = (l - 595.8f) / 33.33f, k2 = (l - 446.8f) / 19.44f;
+    return 1.065f * om_expf(-0.5f * k1 * k1) + 0.366f * om_expf(-0.5f * k2 * k2);
+}
+static float sp_fy(float l) { const float k = (om_logf(l) - 6.3213077f) / 0.075f; return 1.014f * om_expf(-0.5f * k * k); }
+static float sp_fz(float l) { const float k = (om_logf(l) - 6.1088030f) / 0.051f; return 1.839f * om_expf(-0.5f * k * k); }
+/* SampleCIE1931 (sample_ciexyz.cuh:288-325) */
+static void sp_sample(float r0, float r1, float r2, float* lambda, float* pdf)
+{
+    const float total = 0.1f + 1.0f + 1.0f + 1.0f;
+    const float ur = 0.1f / total, xr = 1.0f / total, yr = 1.0f / total, zr = 1.0f / total;
+    float l;
+    if (r0 < ur) {
+        l = r1 * (780.0f - 360.0f) + 360.0f;
+    } else if (r0 < ur + xr) {
+        float h;
+        if (r1 < 0.8330258723493694f) {
+            const float t0 = 7.4884543e-13f + r2 * (0.9999999836707862f - 7.4884543e-13f);
+            h = 595.7999999999999545f + 33.3299999999999983f * sp_ndtri(t0);
+        } else {
+            const float t1 = 0.0000040030528583f + r2 * (1.0f - 0.0000040030528583f);
+            h = 446.8000000000000114f + 19.4400000000000013f * sp_ndtri(t1);
+        }
+        l = sp_clamp_l(h);
+    } else if (r0 < ur + xr + yr) {
+        const float t = 0.0000000020798312f + r1 * (0.9999953206338883f - 0.0000000020798312f);
+        l = sp_clamp_l(om_expf(6.3269327170812479f + 0.0750000000000000f * sp_ndtri(t)));
+    } else {
+        const float t = 0.0000049890553249f + r1 * (1.0f - 0.0000049890553249f);
+        l = sp_clamp_l(om_expf(6.1114040395252154f + 0.0510000000000000f * sp_ndtri(t)));
+    }
+    const float pMix = ur * 1.0f / (780.0f - 360.0f) + xr * (sp_fx(l) / 106.81109281f) + yr * (sp_fy(l) / 106.34513640f) +
+                       zr * (sp_fz(l) / 105.88243587f);
+    *lambda = l;
+    *pdf = fmaxf(pMix, 1e-16f);
+}
+/* IORFromAbbeNM / SigmaAFromTiltNM (spectrum.cuh:8-54) */
+static float sp_ior(float l, float nd, float vd)
+{
+    if (!(l > 0.0f)) return nd;
+    const float invF = 1.0f / 486.1327f, invC = 1.0f / 656.2725f, invD = 1.0f / 587.5618f;
+    const float K = (vd > 0.0f) ? (nd - 1.0f) / (vd * (invF - invC)) : 0.0f;
+    return nd + K * (1.0f / l - invD);
+}
+static float sp_sigma(float sA, float l, float tilt)
+{
+    const float invF = 1.0f / 486.1327f, invC = 1.0f / 656.2725f, invD = 1.0f / 587.5618f;
+    const float u = 1.0f / fmaxf(l, 1.0e-6f);
+    const float du = (u - invD) / (invF - invC);
+    return fmaxf(0.0f, sA * (1.0f + 1.0f * tilt * du));
+}
+/* networks (spectrum_basis.cuh:2262-2459): residual width-32 MLPs, layers
+ * accumulated in input order with fma (tensor::LinearRowMajor) */
+static void sp_block(float* h, const float* W, const float* B)
+{
+    float t[32];
+    for (int i = 0; i < 32; ++i) {
+        float a = B[i];
+        for (int j = 0; j < 32; ++j) a = fmaf(h[j], W[i * 32 + j], a);
+        t[i] = fmaxf(a, 0.0f);
+    }
+    for (int i = 0; i < 32; ++i) h[i] = h[i] + t[i];
+}
+static void sp_out(const float* h, const float* W, float* o)
+{
+    for (int i = 0; i < 4; ++i) {
+        float a = 0.0f;
+        for (int j = 0; j < 32; ++j) a = fmaf(h[j], W[i * 32 + j], a);
+        o[i] = a;
+    }
+}
+static void sp_rgb_encode(const float* tab, float r, float g, float b, float* k)
+{
+    const float scale = fmaxf(fmaxf(r, g), b);
+    const float inv = 1.0f / (scale + 0.001f);
+    const float in[3] = {r, g, b};
+    float sv[32], h[32];
+    for (int c = 0; c < 3; ++c)
+        for (int q = 0; q < 4; ++q) om_sincosf(in[c] * inv * SP_PI * (float)(q + 1), &sv[8 * c + q], &sv[8 * c + q + 4]);
+    for (int q = 0; q < 4; ++q) om_sincosf(scale * SP_PI * (float)(q + 1), &sv[24 + q], &sv[28 + q]);
+    for (int i = 0; i < 32; ++i) {
+        float a = tab[SP_RGB_IN_B + i];
+        for (int j = 0; j < 32; ++j) a = fmaf(sv[j], tab[SP_RGB_IN_W + i * 32 + j], a);
+        h[i] = fmaxf(a, 0.0f);
+    }
+    for (int blk = 0; blk < 7; ++blk) sp_block(h, tab + SP_RGB_BLK_W + blk * 1024, tab + SP_RGB_BLK_B + blk * 32);
+    sp_out(h, tab + SP_RGB_OUT_W, k);
+    for (int i = 0; i < 4; ++i) k[i] *= scale;
+}
+static void sp_lambda_encode(const float* tab, float l, float* k)
+{
+    const float x = fminf(fmaxf((l - 360.0f) / (780.0f - 360.0f), 0.0f), 1.0f);
+    float h[32];
+    for (int q = 0; q < 16; ++q) om_sincosf(x * SP_PI * (float)(q + 1), &h[q], &h[q + 16]);
+    for (int blk = 0; blk < 7; ++blk) sp_block(h, tab + SP_LAM_BLK_W + blk * 1024, tab + SP_LAM_BLK_B + blk * 32);
+    sp_out(h, tab + SP_LAM_OUT_W, k);
+}
+/* QueryLambda / QueryRGBBasis / Interact (spectrum_lut.cuh:92-236) */
+static void sp_linear(float g, int res, int* i0, int* i1, float* t)
+{
+    const float f = floorf(g);
+    *i0 = (int)f;
+    *i1 = *i0 + 1;
+    if (*i1 >= res) *i1 = res - 1;
+    *t = g - f;
+    if (*i0 == *i1) *t = 0.0f;
+}
+static void sp_query_lambda(const or_scene* s, float l, float* k)
+{
+    float u = (l - 360.0f) / (780.0f - 360.0f);
+    u = fminf(fmaxf(u, 0.0f), 1.0f);
+    float g = u * (float)SP_LAMBDA_RES - 0.5f;
+    g = fminf(fmaxf(g, 0.0f), (float)SP_LAMBDA_RES - 1.0f);
+    int i0, i1;
+    float t;
+    sp_linear(g, SP_LAMBDA_RES, &i0, &i1, &t);
+    const float w0 = 1.0f - t, w1 = t;
+    for (int q = 0; q < 4; ++q) k[q] = s->lut_lam[4 * i0 + q] * w0 + s->lut_lam[4 * i1 + q] * w1;
+}
+static void sp_acc(const float* v, float w, float* o) { for (int q = 0; q < 4; ++q) o[q] = fmaf(w, v[q], o[q]); }
+static void sp_query_rgb(const or_scene* s, V3 c, float* k)
+{
+    const int res = s->spec_res;
+    const float mx = (float)res - 1.0f;
+    const float gx = fminf(fmaxf(c.x * (float)res - 0.5f, 0.0f), mx);
+    const float gy = fminf(fmaxf(c.y * (float)res - 0.5f, 0.0f), mx);
+    const float gz = fminf(fmaxf(c.z * (float)res - 0.5f, 0.0f), mx);
+    int x0, x1, y0, y1, z0, z1;
+    float tx, ty, tz;
+    sp_linear(gx, res, &x0, &x1, &tx);
+    sp_linear(gy, res, &y0, &y1, &ty);
+    sp_linear(gz, res, &z0, &z1, &tz);
+    const float wx0 = 1.0f - tx, wx1 = tx, wy0 = 1.0f - ty, wy1 = ty, wz0 = 1.0f - tz, wz1 = tz;
+    const float* L = s->lut_rgb;
+    const size_t sy = (size_t)res, sz = (size_t)res * res;
+    k[0] = k[1] = k[2] = k[3] = 0.0f;
+    sp_acc(L + 4 * (x0 + y0 * sy + z0 * sz), wx0 * wy0 * wz0, k);
+    sp_acc(L + 4 * (x1 + y0 * sy + z0 * sz), wx1 * wy0 * wz0, k);
+    sp_acc(L + 4 * (x0 + y1 * sy + z0 * sz), wx0 * wy1 * wz0, k);
+    sp_acc(L + 4 * (x1 + y1 * sy + z0 * sz), wx1 * wy1 * wz0, k);
+    sp_acc(L + 4 * (x0 + y0 * sy + z1 * sz), wx0 * wy0 * wz1, k);
+    sp_acc(L + 4 * (x1 + y0 * sy + z1 * sz), wx1 * wy0 * wz1, k);
+    sp_acc(L + 4 * (x0 + y1 * sy + z1 * sz), wx0 * wy1 * wz1, k);
+    sp_acc(L + 4 * (x1 + y1 * sy + z1 * sz), wx1 * wy1 * wz1, k);
+}
+static float sp_dot(const float* a, const float* b)
+{
+    float acc = 0.0f;
+    for (int i = 0; i < 4; ++i) acc = fmaf(a[i], b[i], acc);
+    return fminf(fmaxf(acc, 0.0f), 1.0f);
+}
+static float sp_interact(const or_scene* s, const float* lk, V3 rgb)
+{
+    const float lum = fmaxf(rgb.x, fmaxf(rgb.y, rgb.z));
+    float k[4];
+    if (lum > 1.0f) {
+        sp_query_rgb(s, v3(rgb.x / lum, rgb.y / lum, rgb.z / lum), k);
+        return sp_dot(k, lk) * lum;
+    }
+    sp_query_rgb(s, rgb, k);
+    return sp_dot(k, lk);
+}
+
+/* Spectral tables and the lookup tables built from them (PrecomputeRGBLUTKernel /
+ * PrecomputeLambdaLUTKernel, spectrum_lut.cuh:12-58). */
+int or_scene_set_spectral(or_scene* s, const float* tables, size_t count, int res, int threads)
+{
+    if (count != SP_FLOATS || res < 2 || res > 512) return -1;
+    free(s->spec_tab); free(s->lut_lam); free(s->lut_rgb);
+    s->spec_tab = (float*)malloc(count * sizeof(float));
+    memcpy(s->spec_tab, tables, count * sizeof(float));
+    s->lut_lam = (float*)malloc(SP_LAMBDA_RES * 4 * sizeof(float));
+    const size_t nrgb = (size_t)res * res * res;
+    s->lut_rgb = (float*)malloc(nrgb * 4 * sizeof(float));
+    s->spec_res = res;
+    const float step = (780.0f - 360.0f) / (float)SP_LAMBDA_RES;
+    for (int i = 0; i < SP_LAMBDA_RES; ++i) sp_lambda_encode(s->spec_tab, 360.0f + ((float)i + 0.5f) * step, s->lut_lam + 4 * i);
+    const float invRes = 1.0f / (float)res;
+#ifdef _OPENMP
+    const int nthreads = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+#endif
+    for (int64_t v = 0; v < (int64_t)nrgb; ++v) {
+        const int x = (int)(v % res), y = (int)((v / res) % res), z = (int)(v / ((int64_t)res * res));
+        sp_rgb_encode(s->spec_tab, ((float)x + 0.5f) * invRes, ((float)y + 0.5f) * invRes, ((float)z + 0.5f) * invRes,
+                      s->lut_rgb + 4 * v);
+    }
+    return 0;
+}
+void or_spectral_luts(const or_scene* s, float* lam, float* rgb)
+{
+    if (lam) memcpy(lam, s->lut_lam, SP_LAMBDA_RES * 4 * sizeof(float));
+    if (rgb) memcpy(rgb, s->lut_rgb, (size_t)s->spec_res * s->spec_res * s->spec_res * 4 * sizeof(float));
+}
+void or_spectral_sample(const float* u3, int64_t n, float* lambda, float* pdf)
+{
+    for (int64_t i = 0; i < n; ++i) sp_sample(u3[3 * i], u3[3 * i + 1], u3[3 * i + 2], &lambda[i], &pdf[i]);
+}
+void or_spectral_encode(const float* tables, const float* rgb, const float* lambda, int64_t n, float* rgb_k, float* lam_k)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        if (rgb) sp_rgb_encode(tables, rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2], rgb_k + 4 * i);
+        if (lambda) sp_lambda_encode(tables, lambda[i], lam_k + 4 * i);
+    }
+}
+/* Interact at wavelengths lambda[i] of colours rgb[i] through the scene's tables;
+ * also D65Norm and the colour matching functions there. */
+void or_spectral_interact(const or_scene* s, const float* lambda, const float* rgb, int64_t n, float* resp, float* d65,
+                          float* xyz)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        float lk[4];
+        sp_query_lambda(s, lambda[i], lk);
+        resp[i] = sp_interact(s, lk, v3(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2]));
+        d65[i] = sp_d65(s->spec_tab, lambda[i]);
+        const V3 c = sp_cmf(s->spec_tab, lambda[i]);
+        xyz[3 * i] = c.x; xyz[3 * i + 1] = c.y; xyz[3 * i + 2] = c.z;
+    }
+}
+
+/* the path's wavelength and the values that follow from it */
+typedef struct { int on; float lambda, pdf, d65; float lk[4]; } Spec;
+
+/* the hit's G-buffer at the path's wavelength (EvaluateMaterial, spectral) */
+static void sp_apply(const or_scene* s, const Spec* sp, Isect* ic, const ar_material* m)
+{
+    const float a = sp_interact(s, sp->lk, ic->albedo);
+    const float e = sp_interact(s, sp->lk, ic->emissive);
+    ic->albedo = v3(a, a, a);
+    ic->emissive = v3(e, e, e);
+    ic->ior = sp_ior(sp->lambda, ic->ior, m->abbe_number);
+    ic->sigma_a = sp_sigma(ic->sigma_a, sp->lambda, m->tilt_number);
+    ic->spectral = 1;
+}
+
 typedef struct { V3 radiance; int segments, nee_rays, nee_mask; int hits[AR_DEBUG_MAX_HITS]; } PathOut;
 
 /* CalculateRadiance<bUseBVH=true, bUseNEE, bUsePathGuiding=false>, RGB
@@ -1534,6 +1863,16 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
                                Rng* g, V3 ro, V3 rd, PathOut* po, Counters* cnt)
 {
     int nonDelta = 0;
+    Spec sp;
+    memset(&sp, 0, sizeof(sp));
+    sp.d65 = 1.0f;
+    if (p->spectral && s->spec_tab) {  /* SampleCIE1931(Rand3(seed)) (render.cuh:467-473) */
+        const float r0 = rng1(g), r1 = rng1(g), r2 = rng1(g);
+        sp.on = 1;
+        sp_sample(r0, r1, r2, &sp.lambda, &sp.pdf);
+        sp_query_lambda(s, sp.lambda, sp.lk);
+        sp.d65 = sp_d65(s->spec_tab, sp.lambda);
+    }
     rd = vnormalize(rd);
     V3 radiance = v3(0.0f, 0.0f, 0.0f);
     V3 mask = v3(1.0f, 1.0f, 1.0f);
@@ -1578,6 +1917,7 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
         }
         if (hit) {
             model = s->o[ic.obj].mat.shading_model;
+            if (sp.on) sp_apply(s, &sp, &ic, &s->o[ic.obj].mat);
             const SCtx sb = sample_bsdf(g, model, crd, &ic, &media);
             sc = sb;
             sc.media.obj = ic.obj;
@@ -1589,6 +1929,7 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
             sc.next = crd;
             sc.pdf = 1.0f;
             sc.emis = sky_lighting(crd, p->sky);
+            if (sp.on) { const float e = sp_interact(s, sp.lk, sc.emis); sc.emis = v3(e, e, e); }
             sc.media.inside = 0;
         }
         {
@@ -1601,7 +1942,7 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
         media = sc.media;
         /* ---- emission (render.cuh:648-723) ---- */
         if (!hit) {
-            if (!sc.miss_thin) radiance = vadd(radiance, vmul(mask, sc.emis));
+            if (!sc.miss_thin) radiance = vadd(radiance, vscale(vmul(mask, sc.emis), sp.d65));
         } else if (ic.light >= 0) {
             float misW = 1.0f;
             if (p->use_nee && depth > 0 && prevDidNEE) {
@@ -1609,16 +1950,17 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
                 const float pL = pdf_light_from_hit(s, ic.obj, prevPos, ic.pos, ic.nrm);
                 if (pL >= 0.0f && pB > 0.0f) misW = power_heuristic(pB, pL);
             }
-            radiance = vadd(radiance, vscale(vmul(mask, sc.emis), misW));
+            radiance = vadd(radiance, vscale(vscale(vmul(mask, sc.emis), sp.d65), misW));
         }
         if ((!hit && !sc.miss_thin) || sc.terminate) break;
         /* ---- NEE (render.cuh:766-827) ---- */
         if (!sc.miss_thin) {
-            const float lum = luminance3(mask);
+            const float lum = sp.on ? mask.x : luminance3(mask);
             const float useNEERate = sqrtf(saturatef_(lum));
             int neeValid = 0;
             if (p->use_nee && nonDelta < 10 && !sc.delta && !media.inside && rng1(g) < useNEERate) {
-                const LSmp ls = sample_light(s, ic.pos, g);
+                LSmp ls = sample_light(s, ic.pos, g);
+                if (sp.on) { const float e = sp_interact(s, sp.lk, ls.emis); ls.emis = v3(e, e, e); }
                 if (ls.valid) {
                     const float pATotal = fmaxf(1e-20f, ls.pA * ls.pFacet);
                     const V3 lu = vsub(ls.p, ic.pos);
@@ -1645,7 +1987,7 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
                             const float pL = area_to_solid_angle(ic.pos, ls.p, ls.n, ls.pFacet * ls.pA);
                             const float pB = fmaxf(bsdf_pdf(model, &ic, ic.nrm, crd, ld), 0.0f);
                             const float w = power_heuristic(pL, pB);
-                            radiance = vadd(radiance, vmul(mask, vscale(contrib, w)));
+                            radiance = vadd(radiance, vscale(vmul(mask, vscale(contrib, w)), sp.d65));
                         }
                     }
                 }
@@ -1658,8 +2000,8 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
                               sc.brdf.z / fmaxf(sc.pdf, 1e-12f));
         float q = 1.0f;
         if (nonDelta >= p->rr_depth) {
-            const float lum = luminance3(mask);
-            const float mx = max3f(mask);
+            const float lum = sp.on ? mask.x : luminance3(mask);
+            const float mx = sp.on ? mask.x : max3f(mask);
             const float basic = clampf_(lum * 0.5f + mx * 0.5f, 0.05f, 0.95f);
             q = lerpf_(basic, 1.0f, media.inside ? 0.99f : 0.0f);
             if (rng1(g) > q) break;
@@ -1670,9 +2012,15 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
         crd = sc.next;
         if (!sc.delta) nonDelta++;
     }
-    /* checkNanInf + clamp (render.cuh:969), max(0, .) (scene.cu:238) */
-    V3 out = v3(clampf_(fix_nan_inf(radiance.x), 0.0f, 1.0e3f), clampf_(fix_nan_inf(radiance.y), 0.0f, 1.0e3f),
-                clampf_(fix_nan_inf(radiance.z), 0.0f, 1.0e3f));
+    /* checkNanInf + clamp (render.cuh:966-969), max(0, .) (scene.cu:238); spectral:
+     * lambdaXYZ * radiance / pdf, linear CIE XYZ */
+    V3 v = v3(fix_nan_inf(radiance.x), fix_nan_inf(radiance.y), fix_nan_inf(radiance.z));
+    if (sp.on) {
+        const V3 c = sp_cmf(s->spec_tab, sp.lambda);
+        const float r = fix_nan_inf(radiance.x);
+        v = v3((c.x * r) / sp.pdf, (c.y * r) / sp.pdf, (c.z * r) / sp.pdf);
+    }
+    V3 out = v3(clampf_(v.x, 0.0f, 1.0e3f), clampf_(v.y, 0.0f, 1.0e3f), clampf_(v.z, 0.0f, 1.0e3f));
     po->radiance = vmaxs(out, 0.0f);
 }
 

@@ -128,6 +128,19 @@ void or_object_isect(const or_scene* s, int32_t obj, const float* rays, int64_t 
 /* The float grid of SDF volume v as an object of the scene uses it. */
 void or_volume_grid(const or_scene* s, int32_t v, float* out);
 
+/* Spectral mode: the reference's tables (17780 floats, ar_scene_set_spectral
+ * layout) and lookup tables built from them at RGB resolution res.  0 on success. */
+int or_scene_set_spectral(or_scene* s, const float* tables, size_t count, int res, int threads);
+void or_spectral_luts(const or_scene* s, float* lambda_lut, float* rgb_lut);
+/* SampleCIE1931 for n triples of uniforms. */
+void or_spectral_sample(const float* u3, int64_t n, float* lambda, float* pdf);
+/* RGBEncode of rgb[3n] and LambdaEncode of lambda[n] (either may be NULL). */
+void or_spectral_encode(const float* tables, const float* rgb, const float* lambda, int64_t n, float* rgb_k,
+                        float* lam_k);
+/* Interact, D65Norm and the colour matching functions through a scene's tables. */
+void or_spectral_interact(const or_scene* s, const float* lambda, const float* rgb, int64_t n, float* resp,
+                          float* d65, float* xyz);
+
 float or_sinf(float x);
 float or_cosf(float x);
 float or_expf(float x);

@@ -66,6 +66,12 @@ def load():
     lib.or_powf.restype = c_float
     lib.or_object_isect.argtypes = [c_void_p, c_int32, c_void_p, c_int64, c_int32, c_void_p, c_void_p, c_void_p]
     lib.or_volume_grid.argtypes = [c_void_p, c_int32, c_void_p]
+    lib.or_scene_set_spectral.argtypes = [c_void_p, c_void_p, c_size_t, c_int, c_int]
+    lib.or_scene_set_spectral.restype = c_int
+    lib.or_spectral_luts.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.or_spectral_sample.argtypes = [c_void_p, c_int64, c_void_p, c_void_p]
+    lib.or_spectral_encode.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p]
+    lib.or_spectral_interact.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p]
     lib.or_tonemap.argtypes = [c_void_p, c_int64, c_int, c_float, c_int, c_void_p]
     lib.or_trace_detail.argtypes = [c_void_p, c_void_p, c_int64, c_int] + [c_void_p] * 5 + [c_int]
     lib.or_segments_occluded.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p, c_int]
@@ -175,6 +181,27 @@ class OracleScene:
         _lib.or_volume_grid(self._h, v, _p(out))
         return out
 
+    def set_spectral(self, tables: np.ndarray, res: int = 64, threads: int = 0) -> None:
+        t = np.ascontiguousarray(tables, np.float32)
+        if _lib.or_scene_set_spectral(self._h, _p(t), t.size, res, threads) != 0:
+            raise ValueError("bad spectral tables or resolution")
+        self.spec_res = res
+
+    def spectral_luts(self):
+        lam = np.zeros((840, 4), np.float32)
+        rgb = np.zeros((self.spec_res ** 3, 4), np.float32)
+        _lib.or_spectral_luts(self._h, _p(lam), _p(rgb))
+        return lam, rgb
+
+    def spectral_interact(self, lam, rgb):
+        """(Interact response, D65Norm, CMF xyz[n,3]) at wavelengths lam for colours rgb[n,3]."""
+        lam = np.ascontiguousarray(lam, np.float32)
+        rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)
+        n = lam.size
+        resp, d65, xyz = np.empty(n, np.float32), np.empty(n, np.float32), np.empty((n, 3), np.float32)
+        _lib.or_spectral_interact(self._h, _p(lam), _p(rgb), n, _p(resp), _p(d65), _p(xyz))
+        return resp, d65, xyz
+
     def trace_brute(self, rays, any_hit=False, threads=0):
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
         n = rays.shape[0]
@@ -240,3 +267,24 @@ def tonemap(rgb: np.ndarray, tone: int, exposure: float = 1.0, xyz_input: bool =
     out = np.empty(len(rgb), np.uint32)
     load().or_tonemap(_p(rgb), len(rgb), tone, exposure, int(xyz_input), _p(out))
     return out
+
+
+def spectral_sample(u3: np.ndarray):
+    """SampleCIE1931 for uniforms u3[n, 3]: (lambda, pdf)."""
+    u3 = np.ascontiguousarray(u3, np.float32).reshape(-1, 3)
+    lam, pdf = np.empty(len(u3), np.float32), np.empty(len(u3), np.float32)
+    load().or_spectral_sample(_p(u3), len(u3), _p(lam), _p(pdf))
+    return lam, pdf
+
+
+def spectral_encode(tables: np.ndarray, rgb=None, lam=None):
+    """(RGBEncode kernels [n,4] or None, LambdaEncode kernels [n,4] or None)."""
+    t = np.ascontiguousarray(tables, np.float32)
+    n = len(rgb) if rgb is not None else len(lam)
+    rk = np.empty((n, 4), np.float32) if rgb is not None else None
+    lk = np.empty((n, 4), np.float32) if lam is not None else None
+    r = np.ascontiguousarray(rgb, np.float32) if rgb is not None else None
+    l_ = np.ascontiguousarray(lam, np.float32) if lam is not None else None
+    load().or_spectral_encode(_p(t), _p(r) if r is not None else None, _p(l_) if l_ is not None else None, n,
+                              _p(rk) if rk is not None else None, _p(lk) if lk is not None else None)
+    return rk, lk

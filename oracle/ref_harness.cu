@@ -28,6 +28,8 @@
 #include "render/intersection.cuh"
 #include "render/material.cuh"
 #include "tonemap.cuh"
+#include "spectrum/ciexyz.cuh"
+#include "spectrum/sample_ciexyz.cuh"
 
 #include "../include/aperture_b200.h"
 
@@ -286,6 +288,59 @@ void ref_fill_torus(const int32_t* dims, float R, float r, float* out)
                 const float nz = (dims[2] > 1) ? static_cast<float>(z) / static_cast<float>(dims[2] - 1) : 0.0f;
                 out[i] = f(make_float3(nx, ny, nz) - 0.5f, info);
             }
+}
+
+// Spectral pieces, on the host: RGBEncode / LambdaEncode (spectrum_basis.cuh),
+// SampleCIE1931 (sample_ciexyz.cuh), D65Norm and LambdaToCIE1931_XYZ
+// (ciexyz.cuh), and the network weights as compiled (to check their extraction).
+void ref_spectral_encode(const float* rgb, const float* lambda, int64_t n, float* rgb_k, float* lam_k)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        if (rgb) spectrum::query::RGBEncode(rgb + 3 * i, rgb_k + 4 * i);
+        if (lambda) spectrum::query::LambdaEncode(lambda + i, lam_k + 4 * i);
+    }
+}
+
+void ref_spectral_sample(const float* u3, int64_t n, float* lambda, float* pdf)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        const spectrum::sample::SpectrumSample smp =
+            spectrum::sample::SampleCIE1931(make_float3(u3[3 * i], u3[3 * i + 1], u3[3 * i + 2]));
+        lambda[i] = smp.lambda_;
+        pdf[i] = smp.pdf_;
+    }
+}
+
+void ref_spectral_weights(const float* lambda, int64_t n, float* d65, float* xyz)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        d65[i] = spectrum::D65Norm(lambda[i]);
+        const float3 c = spectrum::LambdaToCIE1931_XYZ(lambda[i]);
+        xyz[3 * i] = c.x; xyz[3 * i + 1] = c.y; xyz[3 * i + 2] = c.z;
+    }
+}
+
+// The table block in ar_scene_set_spectral order (17780 floats).
+void ref_spectral_tables(float* out)
+{
+    using namespace spectrum::query;
+    size_t o = 0;
+    auto put = [&](const float* a, size_t n) { for (size_t i = 0; i < n; ++i) out[o++] = a[i]; };
+    for (int i = 0; i < spectrum::CIEXYZ_COUNT; ++i) {
+        out[o++] = spectrum::CIEXYZ_CMF[i].x; out[o++] = spectrum::CIEXYZ_CMF[i].y; out[o++] = spectrum::CIEXYZ_CMF[i].z;
+    }
+    put(spectrum::D65_SPD, spectrum::D65_COUNT);
+    put(RGB_IN_W, 1024); put(RGB_IN_B, 32);
+    const float* rw[7] = {RGB_BLK0_W, RGB_BLK1_W, RGB_BLK2_W, RGB_BLK3_W, RGB_BLK4_W, RGB_BLK5_W, RGB_BLK6_W};
+    const float* rb[7] = {RGB_BLK0_B, RGB_BLK1_B, RGB_BLK2_B, RGB_BLK3_B, RGB_BLK4_B, RGB_BLK5_B, RGB_BLK6_B};
+    const float* lw[7] = {LAM_BLK0_W, LAM_BLK1_W, LAM_BLK2_W, LAM_BLK3_W, LAM_BLK4_W, LAM_BLK5_W, LAM_BLK6_W};
+    const float* lb[7] = {LAM_BLK0_B, LAM_BLK1_B, LAM_BLK2_B, LAM_BLK3_B, LAM_BLK4_B, LAM_BLK5_B, LAM_BLK6_B};
+    for (int k = 0; k < 7; ++k) put(rw[k], 1024);
+    for (int k = 0; k < 7; ++k) put(rb[k], 32);
+    put(RGB_OUT_W, 128);
+    for (int k = 0; k < 7; ++k) put(lw[k], 1024);
+    for (int k = 0; k < 7; ++k) put(lb[k], 32);
+    put(LAM_OUT_W, 128);
 }
 
 // INTERSECT_EPS (config.cuh:3) as the reference's host pass evaluates it.

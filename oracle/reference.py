@@ -49,6 +49,10 @@ def load():
     lib.ref_object_isect.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int64, c_int, c_void_p,
                                      c_void_p, c_void_p]
     lib.ref_fill_torus.argtypes = [c_void_p, c_float, c_float, c_void_p]
+    lib.ref_spectral_encode.argtypes = [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]
+    lib.ref_spectral_sample.argtypes = [c_void_p, c_int64, c_void_p, c_void_p]
+    lib.ref_spectral_weights.argtypes = [c_void_p, c_int64, c_void_p, c_void_p]
+    lib.ref_spectral_tables.argtypes = [c_void_p]
     lib.ref_tonemap.argtypes = [c_void_p, c_int64, c_int, c_float, c_int, c_void_p]
     lib.ref_intersect_eps.argtypes = [c_int]
     lib.ref_intersect_eps.restype = c_float
@@ -156,4 +160,35 @@ def fill_torus(dims, R: float, r: float) -> np.ndarray:
     d = np.asarray(dims, np.int32)
     out = np.empty(int(np.prod(dims)), np.float32)
     load().ref_fill_torus(_p(d), R, r, _p(out))
+    return out
+
+
+def spectral_encode(rgb=None, lam=None):
+    n = len(rgb) if rgb is not None else len(lam)
+    r = np.ascontiguousarray(rgb, np.float32) if rgb is not None else None
+    l_ = np.ascontiguousarray(lam, np.float32) if lam is not None else None
+    rk = np.empty((n, 4), np.float32) if r is not None else None
+    lk = np.empty((n, 4), np.float32) if l_ is not None else None
+    load().ref_spectral_encode(_p(r) if r is not None else None, _p(l_) if l_ is not None else None, n,
+                               _p(rk) if rk is not None else None, _p(lk) if lk is not None else None)
+    return rk, lk
+
+
+def spectral_sample(u3):
+    u3 = np.ascontiguousarray(u3, np.float32).reshape(-1, 3)
+    lam, pdf = np.empty(len(u3), np.float32), np.empty(len(u3), np.float32)
+    load().ref_spectral_sample(_p(u3), len(u3), _p(lam), _p(pdf))
+    return lam, pdf
+
+
+def spectral_weights(lam):
+    lam = np.ascontiguousarray(lam, np.float32)
+    d65, xyz = np.empty(lam.size, np.float32), np.empty((lam.size, 3), np.float32)
+    load().ref_spectral_weights(_p(lam), lam.size, _p(d65), _p(xyz))
+    return d65, xyz
+
+
+def spectral_tables() -> np.ndarray:
+    out = np.empty(17780, np.float32)
+    load().ref_spectral_tables(_p(out))
     return out

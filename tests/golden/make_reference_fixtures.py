@@ -10,7 +10,9 @@ AnyHitSegmentBVH (372-397), Overlap (399-414), BSDF_PDF (RGB,
 core/render/material.cuh:332-387), INTERSECT_EPS (core/config.cuh:3) and the
 Tonemap kernel's curves (core/tonemap.cuh) at exposure 1.7, and the SDF
 intersector (IntersectBase / sdf::IntersectSDFObject with the torus and
-volume functors, core/object/sdf/) with the grid FillSDFVolume writes.
+volume functors, core/object/sdf/) with the grid FillSDFVolume writes, and the
+spectral pieces (RGBEncode / LambdaEncode, SampleCIE1931, D65Norm,
+LambdaToCIE1931_XYZ).
 
 Scenes: config 1 (scenes.box_scene()) and a small sphere field
 (scenes.spheres_scene(n_spheres=24, n_lights=4, box=20, subdivisions=1):
@@ -144,6 +146,17 @@ def main():
         for depth in (0, 5):
             t, pos, nrm = rs.object_isect(obj, rays, depth, grid, dims)
             out[f"sdf_o{obj}_d{depth}"] = np.concatenate([t[:, None], pos, nrm], 1).astype(np.float32)
+    # spectral: the reference's encoders on its own self-test inputs, wavelength
+    # sampling for uniform triples, D65 and colour-matching weights there
+    import spectral_tables
+    tab, it, gt = spectral_tables.load()
+    rk, lk = reference.spectral_encode(it[:3].T.copy(), it[3].copy())
+    out["spec_rgb_k"], out["spec_lam_k"] = rk, lk
+    u3 = rng.random((500, 3)).astype(np.float32)
+    lam, pdf = reference.spectral_sample(u3)
+    d65, xyz = reference.spectral_weights(lam)
+    out.update({"spec_u3": u3, "spec_lambda": lam, "spec_pdf": pdf, "spec_d65": d65, "spec_xyz": xyz,
+                "spec_tables_sha256": np.frombuffer(hashlib.sha256(tab.tobytes()).digest(), np.uint8)})
     np.savez_compressed(OUT, **out)
     print(f"wrote {OUT} ({os.path.getsize(OUT)} bytes)")
 
