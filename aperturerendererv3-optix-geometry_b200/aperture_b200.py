@@ -85,7 +85,7 @@ class Camera(ctypes.Structure):
 class RenderParams(ctypes.Structure):
     _fields_ = [("spp", c_int32), ("max_depth", c_int32), ("rr_depth", c_int32), ("use_nee", c_int32),
                 ("sky", c_int32), ("frame_offset", c_int32), ("seed", c_uint64), ("sort_rays", c_int32),
-                ("wave_paths", c_int32), ("spectral", c_int32), ("reserved", c_int32)]
+                ("wave_paths", c_int32), ("spectral", c_int32), ("tri_light_nee", c_int32)]
 
 
 class PathRecord(ctypes.Structure):
@@ -187,9 +187,10 @@ def make_camera(position, direction, fov_y_deg, width, height) -> Camera:
 
 
 def make_params(spp=1, max_depth=8, rr_depth=3, use_nee=1, sky=1, frame_offset=0, seed=REFERENCE_SEED,
-                sort_rays=0, wave_paths=0, spectral=0) -> RenderParams:
+                sort_rays=0, wave_paths=0, spectral=0, tri_light_nee=0) -> RenderParams:
     return RenderParams(int(spp), int(max_depth), int(rr_depth), int(use_nee), int(sky), int(frame_offset),
-                        int(seed) & 0xFFFFFFFFFFFFFFFF, int(sort_rays), int(wave_paths), int(spectral), 0)
+                        int(seed) & 0xFFFFFFFFFFFFFFFF, int(sort_rays), int(wave_paths), int(spectral),
+                        int(tri_light_nee))
 
 
 class Scene:

@@ -219,6 +219,8 @@ ar_status check_params(const ar_render_params* p)
     if (p->rr_depth < 0) return fail(AR_ERR_INVALID_ARGUMENT, "rr_depth must be >= 0");
     if (p->frame_offset < 0) return fail(AR_ERR_INVALID_ARGUMENT, "frame_offset must be >= 0");
     if (p->spectral != 0 && p->spectral != 1) return fail(AR_ERR_INVALID_ARGUMENT, "spectral must be 0 or 1");
+    if (p->tri_light_nee != 0 && p->tri_light_nee != 1)
+        return fail(AR_ERR_INVALID_ARGUMENT, "tri_light_nee must be 0 or 1");
     return AR_OK;
 }
 
@@ -252,6 +254,7 @@ ar::FrameParams make_frame(const ar_scene* s, const ar_camera* c, const ar_rende
         fp.sky = p->sky;
         fp.seed = p->seed;
         fp.frame0 = static_cast<uint64_t>(p->frame_offset);
+        fp.tri_light_nee = p->tri_light_nee;
         if (p->spectral) {
             fp.spectral = 1;
             fp.spec.tables = s->spec_tables;
@@ -436,6 +439,7 @@ ar_status ar_scene_create_ex(const ar_object_desc* objects, size_t count, const 
         v.materials = static_cast<const ar::MaterialRec*>(own(upload(hs.materials, "materials"), hs.materials.size() * sizeof(ar::MaterialRec)));
         v.light_object = static_cast<const int32_t*>(own(upload(hs.light_object, "lights"), hs.light_object.size() * 4));
         v.light_prob = static_cast<const float*>(own(upload(hs.light_prob, "lights"), hs.light_prob.size() * 4));
+        v.light_tri = static_cast<const float4*>(own(upload(hs.light_tri, "light triangles"), hs.light_tri.size() * 16));
         {
             static const std::vector<uint32_t> jt = ar::xorwow_jump_table_2p32();
             s->jump_table = static_cast<const uint32_t*>(own(upload(jt, "rng jump table"), jt.size() * 4));

@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             float misW = 1.0f;
             if (fp.use_nee && depth > 0 && (flags & kFlagPrevNEE)) {
                 const float pB = fmaxf(pr.prev.w, 0.0f);
-                const float pL = pdf_light_from_hit(s, hr.x, xyz(pr.prev), pos, nrm);
+                const float pL = pdf_light_from_hit(s, hr.x, xyz(pr.prev), pos, nrm, fp.tri_light_nee != 0);
                 if (pL >= 0.0f && pB > 0.0f) misW = power_heuristic(pB, pL);
             }
             radiance = radiance + ((mask * emis) * d65) * misW;
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                 const float lum = kSpec ? mask.x : luminance(mask);
                 const float rate = sqrtf(saturate(lum));
                 if (fp.use_nee && nonDelta < 10 && !delta && !mInside && g.next() < rate) {
-                    LightSample ls = sample_light(s, pos, g);
+                    LightSample ls = sample_light(s, pos, g, fp.tri_light_nee != 0);
                     if (kSpec) {
                         const float e = interact(fp.spec.lut_rgb, fp.spec.res, lk, ls.emis);
                         ls.emis = mk(e, e, e);

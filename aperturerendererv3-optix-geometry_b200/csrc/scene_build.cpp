@@ -405,6 +405,20 @@ HostScene build_scene(const ar_object_desc* objs, size_t n, const ar_sdf_volume*
             }
         }
         if (d.material.shading_model == AR_MAT_LIGHT) {
+            // triangle lights: world-space vertices for the optional triangle NEE sampler
+            float4_ t0 = {0, 0, 0, 0}, t1 = {0, 0, 0, 0}, t2 = {0, 0, 0, 0};
+            if (d.type == AR_OBJ_TRIANGLE) {
+                const f3 p0 = mul(o2w, from_ar(d.tri[0].position)) + center;
+                const f3 e1 = (mul(o2w, from_ar(d.tri[1].position)) + center) - p0;
+                const f3 e2 = (mul(o2w, from_ar(d.tri[2].position)) + center) - p0;
+                const float wa = 0.5f * length(cross(e1, e2));
+                t0 = {p0.x, p0.y, p0.z, wa};
+                t1 = {e1.x, e1.y, e1.z, 0.0f};
+                t2 = {e2.x, e2.y, e2.z, 0.0f};
+            }
+            hs.light_tri.push_back(t0);
+            hs.light_tri.push_back(t1);
+            hs.light_tri.push_back(t2);
             // scene.cu:1060-1076
             oi.light = static_cast<int32_t>(hs.light_object.size());
             const float w = std::max(area * luminance(from_ar(d.material.emissive)), 1.0e-20f);

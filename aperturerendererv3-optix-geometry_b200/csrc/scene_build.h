@@ -12,6 +12,8 @@
 namespace ar {
 
 // A signed-distance volume as uploaded: float or half values, x fastest.
+struct float4_ { float x, y, z, w; };
+
 struct HostVolume {
     int dims[3] = {0, 0, 0};
     bool fp16 = false;
@@ -28,6 +30,7 @@ struct HostScene {
     std::vector<WideNode> nodes;
     std::vector<SdfRec> sdf;           // data pointers index `volumes` until upload
     std::vector<HostVolume> volumes;
+    std::vector<float4_> light_tri;        // per light: v0 + area, e1, e2 (world; triangles only)
     std::vector<int32_t> light_object;
     std::vector<float> light_prob;
     int64_t triangles = 0;

@@ -293,10 +293,23 @@ __device__ __forceinline__ float facing_weight(f3 fn, f3 fc, f3 sp, float area)
 }
 
 // NEEPDFOmegaFromHit (nee.cuh:64-151, 254-271, 313-327)
-__device__ float pdf_light_from_hit(const SceneView& s, int obj, f3 sp, f3 lp, f3 ln)
+// Face normal of light triangle l, turned towards the point p.
+__device__ __forceinline__ f3 light_tri_normal(const SceneView& s, int l, f3 p, f3 lp)
+{
+    const float4 b = s.light_tri[3 * l + 1], c = s.light_tri[3 * l + 2];
+    const f3 n = normalize(cross(mk(b.x, b.y, b.z), mk(c.x, c.y, c.z)));
+    return dot(n, p - lp) < 0.0f ? -n : n;
+}
+
+__device__ float pdf_light_from_hit(const SceneView& s, int obj, f3 sp, f3 lp, f3 ln, bool tri = false)
 {
     const ObjInfo oi = s.objects[obj];
     const float sel = s.light_prob[oi.light];
+    if (tri && oi.type == AR_OBJ_TRIANGLE) {  // extension: triangle lights, uniform area density
+        const float area = s.light_tri[3 * oi.light].w;
+        if (!(area > 0.0f)) return 0.0f;
+        return area_to_solid_angle(sp, lp, light_tri_normal(s, oi.light, sp, lp), sel * (1.0f / area));
+    }
     if (oi.type == AR_OBJ_CUBE) {
         const Analytic& an = s.analytic[oi.aux];
         Box6 b;
@@ -341,7 +354,7 @@ struct LightSample {
 };
 
 // NEESampleLight (nee.cuh:330-377) with the box and sphere samplers
-__device__ LightSample sample_light(const SceneView& s, f3 sp, Rng& g)
+__device__ LightSample sample_light(const SceneView& s, f3 sp, Rng& g, bool tri = false)
 {
     LightSample ls;
     ls.valid = false;
@@ -392,6 +405,19 @@ __device__ LightSample sample_light(const SceneView& s, f3 sp, Rng& g)
         ls.emis = mk(mr.emissive[0], mr.emissive[1], mr.emissive[2]);
         ls.pFacet = 1.0f * (vw[slot] / wsum);
         ls.pA = 1.0f / b.area[fi];
+        ls.valid = true;
+    } else if (tri && oi.type == AR_OBJ_TRIANGLE) {
+        // extension: uniform point on the triangle (square-root warp of two
+        // uniforms), two-sided emitter
+        const float4 a = s.light_tri[3 * pick], b = s.light_tri[3 * pick + 1], c = s.light_tri[3 * pick + 2];
+        if (!(a.w > 0.0f)) return ls;
+        const float u1 = g.next(), u2 = g.next();
+        const float su = sqrtf(u1);
+        ls.p = mk(a.x, a.y, a.z) + mk(b.x, b.y, b.z) * (su * (1.0f - u2)) + mk(c.x, c.y, c.z) * (su * u2);
+        ls.n = light_tri_normal(s, pick, sp, ls.p);
+        ls.emis = mk(mr.emissive[0], mr.emissive[1], mr.emissive[2]);
+        ls.pFacet = 1.0f;
+        ls.pA = 1.0f / a.w;
         ls.valid = true;
     } else if (oi.type == AR_OBJ_SPHERE) {
         const Analytic& an = s.analytic[oi.aux];

@@ -32,6 +32,7 @@ struct SceneView {
     const int32_t* light_object;
     const float* light_prob;
     const SdfRec* sdf;       // SDF objects, tested after the BVH
+    const float4* light_tri; // per light: v0 + area, e1, e2 (triangle lights)
     int32_t num_nodes;
     int32_t num_objects;
     int32_t num_lights;

@@ -101,6 +101,7 @@ struct FrameParams {
     uint64_t frame0;         // TOTAL_FRAME_INDEX of the first sample
     float eps_tab[9];        // INTERSECT_EPS(0..8)
     int32_t spectral;        // 1: one hero wavelength per path, XYZ output
+    int32_t tri_light_nee;   // 1: NEE also samples triangle lights (extension)
     SpectralView spec;       // tables and lookup tables of the spectral mode
 };
 

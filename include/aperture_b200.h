@@ -129,7 +129,10 @@ typedef struct ar_render_params {
     int32_t spectral;      /* 1 = USE_SPECTRUM_RENDERING: one hero wavelength per path
                               (SampleCIE1931), output linear CIE XYZ; needs
                               ar_scene_set_spectral.  0 = RGB                        */
-    int32_t reserved;
+    int32_t tri_light_nee; /* 1 = NEE also samples emissive triangles (uniform area
+                              sampling, two-sided, MIS with BSDF hits).  The
+                              reference samples cube and sphere lights only
+                              (nee.cuh:362-369), which 0 reproduces.               */
 } ar_render_params;
 
 /* Per-path record of ar_render_debug_paths (one per pixel and sample). */

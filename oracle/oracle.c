@@ -1427,7 +1427,33 @@ static LSmp sample_sphere(Rng* g, const OObj* o, V3 cp)
 }
 
 /* NEESampleLight (nee.cuh:330-377) */
-static LSmp sample_light(const or_scene* s, V3 sp, Rng* g)
+/* Extension (not in the reference): emissive triangles as NEE lights, a
+ * uniform point by the square-root warp, two-sided (normal turned to p). */
+static V3 tri_light_normal(const OObj* o, V3 p, V3 lp)
+{
+    const V3 n = vnormalize(cross3(vsub(o->p1, o->p0), vsub(o->p2, o->p0)));
+    return dot3(n, vsub(p, lp)) < 0.0f ? vneg(n) : n;
+}
+static float tri_light_area(const OObj* o) { return 0.5f * len3(cross3(vsub(o->p1, o->p0), vsub(o->p2, o->p0))); }
+static LSmp sample_triangle(Rng* g, const OObj* o, V3 sp)
+{
+    LSmp ls;
+    memset(&ls, 0, sizeof(ls));
+    const float area = tri_light_area(o);
+    if (!(area > 0.0f)) return ls;
+    const float u1 = rng1(g), u2 = rng1(g);
+    const float su = sqrtf(u1);
+    const V3 e1 = vsub(o->p1, o->p0), e2 = vsub(o->p2, o->p0);
+    ls.p = vadd(vadd(o->p0, vscale(e1, su * (1.0f - u2))), vscale(e2, su * u2));
+    ls.n = tri_light_normal(o, sp, ls.p);
+    ls.emis = from_ar(o->mat.emissive);
+    ls.pFacet = 1.0f;
+    ls.pA = 1.0f / area;
+    ls.valid = 1;
+    return ls;
+}
+
+static LSmp sample_light(const or_scene* s, V3 sp, Rng* g, int tri)
 {
     LSmp none;
     memset(&none, 0, sizeof(none));
@@ -1447,18 +1473,25 @@ static LSmp sample_light(const or_scene* s, V3 sp, Rng* g)
     LSmp ls = none;
     if (lo->type == AR_OBJ_CUBE) ls = sample_box(g, lo, sp);
     else if (lo->type == AR_OBJ_SPHERE) ls = sample_sphere(g, lo, sp);
+    else if (tri && lo->type == AR_OBJ_TRIANGLE) ls = sample_triangle(g, lo, sp);
     if (!ls.valid) return none;
     ls.obj = s->lobj[pick];
     ls.pFacet = ls.pFacet * pprob;
     return ls;
 }
 
-static float pdf_light_from_hit(const or_scene* s, int obj, V3 sp, V3 lp, V3 ln)
+static float area_to_solid_angle(V3 sp, V3 lp, V3 ln, float pA);
+static float pdf_light_from_hit(const or_scene* s, int obj, V3 sp, V3 lp, V3 ln, int tri)
 {
     const OObj* o = &s->o[obj];
     const float sel = s->lprob[o->light_index];
     if (o->type == AR_OBJ_CUBE) return pdf_box(o, sel, sp, lp, ln);
     if (o->type == AR_OBJ_SPHERE) return pdf_sphere(o, sel, sp, lp, ln);
+    if (tri && o->type == AR_OBJ_TRIANGLE) {
+        const float area = tri_light_area(o);
+        if (!(area > 0.0f)) return 0.0f;
+        return area_to_solid_angle(sp, lp, tri_light_normal(o, sp, lp), sel * (1.0f / area));
+    }
     return 0.0f;
 }
 
@@ -1947,7 +1980,7 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
             float misW = 1.0f;
             if (p->use_nee && depth > 0 && prevDidNEE) {
                 const float pB = fmaxf(prevPdf, 0.0f);
-                const float pL = pdf_light_from_hit(s, ic.obj, prevPos, ic.pos, ic.nrm);
+                const float pL = pdf_light_from_hit(s, ic.obj, prevPos, ic.pos, ic.nrm, p->tri_light_nee);
                 if (pL >= 0.0f && pB > 0.0f) misW = power_heuristic(pB, pL);
             }
             radiance = vadd(radiance, vscale(vscale(vmul(mask, sc.emis), sp.d65), misW));
@@ -1959,7 +1992,7 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
             const float useNEERate = sqrtf(saturatef_(lum));
             int neeValid = 0;
             if (p->use_nee && nonDelta < 10 && !sc.delta && !media.inside && rng1(g) < useNEERate) {
-                LSmp ls = sample_light(s, ic.pos, g);
+                LSmp ls = sample_light(s, ic.pos, g, p->tri_light_nee);
                 if (sp.on) { const float e = sp_interact(s, sp.lk, ls.emis); ls.emis = v3(e, e, e); }
                 if (ls.valid) {
                     const float pATotal = fmaxf(1e-20f, ls.pA * ls.pFacet);
