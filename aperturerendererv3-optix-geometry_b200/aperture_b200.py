@@ -108,6 +108,17 @@ class RenderStats(ctypes.Structure):
 
 assert ctypes.sizeof(ObjectDesc) == 208
 assert ctypes.sizeof(PathRecord) == 96
+class Job(ctypes.Structure):
+    _fields_ = [("scene", c_void_p), ("camera", Camera), ("params", RenderParams), ("out_rgb", c_void_p),
+                ("accum", c_void_p)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("total_ms", c_float), ("iterations_per_graph", c_int32), ("paths", c_int64),
+                ("extension_rays", c_int64), ("shadow_rays", c_int64), ("graph_launches", c_int64),
+                ("graph_nodes", c_int64), ("kernel_launches", c_int64)]
+
+
 OBJECT_DTYPE = np.dtype(ObjectDesc)
 RECORD_DTYPE = np.dtype(PathRecord)
 
@@ -115,7 +126,7 @@ EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create",
                     "ar_scene_destroy",
                     "ar_scene_get_info", "ar_render", "ar_trace_rays", "ar_trace_rays_static",
                     "ar_render_debug_paths", "ar_rng_tape", "ar_tonemap", "ar_accum_resolve", "ar_tone_curve",
-                    "ar_scene_set_spectral", "ar_scene_get_spectral_luts")
+                    "ar_scene_set_spectral", "ar_scene_get_spectral_luts", "ar_render_batch")
 
 
 class ArError(RuntimeError):
@@ -167,6 +178,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_scene_set_spectral.restype = c_int32
     lib.ar_scene_get_spectral_luts.argtypes = [c_void_p, c_void_p, c_void_p]
     lib.ar_scene_get_spectral_luts.restype = c_int32
+    lib.ar_render_batch.argtypes = [c_void_p, c_int32, c_int32, c_int64, POINTER(BatchStats), c_void_p]
+    lib.ar_render_batch.restype = c_int32
     _lib = lib
     return lib
 
@@ -338,3 +351,18 @@ def make_volume(dims, data: np.ndarray | None = None, precision: int = 32, fill_
     v.fill_kind = fill_kind
     v.fill_info[:] = [float(x) for x in fill_info]
     return v, keep
+
+
+def render_batch(jobs, iterations_per_graph: int = 0, path_budget: int = 0, stream: int = 0) -> BatchStats:
+    """jobs: sequence of (Scene, Camera, RenderParams, out_rgb device pointer, accum device pointer or None)."""
+    lib = load_library()
+    arr = (Job * len(jobs))()
+    for k, (scene, cam, params, out_ptr, acc_ptr) in enumerate(jobs):
+        arr[k].scene = scene.handle
+        arr[k].camera = cam
+        arr[k].params = params
+        arr[k].out_rgb = out_ptr
+        arr[k].accum = acc_ptr
+    st = BatchStats()
+    _check(lib.ar_render_batch(arr, len(jobs), iterations_per_graph, path_budget, ctypes.byref(st), c_void_p(stream)))
+    return st

@@ -598,6 +598,224 @@ ar_status ar_scene_get_spectral_luts(const ar_scene* s, float* lambda_lut, float
     AR_GUARD_END
 }
 
+// ------------------------------------------------------------------ batches
+namespace {
+
+// Workspace of one job of a batch (the same layout as a scene's own).
+struct JobWs {
+    char* mem = nullptr;
+    ar::PathBuffers B{};
+    uint4* base0 = nullptr;
+    uint2* base1 = nullptr;
+    double* accum = nullptr;
+    ar::PoolCtl* ctl = nullptr;
+    unsigned long long* stats = nullptr;
+    int* err = nullptr;
+    uint32_t* ovf = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    ar::FrameParams fp{};
+    int64_t total = 0, pool = 0, npix = 0;
+    int cur = 0;
+};
+
+void job_alloc(JobWs& w, int64_t pool, int64_t npix, int grid_trace)
+{
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
+    const size_t W = static_cast<size_t>(pool), N = static_cast<size_t>(npix);
+    const size_t o_p0 = take(sizeof(ar::PathRec) * W), o_p1 = take(sizeof(ar::PathRec) * W);
+    const size_t o_hit = take(16 * W), o_qsh = take(4 * W * ar::kShadeBuckets);
+    const size_t o_sh = take(sizeof(ar::ShadowRec) * W), o_rt = take(sizeof(ar::RetireRec) * W);
+    const size_t o_b0 = take(16 * N), o_b1 = take(8 * N), o_acc = take(24 * N);
+    const size_t o_cnt = take(sizeof(ar::PoolCtl)), o_stats = take(64), o_err = take(64);
+    const size_t o_ovf = take(static_cast<size_t>(grid_trace) * ar::kTraceBlock * ar::kStackOverflow * 4);
+    w.mem = dalloc<char>(off, "batch job workspace");
+    char* b = w.mem;
+    w.B.pool[0] = reinterpret_cast<ar::PathRec*>(b + o_p0);
+    w.B.pool[1] = reinterpret_cast<ar::PathRec*>(b + o_p1);
+    w.B.hit = reinterpret_cast<int4*>(b + o_hit);
+    w.B.qsh = reinterpret_cast<int32_t*>(b + o_qsh);
+    w.B.shadow = reinterpret_cast<ar::ShadowRec*>(b + o_sh);
+    w.B.retire = reinterpret_cast<ar::RetireRec*>(b + o_rt);
+    w.B.capacity = static_cast<int32_t>(pool);
+    w.base0 = reinterpret_cast<uint4*>(b + o_b0);
+    w.base1 = reinterpret_cast<uint2*>(b + o_b1);
+    w.accum = reinterpret_cast<double*>(b + o_acc);
+    w.ctl = reinterpret_cast<ar::PoolCtl*>(b + o_cnt);
+    w.stats = reinterpret_cast<unsigned long long*>(b + o_stats);
+    w.err = reinterpret_cast<int*>(b + o_err);
+    w.ovf = reinterpret_cast<uint32_t*>(b + o_ovf);
+}
+
+struct BatchResources {
+    std::vector<JobWs> jobs;
+    cudaEvent_t fork = nullptr;
+    cudaStream_t orch = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t* retired_host = nullptr;
+    ~BatchResources()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (fork) cudaEventDestroy(fork);
+        if (retired_host) cudaFreeHost(retired_host);
+        if (orch) cudaStreamDestroy(orch);
+        for (JobWs& w : jobs) {
+            if (w.done) cudaEventDestroy(w.done);
+            if (w.st) cudaStreamDestroy(w.st);
+            if (w.mem) cudaFree(w.mem);
+        }
+    }
+};
+
+}  // namespace
+
+ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_per_graph, int64_t path_budget,
+                          ar_batch_stats* stats, void* stream)
+{
+    g_last_error.clear();
+    if (njobs <= 0 || !jobs) return fail(AR_ERR_INVALID_ARGUMENT, "jobs is NULL or empty");
+    if (iterations_per_graph < 0 || iterations_per_graph > 256)
+        return fail(AR_ERR_INVALID_ARGUMENT, "iterations_per_graph must be in [0, 256]");
+    const ar_scene* s0 = jobs[0].scene;
+    for (int j = 0; j < njobs; ++j) {
+        const ar_job& jb = jobs[j];
+        if (!jb.scene) return fail(AR_ERR_INVALID_ARGUMENT, "job " + std::to_string(j) + ": scene is NULL");
+        if (jb.scene->device != s0->device) return fail(AR_ERR_INVALID_ARGUMENT, "jobs span several devices");
+        if (ar_status e = check_camera(&jb.camera)) return e;
+        if (ar_status e = check_params(&jb.params)) return e;
+        if (!jb.out_rgb && !jb.accum) return fail(AR_ERR_INVALID_ARGUMENT, "job " + std::to_string(j) + ": no output");
+        if (jb.params.spectral && !jb.scene->spec_tables)
+            return fail(AR_ERR_UNSUPPORTED, "job " + std::to_string(j) + ": spectral tables not set");
+    }
+    AR_GUARD_BEGIN
+    DeviceGuard g(s0->device);
+    cudaStream_t user = static_cast<cudaStream_t>(stream);
+    int K = iterations_per_graph > 0 ? iterations_per_graph : 16;
+    K += K & 1;  // even: both pool buffers back in place after a replay
+    // In-flight paths: a shared budget split by each job's share of the work
+    // (a job never gets more than it has paths, nor fewer than 2^14).
+    int64_t totalAll = 0;
+    for (int j = 0; j < njobs; ++j)
+        totalAll += static_cast<int64_t>(jobs[j].camera.width) * jobs[j].camera.height * jobs[j].params.spp;
+    const int64_t budget = path_budget > 0 ? path_budget : (int64_t(1) << 22);
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    ck(cudaEventCreate(&t0), "event");
+    ck(cudaEventCreate(&t1), "event");
+    struct Ev { cudaEvent_t a, b; ~Ev() { cudaEventDestroy(a); cudaEventDestroy(b); } } evs{t0, t1};
+    BatchResources R;
+    R.jobs.resize(static_cast<size_t>(njobs));
+    ck(cudaMallocHost(&R.retired_host, sizeof(int64_t) * njobs), "pinned poll buffer");
+    ck(cudaEventCreateWithFlags(&R.fork, cudaEventDisableTiming), "event");
+    // the batch runs on a stream of its own (the legacy default stream cannot
+    // be captured), ordered after the caller's stream
+    ck(cudaStreamCreateWithFlags(&R.orch, cudaStreamNonBlocking), "stream");
+    cudaStream_t st = R.orch;
+    ck(cudaEventRecord(R.fork, user), "event record");
+    ck(cudaStreamWaitEvent(st, R.fork, 0), "order after caller");
+    ck(cudaEventRecord(t0, st), "event record");
+    ck(cudaEventRecord(R.fork, st), "event record");
+    for (int j = 0; j < njobs; ++j) {
+        JobWs& w = R.jobs[j];
+        const ar_job& jb = jobs[j];
+        w.npix = static_cast<int64_t>(jb.camera.width) * jb.camera.height;
+        w.total = w.npix * jb.params.spp;
+        int64_t pool = static_cast<int64_t>(static_cast<double>(budget) * static_cast<double>(w.total) /
+                                            static_cast<double>(totalAll));
+        if (jb.params.wave_paths > 0) pool = jb.params.wave_paths;
+        pool = std::max<int64_t>(std::min<int64_t>(pool, kMaxPool), int64_t(1) << 14);
+        w.pool = std::max<int64_t>(1, std::min<int64_t>(pool, w.total));
+        w.fp = make_frame(jb.scene, &jb.camera, &jb.params);
+        w.fp.pool = static_cast<int32_t>(w.pool);
+        job_alloc(w, w.pool, w.npix, jb.scene->grid_trace);
+        ck(cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking), "stream");
+        ck(cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming), "event");
+        ck(cudaStreamWaitEvent(w.st, R.fork, 0), "fork");
+        ck(cudaMemsetAsync(w.accum, 0, sizeof(double) * 3 * w.npix, w.st), "memset");
+        ck(cudaMemsetAsync(w.stats, 0, 64, w.st), "memset");
+        ck(cudaMemsetAsync(w.err, 0, 64, w.st), "memset");
+        ck(ar::launch_rng_init(w.fp, w.base0, w.base1, w.st), "rng init");
+        ck(ar::launch_pool_init(w.ctl, w.total, w.st), "pool init");
+        ck(cudaEventRecord(w.done, w.st), "event record");
+        ck(cudaStreamWaitEvent(st, w.done, 0), "join");
+    }
+    // One graph: K wavefront iterations of every job, each job on its own
+    // branch, plus the copy of every job's retired count.
+    ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    ck(cudaEventRecord(R.fork, st), "fork");
+    int64_t launches = 0;
+    for (int j = 0; j < njobs; ++j) {
+        JobWs& w = R.jobs[j];
+        const ar_job& jb = jobs[j];
+        ck(cudaStreamWaitEvent(w.st, R.fork, 0), "fork");
+        ck(ar::launch_iterations(jb.scene->view, w.fp, w.B, w.ctl, w.base0, w.base1, jb.scene->jump_table, w.stats,
+                                 w.ovf, w.err, w.accum, nullptr, K, &w.cur, jb.scene->grid_trace,
+                                 jb.scene->sm_count * 4, w.st, &launches, nullptr),
+           "capture iterations");
+        ck(cudaMemcpyAsync(R.retired_host + j, &w.ctl->retired, sizeof(int64_t), cudaMemcpyDeviceToHost, w.st),
+           "capture poll");
+        ck(cudaEventRecord(w.done, w.st), "join");
+        ck(cudaStreamWaitEvent(st, w.done, 0), "join");
+    }
+    ck(cudaStreamEndCapture(st, &R.graph), "end capture");
+    ck(cudaGraphInstantiate(&R.exec, R.graph, 0), "graph instantiate");
+    size_t nodes = 0;
+    cudaGraphGetNodes(R.graph, nullptr, &nodes);
+    int64_t maxDepth = 0, maxRatio = 0;
+    for (int j = 0; j < njobs; ++j) {
+        maxDepth = std::max<int64_t>(maxDepth, jobs[j].params.max_depth);
+        maxRatio = std::max<int64_t>(maxRatio, R.jobs[j].total / R.jobs[j].pool + 2);
+    }
+    const int64_t maxReplays = (maxRatio * (maxDepth + 2)) / K + 2;
+    int64_t replays = 0;
+    for (;;) {
+        ck(cudaGraphLaunch(R.exec, st), "graph launch");
+        ck(cudaStreamSynchronize(st), "sync");
+        ++replays;
+        bool all = true;
+        for (int j = 0; j < njobs; ++j) all = all && (R.retired_host[j] >= R.jobs[j].total);
+        if (all) break;
+        if (replays > maxReplays) return fail(AR_ERR_DEVICE_FAULT, "batch path pools did not drain");
+    }
+    // outputs, counters, error words
+    unsigned long long ext = 0, sh = 0;
+    for (int j = 0; j < njobs; ++j) {
+        JobWs& w = R.jobs[j];
+        const ar_job& jb = jobs[j];
+        const int64_t n = w.npix * 3;
+        if (jb.out_rgb) ck(ar::launch_mean(w.accum, n, 1.0 / static_cast<double>(jb.params.spp), jb.out_rgb, st), "mean");
+        if (jb.accum) ck(ar::launch_add(w.accum, n, jb.accum, st), "accumulate");
+        unsigned long long h[2];
+        int e = 0;
+        ck(cudaMemcpyAsync(h, w.stats, sizeof(h), cudaMemcpyDeviceToHost, st), "stats");
+        ck(cudaMemcpyAsync(&e, w.err, sizeof(int), cudaMemcpyDeviceToHost, st), "error word");
+        ck(cudaStreamSynchronize(st), "sync");
+        if (e != 0) return fail(AR_ERR_DEVICE_FAULT, "job " + std::to_string(j) + ": traversal stack overflow");
+        ext += h[0];
+        sh += h[1];
+    }
+    ck(cudaEventRecord(t1, st), "event record");
+    ck(cudaEventSynchronize(t1), "sync");
+    ck(cudaStreamWaitEvent(user, t1, 0), "order caller after batch");
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, t0, t1);
+        stats->total_ms = ms;
+        stats->paths = totalAll;
+        stats->extension_rays = static_cast<int64_t>(ext);
+        stats->shadow_rays = static_cast<int64_t>(sh);
+        stats->graph_launches = replays;
+        stats->graph_nodes = static_cast<int64_t>(nodes);
+        stats->kernel_launches = launches * replays;
+        stats->iterations_per_graph = K;
+    }
+    return AR_OK;
+    AR_GUARD_END
+}
+
 ar_status ar_accum_resolve(const double* accum, size_t n, double scale, float* out, int32_t mem_kind, void* stream)
 {
     g_last_error.clear();

@@ -272,6 +272,39 @@ ar_status ar_scene_set_spectral(ar_scene* scene, const float* tables, size_t cou
  * fastest); either pointer may be NULL. */
 ar_status ar_scene_get_spectral_luts(const ar_scene* scene, float* lambda_lut, float* rgb_lut);
 
+/* One job of a batch: a scene (shared between jobs if wanted), a camera, the
+ * render parameters and device outputs (mean image and/or FP64 sums added). */
+typedef struct ar_job {
+    ar_scene* scene;
+    ar_camera camera;
+    ar_render_params params;
+    float* out_rgb;        /* device, width*height*3 floats, or NULL          */
+    double* accum;         /* device, width*height*3 doubles (sums added), or NULL */
+} ar_job;
+
+typedef struct ar_batch_stats {
+    float total_ms;        /* device time of the whole batch                   */
+    int32_t iterations_per_graph;
+    int64_t paths;
+    int64_t extension_rays;
+    int64_t shadow_rays;
+    int64_t graph_launches;/* replays of the batch graph                       */
+    int64_t graph_nodes;   /* nodes of the batch graph                         */
+    int64_t kernel_launches;/* kernels run (graph nodes x replays)             */
+} ar_batch_stats;
+
+/* Many render jobs of uneven resolution, scene and spp at once (config 5 of
+ * the benchmark; the reference renders one camera at a time, scene.cu:276-306).
+ * Every job keeps its own wavefront pool; one CUDA graph holds
+ * iterations_per_graph (0 = 16; rounded up to even) wavefront iterations of
+ * every job, each job on its own branch so small jobs run side by side, and is
+ * replayed until every job has retired all of its paths.  path_budget (0 =
+ * 2^22) paths in flight are shared among the jobs by their share of the work
+ * (a job's own params.wave_paths overrides).  All scenes on one device.
+ * Outputs are written on `stream`; the call returns when they are complete. */
+ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_per_graph, int64_t path_budget,
+                          ar_batch_stats* stats, void* stream);
+
 /* Running-mean resolve for progressive rendering: out[i] = (float)(accum[i] *
  * scale) for n values (scale = 1 / samples so far).  With ar_render's FP64
  * accum this replaces the reference's per-frame FP32 running mean of the

@@ -1,0 +1,50 @@
+"""Batched jobs (ar_render_batch): uneven resolutions, spp, scenes (a shared
+scene among them), RGB and spectral jobs in one CUDA graph replayed until all
+are done.  Each job's image equals a separate ar_render of the same job:
+paths draw the same random streams whatever pool they share (per-pixel FP64
+sums, added in another order: equal to FP32 rounding)."""
+import numpy as np
+import pytest
+
+import scenes
+import spectral_tables
+from aperture_b200 import Scene, make_params, render_batch
+
+
+@pytest.mark.gpu
+def test_batch_equals_separate_renders(box_objects, small_spheres_objects):
+    import torch
+    box = Scene(box_objects)
+    sph = Scene(small_spheres_objects)
+    spectral = spectral_tables.available()
+    if spectral:
+        box.set_spectral(32)
+    cam_s = scenes.spheres_camera(72, 40)
+    cam_s.position.z = -45.0
+    specs = [
+        (box, scenes.box_camera(64, 48), make_params(spp=4, max_depth=8)),
+        (box, scenes.box_camera(33, 17), make_params(spp=16, max_depth=6, frame_offset=3)),
+        (sph, cam_s, make_params(spp=2, max_depth=10)),
+        (box, scenes.box_camera(20, 20), make_params(spp=8, max_depth=8, spectral=1 if spectral else 0)),
+        (sph, scenes.spheres_camera(16, 9), make_params(spp=1, max_depth=12, use_nee=0)),
+    ]
+    outs, jobs = [], []
+    for scene, cam, p in specs:
+        o = torch.zeros(cam.width * cam.height * 3, dtype=torch.float32, device="cuda")
+        outs.append(o)
+        jobs.append((scene, cam, p, o.data_ptr(), None))
+    st = render_batch(jobs, iterations_per_graph=6, path_budget=1 << 16)
+    torch.cuda.synchronize()
+    assert st.graph_launches >= 1 and st.graph_nodes > 5 * 10 * 6
+    assert st.paths == sum(c.width * c.height * p.spp for _, c, p in specs)
+    for (scene, cam, p), o in zip(specs, outs):
+        ref, _ = scene.render(cam, p)
+        np.testing.assert_allclose(o.cpu().numpy().reshape(cam.height, cam.width, 3), ref, rtol=1e-6, atol=1e-7)
+
+
+@pytest.mark.gpu
+def test_batch_rejects_bad_jobs(box_objects):
+    from aperture_b200 import ArError
+    s = Scene(box_objects)
+    with pytest.raises(ArError):
+        render_batch([(s, scenes.box_camera(8, 8), make_params(spp=1), None, None)])
