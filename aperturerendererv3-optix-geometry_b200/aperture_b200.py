@@ -57,6 +57,13 @@ class SdfVolume(ctypes.Structure):
                 ("fill_info", c_float * 4), ("reserved", c_int32)]
 
 
+class MediumDesc(ctypes.Structure):
+    """ar_medium_desc: a box of heterogeneous participating medium."""
+    _fields_ = [("bounds_min", c_float * 3), ("bounds_max", c_float * 3), ("sigma_t_max", c_float),
+                ("albedo", c_float * 3), ("g", c_float), ("dims", c_int32 * 3), ("precision", c_int32),
+                ("density", c_void_p)]
+
+
 SDF_TORUS, SDF_VOLUME = 0, 1
 SDF_OFFSET = ObjectDesc.tri.offset   # ar_object_desc.sdf overlays tri[0]
 
@@ -126,7 +133,8 @@ EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create",
                     "ar_scene_destroy",
                     "ar_scene_get_info", "ar_render", "ar_trace_rays", "ar_trace_rays_static",
                     "ar_render_debug_paths", "ar_rng_tape", "ar_tonemap", "ar_accum_resolve", "ar_tone_curve",
-                    "ar_scene_set_spectral", "ar_scene_get_spectral_luts", "ar_render_batch")
+                    "ar_scene_set_spectral", "ar_scene_get_spectral_luts", "ar_render_batch",
+                    "ar_scene_set_medium")
 
 
 class ArError(RuntimeError):
@@ -178,6 +186,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_scene_set_spectral.restype = c_int32
     lib.ar_scene_get_spectral_luts.argtypes = [c_void_p, c_void_p, c_void_p]
     lib.ar_scene_get_spectral_luts.restype = c_int32
+    lib.ar_scene_set_medium.argtypes = [c_void_p, c_void_p]
+    lib.ar_scene_set_medium.restype = c_int32
     lib.ar_render_batch.argtypes = [c_void_p, c_int32, c_int32, c_int64, POINTER(BatchStats), c_void_p]
     lib.ar_render_batch.restype = c_int32
     _lib = lib
@@ -204,6 +214,20 @@ def make_params(spp=1, max_depth=8, rr_depth=3, use_nee=1, sky=1, frame_offset=0
     return RenderParams(int(spp), int(max_depth), int(rr_depth), int(use_nee), int(sky), int(frame_offset),
                         int(seed) & 0xFFFFFFFFFFFFFFFF, int(sort_rays), int(wave_paths), int(spectral),
                         int(tri_light_nee))
+
+
+def medium_desc(density: np.ndarray, bounds_min, bounds_max, sigma_t_max, albedo, g) -> MediumDesc:
+    """ar_medium_desc for a [z, y, x] grid (the array must stay alive while used)."""
+    m = MediumDesc()
+    m.bounds_min[:] = [float(x) for x in bounds_min]
+    m.bounds_max[:] = [float(x) for x in bounds_max]
+    m.sigma_t_max = float(sigma_t_max)
+    m.albedo[:] = [float(x) for x in albedo]
+    m.g = float(g)
+    m.dims[:] = [density.shape[2], density.shape[1], density.shape[0]]
+    m.precision = 16 if density.dtype == np.float16 else 32
+    m.density = density.ctypes.data
+    return m
 
 
 class Scene:
@@ -234,6 +258,19 @@ class Scene:
         t = np.ascontiguousarray(tables, np.float32)
         _check(_lib.ar_scene_set_spectral(self._h, _ptr(t), t.size, lut_res))
         self.lut_res = lut_res
+
+    def set_medium(self, density, bounds_min=None, bounds_max=None, sigma_t_max: float = 0.0, albedo=None,
+                   g: float = 0.0) -> None:
+        """Attach a participating medium; density is a [z, y, x] float32 or
+        float16 array (x fastest), None removes the medium."""
+        if density is None:
+            _check(_lib.ar_scene_set_medium(self._h, None))
+            return
+        d = np.ascontiguousarray(density)
+        if d.dtype not in (np.float32, np.float16) or d.ndim != 3:
+            raise ValueError("density must be a 3-d float32 or float16 array")
+        m = medium_desc(d, bounds_min, bounds_max, sigma_t_max, albedo, g)
+        _check(_lib.ar_scene_set_medium(self._h, ctypes.byref(m)))
 
     def spectral_luts(self):
         """(lambda table [840, 4], rgb table [res^3, 4]) as built on the device."""

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -99,6 +100,7 @@ struct ar_scene {
     float4* spec_lut_lam = nullptr;
     float4* spec_lut_rgb = nullptr;
     int spec_res = 0;
+    void* medium_grid = nullptr;                // density grid of the participating medium
     std::vector<ar::SdfRec> h_sdf;              // data pointers into h_volumes
     std::vector<ar::HostVolume> h_volumes;
     // render workspace
@@ -255,6 +257,7 @@ ar::FrameParams make_frame(const ar_scene* s, const ar_camera* c, const ar_rende
         fp.seed = p->seed;
         fp.frame0 = static_cast<uint64_t>(p->frame_offset);
         fp.tri_light_nee = p->tri_light_nee;
+        fp.medium_key = medium_frame_key(fp.seed, fp.frame0);
         if (p->spectral) {
             fp.spectral = 1;
             fp.spec.tables = s->spec_tables;
@@ -295,8 +298,10 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
     LaunchTimers tm;
     LaunchTimers* tmp = stats ? &tm : nullptr;
     constexpr int kBatch = 16;
-    // every iteration retires or advances each path by one segment: a hard bound
-    const int64_t max_iter = (total / pool + 2) * (static_cast<int64_t>(p->max_depth) + 2) + kBatch;
+    // every iteration retires or advances each path by one segment and admits up
+    // to min(pool, npix) new samples (k_plan): a hard bound
+    const int64_t admit = std::max<int64_t>(1, std::min<int64_t>(pool, npix));
+    const int64_t max_iter = (total / admit + 2) * (static_cast<int64_t>(p->max_depth) + 2) + kBatch;
     int cur = 0;
     int64_t iters = 0;
     int64_t retired = 0;
@@ -581,6 +586,66 @@ ar_status ar_scene_set_spectral(ar_scene* s, const float* tables, size_t count, 
     AR_GUARD_END
 }
 
+ar_status ar_scene_set_medium(ar_scene* s, const ar_medium_desc* m)
+{
+    g_last_error.clear();
+    if (!s) return fail(AR_ERR_INVALID_ARGUMENT, "scene is NULL");
+    size_t count = 0;
+    if (m) {
+        for (int a = 0; a < 3; ++a) {
+            if (!(m->bounds_max[a] > m->bounds_min[a]) || !std::isfinite(m->bounds_min[a]) || !std::isfinite(m->bounds_max[a]))
+                return fail(AR_ERR_INVALID_ARGUMENT, "medium bounds must be finite with max > min");
+            if (m->dims[a] < 1 || m->dims[a] > 4096) return fail(AR_ERR_INVALID_ARGUMENT, "medium dims must be in [1, 4096]");
+            if (!(m->albedo[a] >= 0.0f && m->albedo[a] <= 1.0f)) return fail(AR_ERR_INVALID_ARGUMENT, "medium albedo must be in [0, 1]");
+        }
+        if (!(m->sigma_t_max >= 0.0f) || !std::isfinite(m->sigma_t_max))
+            return fail(AR_ERR_INVALID_ARGUMENT, "sigma_t_max must be finite and non-negative");
+        if (!(m->g > -1.0f && m->g < 1.0f)) return fail(AR_ERR_INVALID_ARGUMENT, "g must be in (-1, 1)");
+        if (m->precision != 16 && m->precision != 32) return fail(AR_ERR_INVALID_ARGUMENT, "precision must be 16 or 32");
+        if (!m->density) return fail(AR_ERR_INVALID_ARGUMENT, "density is NULL");
+        count = static_cast<size_t>(m->dims[0]) * m->dims[1] * m->dims[2];
+        if (count > (size_t(1) << 31)) return fail(AR_ERR_INVALID_ARGUMENT, "medium grid above 2^31 values");
+    }
+    AR_GUARD_BEGIN
+    float dmax = 0.0f;
+    for (size_t i = 0; i < count; ++i) {
+        const float v = m->precision == 16 ? __half2float(static_cast<const __half*>(m->density)[i])
+                                           : static_cast<const float*>(m->density)[i];
+        if (!(v >= 0.0f) || !std::isfinite(v)) return fail(AR_ERR_INVALID_ARGUMENT, "density values must be finite and non-negative");
+        dmax = std::max(dmax, v);
+    }
+    DeviceGuard g(s->device);
+    if (s->medium_grid) {
+        for (auto it = s->owned.begin(); it != s->owned.end(); ++it)
+            if (*it == s->medium_grid) { s->owned.erase(it); break; }
+        cudaFree(s->medium_grid);
+        s->medium_grid = nullptr;
+    }
+    s->view.has_medium = 0;
+    std::memset(&s->view.medium, 0, sizeof(s->view.medium));
+    if (!m) return AR_OK;
+    const size_t bytes = count * (m->precision == 16 ? 2 : 4);
+    unsigned char* grid = dalloc<unsigned char>(bytes, "medium grid");
+    s->owned.push_back(grid);
+    s->medium_grid = grid;
+    ck(cudaMemcpy(grid, m->density, bytes, cudaMemcpyHostToDevice), "copy medium grid");
+    ar::MediumRec& r = s->view.medium;
+    for (int a = 0; a < 3; ++a) {
+        r.bmin[a] = m->bounds_min[a];
+        r.bmax[a] = m->bounds_max[a];
+        r.albedo[a] = m->albedo[a];
+        r.dims[a] = m->dims[a];
+    }
+    r.sigma_max = m->sigma_t_max;
+    r.g = m->g;
+    r.majorant = m->sigma_t_max * dmax;
+    r.fp16 = m->precision == 16 ? 1 : 0;
+    r.data = grid;
+    s->view.has_medium = 1;
+    return AR_OK;
+    AR_GUARD_END
+}
+
 ar_status ar_scene_get_spectral_luts(const ar_scene* s, float* lambda_lut, float* rgb_lut)
 {
     g_last_error.clear();
@@ -766,7 +831,8 @@ ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_
     int64_t maxDepth = 0, maxRatio = 0;
     for (int j = 0; j < njobs; ++j) {
         maxDepth = std::max<int64_t>(maxDepth, jobs[j].params.max_depth);
-        maxRatio = std::max<int64_t>(maxRatio, R.jobs[j].total / R.jobs[j].pool + 2);
+        const int64_t admit = std::max<int64_t>(1, std::min<int64_t>(R.jobs[j].pool, R.jobs[j].npix));
+        maxRatio = std::max<int64_t>(maxRatio, R.jobs[j].total / admit + 2);
     }
     const int64_t maxReplays = (maxRatio * (maxDepth + 2)) / K + 2;
     int64_t replays = 0;

@@ -244,17 +244,31 @@ __global__ void k_regen(FrameParams fp, PathBuffers B, PoolCtl* ctl, int cur, ui
 }
 
 // ------------------------------------------------------------------ extend
-template <bool kSdf>
+// Free-flight sampling in the medium along the extension segment [0, tmax):
+// the distance of the first real collision, or -1 (out of line: only scenes
+// with a medium reach it).
+__device__ __noinline__ float medium_collision(const SceneView& s, const PathRec& pr, f3 o, f3 d, float tmax,
+                                               uint32_t key)
+{
+    HashRng h;
+    h.seed = medium_seed(key, static_cast<uint32_t>(ibits(pr.rad.w)), static_cast<uint32_t>(ibits(pr.mask.w)),
+                         static_cast<uint32_t>(ibits(pr.o.w) & 0xFFFF), 0u);
+    h.n = 0;
+    return delta_track(s.medium, o, d, tmax, h);
+}
+
+template <bool kExt>
 struct ExtendIO {
     const PathRec* pool;
     int4* hit;
     int32_t* shade_count;
     int32_t* qsh;
     int cap;
+    uint32_t medium_key;  // medium_frame_key of the render
     // queue the path for shading, bucketed by what it hit (render.cuh:97-118)
     __device__ __forceinline__ void to_shade(const SceneView& s, int k, int obj)
     {
-        const int bucket = obj >= 0 ? s.materials[s.objects[obj].material].model + 1 : 0;
+        const int bucket = obj >= 0 ? s.materials[s.objects[obj].material].model + 1 : (obj == kHitMedium ? kModelMedium + 1 : 0);
         bucket_append(shade_count, qsh, cap, bucket, k);
     }
     __device__ __forceinline__ int load(const SceneView& s, int k, RayState& r)
@@ -266,7 +280,7 @@ struct ExtendIO {
             const int mobj = static_cast<int>(pool[k].rng1.z);
             if (mobj >= 0 && s.objects[mobj].type != AR_OBJ_TRIANGLE) {
                 // solo trace of the medium's object (render.cuh:91-94, intersection.cuh:185-193)
-                const float t = (kSdf && s.objects[mobj].type == AR_OBJ_SDF) ? sdf_solo_t(s, mobj, o, d, e)
+                const float t = (kExt && s.objects[mobj].type == AR_OBJ_SDF) ? sdf_solo_t(s, mobj, o, d, e)
                                                                              : isect_analytic_t(s, mobj, o, d);
                 const bool h = t >= 0.0f && !(t < e);
                 hit[k] = h ? make_int4(mobj, -1, ibits(t), 0) : make_int4(-1, -1, 0, 0);
@@ -281,23 +295,30 @@ struct ExtendIO {
     {
         int32_t obj = r.best.obj, prim = r.best.prim;
         float t = r.best.t;
-        if (kSdf && s.num_sdf > 0) {
+        if (kExt && s.num_sdf > 0) {
             const int32_t before = obj;
             sdf_closest(s, r.o, r.d, r.tmin, c_eps_tab[min(ibits(pool[k].o.w) >> 16, 8)], &t, &obj);
             if (obj != before) prim = -1;
         }
-        hit[k] = obj >= 0 ? make_int4(obj, prim, ibits(t), 0) : make_int4(-1, -1, 0, 0);
+        if (kExt && s.has_medium && !(ibits(pool[k].d.w) & kFlagInside)) {
+            const float tc = medium_collision(s, pool[k], r.o, r.d, obj >= 0 ? t : INFINITY, medium_key);
+            if (tc >= 0.0f) { obj = kHitMedium; prim = -1; t = tc; }
+        }
+        hit[k] = obj >= 0 || obj == kHitMedium ? make_int4(obj, prim, ibits(t), 0) : make_int4(-1, -1, 0, 0);
         to_shade(s, k, obj);
     }
 };
 
-// Trace's closest-hit query (render.cuh:86-99) for every path of the pool.
-template <bool kSdf>
+// Trace's closest-hit query (render.cuh:86-99) for every path of the pool,
+// then (extension) free-flight sampling in the participating medium.
+template <bool kExt>
 __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(SceneView s, PathBuffers B, int cur, PoolCtl* ctl,
-                                                        unsigned long long* stats, uint32_t* ovf, int* err)
+                                                        unsigned long long* stats, uint32_t* ovf, int* err,
+                                                        uint32_t medium_key)
 {
     extern __shared__ uint32_t smem[];
-    ExtendIO<kSdf> io;
+    ExtendIO<kExt> io;
+    io.medium_key = medium_key;
     io.pool = pool_of(B, cur);
     io.hit = B.hit;
     io.shade_count = ctl->shade_count;
@@ -313,7 +334,7 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(SceneVi
 // the shadow query: Trace's material evaluation and hit offset, emission with
 // MIS, light sampling for NEE, throughput and Russian roulette.  kModel is the
 // shading model of every path of this launch's bucket, -1 = miss.
-template <int kModel, bool kSdf, bool kSpec>
+template <int kModel, bool kExt, bool kSpec>
 __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams fp, PathBuffers B, int cur,
                                                        PoolCtl* ctl, ar_path_record* rec)
 {
@@ -351,11 +372,12 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         const bool inside = (flags & kFlagInside) != 0;
         const f3 vloc = xyz(pr.vloc);
         const int4 hr = B.hit[k];
-        constexpr bool hit = kModel >= 0;
+        constexpr bool kMed = kModel == kModelMedium;  // collisions in the participating medium
+        constexpr bool hit = kModel >= 0 && !kMed;
         const float eps = c_eps_tab[min(nonDelta, 8)];
         Rng g;
         rng_from(g, pr.rng0, pr.rng1);
-        if (rec && depth < AR_DEBUG_MAX_HITS) rec[ri].hit_object[depth] = hit ? hr.x : -1;
+        if (rec && depth < AR_DEBUG_MAX_HITS) rec[ri].hit_object[depth] = hit || kMed ? hr.x : -1;
         if (rec) rec[ri].segments = depth + 1;
         // ---- intersection details (re-run of the accepted test)
         f3 pos = mk(0.0f, 0.0f, 0.0f), nrm = mk(0.0f, 0.0f, 0.0f);
@@ -397,12 +419,13 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                 nrm = dot(crd, ni) > 0.0f ? -ni : ni;
             } else if (oi.type == AR_OBJ_CUBE) {
                 isect_cube<true>(s.analytic[oi.aux], cro, crd, &pos, &nrm);
-            } else if (kSdf && oi.type == AR_OBJ_SDF) {
+            } else if (kExt && oi.type == AR_OBJ_SDF) {
                 sdf_surface_of(s, oi.aux, cro, crd, fbits(hr.z), eps, &pos, &nrm);
             } else {
                 isect_sphere<true>(s.analytic[oi.aux], cro, crd, &pos, &nrm);
             }
         }
+        if (kMed) pos = cro + crd * fbits(hr.z);  // no surface: the normal stays zero
         // ---- SampleContext (material.cuh:19-37, 177-330, 389-425)
         f3 next = mk(0.0f, 0.0f, 0.0f), emis = mk(0.0f, 0.0f, 0.0f), brdf = mk(0.0f, 0.0f, 0.0f);
         float pdf = 1.0f;
@@ -410,7 +433,8 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         bool nInside = false;
         f3 nvloc = mk(0.0f, 0.0f, 0.0f);
         int nmobj = -1, nmdepth = 0;
-        if (!hit && inside) {
+        f3 malb = mk(0.0f, 0.0f, 0.0f);  // medium: single-scatter albedo
+        if (!hit && !kMed && inside) {
             missThin = true;
             nvloc = cro;
         }
@@ -476,6 +500,21 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             nmobj = hr.x;
             nmdepth = mdepth + 1;
             brdf = eval_bsdf_cos(kModel, crd, next, N, pos, gb, inside, vloc);
+        } else if (kMed) {
+            // Henyey-Greenstein scattering; phase / pdf = 1, throughput weight = albedo
+            const float u1 = g.next(), u2 = g.next();
+            next = hg_sample(crd, s.medium.g, u1, u2);
+            pdf = hg_phase(s.medium.g, dot(crd, next));
+            malb = mk(s.medium.albedo[0], s.medium.albedo[1], s.medium.albedo[2]);
+            if (kSpec) {
+                const float a = interact(fp.spec.lut_rgb, fp.spec.res, lk, malb);
+                malb = mk(a, a, a);
+            }
+            brdf = malb * pdf;
+            nInside = false;
+            nvloc = pos;
+            nmobj = static_cast<int>(pr.rng1.z);
+            nmdepth = mdepth;
         } else {
             brdf = mk(1.0f, 1.0f, 1.0f);
             next = crd;
@@ -487,7 +526,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             }
             nInside = false;
         }
-        {   // hit offset, always one uniform (render.cuh:156-160)
+        if (!kMed) {   // hit offset, always one uniform (render.cuh:156-160)
             const float offEps = eps * fmaxf(1.0f, length(pos));
             const float sg = signf(dot(nrm, next));
             const float r = g.next();
@@ -495,9 +534,9 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         }
         const bool mInside = nInside;  // media state after this segment
         // ---- emission (render.cuh:648-723)
-        if (!hit) {
+        if (!hit && !kMed) {
             if (!missThin) radiance = radiance + (mask * emis) * d65;
-        } else if (light >= 0) {
+        } else if (hit && light >= 0) {
             float misW = 1.0f;
             if (fp.use_nee && depth > 0 && (flags & kFlagPrevNEE)) {
                 const float pB = fmaxf(pr.prev.w, 0.0f);
@@ -506,7 +545,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             }
             radiance = radiance + ((mask * emis) * d65) * misW;
         }
-        const bool brk = (!hit && !missThin) || terminate;
+        const bool brk = (!hit && !kMed && !missThin) || terminate;
         bool cont = false, shadow = false, cosOK = false;
         f3 pending = mk(0.0f, 0.0f, 0.0f), lightP = mk(0.0f, 0.0f, 0.0f);
         float4 prevOut = pr.prev;
@@ -526,15 +565,17 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                         const f3 lu = ls.p - pos;
                         const float d2 = fmaxf(dot(lu, lu), 1.0e-12f);
                         const f3 ld = lu * rsqrt_ieee(d2);
-                        const float cosX = fmaxf(0.0f, dot(nrm, ld));
+                        const float cosX = kMed ? 1.0f : fmaxf(0.0f, dot(nrm, ld));
                         const float cosY = fmaxf(0.0f, dot(ls.n, -ld));
                         if (cosX > 0.0f && cosY > 0.0f) {
                             cosOK = true;
-                            const f3 fcos = eval_bsdf_cos(kModel, crd, ld, nrm, pos, gb, false, mk(0.0f, 0.0f, 0.0f));
+                            const f3 fcos = kMed ? malb * hg_phase(s.medium.g, dot(crd, ld))
+                                                 : eval_bsdf_cos(kModel, crd, ld, nrm, pos, gb, false, mk(0.0f, 0.0f, 0.0f));
                             const float G = cosY / d2;
                             const f3 contrib = (fcos * ls.emis) * (G / pATotal);
                             const float pL = area_to_solid_angle(pos, ls.p, ls.n, ls.pFacet * ls.pA);
-                            const float pB = fmaxf(bsdf_pdf(kModel, gb, nrm, crd, ld), 0.0f);
+                            const float pB = kMed ? hg_phase(s.medium.g, dot(crd, ld))
+                                                  : fmaxf(bsdf_pdf(kModel, gb, nrm, crd, ld), 0.0f);
                             pending = (mask * (contrib * power_heuristic(pL, pB))) * d65;
                         }
                         shadow = true;
@@ -596,29 +637,42 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             ShadowRec sr;
             sr.src = f4(pos, c_eps_tab[min(depth, 8)]);
             sr.dst = f4(lightP, fbits(target));
-            sr.nee = f4(pending, fbits(cosOK ? 1 : 0));
+            const uint32_t mseed = kExt && s.has_medium
+                ? medium_seed(fp.medium_key, static_cast<uint32_t>(sidx), static_cast<uint32_t>(pixel), static_cast<uint32_t>(depth), 1u) & ~1u
+                : 0u;
+            sr.nee = f4(pending, fbits(static_cast<int>(mseed | (cosOK ? 1u : 0u))));
             B.shadow[m] = sr;
         }
     }
 }
 
 // ------------------------------------------------------------------ shadow
+// Transmittance of the medium along an unoccluded shadow segment (out of line).
+__device__ __noinline__ float shadow_transmittance(const SceneView& s, f3 o, f3 d, float tmax, uint32_t seed)
+{
+    HashRng h;
+    h.seed = seed;
+    h.n = 0;
+    return ratio_track(s.medium, o, d, tmax, h);
+}
+
 // SegmentTrace -> AnyHitSegmentBVH (render.cuh:167-183, intersection.cuh:372-397)
 // and the remainder of NEE (render.cuh:242-343): the pending term is added when
 // the segment is unoccluded, and previousDidNEE_ becomes "occluded or cos > 0".
-template <bool kSdf>
+template <bool kExt>
 struct ShadowIO {
     const ShadowRec* rec;
     PathRec* next_pool;
     RetireRec* retire;
     unsigned long long traced;
-    __device__ __forceinline__ void finish(int m, bool occ)
+    __device__ __forceinline__ void finish(int m, bool occ, float tr = 1.0f)
     {
         const float4 dst = rec[m].dst;
-        const float4 nee = rec[m].nee;
+        float4 nee = rec[m].nee;
         const int target = ibits(dst.w);
-        const bool cosOK = ibits(nee.w) != 0;
+        const bool cosOK = (ibits(nee.w) & 1) != 0;
         const bool add = !occ && cosOK;
+        if (kExt) { nee.x *= tr; nee.y *= tr; nee.z *= tr; }  // medium transmittance
         if (target >= 0) {
             PathRec& p = next_pool[target];
             if (add) {
@@ -657,18 +711,20 @@ struct ShadowIO {
     __device__ __forceinline__ void store(const SceneView& s, int m, const RayState& r)
     {
         bool occ = r.best.obj >= 0;
-        if (kSdf && !occ && s.num_sdf > 0) occ = sdf_any(s, r.o, r.d, 0.0f, r.best.t, rec[m].src.w) >= 0;
-        finish(m, occ);
+        if (kExt && !occ && s.num_sdf > 0) occ = sdf_any(s, r.o, r.d, 0.0f, r.best.t, rec[m].src.w) >= 0;
+        float tr = 1.0f;
+        if (kExt && !occ && s.has_medium) tr = shadow_transmittance(s, r.o, r.d, r.best.t, static_cast<uint32_t>(ibits(rec[m].nee.w)) & ~1u);
+        finish(m, occ, tr);
     }
 };
 
-template <bool kSdf>
+template <bool kExt>
 __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks - 1) k_shadow(SceneView s, PathBuffers B, int cur, PoolCtl* ctl,
                                                         unsigned long long* stats, uint32_t* ovf, int* err)
 {
     extern __shared__ uint32_t smem[];
     const int n = ctl->shadow_count;
-    ShadowIO<kSdf> io;
+    ShadowIO<kExt> io;
     io.rec = B.shadow;
     io.next_pool = pool_of(B, 1 - cur);
     io.retire = B.retire;
@@ -792,15 +848,16 @@ cudaError_t launch_pool_init(PoolCtl* ctl, int64_t total, cudaStream_t st)
 }
 
 // The five per-material shading launches of one iteration.
-template <bool kSdf, bool kSpec>
+template <bool kExt, bool kSpec>
 void launch_shade(const SceneView& s, const FrameParams& fp, const PathBuffers& B, int c, PoolCtl* ctl,
                   ar_path_record* rec, int grid, cudaStream_t st)
 {
-    k_shade<-1, kSdf, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_DIFFUSE, kSdf, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_LIGHT, kSdf, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_GLASS, kSdf, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_GGX, kSdf, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<-1, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_DIFFUSE, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_LIGHT, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_GLASS, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_GGX, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    if (kExt && s.has_medium) k_shade<kModelMedium, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
 }
 
 cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const PathBuffers& B, PoolCtl* ctl,
@@ -808,29 +865,30 @@ cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const P
                               uint32_t* ovf, int* err, double* accum, ar_path_record* rec, int iterations, int* cur,
                               int grid_trace, int grid_other, cudaStream_t st, int64_t* launches, LaunchTimers* tm)
 {
+    const bool ext = s.num_sdf > 0 || s.has_medium;
     for (int it = 0; it < iterations; ++it) {
         const int c = *cur;
         k_plan<<<1, 1, 0, st>>>(ctl, c, fp.npix, B.capacity);
         k_regen<<<grid_other, kShadeBlock, 0, st>>>(fp, B, ctl, c, b0, b1, jump_table, rec);
         const bool te = tm && tm->n_extend < tm->cap;
         if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend], st);
-        if (s.num_sdf > 0) k_extend<true><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
-        else k_extend<false><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
+        if (ext) k_extend<true><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err, fp.medium_key);
+        else k_extend<false><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err, fp.medium_key);
         if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend++ + 1], st);
         if (fp.spectral) {
-            if (s.num_sdf > 0) launch_shade<true, true>(s, fp, B, c, ctl, rec, grid_other, st);
+            if (ext) launch_shade<true, true>(s, fp, B, c, ctl, rec, grid_other, st);
             else launch_shade<false, true>(s, fp, B, c, ctl, rec, grid_other, st);
         } else {
-            if (s.num_sdf > 0) launch_shade<true, false>(s, fp, B, c, ctl, rec, grid_other, st);
+            if (ext) launch_shade<true, false>(s, fp, B, c, ctl, rec, grid_other, st);
             else launch_shade<false, false>(s, fp, B, c, ctl, rec, grid_other, st);
         }
         const bool ts = tm && tm->n_shadow < tm->cap;
         if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow], st);
-        if (s.num_sdf > 0) k_shadow<true><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
+        if (ext) k_shadow<true><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
         else k_shadow<false><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
         if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow++ + 1], st);
         k_retire<<<grid_other, kShadeBlock, 0, st>>>(fp, B, ctl, accum, rec);
-        *launches += 10;
+        *launches += s.has_medium ? 11 : 10;
         *cur = 1 - c;
     }
     return cudaGetLastError();

@@ -18,6 +18,7 @@
 #include "detmath.h"
 #include "../../include/aperture_b200.h"
 #include "scene_types.h"
+#include "medium.cuh"
 #include "sdf.cuh"
 
 namespace ar {
@@ -37,6 +38,8 @@ struct SceneView {
     int32_t num_objects;
     int32_t num_lights;
     int32_t num_sdf;
+    int32_t has_medium;      // 1: `medium` holds the participating medium
+    MediumRec medium;
 };
 
 constexpr float kSlabWiden = 1.000001f;

@@ -33,7 +33,9 @@ enum : int32_t {
     kFlagInside = 2,       // MediaContext::bInsideMedia_
 };
 
-constexpr int kShadeBuckets = 5;  // miss, then shading model + 1
+constexpr int kModelMedium = 4;   // shade bucket of collisions in the participating medium
+constexpr int kShadeBuckets = 6;  // miss, then shading model + 1 (medium: kModelMedium + 1)
+constexpr int32_t kHitMedium = -2; // hit object of a medium collision
 
 struct alignas(16) PathRec {
     float4 o;     // ray origin xyz; w: depth | nonDeltaDepth << 16 (int bits)
@@ -50,7 +52,8 @@ static_assert(sizeof(PathRec) == 128, "PathRec must be one 128-byte line");
 struct alignas(16) ShadowRec {
     float4 src;   // segment start xyz; w segment eps
     float4 dst;   // segment end xyz; w target: >= 0 next-pool index, < 0 ~retire index
-    float4 nee;   // pending radiance rgb (throughput applied); w 1 if cosX > 0 && cosY > 0
+    float4 nee;   // pending radiance rgb (throughput applied); w bit 0: cosX > 0 && cosY > 0,
+                  // bits 1-31: seed of the medium transmittance estimate
 };
 
 struct alignas(16) RetireRec {
@@ -103,6 +106,7 @@ struct FrameParams {
     int32_t spectral;        // 1: one hero wavelength per path, XYZ output
     int32_t tri_light_nee;   // 1: NEE also samples triangle lights (extension)
     SpectralView spec;       // tables and lookup tables of the spectral mode
+    uint32_t medium_key;     // medium_frame_key(seed, frame0)
 };
 
 }  // namespace ar

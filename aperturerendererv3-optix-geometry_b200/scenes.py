@@ -282,3 +282,42 @@ def sdf_box_scene(seed: int = SEED_BASE + 3, precision: int = 32, grid: int = 64
     ggx(vol, (0.9, 0.6, 0.3), 0.3, 1.0, 0.5)
     volumes = [make_volume((grid, grid, grid), None, precision, SDF_TORUS, (0.32, 0.14, 0.0, 0.0))]
     return np.concatenate([base, tor, vol]), volumes
+
+
+def fbm_density(seed: int = SEED_BASE + 3, n: int = 128, octaves: int = 6, base: int = 4) -> np.ndarray:
+    """[n, n, n] float32 density in [0, 1]: fractal Brownian motion of seeded
+    value noise (lattice values U(0, 1), trilinear), frequencies base * 2^o with
+    gain 1/2, then a soft threshold that leaves clouds and clear gaps."""
+    rng = np.random.default_rng(seed)
+    x = (np.arange(n, dtype=np.float64) + 0.5) / n
+    acc = np.zeros((n, n, n), np.float64)
+    amp, norm = 1.0, 0.0
+    for o in range(octaves):
+        f = base << o
+        lat = rng.random((f + 1, f + 1, f + 1))
+        g = x * f
+        i0 = np.minimum(np.floor(g).astype(np.int64), f - 1)
+        t = g - i0
+        # separable trilinear: interpolate along x, then y, then z
+        a = lat[:, :, i0] * (1 - t) + lat[:, :, i0 + 1] * t
+        a = a[:, i0, :] * (1 - t)[None, :, None] + a[:, i0 + 1, :] * t[None, :, None]
+        a = a[i0, :, :] * (1 - t)[:, None, None] + a[i0 + 1, :, :] * t[:, None, None]
+        acc += amp * a
+        norm += amp
+        amp *= 0.5
+    v = acc / norm
+    return np.clip((v - 0.42) * 4.0, 0.0, 1.0).astype(np.float32)
+
+
+def medium_box_scene(seed: int = SEED_BASE + 3, precision: int = 16, grid: int = 256, medium_grid: int = 128):
+    """Config 3: the SDF box scene (a grid^3 sampled torus, float or half) plus a
+    heterogeneous medium filling the box: a medium_grid^3 fBm density (6
+    octaves, seeded) scaled to sigma_t max 2.0, single-scatter albedo 0.8,
+    Henyey-Greenstein g = 0.3.  Returns (objects, volumes, medium) where
+    medium holds the keyword arguments of Scene.set_medium."""
+    objects, volumes = sdf_box_scene(seed, precision, grid)
+    d = fbm_density(seed, medium_grid)
+    medium = dict(density=d.astype(np.float16 if precision == 16 else np.float32),
+                  bounds_min=(-0.5, -0.5, -0.5), bounds_max=(0.5, 0.5, 0.5),
+                  sigma_t_max=2.0, albedo=(0.8, 0.8, 0.8), g=0.3)
+    return objects, volumes, medium

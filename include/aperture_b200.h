@@ -144,7 +144,8 @@ typedef struct ar_path_record {
     int32_t nee_rays;      /* shadow rays cast                                        */
     int32_t nee_depth_mask;/* bit d set: a shadow ray was cast at loop depth d (< 32) */
     int32_t reserved;
-    int32_t hit_object[AR_DEBUG_MAX_HITS]; /* closest-hit object per segment, -1 = miss */
+    int32_t hit_object[AR_DEBUG_MAX_HITS]; /* closest-hit object per segment, -1 = miss,
+                                              -2 = collision in the participating medium */
 } ar_path_record;          /* 96 bytes */
 
 typedef struct ar_scene_info {
@@ -271,6 +272,31 @@ ar_status ar_scene_set_spectral(ar_scene* scene, const float* tables, size_t cou
 /* Copies of the spectral lookup tables (840 x 4 and lut_res^3 x 4 floats, x
  * fastest); either pointer may be NULL. */
 ar_status ar_scene_get_spectral_luts(const ar_scene* scene, float* lambda_lut, float* rgb_lut);
+
+/* A heterogeneous participating medium (extension: the reference has no
+ * volumetric media; its Henyey-Greenstein helpers, core/render/sample.cuh:110-145,
+ * have no call site).  One axis-aligned box of world space holds a density grid
+ * (dims[0] x dims[1] x dims[2] values, x fastest, trilinear between voxel
+ * centres, clamped at the faces); extinction = sigma_t_max * density.  Free
+ * flights are sampled by delta tracking, scattering by the Henyey-Greenstein
+ * phase function with asymmetry g; every collision scatters with throughput
+ * weight `albedo`.  Shadow rays are attenuated by ratio-tracking estimates of
+ * the transmittance.  The interior of a dielectric object (a path inside
+ * glass) is not part of the medium. */
+typedef struct ar_medium_desc {
+    float bounds_min[3];
+    float bounds_max[3];
+    float sigma_t_max;     /* extinction of density 1, world units^-1               */
+    float albedo[3];       /* single-scatter albedo, each in [0, 1]                 */
+    float g;               /* Henyey-Greenstein asymmetry, (-1, 1)                  */
+    int32_t dims[3];
+    int32_t precision;     /* 32 = float, 16 = half                                 */
+    const void* density;   /* host memory, non-negative finite values               */
+} ar_medium_desc;
+
+/* Attach (or with NULL remove) the scene's medium; copies the grid to the
+ * scene's device. */
+ar_status ar_scene_set_medium(ar_scene* scene, const ar_medium_desc* medium);
 
 /* One job of a batch: a scene (shared between jobs if wanted), a camera, the
  * render parameters and device outputs (mean image and/or FP64 sums added). */

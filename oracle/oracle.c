@@ -147,6 +147,11 @@ struct or_scene {
     int flags;
     int fallbacks;
     float eps_tab[9];
+    /* participating medium (or_scene_set_medium; extension, no reference counterpart) */
+    int has_medium;
+    float m_bmin[3], m_bmax[3], m_sigma, m_g, m_albedo[3], m_major;
+    int m_dims[3];
+    float* m_grid;         /* density values as float (half grids converted exactly) */
 };
 
 /* float3x3::rotX/Y/Z and mul (vector.cuh:378-416), host libm as in the
@@ -539,6 +544,7 @@ void or_scene_destroy(or_scene* s)
     for (int v = 0; v < s->nvol; ++v) free(s->vols[v]);
     free(s->vols);
     free(s->spec_tab); free(s->lut_lam); free(s->lut_rgb);
+    free(s->m_grid);
     free(s->o); free(s->nodes); free(s->idx); free(s->lobj); free(s->lprob); free(s);
 }
 
@@ -1550,6 +1556,189 @@ static int closest(const or_scene* s, V3 ro, V3 rd, float tMin, Isect* out)
 }
 
 /* AnyHitSegmentBVH (intersection.cuh:372-397) */
+/* ------------------------------------------------------------------------ */
+/* Heterogeneous participating medium (extension; no reference counterpart:   */
+/* the reference's Henyey-Greenstein helpers, sample.cuh:110-145, are unused). */
+/* Same arithmetic, in the same order, as the device code: delta tracking     */
+/* (Woodcock) for free flights, ratio tracking for shadow transmittance,      */
+/* Henyey-Greenstein by CDF inversion, lowbias32 counter-based uniforms.      */
+/* ------------------------------------------------------------------------ */
+static uint32_t lowbias32(uint32_t x)
+{
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+typedef struct { uint32_t seed, n; } HashRng;
+static float hash_next(HashRng* h)
+{
+    const uint32_t v = lowbias32(h->seed ^ lowbias32(h->n++ * 0x9E3779B9u + 0x632BE5ABu));
+    return ((float)(v >> 8) + 0.5f) * (1.0f / 16777216.0f);
+}
+static uint32_t medium_frame_key(uint64_t seed, uint64_t frame0)
+{
+    uint32_t h = lowbias32((uint32_t)seed ^ 0x6D2B79F5u);
+    h = lowbias32(h ^ (uint32_t)(seed >> 32));
+    h = lowbias32(h ^ (uint32_t)frame0);
+    return lowbias32(h ^ (uint32_t)(frame0 >> 32));
+}
+static uint32_t medium_seed(uint32_t key, uint32_t sample, uint32_t pixel, uint32_t depth, uint32_t salt)
+{
+    uint32_t h = lowbias32(key ^ sample);
+    h = lowbias32(h ^ pixel);
+    return lowbias32(h ^ (depth * 2u + salt));
+}
+static int clamp_index(int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); }
+/* trilinear between voxel centres, clamped at the faces */
+static float medium_density(const or_scene* s, V3 p)
+{
+    const float gx = (p.x - s->m_bmin[0]) / (s->m_bmax[0] - s->m_bmin[0]) * (float)s->m_dims[0] - 0.5f;
+    const float gy = (p.y - s->m_bmin[1]) / (s->m_bmax[1] - s->m_bmin[1]) * (float)s->m_dims[1] - 0.5f;
+    const float gz = (p.z - s->m_bmin[2]) / (s->m_bmax[2] - s->m_bmin[2]) * (float)s->m_dims[2] - 0.5f;
+    const float fx0 = floorf(gx), fy0 = floorf(gy), fz0 = floorf(gz);
+    const float tx = gx - fx0, ty = gy - fy0, tz = gz - fz0;
+    const int X = s->m_dims[0] - 1, Y = s->m_dims[1] - 1, Z = s->m_dims[2] - 1;
+    const int x0 = clamp_index((int)fx0, X), x1 = clamp_index((int)fx0 + 1, X);
+    const int y0 = clamp_index((int)fy0, Y), y1 = clamp_index((int)fy0 + 1, Y);
+    const int z0 = clamp_index((int)fz0, Z), z1 = clamp_index((int)fz0 + 1, Z);
+    const size_t sy = (size_t)s->m_dims[0], sz = (size_t)s->m_dims[0] * (size_t)s->m_dims[1];
+    const float* g = s->m_grid;
+    const float c000 = g[x0 + y0 * sy + z0 * sz], c100 = g[x1 + y0 * sy + z0 * sz];
+    const float c010 = g[x0 + y1 * sy + z0 * sz], c110 = g[x1 + y1 * sy + z0 * sz];
+    const float c001 = g[x0 + y0 * sy + z1 * sz], c101 = g[x1 + y0 * sy + z1 * sz];
+    const float c011 = g[x0 + y1 * sy + z1 * sz], c111 = g[x1 + y1 * sy + z1 * sz];
+    const float c00 = c000 * (1.0f - tx) + c100 * tx, c10 = c010 * (1.0f - tx) + c110 * tx;
+    const float c01 = c001 * (1.0f - tx) + c101 * tx, c11 = c011 * (1.0f - tx) + c111 * tx;
+    const float c0 = c00 * (1.0f - ty) + c10 * ty, c1 = c01 * (1.0f - ty) + c11 * ty;
+    return c0 * (1.0f - tz) + c1 * tz;
+}
+static int medium_span(const or_scene* s, V3 o, V3 d, float tmax, float* t0, float* t1)
+{
+    const V3 inv = v3(inv_safe(d.x), inv_safe(d.y), inv_safe(d.z));
+    const V3 a = vmul(vsub(v3(s->m_bmin[0], s->m_bmin[1], s->m_bmin[2]), o), inv);
+    const V3 b = vmul(vsub(v3(s->m_bmax[0], s->m_bmax[1], s->m_bmax[2]), o), inv);
+    const V3 lo = vmin3(a, b), hi = vmax3(a, b);
+    *t0 = fmaxf(fmaxf(fmaxf(lo.x, lo.y), lo.z), 0.0f);
+    *t1 = fminf(fminf(fminf(hi.x, hi.y), hi.z), tmax);
+    return *t0 < *t1 && s->m_major > 0.0f;
+}
+#define OR_MEDIUM_MAX_STEPS 4096
+static float delta_track(const or_scene* s, V3 o, V3 d, float tmax, HashRng* h)
+{
+    float t0, t1;
+    if (!medium_span(s, o, d, tmax, &t0, &t1)) return -1.0f;
+    float t = t0;
+    for (int i = 0; i < OR_MEDIUM_MAX_STEPS; ++i) {
+        t = t - om_logf(1.0f - hash_next(h) * 0.99999994f) / s->m_major;
+        if (t >= t1) return -1.0f;
+        const float sg = medium_density(s, vadd(o, vscale(d, t))) * s->m_sigma;
+        if (hash_next(h) * s->m_major < sg) return t;
+    }
+    return -1.0f;
+}
+static float ratio_track(const or_scene* s, V3 o, V3 d, float tmax, HashRng* h)
+{
+    float t0, t1;
+    if (!medium_span(s, o, d, tmax, &t0, &t1)) return 1.0f;
+    float t = t0, tr = 1.0f;
+    for (int i = 0; i < OR_MEDIUM_MAX_STEPS; ++i) {
+        t = t - om_logf(1.0f - hash_next(h) * 0.99999994f) / s->m_major;
+        if (t >= t1) break;
+        tr = tr * (1.0f - medium_density(s, vadd(o, vscale(d, t))) * s->m_sigma / s->m_major);
+        if (tr <= 0.0f) return 0.0f;
+    }
+    return tr;
+}
+static float hg_phase(float g, float cosT)
+{
+    const float den = 1.0f + g * g - 2.0f * g * cosT;
+    return (1.0f - g * g) / (4.0f * 3.14159265358979f * den * sqrtf(den));
+}
+static V3 hg_sample(V3 d, float g, float u1, float u2)
+{
+    float cosT;
+    if (fabsf(g) < 1e-3f) {
+        cosT = 1.0f - 2.0f * u1;
+    } else {
+        const float sq = (1.0f - g * g) / (1.0f - g + 2.0f * g * u1);
+        cosT = (1.0f + g * g - sq * sq) / (2.0f * g);
+    }
+    cosT = fminf(fmaxf(cosT, -1.0f), 1.0f);
+    const float sinT = sqrtf(fmaxf(0.0f, 1.0f - cosT * cosT));
+    float sp, cp;
+    om_sincosf(2.0f * 3.14159265358979f * u2, &sp, &cp);
+    const V3 a = fabsf(d.z) < 0.999f ? v3(0.0f, 0.0f, 1.0f) : v3(1.0f, 0.0f, 0.0f);
+    const V3 t = vnormalize(cross3(a, d));
+    const V3 b = cross3(d, t);
+    return vnormalize(vadd(vadd(vscale(t, sinT * cp), vscale(b, sinT * sp)), vscale(d, cosT)));
+}
+/* transmittance of an unoccluded shadow segment, with the geometry of
+ * segment_occluded (1 when the segment is too short to be traced) */
+static float segment_transmittance(const or_scene* s, float eps_d, V3 src, V3 dst, uint32_t seed)
+{
+    V3 dir = vsub(dst, src);
+    const float dist = len3(dir);
+    if (dist <= 0.0f) return 1.0f;
+    dir = vdivs(dir, dist);
+    const float eps = eps_d * fmaxf(1.0f, fmaxf(len3(src), len3(dst)));
+    const float tMax = fmaxf(0.0f, dist - eps);
+    if (tMax <= 0.0f) return 1.0f;
+    HashRng h;
+    h.seed = seed; h.n = 0;
+    return ratio_track(s, src, dir, tMax, &h);
+}
+
+int or_scene_set_medium(or_scene* s, const ar_medium_desc* m)
+{
+    free(s->m_grid);
+    s->m_grid = NULL;
+    s->has_medium = 0;
+    if (!m) return 0;
+    const size_t n = (size_t)m->dims[0] * (size_t)m->dims[1] * (size_t)m->dims[2];
+    s->m_grid = (float*)malloc(n * sizeof(float));
+    float mx = 0.0f;
+    for (size_t i = 0; i < n; ++i) {
+        const float v = m->precision == 16 ? half_to_float(((const uint16_t*)m->density)[i]) : ((const float*)m->density)[i];
+        s->m_grid[i] = v;
+        mx = fmaxf(mx, v);
+    }
+    for (int a = 0; a < 3; ++a) {
+        s->m_bmin[a] = m->bounds_min[a]; s->m_bmax[a] = m->bounds_max[a];
+        s->m_albedo[a] = m->albedo[a]; s->m_dims[a] = m->dims[a];
+    }
+    s->m_sigma = m->sigma_t_max;
+    s->m_g = m->g;
+    s->m_major = m->sigma_t_max * mx;
+    s->has_medium = 1;
+    return 0;
+}
+
+float or_medium_density(const or_scene* s, const float* p3) { return medium_density(s, v3(p3[0], p3[1], p3[2])); }
+
+void or_hg_sample(const float* d3, float g, const float* u2, int64_t n, float* out3)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        const V3 r = hg_sample(v3(d3[0], d3[1], d3[2]), g, u2[2 * i], u2[2 * i + 1]);
+        out3[3 * i] = r.x; out3[3 * i + 1] = r.y; out3[3 * i + 2] = r.z;
+    }
+}
+
+float or_hg_phase(float g, float cosT) { return hg_phase(g, cosT); }
+
+void or_medium_track(const or_scene* s, const float* rays8, int64_t n, const uint32_t* seeds, int ratio, float* out)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        const float* r = rays8 + 8 * i;
+        HashRng h;
+        h.seed = seeds[i]; h.n = 0;
+        const V3 o = v3(r[0], r[1], r[2]), d = v3(r[4], r[5], r[6]);
+        out[i] = ratio ? ratio_track(s, o, d, r[7], &h) : delta_track(s, o, d, r[7], &h);
+    }
+}
+
 static int segment_occluded(const or_scene* s, float eps_d, V3 src, V3 dst, Counters* cnt)
 {
     V3 dir = vsub(dst, src);
@@ -1893,7 +2082,8 @@ typedef struct { V3 radiance; int segments, nee_rays, nee_mask; int hits[AR_DEBU
  * (render.cuh:460-999), with camera_inside = intersection::Overlap at the
  * camera position (render.cuh:536-538). */
 static void calculate_radiance(const or_scene* s, const ar_render_params* p, int camera_inside,
-                               Rng* g, V3 ro, V3 rd, PathOut* po, Counters* cnt)
+                               Rng* g, V3 ro, V3 rd, PathOut* po, Counters* cnt,
+                               uint32_t mkey, uint32_t sample, uint32_t pixel)
 {
     int nonDelta = 0;
     Spec sp;
@@ -1937,6 +2127,74 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
             else { memset(&ic, 0, sizeof(ic)); ic.obj = -1; ic.light = -1; }
         } else {
             hit = closest(s, cro, crd, eps, &ic);
+        }
+        if (s->has_medium && !media.inside) {
+            /* free flight in the medium up to the surface (extension) */
+            HashRng hr;
+            hr.seed = medium_seed(mkey, sample, pixel, (uint32_t)depth, 0u); hr.n = 0;
+            const float tc = delta_track(s, cro, crd, hit ? ic.dist : INFINITY, &hr);
+            if (tc >= 0.0f) {
+                if (po->segments < AR_DEBUG_MAX_HITS) po->hits[po->segments] = -2;
+                po->segments++;
+                const V3 pos = vadd(cro, vscale(crd, tc));
+                const float u1 = rng1(g), u2 = rng1(g);
+                const V3 next = hg_sample(crd, s->m_g, u1, u2);
+                const float pdf = hg_phase(s->m_g, dot3(crd, next));
+                V3 alb = v3(s->m_albedo[0], s->m_albedo[1], s->m_albedo[2]);
+                if (sp.on) { const float a = sp_interact(s, sp.lk, alb); alb = v3(a, a, a); }
+                const V3 brdf = vscale(alb, pdf);
+                const float lum = sp.on ? mask.x : luminance3(mask);
+                const float useNEERate = sqrtf(saturatef_(lum));
+                int neeValid = 0;
+                if (p->use_nee && nonDelta < 10 && rng1(g) < useNEERate) {
+                    LSmp ls = sample_light(s, pos, g, p->tri_light_nee);
+                    if (sp.on) { const float e = sp_interact(s, sp.lk, ls.emis); ls.emis = v3(e, e, e); }
+                    if (ls.valid) {
+                        const float pATotal = fmaxf(1e-20f, ls.pA * ls.pFacet);
+                        const V3 lu = vsub(ls.p, pos);
+                        const float d2 = fmaxf(dot3(lu, lu), 1.0e-12f);
+                        const V3 ld = vscale(lu, om_rsqrtf(d2));
+                        po->nee_rays++;
+                        if (depth < 32) po->nee_mask |= (int)(1u << depth);
+                        const float epsS = s->eps_tab[depth < 8 ? depth : 8];
+                        if (segment_occluded(s, epsS, pos, ls.p, cnt)) {
+                            neeValid = 1;
+                        } else {
+                            const float cosY = fmaxf(0.0f, dot3(ls.n, vneg(ld)));
+                            if (cosY > 0.0f) {
+                                const V3 f = vscale(alb, hg_phase(s->m_g, dot3(crd, ld)));
+                                const float G = cosY / d2;
+                                const V3 contrib = vscale(vmul(f, ls.emis), G / pATotal);
+                                neeValid = 1;
+                                const float pL = area_to_solid_angle(pos, ls.p, ls.n, ls.pFacet * ls.pA);
+                                const float pB = hg_phase(s->m_g, dot3(crd, ld));
+                                const float w = power_heuristic(pL, pB);
+                                const float tr = segment_transmittance(
+                                    s, epsS, pos, ls.p, medium_seed(mkey, sample, pixel, (uint32_t)depth, 1u) & ~1u);
+                                radiance = vadd(radiance, vscale(vscale(vmul(mask, vscale(contrib, w)), sp.d65), tr));
+                            }
+                        }
+                    }
+                }
+                prevDidNEE = neeValid;
+                prevPdf = pdf;
+                prevPos = pos;
+                const V3 contrib = v3(brdf.x / fmaxf(pdf, 1e-12f), brdf.y / fmaxf(pdf, 1e-12f), brdf.z / fmaxf(pdf, 1e-12f));
+                float q = 1.0f;
+                if (nonDelta >= p->rr_depth) {
+                    const float mx = sp.on ? mask.x : max3f(mask);
+                    const float basic = clampf_(lum * 0.5f + mx * 0.5f, 0.05f, 0.95f);
+                    q = lerpf_(basic, 1.0f, 0.0f);
+                    if (rng1(g) > q) break;
+                }
+                mask = vmul(mask, contrib);
+                mask = vdivs(mask, q);
+                cro = pos;
+                crd = next;
+                media.vloc = pos;
+                nonDelta++;
+                continue;
+            }
         }
         if (po->segments < AR_DEBUG_MAX_HITS) po->hits[po->segments] = hit ? ic.obj : -1;
         po->segments++;
@@ -2020,7 +2278,11 @@ static void calculate_radiance(const or_scene* s, const ar_render_params* p, int
                             const float pL = area_to_solid_angle(ic.pos, ls.p, ls.n, ls.pFacet * ls.pA);
                             const float pB = fmaxf(bsdf_pdf(model, &ic, ic.nrm, crd, ld), 0.0f);
                             const float w = power_heuristic(pL, pB);
-                            radiance = vadd(radiance, vscale(vmul(mask, vscale(contrib, w)), sp.d65));
+                            const float tr = s->has_medium
+                                ? segment_transmittance(s, s->eps_tab[depth < 8 ? depth : 8], ic.pos, ls.p,
+                                                        medium_seed(mkey, sample, pixel, (uint32_t)depth, 1u) & ~1u)
+                                : 1.0f;
+                            radiance = vadd(radiance, vscale(vscale(vmul(mask, vscale(contrib, w)), sp.d65), tr));
                         }
                     }
                 }
@@ -2108,6 +2370,7 @@ int64_t or_render_paths(const or_scene* s, const ar_camera* cam, const ar_render
 {
     const int64_t W = cam->width, H = cam->height, S = p->spp;
     const int inside = camera_overlap(s, from_ar(cam->position));
+    const uint32_t mkey = medium_frame_key(p->seed, (uint64_t)p->frame_offset);
     int64_t overflow = 0;
 #ifdef _OPENMP
     const int nthreads = threads > 0 ? threads : omp_get_max_threads();
@@ -2115,6 +2378,7 @@ int64_t or_render_paths(const or_scene* s, const ar_camera* cam, const ar_render
 #endif
     for (int64_t k = 0; k < W * H * S; ++k) {
         const int i = (int)(k % W), j = (int)((k / W) % H);
+        const uint32_t smp = (uint32_t)(k / (W * H)), pix = (uint32_t)(k % (W * H));
         Rng g;
         g.tape = tape + k * per_path; g.limit = per_path; g.pos = 0; g.overflow = 0; g.state = 0;
         const float jx = rng1(&g), jy = rng1(&g);
@@ -2123,7 +2387,8 @@ int64_t or_render_paths(const or_scene* s, const ar_camera* cam, const ar_render
         PathOut po;
         Counters cnt;
         memset(&cnt, 0, sizeof(cnt));
-        calculate_radiance(s, p, inside, &g, v3(ray[0], ray[1], ray[2]), v3(ray[4], ray[5], ray[6]), &po, &cnt);
+        calculate_radiance(s, p, inside, &g, v3(ray[0], ray[1], ray[2]), v3(ray[4], ray[5], ray[6]), &po, &cnt,
+                           mkey, smp, pix);
         ar_path_record* r = &rec[k];
         memset(r, 0, sizeof(*r));
         r->radiance[0] = po.radiance.x; r->radiance[1] = po.radiance.y; r->radiance[2] = po.radiance.z;
@@ -2142,6 +2407,7 @@ void or_render_image(const or_scene* s, const ar_camera* cam, const ar_render_pa
 {
     const int64_t W = cam->width;
     const int inside = camera_overlap(s, from_ar(cam->position));
+    const uint32_t mkey = medium_frame_key(p->seed, (uint64_t)p->frame_offset);
     int64_t e = 0, sh = 0;
     if (step < 1) step = 1;
     const int64_t count = (pe - pb + step - 1) / step;
@@ -2163,7 +2429,8 @@ void or_render_image(const or_scene* s, const ar_camera* cam, const ar_render_pa
             float ray[8];
             or_camera_ray(cam, i, j, jx, jy, ray);
             PathOut po;
-            calculate_radiance(s, p, inside, &g, v3(ray[0], ray[1], ray[2]), v3(ray[4], ray[5], ray[6]), &po, &cnt);
+            calculate_radiance(s, p, inside, &g, v3(ray[0], ray[1], ray[2]), v3(ray[4], ray[5], ray[6]), &po, &cnt,
+                               mkey, (uint32_t)smp, (uint32_t)pix);
             acc[0] += po.radiance.x; acc[1] += po.radiance.y; acc[2] += po.radiance.z;
         }
         accum[3 * pix + 0] += acc[0]; accum[3 * pix + 1] += acc[1]; accum[3 * pix + 2] += acc[2];
@@ -2184,6 +2451,7 @@ int64_t or_collect_rays(const or_scene* s, const ar_camera* cam, const ar_render
 {
     const int64_t W = cam->width;
     const int inside = camera_overlap(s, from_ar(cam->position));
+    const uint32_t mkey = medium_frame_key(p->seed, (uint64_t)p->frame_offset);
     Counters cnt;
     memset(&cnt, 0, sizeof(cnt));
     cnt.ext_out = ext; cnt.ext_cap = ext_cap; cnt.sh_out = sh; cnt.sh_cap = sh_cap;
@@ -2197,7 +2465,8 @@ int64_t or_collect_rays(const or_scene* s, const ar_camera* cam, const ar_render
             float ray[8];
             or_camera_ray(cam, i, j, jx, jy, ray);
             PathOut po;
-            calculate_radiance(s, p, inside, &g, v3(ray[0], ray[1], ray[2]), v3(ray[4], ray[5], ray[6]), &po, &cnt);
+            calculate_radiance(s, p, inside, &g, v3(ray[0], ray[1], ray[2]), v3(ray[4], ray[5], ray[6]), &po, &cnt,
+                               mkey, (uint32_t)smp, (uint32_t)pix);
         }
     }
     *n_ext = cnt.ext_rays < ext_cap ? cnt.ext_rays : ext_cap;

@@ -102,6 +102,17 @@ void or_render_image(const or_scene* s, const ar_camera* cam, const ar_render_pa
 int64_t or_collect_rays(const or_scene* s, const ar_camera* cam, const ar_render_params* p, int64_t pb, int64_t pe,
                         float* ext, int64_t ext_cap, int64_t* n_ext, float* sh, int64_t sh_cap, int64_t* n_sh);
 
+/* Participating medium (extension): attach (NULL removes) a density box; the
+ * medium's pieces for their own tests: density at a point, Henyey-Greenstein
+ * sampling (n pairs of uniforms around d3) and value, and per ray (8 floats,
+ * tmax in [7]) delta tracking (first collision or -1) or, with ratio = 1,
+ * ratio-tracking transmittance, from counter-based uniforms of seeds[i]. */
+int or_scene_set_medium(or_scene* s, const ar_medium_desc* m);
+float or_medium_density(const or_scene* s, const float* p3);
+void or_hg_sample(const float* d3, float g, const float* u2, int64_t n, float* out3);
+float or_hg_phase(float g, float cosT);
+void or_medium_track(const or_scene* s, const float* rays8, int64_t n, const uint32_t* seeds, int ratio, float* out);
+
 /* Deterministic transcendental functions (exported for their own tests). */
 /* Closest hit plus the hit's world position, normal and inside flag
  * (IntersectionContext fields), per ray; misses leave zeros. */

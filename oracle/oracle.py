@@ -79,6 +79,14 @@ def load():
     lib.or_bsdf_pdf.argtypes = [c_int, c_void_p, c_void_p, c_void_p, c_void_p]
     lib.or_bsdf_pdf.restype = c_float
     lib.or_power_heuristic.argtypes = [c_float, c_float]
+    lib.or_scene_set_medium.argtypes = [c_void_p, c_void_p]
+    lib.or_scene_set_medium.restype = c_int
+    lib.or_medium_density.argtypes = [c_void_p, c_void_p]
+    lib.or_medium_density.restype = c_float
+    lib.or_hg_sample.argtypes = [c_void_p, c_float, c_void_p, c_int64, c_void_p]
+    lib.or_hg_phase.argtypes = [c_float, c_float]
+    lib.or_hg_phase.restype = c_float
+    lib.or_medium_track.argtypes = [c_void_p, c_void_p, c_int64, c_void_p, c_int, c_void_p]
     lib.or_power_heuristic.restype = c_float
     _lib = lib
     return lib
@@ -187,6 +195,27 @@ class OracleScene:
             raise ValueError("bad spectral tables or resolution")
         self.spec_res = res
 
+    def set_medium(self, density, bounds_min=None, bounds_max=None, sigma_t_max=0.0, albedo=None, g=0.0) -> None:
+        """The participating medium of Scene.set_medium (same arguments)."""
+        from aperture_b200 import medium_desc
+        if density is None:
+            _lib.or_scene_set_medium(self._h, None)
+            return
+        d = np.ascontiguousarray(density)
+        m = medium_desc(d, bounds_min, bounds_max, sigma_t_max, albedo, g)
+        _lib.or_scene_set_medium(self._h, ctypes.byref(m))
+
+    def medium_density(self, p3) -> float:
+        p = np.ascontiguousarray(p3, np.float32)
+        return float(_lib.or_medium_density(self._h, _p(p)))
+
+    def medium_track(self, rays, seeds, ratio: bool = False) -> np.ndarray:
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        sd = np.ascontiguousarray(seeds, np.uint32)
+        out = np.zeros(len(r), np.float32)
+        _lib.or_medium_track(self._h, _p(r), len(r), _p(sd), 1 if ratio else 0, _p(out))
+        return out
+
     def spectral_luts(self):
         lam = np.zeros((840, 4), np.float32)
         rgb = np.zeros((self.spec_res ** 3, 4), np.float32)
@@ -288,3 +317,16 @@ def spectral_encode(tables: np.ndarray, rgb=None, lam=None):
     load().or_spectral_encode(_p(t), _p(r) if r is not None else None, _p(l_) if l_ is not None else None, n,
                               _p(rk) if rk is not None else None, _p(lk) if lk is not None else None)
     return rk, lk
+
+
+def hg_sample(d, g: float, u2) -> np.ndarray:
+    """Henyey-Greenstein directions around d for an [n, 2] array of uniforms."""
+    dd = np.ascontiguousarray(d, np.float32)
+    u = np.ascontiguousarray(u2, np.float32).reshape(-1, 2)
+    out = np.zeros((len(u), 3), np.float32)
+    load().or_hg_sample(_p(dd), g, _p(u), len(u), _p(out))
+    return out
+
+
+def hg_phase(g: float, cos_t: float) -> float:
+    return float(load().or_hg_phase(g, cos_t))
