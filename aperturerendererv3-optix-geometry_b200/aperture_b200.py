@@ -120,6 +120,35 @@ class Job(ctypes.Structure):
                 ("accum", c_void_p)]
 
 
+class NrcConfig(ctypes.Structure):
+    _fields_ = [("levels", c_int32), ("log2_entries", c_int32), ("base_resolution", c_int32),
+                ("max_resolution", c_int32), ("bounds_min", c_float * 3), ("bounds_max", c_float * 3),
+                ("train_paths", c_int32), ("train_batch", c_int32), ("train_steps", c_int32),
+                ("max_train_vertices", c_int32), ("learning_rate", c_float), ("spread_c", c_float),
+                ("seed", ctypes.c_uint64)]
+
+
+class NrcFrameStats(ctypes.Structure):
+    _fields_ = [("total_ms", c_float), ("render_ms", c_float), ("infer_ms", c_float), ("train_ms", c_float),
+                ("queries", c_int64), ("train_samples", c_int64), ("extension_rays", c_int64),
+                ("shadow_rays", c_int64), ("loss", c_float), ("reserved", c_int32)]
+
+
+NRC_PARAMS = 21504
+
+
+def nrc_config(levels=16, log2_entries=19, base_resolution=16, max_resolution=2048, bounds=None,
+               train_paths=65536, train_batch=16384, train_steps=4, max_train_vertices=8, learning_rate=1e-2,
+               spread_c=0.01, seed=1) -> NrcConfig:
+    c = NrcConfig(levels, log2_entries, base_resolution, max_resolution)
+    if bounds is not None:
+        c.bounds_min[:] = [float(x) for x in bounds[0]]
+        c.bounds_max[:] = [float(x) for x in bounds[1]]
+    c.train_paths, c.train_batch, c.train_steps = train_paths, train_batch, train_steps
+    c.max_train_vertices, c.learning_rate, c.spread_c, c.seed = max_train_vertices, learning_rate, spread_c, seed
+    return c
+
+
 class BatchStats(ctypes.Structure):
     _fields_ = [("total_ms", c_float), ("iterations_per_graph", c_int32), ("paths", c_int64),
                 ("extension_rays", c_int64), ("shadow_rays", c_int64), ("graph_launches", c_int64),
@@ -134,7 +163,8 @@ EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create",
                     "ar_scene_get_info", "ar_render", "ar_trace_rays", "ar_trace_rays_static",
                     "ar_render_debug_paths", "ar_rng_tape", "ar_tonemap", "ar_accum_resolve", "ar_tone_curve",
                     "ar_scene_set_spectral", "ar_scene_get_spectral_luts", "ar_render_batch",
-                    "ar_scene_set_medium")
+                    "ar_scene_set_medium", "ar_nrc_create", "ar_nrc_destroy", "ar_nrc_render_frame",
+                    "ar_nrc_get_params", "ar_nrc_set_params", "ar_nrc_infer", "ar_nrc_train", "ar_nrc_gradients")
 
 
 class ArError(RuntimeError):
@@ -190,6 +220,18 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_scene_set_medium.restype = c_int32
     lib.ar_render_batch.argtypes = [c_void_p, c_int32, c_int32, c_int64, POINTER(BatchStats), c_void_p]
     lib.ar_render_batch.restype = c_int32
+    lib.ar_nrc_create.argtypes = [c_void_p, POINTER(NrcConfig), POINTER(c_void_p)]
+    lib.ar_nrc_destroy.argtypes = [c_void_p]
+    lib.ar_nrc_render_frame.argtypes = [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p,
+                                        c_int32, POINTER(NrcFrameStats), c_void_p]
+    lib.ar_nrc_get_params.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.ar_nrc_set_params.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.ar_nrc_infer.argtypes = [c_void_p, c_void_p, c_size_t, c_void_p]
+    lib.ar_nrc_train.argtypes = [c_void_p, c_void_p, c_size_t, c_int32, c_void_p]
+    lib.ar_nrc_gradients.argtypes = [c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p]
+    for f in ("ar_nrc_create", "ar_nrc_destroy", "ar_nrc_render_frame", "ar_nrc_get_params", "ar_nrc_set_params",
+              "ar_nrc_infer", "ar_nrc_train", "ar_nrc_gradients"):
+        getattr(lib, f).restype = c_int32
     _lib = lib
     return lib
 
@@ -403,3 +445,68 @@ def render_batch(jobs, iterations_per_graph: int = 0, path_budget: int = 0, stre
     st = BatchStats()
     _check(lib.ar_render_batch(arr, len(jobs), iterations_per_graph, path_budget, ctypes.byref(st), c_void_p(stream)))
     return st
+
+
+class RadianceCache:
+    """ar_nrc: the learned radiance cache of a scene."""
+
+    def __init__(self, scene: "Scene", config: NrcConfig | None = None):
+        lib = load_library()
+        self.config = config or nrc_config()
+        self._scene = scene
+        h = c_void_p()
+        _check(lib.ar_nrc_create(scene.handle, ctypes.byref(self.config), ctypes.byref(h)))
+        self._h = h
+        self.table_floats = self.config.levels * (1 << self.config.log2_entries) * 2
+
+    def render_frame(self, camera: Camera, params: RenderParams, out_ptr: int | None, accum_ptr: int | None,
+                     train: bool = True, stats: bool = False, stream: int = 0):
+        st = NrcFrameStats() if stats else None
+        _check(_lib.ar_nrc_render_frame(self._h, ctypes.byref(camera), ctypes.byref(params),
+                                        c_void_p(out_ptr) if out_ptr else None,
+                                        c_void_p(accum_ptr) if accum_ptr else None, int(train),
+                                        ctypes.byref(st) if st is not None else None, c_void_p(stream)))
+        return st
+
+    def params(self):
+        t = np.empty(self.table_floats, np.float32)
+        w = np.empty(NRC_PARAMS, np.float32)
+        _check(_lib.ar_nrc_get_params(self._h, _ptr(t), _ptr(w)))
+        return t, w
+
+    def set_params(self, table: np.ndarray | None, weights: np.ndarray | None) -> None:
+        t = None if table is None else np.ascontiguousarray(table, np.float32)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        _check(_lib.ar_nrc_set_params(self._h, _ptr(t) if t is not None else None, _ptr(w) if w is not None else None))
+
+    def infer(self, vertices: np.ndarray) -> np.ndarray:
+        v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 16)
+        out = np.empty((len(v), 3), np.float32)
+        _check(_lib.ar_nrc_infer(self._h, _ptr(v), len(v), _ptr(out)))
+        return out
+
+    def train(self, samples: np.ndarray, steps: int) -> np.ndarray:
+        s = np.ascontiguousarray(samples, np.float32).reshape(-1, 16)
+        losses = np.zeros(max(steps, 1), np.float32)
+        _check(_lib.ar_nrc_train(self._h, _ptr(s), len(s), steps, _ptr(losses)))
+        return losses[:steps]
+
+    def gradients(self, samples: np.ndarray):
+        s = np.ascontiguousarray(samples, np.float32).reshape(-1, 16)
+        tg = np.empty(self.table_floats, np.float32)
+        wg = np.empty(NRC_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        _check(_lib.ar_nrc_gradients(self._h, _ptr(s), len(s), _ptr(tg), _ptr(wg), _ptr(loss)))
+        return tg, wg, float(loss[0])
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.ar_nrc_destroy(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <memory>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -101,6 +102,7 @@ struct ar_scene {
     float4* spec_lut_rgb = nullptr;
     int spec_res = 0;
     void* medium_grid = nullptr;                // density grid of the participating medium
+    float bounds[6] = {0, 0, 0, 0, 0, 0};       // box of the BVH root (min xyz, max xyz)
     std::vector<ar::SdfRec> h_sdf;              // data pointers into h_volumes
     std::vector<ar::HostVolume> h_volumes;
     // render workspace
@@ -271,7 +273,7 @@ ar::FrameParams make_frame(const ar_scene* s, const ar_camera* c, const ar_rende
 }
 
 ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* p, ar_path_record* rec_dev,
-                     cudaStream_t st, ar_render_stats* stats)
+                     cudaStream_t st, ar_render_stats* stats, const ar::NrcFrame* nrc = nullptr)
 {
     using namespace ar;
     if (p->spectral && !s->spec_tables)
@@ -282,6 +284,7 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
     int64_t pool = p->wave_paths > 0 ? std::min<int64_t>(p->wave_paths, kMaxPool) : kMaxPool;
     pool = std::max<int64_t>(1, std::min<int64_t>(pool, total));
     fp.pool = static_cast<int32_t>(pool);
+    if (nrc) fp.nrc = *nrc;
     ensure_workspace(s, pool, npix);
     PathBuffers B = s->bufs;
     B.capacity = static_cast<int32_t>(pool);
@@ -432,6 +435,21 @@ ar_status ar_scene_create_ex(const ar_object_desc* objects, size_t count, const 
     DeviceGuard g(device);
     ar_scene* s = new ar_scene();
     s->device = device;
+    if (!hs.nodes.empty()) {   // root box: origin + the largest quantised child upper bound
+        const ar::WideNode& r = hs.nodes[0];
+        const float o[3] = {r.ox, r.oy, r.oz};
+        const uint8_t* qhi[3] = {r.qhi_x, r.qhi_y, r.qhi_z};
+        const uint8_t* qlo[3] = {r.qlo_x, r.qlo_y, r.qlo_z};
+        for (int a = 0; a < 3; ++a) {
+            const int e = static_cast<int>((r.exps >> (8 * a)) & 0xFFu) - 127;
+            const float sc = std::ldexp(1.0f, e);
+            float hi = o[a];
+            for (int k = 0; k < 8; ++k)
+                if (qlo[a][k] <= qhi[a][k]) hi = std::max(hi, o[a] + static_cast<float>(qhi[a][k]) * sc);
+            s->bounds[a] = o[a];
+            s->bounds[3 + a] = hi;
+        }
+    }
     cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, device);
     try {
         auto own = [&](void* p, size_t bytes) { s->owned.push_back(p); s->device_bytes += static_cast<int64_t>(bytes); return p; };
@@ -1023,3 +1041,359 @@ ar_status ar_rng_tape(const ar_camera* cam, const ar_render_params* p, int32_t p
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ learned radiance cache
+struct ar_nrc {
+    ar_scene* scene = nullptr;
+    ar_nrc_config cfg{};
+    ar::NrcGrid grid{};
+    ar::NrcParams P{};
+    ar::NrcTrainBuffers T{};
+    int step = 0;
+    ar::NrcQuery* queries = nullptr;
+    int64_t query_cap = 0;
+    ar::NrcTrainVertex* tverts = nullptr;
+    ar::NrcSample* samples = nullptr;
+    int32_t* counters = nullptr;   // [0] queries, [1] samples, [2..] slot vertex counts
+    int slots = 0, sample_cap = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::vector<void*> owned;
+
+    ar::NrcNet net() const
+    {
+        ar::NrcNet n;
+        n.grid = grid;
+        n.table = P.table_h;
+        n.w = P.w_bf;
+        n.wt = P.wt_bf;
+        return n;
+    }
+    ~ar_nrc()
+    {
+        DeviceGuard g(scene->device);
+        for (void* p : owned) cudaFree(p);
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
+namespace {
+
+template <class T>
+T* nrc_alloc(ar_nrc* c, size_t count, const char* what)
+{
+    T* p = dalloc<T>(count, what);
+    c->owned.push_back(p);
+    return p;
+}
+
+void nrc_ensure_queries(ar_nrc* c, int64_t n)
+{
+    if (n <= c->query_cap) return;
+    for (auto it = c->owned.begin(); it != c->owned.end(); ++it)
+        if (*it == c->queries) { c->owned.erase(it); break; }
+    if (c->queries) cudaFree(c->queries);
+    c->queries = nrc_alloc<ar::NrcQuery>(c, static_cast<size_t>(n), "cache queries");
+    c->query_cap = n;
+}
+
+ar_status nrc_train_steps(ar_nrc* c, const ar::NrcSample* samples, const int32_t* count, int steps, cudaStream_t st)
+{
+    for (int k = 0; k < steps; ++k)
+        ck(ar::nrc_train_step(c->net(), c->P, samples, count, k * c->cfg.train_batch, c->cfg.train_batch, c->T,
+                              c->cfg.learning_rate, ++c->step, c->scene->sm_count, st), "cache training");
+    return AR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ar_status ar_nrc_create(ar_scene* s, const ar_nrc_config* cfg, ar_nrc** out)
+{
+    g_last_error.clear();
+    if (!s || !cfg || !out) return fail(AR_ERR_INVALID_ARGUMENT, "scene, config or out is NULL");
+    *out = nullptr;
+    if (cfg->levels < 1 || cfg->levels > ar::kNrcMaxLevels) return fail(AR_ERR_INVALID_ARGUMENT, "levels must be in [1, 16]");
+    if (cfg->log2_entries < 8 || cfg->log2_entries > 24) return fail(AR_ERR_INVALID_ARGUMENT, "log2_entries must be in [8, 24]");
+    if (cfg->base_resolution < 2 || cfg->max_resolution < cfg->base_resolution || cfg->max_resolution > (1 << 16))
+        return fail(AR_ERR_INVALID_ARGUMENT, "need 2 <= base_resolution <= max_resolution <= 65536");
+    if (cfg->train_paths < 1 || cfg->train_batch < 32 || cfg->train_steps < 0 || cfg->max_train_vertices < 1 ||
+        cfg->max_train_vertices > 64)
+        return fail(AR_ERR_INVALID_ARGUMENT, "bad training sizes");
+    if (!(cfg->learning_rate > 0.0f) || !(cfg->spread_c > 0.0f)) return fail(AR_ERR_INVALID_ARGUMENT, "learning_rate and spread_c must be positive");
+    float bmin[3], bmax[3];
+    bool given = true;
+    for (int a = 0; a < 3; ++a) given = given && cfg->bounds_max[a] > cfg->bounds_min[a];
+    for (int a = 0; a < 3; ++a) {
+        bmin[a] = given ? cfg->bounds_min[a] : s->bounds[a];
+        bmax[a] = given ? cfg->bounds_max[a] : s->bounds[3 + a];
+        if (!(bmax[a] > bmin[a])) return fail(AR_ERR_INVALID_ARGUMENT, "scene has no extent: give bounds");
+    }
+    AR_GUARD_BEGIN
+    DeviceGuard g(s->device);
+    std::unique_ptr<ar_nrc> c(new ar_nrc());
+    c->scene = s;
+    c->cfg = *cfg;
+    ar::NrcGrid& gr = c->grid;
+    gr.levels = cfg->levels;
+    const uint32_t entries = 1u << cfg->log2_entries;
+    gr.mask = entries - 1u;
+    const double b = cfg->levels > 1 ? std::exp((std::log(static_cast<double>(cfg->max_resolution)) -
+                                                 std::log(static_cast<double>(cfg->base_resolution))) / (cfg->levels - 1))
+                                     : 1.0;
+    for (int l = 0; l < ar::kNrcMaxLevels; ++l) {
+        const int r = l < cfg->levels ? static_cast<int>(std::floor(cfg->base_resolution * std::pow(b, l) + 1e-6)) : 1;
+        gr.res[l] = r;
+        const double cells = std::pow(static_cast<double>(r + 1), 3.0);
+        gr.dense[l] = cells <= static_cast<double>(entries) ? 1 : 0;
+    }
+    for (int a = 0; a < 3; ++a) {
+        gr.bmin[a] = bmin[a];
+        gr.inv_ext[a] = 1.0f / (bmax[a] - bmin[a]);
+    }
+    ar::NrcParams& P = c->P;
+    P.table_floats = static_cast<int64_t>(cfg->levels) * entries * 2;
+    const size_t tf = static_cast<size_t>(P.table_floats);
+    P.table_f32 = nrc_alloc<float>(c.get(), tf, "cache table");
+    P.table_m = nrc_alloc<float>(c.get(), tf, "cache table moments");
+    P.table_v = nrc_alloc<float>(c.get(), tf, "cache table moments");
+    P.table_g = nrc_alloc<float>(c.get(), tf, "cache table gradients");
+    P.table_h = nrc_alloc<__half2>(c.get(), tf / 2, "cache table half");
+    P.w_f32 = nrc_alloc<float>(c.get(), ar::kNrcParams, "cache weights");
+    P.w_m = nrc_alloc<float>(c.get(), ar::kNrcParams, "cache weights");
+    P.w_v = nrc_alloc<float>(c.get(), ar::kNrcParams, "cache weights");
+    P.w_g = nrc_alloc<float>(c.get(), ar::kNrcParams, "cache weights");
+    P.w_bf = nrc_alloc<__nv_bfloat16>(c.get(), ar::kNrcParams, "cache weights bf16");
+    P.wt_bf = nrc_alloc<__nv_bfloat16>(c.get(), ar::kNrcParams, "cache weights bf16");
+    ck(cudaMemset(P.table_m, 0, tf * 4), "memset");
+    ck(cudaMemset(P.table_v, 0, tf * 4), "memset");
+    ck(cudaMemset(P.table_g, 0, tf * 4), "memset");
+    ck(cudaMemset(P.w_m, 0, ar::kNrcParams * 4), "memset");
+    ck(cudaMemset(P.w_v, 0, ar::kNrcParams * 4), "memset");
+    ck(cudaMemset(P.w_g, 0, ar::kNrcParams * 4), "memset");
+    const size_t B = static_cast<size_t>(cfg->train_batch);
+    ar::NrcTrainBuffers& T = c->T;
+    T.acts = nrc_alloc<__nv_bfloat16>(c.get(), B * ar::kNrcIn * ar::kNrcLayers, "cache activations");
+    T.dz = nrc_alloc<__nv_bfloat16>(c.get(), B * ar::kNrcIn * ar::kNrcLayers, "cache gradients");
+    T.raw = nrc_alloc<float>(c.get(), B * 4, "cache outputs");
+    T.dx = nrc_alloc<float>(c.get(), B * 32, "cache input gradients");
+    T.loss = nrc_alloc<float>(c.get(), 1, "cache loss");
+    c->slots = cfg->train_paths + 1;
+    c->sample_cap = std::max(cfg->train_paths * cfg->max_train_vertices, cfg->train_batch * std::max(cfg->train_steps, 1));
+    c->tverts = nrc_alloc<ar::NrcTrainVertex>(c.get(), static_cast<size_t>(c->slots) * cfg->max_train_vertices, "cache training vertices");
+    c->samples = nrc_alloc<ar::NrcSample>(c.get(), static_cast<size_t>(c->sample_cap), "cache samples");
+    c->counters = nrc_alloc<int32_t>(c.get(), static_cast<size_t>(c->slots) + 2, "cache counters");
+    ck(ar::nrc_init_params(P, cfg->seed, nullptr), "cache init");
+    for (cudaEvent_t& e : c->ev) ck(cudaEventCreate(&e), "event");
+    ck(cudaDeviceSynchronize(), "cache init");
+    *out = c.release();
+    return AR_OK;
+    AR_GUARD_END
+}
+
+ar_status ar_nrc_destroy(ar_nrc* c)
+{
+    g_last_error.clear();
+    delete c;
+    return AR_OK;
+}
+
+ar_status ar_nrc_render_frame(ar_nrc* c, const ar_camera* cam, const ar_render_params* p, float* out_rgb,
+                              double* accum, int32_t train, ar_nrc_frame_stats* stats, void* stream)
+{
+    g_last_error.clear();
+    if (!c) return fail(AR_ERR_INVALID_ARGUMENT, "cache is NULL");
+    if (ar_status e = check_camera(cam)) return e;
+    if (ar_status e = check_params(p)) return e;
+    if (p->spp != 1) return fail(AR_ERR_INVALID_ARGUMENT, "cache frames take spp = 1");
+    if (p->spectral) return fail(AR_ERR_UNSUPPORTED, "the cache is RGB only");
+    if (!out_rgb && !accum) return fail(AR_ERR_INVALID_ARGUMENT, "out_rgb and accum are both NULL");
+    AR_GUARD_BEGIN
+    ar_scene* s = c->scene;
+    DeviceGuard g(s->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t npix = static_cast<int64_t>(cam->width) * cam->height;
+    nrc_ensure_queries(c, npix);
+    ck(cudaMemsetAsync(c->counters, 0, sizeof(int32_t) * (static_cast<size_t>(c->slots) + 2), st), "memset");
+    if (stats) ck(cudaMemsetAsync(c->T.loss, 0, sizeof(float), st), "memset");
+    ar::NrcFrame f{};
+    f.enabled = 1;
+    f.stride = static_cast<int32_t>(std::max<int64_t>(1, npix / c->cfg.train_paths));
+    f.offset = static_cast<int32_t>(ar::lowbias32(static_cast<uint32_t>(p->frame_offset) * 0x9E3779B9u ^
+                                                  static_cast<uint32_t>(p->seed)) % static_cast<uint32_t>(f.stride));
+    f.max_train_vertices = c->cfg.max_train_vertices;
+    f.spread_c = c->cfg.spread_c;
+    f.query_cap = static_cast<int32_t>(c->query_cap);
+    f.sample_cap = c->sample_cap;
+    f.slots = c->slots;
+    f.queries = c->queries;
+    f.query_count = c->counters;
+    f.train_vertices = c->tverts;
+    f.slot_count = c->counters + 2;
+    f.samples = c->samples;
+    f.sample_count = c->counters + 1;
+    ar_render_stats rs;
+    ck(cudaEventRecord(c->ev[0], st), "event");
+    if (ar_status e = run_render(s, cam, p, nullptr, st, stats ? &rs : nullptr, &f)) return e;
+    ck(cudaEventRecord(c->ev[1], st), "event");
+    ck(ar::nrc_infer(c->net(), c->queries, c->counters, static_cast<int>(c->query_cap), s->accum, nullptr,
+                     s->sm_count, st), "cache inference");
+    ck(cudaEventRecord(c->ev[2], st), "event");
+    if (train) nrc_train_steps(c, c->samples, c->counters + 1, c->cfg.train_steps, st);
+    ck(cudaEventRecord(c->ev[3], st), "event");
+    const int64_t n = npix * 3;
+    if (out_rgb) ck(ar::launch_mean(s->accum, n, 1.0, out_rgb, st), "mean");
+    if (accum) ck(ar::launch_add(s->accum, n, accum, st), "accumulate");
+    if (stats) {
+        int32_t cnt[2];
+        float loss = 0.0f;
+        ck(cudaMemcpyAsync(cnt, c->counters, sizeof(cnt), cudaMemcpyDeviceToHost, st), "copy counters");
+        ck(cudaMemcpyAsync(&loss, c->T.loss, sizeof(float), cudaMemcpyDeviceToHost, st), "copy loss");
+        ck(cudaStreamSynchronize(st), "sync");
+        std::memset(stats, 0, sizeof(*stats));
+        cudaEventElapsedTime(&stats->total_ms, c->ev[0], c->ev[3]);
+        cudaEventElapsedTime(&stats->render_ms, c->ev[0], c->ev[1]);
+        cudaEventElapsedTime(&stats->infer_ms, c->ev[1], c->ev[2]);
+        cudaEventElapsedTime(&stats->train_ms, c->ev[2], c->ev[3]);
+        stats->queries = cnt[0];
+        stats->train_samples = cnt[1];
+        stats->extension_rays = rs.extension_rays;
+        stats->shadow_rays = rs.shadow_rays;
+        stats->loss = train && c->cfg.train_steps > 0 ? loss / static_cast<float>(c->cfg.train_steps) : 0.0f;
+    }
+    return check_err(s, st);
+    AR_GUARD_END
+}
+
+ar_status ar_nrc_get_params(const ar_nrc* c, float* table, float* weights)
+{
+    g_last_error.clear();
+    if (!c) return fail(AR_ERR_INVALID_ARGUMENT, "cache is NULL");
+    AR_GUARD_BEGIN
+    DeviceGuard g(c->scene->device);
+    if (table) ck(cudaMemcpy(table, c->P.table_f32, static_cast<size_t>(c->P.table_floats) * 4, cudaMemcpyDeviceToHost), "copy table");
+    if (weights) ck(cudaMemcpy(weights, c->P.w_f32, ar::kNrcParams * 4, cudaMemcpyDeviceToHost), "copy weights");
+    return AR_OK;
+    AR_GUARD_END
+}
+
+ar_status ar_nrc_set_params(ar_nrc* c, const float* table, const float* weights)
+{
+    g_last_error.clear();
+    if (!c) return fail(AR_ERR_INVALID_ARGUMENT, "cache is NULL");
+    AR_GUARD_BEGIN
+    DeviceGuard g(c->scene->device);
+    if (table) ck(cudaMemcpy(c->P.table_f32, table, static_cast<size_t>(c->P.table_floats) * 4, cudaMemcpyHostToDevice), "copy table");
+    if (weights) ck(cudaMemcpy(c->P.w_f32, weights, ar::kNrcParams * 4, cudaMemcpyHostToDevice), "copy weights");
+    ck(ar::nrc_publish(c->P, nullptr), "publish");
+    ck(cudaDeviceSynchronize(), "sync");
+    return AR_OK;
+    AR_GUARD_END
+}
+
+ar_status ar_nrc_infer(ar_nrc* c, const float* vertices, size_t n, float* out_rgb)
+{
+    g_last_error.clear();
+    if (!c || (n && (!vertices || !out_rgb))) return fail(AR_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n > static_cast<size_t>(INT32_MAX)) return fail(AR_ERR_INVALID_ARGUMENT, "too many vertices");
+    if (n == 0) return AR_OK;
+    AR_GUARD_BEGIN
+    DeviceGuard g(c->scene->device);
+    ar::NrcQuery* q = dalloc<ar::NrcQuery>(n, "queries");
+    float* out = nullptr;
+    int32_t* cnt = nullptr;
+    cudaError_t e = cudaSuccess;
+    try {
+        out = dalloc<float>(n * 3, "predictions");
+        cnt = dalloc<int32_t>(1, "count");
+        std::vector<ar::NrcQuery> h(n);
+        for (size_t i = 0; i < n; ++i) {
+            std::memcpy(&h[i].v, vertices + 16 * i, sizeof(ar::NrcVertex));
+            h[i].t = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        }
+        const int32_t ni = static_cast<int32_t>(n);
+        ck(cudaMemcpy(q, h.data(), n * sizeof(ar::NrcQuery), cudaMemcpyHostToDevice), "copy vertices");
+        ck(cudaMemcpy(cnt, &ni, 4, cudaMemcpyHostToDevice), "copy count");
+        e = ar::nrc_infer(c->net(), q, cnt, ni, nullptr, out, c->scene->sm_count, nullptr);
+        if (e == cudaSuccess) e = cudaMemcpy(out_rgb, out, n * 12, cudaMemcpyDeviceToHost);
+    } catch (...) {
+        cudaFree(q); cudaFree(out); cudaFree(cnt);
+        throw;
+    }
+    cudaFree(q); cudaFree(out); cudaFree(cnt);
+    ck(e, "cache inference");
+    return AR_OK;
+    AR_GUARD_END
+}
+
+ar_status ar_nrc_gradients(ar_nrc* c, const float* samples, size_t n, float* table_grad, float* weight_grad,
+                           float* loss)
+{
+    g_last_error.clear();
+    if (!c || !samples || n == 0) return fail(AR_ERR_INVALID_ARGUMENT, "bad argument");
+    if (n > static_cast<size_t>(c->cfg.train_batch)) return fail(AR_ERR_INVALID_ARGUMENT, "n exceeds train_batch");
+    AR_GUARD_BEGIN
+    DeviceGuard g(c->scene->device);
+    ar::NrcSample* d = dalloc<ar::NrcSample>(n, "samples");
+    int32_t* cnt = nullptr;
+    try {
+        cnt = dalloc<int32_t>(1, "count");
+        const int32_t ni = static_cast<int32_t>(n);
+        ck(cudaMemcpy(d, samples, n * sizeof(ar::NrcSample), cudaMemcpyHostToDevice), "copy samples");
+        ck(cudaMemcpy(cnt, &ni, 4, cudaMemcpyHostToDevice), "copy count");
+        ck(cudaMemset(c->T.loss, 0, 4), "memset");
+        ck(ar::nrc_train_step(c->net(), c->P, d, cnt, 0, c->cfg.train_batch, c->T, c->cfg.learning_rate, c->step + 1,
+                              c->scene->sm_count, nullptr, false), "cache gradients");
+        const size_t tf = static_cast<size_t>(c->P.table_floats);
+        std::vector<float> tg(tf), wg(ar::kNrcParams);
+        ck(cudaMemcpy(tg.data(), c->P.table_g, tf * 4, cudaMemcpyDeviceToHost), "copy gradients");
+        ck(cudaMemcpy(wg.data(), c->P.w_g, ar::kNrcParams * 4, cudaMemcpyDeviceToHost), "copy gradients");
+        if (loss) ck(cudaMemcpy(loss, c->T.loss, 4, cudaMemcpyDeviceToHost), "copy loss");
+        ck(cudaMemset(c->P.table_g, 0, tf * 4), "memset");
+        ck(cudaMemset(c->P.w_g, 0, ar::kNrcParams * 4), "memset");
+        const float inv = 1.0f / ar::kNrcLossScale;
+        if (table_grad) for (size_t i = 0; i < tf; ++i) table_grad[i] = tg[i] * inv;
+        if (weight_grad) for (int i = 0; i < ar::kNrcParams; ++i) weight_grad[i] = wg[static_cast<size_t>(i)] * inv;
+    } catch (...) {
+        cudaFree(d); cudaFree(cnt);
+        throw;
+    }
+    cudaFree(d); cudaFree(cnt);
+    return AR_OK;
+    AR_GUARD_END
+}
+
+ar_status ar_nrc_train(ar_nrc* c, const float* samples, size_t n, int32_t steps, float* losses)
+{
+    g_last_error.clear();
+    if (!c || (n && !samples) || steps < 0) return fail(AR_ERR_INVALID_ARGUMENT, "bad argument");
+    if (n > static_cast<size_t>(INT32_MAX)) return fail(AR_ERR_INVALID_ARGUMENT, "too many samples");
+    AR_GUARD_BEGIN
+    DeviceGuard g(c->scene->device);
+    ar::NrcSample* d = dalloc<ar::NrcSample>(std::max<size_t>(n, 1), "samples");
+    int32_t* cnt = nullptr;
+    try {
+        cnt = dalloc<int32_t>(1, "count");
+        const int32_t ni = static_cast<int32_t>(n);
+        if (n) ck(cudaMemcpy(d, samples, n * sizeof(ar::NrcSample), cudaMemcpyHostToDevice), "copy samples");
+        ck(cudaMemcpy(cnt, &ni, 4, cudaMemcpyHostToDevice), "copy count");
+        for (int k = 0; k < steps; ++k) {
+            ck(cudaMemset(c->T.loss, 0, 4), "memset");
+            ck(ar::nrc_train_step(c->net(), c->P, d, cnt, k * c->cfg.train_batch, c->cfg.train_batch, c->T,
+                                  c->cfg.learning_rate, ++c->step, c->scene->sm_count, nullptr), "cache training");
+            float l = 0.0f;
+            ck(cudaMemcpy(&l, c->T.loss, 4, cudaMemcpyDeviceToHost), "copy loss");
+            if (losses) losses[k] = l;
+        }
+    } catch (...) {
+        cudaFree(d); cudaFree(cnt);
+        throw;
+    }
+    cudaFree(d); cudaFree(cnt);
+    return AR_OK;
+    AR_GUARD_END
+}
+
+}  // extern "C"
+

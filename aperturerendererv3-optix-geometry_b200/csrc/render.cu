@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(SceneVi
 // the shadow query: Trace's material evaluation and hit offset, emission with
 // MIS, light sampling for NEE, throughput and Russian roulette.  kModel is the
 // shading model of every path of this launch's bucket, -1 = miss.
-template <int kModel, bool kExt, bool kSpec>
+template <int kModel, bool kExt, bool kSpec, bool kNrc>
 __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams fp, PathBuffers B, int cur,
                                                        PoolCtl* ctl, ar_path_record* rec)
 {
@@ -426,6 +426,44 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             }
         }
         if (kMed) pos = cro + crd * fbits(hr.z);  // no surface: the normal stays zero
+        // ---- learned radiance cache (extension): path spread (Mueller et al. 2021,
+        // a = (sum_i sqrt(|x_i-1 - x_i|^2 / (p_i |cos_i|)))^2 against
+        // a0 = |x_0 - x_1|^2 / (4 pi |cos_1|)), training vertices, termination
+        bool nrcQuery = false;
+        float nrcS = 0.0f, nrcA = 0.0f;
+        NrcVertex nv;
+        if (kNrc) {
+            nrcS = __uint_as_float(pr.rng1.w);
+            nrcA = pr.vloc.w;
+            if (hit && !inside && kModel != AR_MAT_LIGHT && kModel != AR_MAT_GLASS) {
+                const float tt = fbits(hr.z);
+                const float cosT = fmaxf(fabsf(dot(nrm, crd)), 1e-4f);
+                if (depth == 0) {
+                    nrcA = tt / sqrtf(4.0f * kPi * cosT);
+                    nrcS = 0.0f;
+                } else {
+                    nrcS = nrcS + tt / sqrtf(fmaxf(pr.prev.w, 1e-12f) * cosT);
+                }
+                nv.p = make_float4(pos.x, pos.y, pos.z, fbits(pixel));
+                nv.d = make_float4(-crd.x, -crd.y, -crd.z, kModel == AR_MAT_GGX ? gb.roughness : 1.0f);
+                nv.n = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
+                nv.a = make_float4(gb.albedo.x, gb.albedo.y, gb.albedo.z, 0.0f);
+                int slot;
+                if (nrc_train_slot(fp.nrc, pixel, &slot)) {
+                    const int kv = fp.nrc.slot_count[slot];
+                    if (kv < fp.nrc.max_train_vertices) {
+                        NrcTrainVertex tv;
+                        tv.v = nv;
+                        tv.t = f4(mask, 0.0f);
+                        tv.lb = f4(radiance, 0.0f);
+                        fp.nrc.train_vertices[static_cast<int64_t>(slot) * fp.nrc.max_train_vertices + kv] = tv;
+                        fp.nrc.slot_count[slot] = kv + 1;
+                    }
+                } else if (depth >= 1 && nrcS > sqrtf(fp.nrc.spread_c) * nrcA) {
+                    nrcQuery = true;
+                }
+            }
+        }
         // ---- SampleContext (material.cuh:19-37, 177-330, 389-425)
         f3 next = mk(0.0f, 0.0f, 0.0f), emis = mk(0.0f, 0.0f, 0.0f), brdf = mk(0.0f, 0.0f, 0.0f);
         float pdf = 1.0f;
@@ -536,7 +574,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         // ---- emission (render.cuh:648-723)
         if (!hit && !kMed) {
             if (!missThin) radiance = radiance + (mask * emis) * d65;
-        } else if (hit && light >= 0) {
+        } else if (hit && light >= 0 && !nrcQuery) {
             float misW = 1.0f;
             if (fp.use_nee && depth > 0 && (flags & kFlagPrevNEE)) {
                 const float pB = fmaxf(pr.prev.w, 0.0f);
@@ -545,7 +583,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             }
             radiance = radiance + ((mask * emis) * d65) * misW;
         }
-        const bool brk = (!hit && !kMed && !missThin) || terminate;
+        const bool brk = (!hit && !kMed && !missThin) || terminate || nrcQuery;
         bool cont = false, shadow = false, cosOK = false;
         f3 pending = mk(0.0f, 0.0f, 0.0f), lightP = mk(0.0f, 0.0f, 0.0f);
         float4 prevOut = pr.prev;
@@ -588,7 +626,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                 }
                 // previousDidNEE_ is decided by the shadow query when one is cast
                 flags &= ~kFlagPrevNEE;
-                prevOut = f4(pos, pdf);
+                prevOut = f4(pos, (kNrc && delta) ? INFINITY : pdf);
             }
             // ---- throughput and Russian roulette (render.cuh:829-907)
             const f3 contrib = mk(brdf.x / fmaxf(pdf, 1e-12f), brdf.y / fmaxf(pdf, 1e-12f), brdf.z / fmaxf(pdf, 1e-12f));
@@ -613,6 +651,15 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         int target;
         const int j = warp_alloc(&ctl->count[1 - cur], cont);
         const int r = warp_alloc(&ctl->retire_count, !cont);
+        if (kNrc) {   // the path ends here; the cache supplies the rest
+            const int qi = warp_alloc(fp.nrc.query_count, nrcQuery);
+            if (nrcQuery && qi < fp.nrc.query_cap) {
+                NrcQuery qq;
+                qq.v = nv;
+                qq.t = f4(mask, 0.0f);
+                fp.nrc.queries[qi] = qq;
+            }
+        }
         if (cont) {
             PathRec out;
             out.o = f4(pos, fbits((depth + 1) | (nonDelta << 16)));
@@ -620,9 +667,9 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             out.mask = kSpec ? make_float4(mask.x, lambda, lpdf, fbits(pixel)) : f4(mask, fbits(pixel));
             out.rad = kSpec ? make_float4(radiance.x, 0.0f, 0.0f, fbits(sidx)) : f4(radiance, fbits(sidx));
             out.rng0 = make_uint4(g.st.d, g.st.v[0], g.st.v[1], g.st.v[2]);
-            out.rng1 = make_uint4(g.st.v[3], g.st.v[4], static_cast<uint32_t>(nmobj), used);
+            out.rng1 = make_uint4(g.st.v[3], g.st.v[4], static_cast<uint32_t>(nmobj), kNrc ? __float_as_uint(nrcS) : used);
             out.prev = prevOut;
-            out.vloc = f4(nvloc, 0.0f);
+            out.vloc = f4(nvloc, kNrc ? nrcA : 0.0f);
             next_pool[j] = out;
             target = j;
         } else {
@@ -764,6 +811,28 @@ __global__ void k_retire(FrameParams fp, PathBuffers B, PoolCtl* ctl, double* ac
         const float y = fmaxf(clampf(v.y, 0.0f, 1.0e3f), 0.0f);
         const float z = fmaxf(clampf(v.z, 0.0f, 1.0e3f), 0.0f);
         const int pixel = ibits(rr.rad.w);
+        int slot;
+        if (fp.nrc.enabled && nrc_train_slot(fp.nrc, pixel, &slot)) {
+            // training targets: radiance gathered after each recorded vertex,
+            // divided by the throughput that reached it
+            const int nvtx = fp.nrc.slot_count[slot];
+            const f3 L = mk(fix_nan_inf(rr.rad.x), fix_nan_inf(rr.rad.y), fix_nan_inf(rr.rad.z));
+            for (int k = 0; k < nvtx; ++k) {
+                const NrcTrainVertex tv = fp.nrc.train_vertices[static_cast<int64_t>(slot) * fp.nrc.max_train_vertices + k];
+                const f3 tgt = mk(tv.t.x > 1e-6f ? (L.x - tv.lb.x) / tv.t.x : 0.0f,
+                                  tv.t.y > 1e-6f ? (L.y - tv.lb.y) / tv.t.y : 0.0f,
+                                  tv.t.z > 1e-6f ? (L.z - tv.lb.z) / tv.t.z : 0.0f);
+                const int si = atomicAdd(fp.nrc.sample_count, 1);
+                if (si < fp.nrc.sample_cap) {
+                    NrcSample sm;
+                    sm.v = tv.v;
+                    sm.v.p.w = fminf(fmaxf(tgt.x, 0.0f), 1.0e3f);
+                    sm.v.n.w = fminf(fmaxf(tgt.y, 0.0f), 1.0e3f);
+                    sm.v.a.w = fminf(fmaxf(tgt.z, 0.0f), 1.0e3f);
+                    fp.nrc.samples[si] = sm;
+                }
+            }
+        }
         double* a = accum + 3 * static_cast<int64_t>(pixel);
         atomicAdd(a + 0, static_cast<double>(x));
         atomicAdd(a + 1, static_cast<double>(y));
@@ -848,16 +917,17 @@ cudaError_t launch_pool_init(PoolCtl* ctl, int64_t total, cudaStream_t st)
 }
 
 // The five per-material shading launches of one iteration.
-template <bool kExt, bool kSpec>
+template <bool kExt, bool kSpec, bool kNrc>
 void launch_shade(const SceneView& s, const FrameParams& fp, const PathBuffers& B, int c, PoolCtl* ctl,
                   ar_path_record* rec, int grid, cudaStream_t st)
 {
-    k_shade<-1, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_DIFFUSE, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_LIGHT, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_GLASS, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_GGX, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    if (kExt && s.has_medium) k_shade<kModelMedium, kExt, kSpec><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<-1, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_DIFFUSE, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_LIGHT, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_GLASS, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_GGX, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    if (kExt && s.has_medium)
+        k_shade<kModelMedium, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
 }
 
 cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const PathBuffers& B, PoolCtl* ctl,
@@ -876,11 +946,14 @@ cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const P
         else k_extend<false><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err, fp.medium_key);
         if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend++ + 1], st);
         if (fp.spectral) {
-            if (ext) launch_shade<true, true>(s, fp, B, c, ctl, rec, grid_other, st);
-            else launch_shade<false, true>(s, fp, B, c, ctl, rec, grid_other, st);
+            if (ext) launch_shade<true, true, false>(s, fp, B, c, ctl, rec, grid_other, st);
+            else launch_shade<false, true, false>(s, fp, B, c, ctl, rec, grid_other, st);
+        } else if (fp.nrc.enabled) {
+            if (ext) launch_shade<true, false, true>(s, fp, B, c, ctl, rec, grid_other, st);
+            else launch_shade<false, false, true>(s, fp, B, c, ctl, rec, grid_other, st);
         } else {
-            if (ext) launch_shade<true, false>(s, fp, B, c, ctl, rec, grid_other, st);
-            else launch_shade<false, false>(s, fp, B, c, ctl, rec, grid_other, st);
+            if (ext) launch_shade<true, false, false>(s, fp, B, c, ctl, rec, grid_other, st);
+            else launch_shade<false, false, false>(s, fp, B, c, ctl, rec, grid_other, st);
         }
         const bool ts = tm && tm->n_shadow < tm->cap;
         if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow], st);

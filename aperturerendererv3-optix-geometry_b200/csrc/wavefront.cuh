@@ -23,6 +23,7 @@
 #include <cstdint>
 
 #include "../../include/aperture_b200.h"
+#include "nrc.cuh"
 #include "spectral.cuh"
 #include "traverse.cuh"
 
@@ -43,9 +44,9 @@ struct alignas(16) PathRec {
     float4 mask;  // throughput rgb (spectral: x throughput, y wavelength, z its pdf); w: pixel (int bits)
     float4 rad;   // radiance rgb (spectral: x); w: sample index (int bits)
     uint4 rng0;   // xorwow d, v0, v1, v2
-    uint4 rng1;   // xorwow v3, v4; z media object; w uniforms consumed
-    float4 prev;  // previous NEE vertex xyz; w previous BSDF pdf
-    float4 vloc;  // media vertex location xyz
+    uint4 rng1;   // xorwow v3, v4; z media object; w uniforms consumed (cache mode: spread sum, float bits)
+    float4 prev;  // previous NEE vertex xyz; w previous BSDF pdf (cache mode: +inf after a delta event)
+    float4 vloc;  // media vertex location xyz; w (cache mode) square root of the primary spread a0
 };
 static_assert(sizeof(PathRec) == 128, "PathRec must be one 128-byte line");
 
@@ -107,6 +108,7 @@ struct FrameParams {
     int32_t tri_light_nee;   // 1: NEE also samples triangle lights (extension)
     SpectralView spec;       // tables and lookup tables of the spectral mode
     uint32_t medium_key;     // medium_frame_key(seed, frame0)
+    NrcFrame nrc;            // learned radiance cache hooks (enabled = 0: plain tracer)
 };
 
 }  // namespace ar

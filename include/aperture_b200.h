@@ -298,6 +298,77 @@ typedef struct ar_medium_desc {
  * scene's device. */
 ar_status ar_scene_set_medium(ar_scene* scene, const ar_medium_desc* medium);
 
+/* ------------------------------------------------------------------------ */
+/* Learned radiance cache (extension; the reference has none).               */
+/* A multiresolution hash-grid encoding of position (half-float tables),     */
+/* degree-4 spherical harmonics of the outgoing direction, roughness,        */
+/* diffuse albedo and normal feed a 64-wide MLP (5 hidden ReLU layers, exp   */
+/* output, bf16 weights and activations, fp32 accumulation) trained online    */
+/* with a relative L2 loss and Adam on radiance estimates of a subset of      */
+/* full-length "training" paths; the other paths end at the first vertex      */
+/* whose path spread exceeds spread_c times the primary footprint and take    */
+/* the cache's prediction there (Mueller et al. 2021).                        */
+/* ------------------------------------------------------------------------ */
+typedef struct ar_nrc ar_nrc;
+
+typedef struct ar_nrc_config {
+    int32_t levels;             /* hash-grid levels, <= 16 (16)                      */
+    int32_t log2_entries;       /* table entries per level = 2^log2_entries (19)    */
+    int32_t base_resolution;    /* coarsest grid resolution (16)                     */
+    int32_t max_resolution;     /* finest grid resolution (2048)                     */
+    float bounds_min[3];        /* box of the position encoding; bounds_max <=      */
+    float bounds_max[3];        /* bounds_min takes the scene's bounding box         */
+    int32_t train_paths;        /* training paths per frame (65536)                  */
+    int32_t train_batch;        /* samples per optimiser step (16384)                */
+    int32_t train_steps;        /* optimiser steps per frame (4)                     */
+    int32_t max_train_vertices; /* vertices recorded per training path (8)           */
+    float learning_rate;        /* Adam (1e-2; beta1 0.9, beta2 0.99)                */
+    float spread_c;             /* termination threshold c (0.01)                    */
+    uint64_t seed;              /* initial weights and tables                        */
+} ar_nrc_config;
+
+typedef struct ar_nrc_frame_stats {
+    float total_ms;             /* device time of the frame                          */
+    float render_ms;            /* path tracing (extension + shade + shadow)         */
+    float infer_ms;             /* cache queries                                     */
+    float train_ms;             /* optimiser steps                                   */
+    int64_t queries;            /* paths terminated into the cache                   */
+    int64_t train_samples;      /* training samples produced                         */
+    int64_t extension_rays;
+    int64_t shadow_rays;
+    float loss;                 /* mean relative L2 loss of the frame's steps         */
+    int32_t reserved;
+} ar_nrc_frame_stats;
+
+/* Cache of one scene (the scene must outlive it). */
+ar_status ar_nrc_create(ar_scene* scene, const ar_nrc_config* config, ar_nrc** out);
+ar_status ar_nrc_destroy(ar_nrc* nrc);
+/* One frame of 1 sample per pixel (params->spp must be 1, RGB): paths that
+ * end in the cache add throughput x prediction; with train != 0 the frame's
+ * training samples then take train_steps optimiser steps.  out_rgb (this
+ * frame's image) and accum (FP64 sums added) are device buffers; either may
+ * be NULL, not both.  stats may be NULL (then no host synchronisation). */
+ar_status ar_nrc_render_frame(ar_nrc* nrc, const ar_camera* camera, const ar_render_params* params,
+                              float* out_rgb, double* accum, int32_t train, ar_nrc_frame_stats* stats,
+                              void* stream);
+/* Parameters as fp32: tables (levels x 2^log2_entries x 2) and MLP weights
+ * (21504: layers 0-4 [64][64], layer 5 [16][64], [out][in]); NULL skips. */
+ar_status ar_nrc_get_params(const ar_nrc* nrc, float* table, float* weights);
+ar_status ar_nrc_set_params(ar_nrc* nrc, const float* table, const float* weights);
+/* Direct use of the network: n vertices of 16 floats (position, pad;
+ * direction, roughness; normal, pad; albedo, pad) -> n x 3 predictions; and
+ * `steps` optimiser steps over n training samples (the vertex layout with
+ * the target radiance in the three pad floats: r at 3, g at 11, b at 15),
+ * batches taken in order, the mean loss of each step to losses[steps].  Host
+ * buffers. */
+ar_status ar_nrc_infer(ar_nrc* nrc, const float* vertices, size_t n, float* out_rgb);
+ar_status ar_nrc_train(ar_nrc* nrc, const float* samples, size_t n, int32_t steps, float* losses);
+/* Gradients of the mean relative L2 loss over n <= train_batch samples with
+ * respect to the table entries and the weights (layouts of
+ * ar_nrc_get_params), without an update; loss may be NULL. */
+ar_status ar_nrc_gradients(ar_nrc* nrc, const float* samples, size_t n, float* table_grad, float* weight_grad,
+                           float* loss);
+
 /* One job of a batch: a scene (shared between jobs if wanted), a camera, the
  * render parameters and device outputs (mean image and/or FP64 sums added). */
 typedef struct ar_job {

@@ -1,0 +1,121 @@
+"""Learned radiance cache on the GPU: inference and gradients of the CUDA
+kernels (bf16 mma.sync MLP, hash-grid encoding and its backward) against the
+numpy restatement (oracle/nrc_oracle.py, itself checked against finite
+differences), training on a known field, and whole frames of the
+cache-terminated tracer converging to the plain tracer's image."""
+import numpy as np
+import pytest
+
+import nrc_oracle as N
+import scenes
+from aperture_b200 import RadianceCache, Scene, make_params, nrc_config
+
+BOUNDS = ((-0.6, -0.6, -0.6), (0.6, 0.6, 0.6))
+
+
+def _cache(**kw):
+    cfg = nrc_config(bounds=BOUNDS, **kw)
+    sc = Scene(scenes.box_scene())
+    return sc, RadianceCache(sc, cfg), cfg
+
+
+def _vertices(n, seed):
+    rng = np.random.default_rng(seed)
+    v = np.zeros((n, 16), np.float32)
+    v[:, 0:3] = rng.uniform(-0.55, 0.55, (n, 3))
+    d = rng.normal(size=(n, 3))
+    v[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    v[:, 7] = rng.uniform(0, 1, n)
+    nr = rng.normal(size=(n, 3))
+    v[:, 8:11] = nr / np.linalg.norm(nr, axis=1, keepdims=True)
+    v[:, 12:15] = rng.uniform(0, 1, (n, 3))
+    return v
+
+
+def _random_params(c, seed, tscale=0.5, wscale=0.25):
+    rng = np.random.default_rng(seed)
+    t = rng.uniform(-tscale, tscale, c.table_floats).astype(np.float32)
+    w = rng.uniform(-wscale, wscale, N.PARAMS).astype(np.float32)
+    c.set_params(t, w)
+    return t.astype(np.float16).astype(np.float32).reshape(-1, 2), w
+
+
+def _geo(cfg):
+    return N.Geometry(cfg.levels, cfg.log2_entries, cfg.base_resolution, cfg.max_resolution, BOUNDS[0], BOUNDS[1])
+
+
+@pytest.mark.gpu
+def test_nrc_inference_equals_oracle():
+    _, c, cfg = _cache(log2_entries=15)
+    table, w = _random_params(c, 1)
+    v = _vertices(5000, 2)
+    g = c.infer(v)
+    o = N.predict(_geo(cfg), v, table, w)
+    rel = np.abs(g - o) / np.maximum(np.abs(o), 1e-6)
+    assert np.median(rel) < 1e-3 and np.mean(rel) < 5e-3, (np.median(rel), np.mean(rel), rel.max())
+    assert np.percentile(rel, 99) < 0.05
+
+
+@pytest.mark.gpu
+def test_nrc_gradients_equal_oracle():
+    _, c, cfg = _cache(log2_entries=15, train_batch=2048)
+    table, w = _random_params(c, 3, 0.3, 0.2)
+    s = _vertices(2000, 4)
+    s[:, [3, 11, 15]] = np.random.default_rng(5).uniform(0.05, 3.0, (2000, 3))
+    tg, wg, loss = c.gradients(s)
+    lo, dT, dW = N.loss_and_gradients(_geo(cfg), s, table, w)
+    assert abs(loss - lo) <= 1e-3 * abs(lo)
+    assert np.linalg.norm(wg - dW) <= 2e-2 * np.linalg.norm(dW)
+    dT = dT.reshape(-1)
+    assert np.linalg.norm(tg - dT) <= 2e-2 * np.linalg.norm(dT)
+    assert np.count_nonzero(dT) > 10000
+
+
+@pytest.mark.gpu
+def test_nrc_training_fits_a_smooth_field():
+    _, c, cfg = _cache(log2_entries=16, train_batch=4096)
+    s = _vertices(4096 * 50, 6)
+    p, d = s[:, 0:3], s[:, 4:7]
+    field = np.stack([1.0 + np.sin(4 * p[:, 0]) * 0.5 + 0.3 * d[:, 1],
+                      0.5 + 0.4 * np.cos(3 * p[:, 1] + p[:, 2]),
+                      0.2 + np.exp(-4 * (p ** 2).sum(1)) + 0.2 * (d[:, 2] > 0)], 1)
+    s[:, [3, 11, 15]] = field
+    losses = c.train(s, 50)
+    losses2 = np.concatenate([c.train(s, 50) for _ in range(3)])
+    assert losses2[-10:].mean() < 0.1 * losses[:3].mean(), (losses[:3], losses2[-10:])
+    test = _vertices(4000, 7)
+    pt, dt = test[:, 0:3], test[:, 4:7]
+    want = np.stack([1.0 + np.sin(4 * pt[:, 0]) * 0.5 + 0.3 * dt[:, 1],
+                     0.5 + 0.4 * np.cos(3 * pt[:, 1] + pt[:, 2]),
+                     0.2 + np.exp(-4 * (pt ** 2).sum(1)) + 0.2 * (dt[:, 2] > 0)], 1)
+    got = c.infer(test)
+    assert np.mean(np.abs(got - want) / want) < 0.1
+
+
+@pytest.mark.gpu
+def test_nrc_frames_converge_to_plain_image():
+    import torch
+    objs = scenes.box_scene()
+    sc = Scene(objs)
+    cam = scenes.box_camera(64, 64)
+    ref, _ = sc.render(cam, make_params(spp=1024, max_depth=8))
+    cfg = nrc_config(bounds=BOUNDS, log2_entries=16, train_paths=1024, train_batch=2048, train_steps=2)
+    c = RadianceCache(sc, cfg)
+    n = 64 * 64 * 3
+    acc = torch.zeros(n, dtype=torch.float64, device="cuda")
+    frames = 256
+    queries = 0
+    for f in range(frames):
+        st = c.render_frame(cam, make_params(spp=1, max_depth=8, frame_offset=f), None, acc.data_ptr(),
+                            train=True, stats=(f % 64 == 63))
+        if st is not None:
+            queries = st.queries
+            assert st.train_samples > 500
+    img = (acc / frames).cpu().numpy().reshape(64, 64, 3)
+    rel = ((img - ref) ** 2 / (ref ** 2 + 1e-2)).mean()
+    assert queries > 1000
+    assert rel < 0.02, rel
+    # the cache removes most of the noise of the plain tracer at equal frames
+    plain, _ = sc.render(cam, make_params(spp=frames, max_depth=8, frame_offset=100000))
+    rel_plain = ((plain - ref) ** 2 / (ref ** 2 + 1e-2)).mean()
+    print("relMSE cache", rel, "plain", rel_plain)
