@@ -113,6 +113,11 @@ struct ar_scene {
     ar::PathBuffers bufs{};
     uint4* base0 = nullptr;
     uint2* base1 = nullptr;
+    // the per-pixel generator states in base0/base1 are those of frame
+    // rng_next_frame for (rng_seed, rng_width, rng_height) when rng_valid
+    bool rng_valid = false;
+    uint64_t rng_seed = 0, rng_next_frame = 0;
+    int rng_width = 0, rng_height = 0;
     double* accum = nullptr;
     float* fout = nullptr;
     ar::PoolCtl* ctl = nullptr;
@@ -157,6 +162,7 @@ void ensure_workspace(ar_scene* s, int64_t pool, int64_t npix)
     s->ws_bytes = off;
     s->ws_wave = pool;
     s->ws_pix = npix;
+    s->rng_valid = false;
     char* b = s->ws;
     ar::PathBuffers& B = s->bufs;
     B.pool[0] = reinterpret_cast<ar::PathRec*>(b + o_p0);
@@ -293,7 +299,14 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
     ck(cudaMemsetAsync(s->err, 0, 64, st), "memset err");
     if (!s->ev0) { ck(cudaEventCreate(&s->ev0), "event"); ck(cudaEventCreate(&s->ev1), "event"); }
     ck(cudaEventRecord(s->ev0, st), "event record");
-    ck(launch_rng_init(fp, s->base0, s->base1, st), "rng init");
+    // curand_init of every pixel (a skip-ahead per pixel) only when the stored
+    // states are not already those of this render's first frame: a render that
+    // continues the previous one (frame_offset = previous offset + spp, same
+    // seed and image) starts from the states the previous one left.
+    if (!(s->rng_valid && s->rng_seed == fp.seed && s->rng_width == fp.width && s->rng_height == fp.height &&
+          s->rng_next_frame == fp.frame0))
+        ck(launch_rng_init(fp, s->base0, s->base1, st), "rng init");
+    s->rng_valid = false;
     ck(launch_pool_init(s->ctl, total, st), "pool init");
     int64_t launches = 2;
     const int grid_trace = s->grid_trace;
@@ -333,6 +346,12 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
         if (retired >= total) break;
         if (iters > max_iter) return fail(AR_ERR_DEVICE_FAULT, "path pool did not drain");
     }
+    // every pixel's state advanced by one frame per sample (k_regen)
+    s->rng_valid = true;
+    s->rng_seed = fp.seed;
+    s->rng_width = fp.width;
+    s->rng_height = fp.height;
+    s->rng_next_frame = fp.frame0 + static_cast<uint64_t>(p->spp);
     ck(cudaEventRecord(s->ev1, st), "event record");
     if (stats) {
         unsigned long long h[6];
@@ -1219,7 +1238,7 @@ ar_status ar_nrc_render_frame(ar_nrc* c, const ar_camera* cam, const ar_render_p
     if (stats) ck(cudaMemsetAsync(c->T.loss, 0, sizeof(float), st), "memset");
     ar::NrcFrame f{};
     f.enabled = 1;
-    f.stride = static_cast<int32_t>(std::max<int64_t>(1, npix / c->cfg.train_paths));
+    f.stride = static_cast<int32_t>(std::max<int64_t>(1, (npix + c->cfg.train_paths - 1) / c->cfg.train_paths));
     f.offset = static_cast<int32_t>(ar::lowbias32(static_cast<uint32_t>(p->frame_offset) * 0x9E3779B9u ^
                                                   static_cast<uint32_t>(p->seed)) % static_cast<uint32_t>(f.stride));
     f.max_train_vertices = c->cfg.max_train_vertices;

@@ -321,3 +321,30 @@ def medium_box_scene(seed: int = SEED_BASE + 3, precision: int = 16, grid: int =
                   bounds_min=(-0.5, -0.5, -0.5), bounds_max=(0.5, 0.5, 0.5),
                   sigma_t_max=2.0, albedo=(0.8, 0.8, 0.8), g=0.3)
     return objects, volumes, medium
+
+
+def spline_cameras(seed: int = SEED_BASE + 4, frames: int = 300, width: int = 1920, height: int = 1080,
+                   fov: float = 60.0, control: int = 8):
+    """Config 4's camera path: a closed Catmull-Rom spline through `control`
+    seeded points on a ring around the config-2 scene (radius U(120, 180),
+    height U(15, 60)), looking at seeded points near the centre; one camera
+    per frame, uniform in the spline parameter."""
+    rng = np.random.default_rng(seed)
+    ang = np.sort(rng.uniform(0.0, 2.0 * np.pi, control))
+    rad = rng.uniform(120.0, 180.0, control)
+    pts = np.stack([rad * np.cos(ang), rng.uniform(15.0, 60.0, control), rad * np.sin(ang)], 1)
+    tgt = rng.uniform(-30.0, 30.0, (control, 3)) * np.array([1.0, 0.3, 1.0])
+
+    def cr(p, i, t):
+        p0, p1, p2, p3 = (p[(i + k) % control] for k in (-1, 0, 1, 2))
+        return 0.5 * ((2 * p1) + (-p0 + p2) * t + (2 * p0 - 5 * p1 + 4 * p2 - p3) * t * t
+                      + (-p0 + 3 * p1 - 3 * p2 + p3) * t * t * t)
+
+    cams = []
+    for f in range(frames):
+        u = f / frames * control
+        i, t = int(u), u - int(u)
+        pos, look = cr(pts, i, t), cr(tgt, i, t)
+        d = look - pos
+        cams.append(make_camera(pos, d / np.linalg.norm(d), fov, width, height))
+    return cams

@@ -36,7 +36,7 @@ ORACLE = os.path.join(ROOT, "oracle")
 sys.path.insert(0, PKG)
 
 import scenes  # noqa: E402
-from aperture_b200 import Camera, RenderParams, RenderStats, Scene, make_params  # noqa: E402
+from aperture_b200 import Camera, RadianceCache, RenderParams, RenderStats, Scene, make_params, nrc_config  # noqa: E402
 from sharding import job_totals, rank_frame_offset, reduce_accumulators  # noqa: E402
 
 METRIC = "Mrays/s"
@@ -147,6 +147,103 @@ def cpu_sample(objs, cam: Camera, params: RenderParams, target_s: float, threads
 
 
 # ----------------------------------------------------------------------------- ours
+NRC_SIZES = {"small": (480, 270, 16384, 4096), "full": (1920, 1080, 16384, 4096)}
+
+
+def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
+    """Config 4 on the config-2 scene: time to reach the plain tracer's relMSE
+    at `target` spp with the cache-terminated tracer (1 spp per frame, online
+    training), both against an FP64 oracle image of `ref` spp (plain tracer,
+    per-pixel FP64 sums on the GPU); then the 300-frame seeded spline camera
+    path at 1920x1080 (frames/s, per-stage times).  Device time (CUDA events
+    on the launching stream) excludes the relMSE evaluations."""
+    w, h, ref_spp, target = NRC_SIZES[mode]
+    npix = w * h
+    cam = scenes.spheres_camera(w, h)
+    out = torch.empty(npix * 3, dtype=torch.float32, device=dev)
+
+    def plain(spp_total: int, offset: int, acc):
+        ms = 0.0
+        chunk = 256
+        for k in range(0, spp_total, chunk):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            scene.render_device(cam, make_params(spp=min(chunk, spp_total - k), max_depth=DEPTH, frame_offset=offset + k),
+                                out.data_ptr(), acc.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+        return ms
+
+    def relmse(acc, n, ref):
+        img = acc / n
+        return float(((img - ref) ** 2 / (ref * ref + 1e-2)).mean())
+
+    with torch.cuda.stream(stream):
+        acc_ref = torch.zeros(npix * 3, dtype=torch.float64, device=dev)
+        ref_ms = plain(ref_spp, 10_000_000, acc_ref)
+        ref = acc_ref / ref_spp
+        acc_p = torch.zeros_like(acc_ref)
+        plain_ms = plain(target, 20_000_000, acc_p)
+        e_plain = relmse(acc_p, target, ref)
+        cache = RadianceCache(scene, nrc_config())
+        acc_n = torch.zeros_like(acc_ref)
+        t_ms, reached, curve = 0.0, None, []
+        max_ms = 3.0 * plain_ms
+        f = 0
+        check = 16
+        while t_ms < max_ms and f < 65536:
+            evs = []
+            for _ in range(check):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                cache.render_frame(cam, make_params(spp=1, max_depth=DEPTH, frame_offset=30_000_000 + f), None,
+                                   acc_n.data_ptr(), train=True, stream=stream.cuda_stream)
+                e1.record(stream)
+                evs.append((e0, e1))
+                f += 1
+            evs[-1][1].synchronize()
+            t_ms += sum(a.elapsed_time(b) for a, b in evs)
+            e = relmse(acc_n, f, ref)
+            curve.append((f, round(t_ms, 2), e))
+            if e <= e_plain:
+                reached = t_ms
+                break
+            check = min(check * 2, 256)
+        best = min(c[2] for c in curve)
+        res = {"workload": f"config4 static view: config-2 scene {w}x{h}, max depth {DEPTH}, 1 spp per frame, "
+                           f"cache trained online (65536 training paths, 4 steps of 16384 per frame)",
+               "oracle_spp": ref_spp, "oracle_ms": round(ref_ms, 1),
+               "plain_spp": target, "plain_ms": round(plain_ms, 2), "plain_relmse": e_plain,
+               "cache_frames": f, "cache_ms": round(t_ms, 2), "cache_relmse": curve[-1][2], "cache_best_relmse": best,
+               "reached": reached is not None,
+               "time_to_relmse_speedup": round(plain_ms / reached, 3) if reached else None,
+               "curve": [(a, b, round(c, 6)) for a, b, c in curve[:: max(1, len(curve) // 12)]]}
+        # the spline camera path at the full config-4 resolution
+        cams = scenes.spline_cameras(frames=300)
+        acc_s = torch.zeros(1920 * 1080 * 3, dtype=torch.float64, device=dev)
+        cache2 = RadianceCache(scene, nrc_config(seed=2))
+        tot = {"render": 0.0, "infer": 0.0, "train": 0.0, "total": 0.0, "q": 0, "rays": 0}
+        for k, c in enumerate(cams):
+            st = cache2.render_frame(c, make_params(spp=1, max_depth=DEPTH, frame_offset=40_000_000 + k), None,
+                                     acc_s.data_ptr(), train=True, stats=True, stream=stream.cuda_stream)
+            if k >= 10:
+                tot["render"] += st.render_ms
+                tot["infer"] += st.infer_ms
+                tot["train"] += st.train_ms
+                tot["total"] += st.total_ms
+                tot["q"] += st.queries
+                tot["rays"] += st.extension_rays + st.shadow_rays
+        n = len(cams) - 10
+        res["spline_1920x1080"] = {
+            "frames": len(cams), "timed_frames": n, "ms_per_frame": round(tot["total"] / n, 3),
+            "render_ms": round(tot["render"] / n, 3), "infer_ms": round(tot["infer"] / n, 3),
+            "train_ms": round(tot["train"] / n, 3), "queries_per_frame": int(tot["q"] / n),
+            "tracer_mrays_per_s": round(tot["rays"] / (tot["render"] / 1e3) / 1e6, 1),
+            "last_loss": round(float(st.loss), 5)}
+    return res
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -287,6 +384,8 @@ def run_ours(args) -> None:
             "gpu_launches": int(tot["launches"]),
             "clocks": clocks,
         }
+        if world == 1 and args.nrc != "off":
+            line["nrc"] = measure_nrc(torch, dev, scene, args.nrc, stream)
         if world == 1 and not args.no_cpu:
             cs = cpu_sample(objs, cam, params, args.cpu_seconds, cpu_threads())
             line["cpu_baseline"] = {"value": round(cs["value"], 4), "unit": "Mrays/s", "cores": cpu_threads(),
@@ -373,6 +472,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU sample length per measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--nrc", choices=("off", "small", "full"), default="small",
+                    help="radiance-cache time-to-relMSE measurement (small: 480x270, full: 1920x1080)")
     ap.add_argument("--profile-queues", action="store_true",
                     help="render the workload once at 1 spp (for ncu captures) and print the per-depth queue sizes")
     args = ap.parse_args()
