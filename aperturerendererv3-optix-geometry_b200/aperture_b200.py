@@ -149,6 +149,11 @@ def nrc_config(levels=16, log2_entries=19, base_resolution=16, max_resolution=20
     return c
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("iterations_per_graph", c_int32), ("candidates", c_int32), ("path_budget", c_int64),
+                ("best_ms", c_float), ("default_ms", c_float)]
+
+
 class BatchStats(ctypes.Structure):
     _fields_ = [("total_ms", c_float), ("iterations_per_graph", c_int32), ("paths", c_int64),
                 ("extension_rays", c_int64), ("shadow_rays", c_int64), ("graph_launches", c_int64),
@@ -164,7 +169,8 @@ EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create",
                     "ar_render_debug_paths", "ar_rng_tape", "ar_tonemap", "ar_accum_resolve", "ar_tone_curve",
                     "ar_scene_set_spectral", "ar_scene_get_spectral_luts", "ar_render_batch",
                     "ar_scene_set_medium", "ar_nrc_create", "ar_nrc_destroy", "ar_nrc_render_frame",
-                    "ar_nrc_get_params", "ar_nrc_set_params", "ar_nrc_infer", "ar_nrc_train", "ar_nrc_gradients")
+                    "ar_nrc_get_params", "ar_nrc_set_params", "ar_nrc_infer", "ar_nrc_train", "ar_nrc_gradients",
+                    "ar_batch_autotune")
 
 
 class ArError(RuntimeError):
@@ -220,6 +226,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_scene_set_medium.restype = c_int32
     lib.ar_render_batch.argtypes = [c_void_p, c_int32, c_int32, c_int64, POINTER(BatchStats), c_void_p]
     lib.ar_render_batch.restype = c_int32
+    lib.ar_batch_autotune.argtypes = [c_void_p, c_int32, c_int32, POINTER(BatchTuning), c_void_p]
+    lib.ar_batch_autotune.restype = c_int32
     lib.ar_nrc_create.argtypes = [c_void_p, POINTER(NrcConfig), POINTER(c_void_p)]
     lib.ar_nrc_destroy.argtypes = [c_void_p]
     lib.ar_nrc_render_frame.argtypes = [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p,
@@ -430,6 +438,27 @@ def make_volume(dims, data: np.ndarray | None = None, precision: int = 32, fill_
     v.fill_kind = fill_kind
     v.fill_info[:] = [float(x) for x in fill_info]
     return v, keep
+
+
+def _job_array(jobs):
+    arr = (Job * len(jobs))()
+    for k, (scene, cam, params, out_ptr, acc_ptr) in enumerate(jobs):
+        arr[k].scene = scene.handle
+        arr[k].camera = cam
+        arr[k].params = params
+        arr[k].out_rgb = out_ptr
+        arr[k].accum = acc_ptr
+    return arr
+
+
+def autotune_batch(jobs, probe_spp: int = 4, stream: int = 0) -> BatchTuning:
+    """ar_batch_autotune: choose graph length and path budget for this batch
+    shape; later render_batch calls with both left at 0 use the choice."""
+    lib = load_library()
+    arr = _job_array(jobs)
+    t = BatchTuning()
+    _check(lib.ar_batch_autotune(arr, len(jobs), probe_spp, ctypes.byref(t), c_void_p(stream)))
+    return t
 
 
 def render_batch(jobs, iterations_per_graph: int = 0, path_budget: int = 0, stream: int = 0) -> BatchStats:

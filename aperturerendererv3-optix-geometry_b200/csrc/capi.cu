@@ -7,7 +7,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -774,6 +777,36 @@ struct BatchResources {
 
 }  // namespace
 
+}  // extern "C"
+
+namespace {
+// Batch shape of the autotuner's memory: job count, pixels, samples, spectral jobs.
+struct BatchKey {
+    int32_t jobs;
+    int32_t spectral;
+    int64_t pixels, samples;
+    bool operator<(const BatchKey& o) const
+    {
+        return std::tie(jobs, spectral, pixels, samples) < std::tie(o.jobs, o.spectral, o.pixels, o.samples);
+    }
+};
+BatchKey batch_key(const ar_job* jobs, int32_t njobs)
+{
+    BatchKey k{njobs, 0, 0, 0};
+    for (int j = 0; j < njobs; ++j) {
+        const int64_t px = static_cast<int64_t>(jobs[j].camera.width) * jobs[j].camera.height;
+        k.pixels += px;
+        k.samples += px * jobs[j].params.spp;
+        k.spectral += jobs[j].params.spectral ? 1 : 0;
+    }
+    return k;
+}
+std::mutex g_tune_mutex;
+std::map<BatchKey, std::pair<int32_t, int64_t>> g_tuned;
+}  // namespace
+
+extern "C" {
+
 ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_per_graph, int64_t path_budget,
                           ar_batch_stats* stats, void* stream)
 {
@@ -791,6 +824,14 @@ ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_
         if (!jb.out_rgb && !jb.accum) return fail(AR_ERR_INVALID_ARGUMENT, "job " + std::to_string(j) + ": no output");
         if (jb.params.spectral && !jb.scene->spec_tables)
             return fail(AR_ERR_UNSUPPORTED, "job " + std::to_string(j) + ": spectral tables not set");
+    }
+    if (iterations_per_graph == 0 && path_budget == 0) {   // autotuned defaults for this batch shape
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tuned.find(batch_key(jobs, njobs));
+        if (it != g_tuned.end()) {
+            iterations_per_graph = it->second.first;
+            path_budget = it->second.second;
+        }
     }
     AR_GUARD_BEGIN
     DeviceGuard g(s0->device);
@@ -1410,6 +1451,59 @@ ar_status ar_nrc_train(ar_nrc* c, const float* samples, size_t n, int32_t steps,
         throw;
     }
     cudaFree(d); cudaFree(cnt);
+    return AR_OK;
+    AR_GUARD_END
+}
+
+ar_status ar_batch_autotune(const ar_job* jobs, int32_t njobs, int32_t probe_spp, ar_batch_tuning* out, void* stream)
+{
+    g_last_error.clear();
+    if (!jobs || njobs <= 0 || !out) return fail(AR_ERR_INVALID_ARGUMENT, "jobs or out is NULL");
+    for (int j = 0; j < njobs; ++j)
+        if (!jobs[j].scene) return fail(AR_ERR_INVALID_ARGUMENT, "job " + std::to_string(j) + ": scene is NULL");
+    if (probe_spp <= 0) probe_spp = 4;
+    AR_GUARD_BEGIN
+    DeviceGuard g(jobs[0].scene->device);
+    std::vector<ar_job> probe(jobs, jobs + njobs);
+    std::vector<float*> scratch;
+    struct Free {
+        std::vector<float*>& v;
+        ~Free() { for (float* p : v) cudaFree(p); }
+    } release{scratch};
+    for (ar_job& jb : probe) {
+        const size_t n = static_cast<size_t>(jb.camera.width) * static_cast<size_t>(jb.camera.height) * 3;
+        float* p = dalloc<float>(std::max<size_t>(n, 1), "autotune scratch");
+        scratch.push_back(p);
+        jb.out_rgb = p;
+        jb.accum = nullptr;
+        jb.params.spp = std::min(jb.params.spp, probe_spp);
+        jb.params.wave_paths = 0;
+    }
+    const int32_t ks[4] = {4, 8, 16, 32};
+    const int64_t bs[4] = {int64_t(1) << 20, int64_t(1) << 21, int64_t(1) << 22, int64_t(1) << 23};
+    ar_batch_stats st;
+    // first use of every workspace (allocations, graph set-up) outside the timing
+    if (ar_status e = ar_render_batch(probe.data(), njobs, 16, bs[2], &st, stream)) return e;
+    ar_batch_tuning best{16, 0, bs[2], 0.0f, 0.0f};
+    double best_rate = -1.0;
+    for (int32_t k : ks)
+        for (int64_t b : bs) {
+            if (ar_status e = ar_render_batch(probe.data(), njobs, k, b, &st, stream)) return e;
+            const double rate = static_cast<double>(st.paths) / std::max(1e-6, static_cast<double>(st.total_ms));
+            if (k == 16 && b == bs[2]) best.default_ms = st.total_ms;
+            ++best.candidates;
+            if (rate > best_rate) {
+                best_rate = rate;
+                best.iterations_per_graph = k;
+                best.path_budget = b;
+                best.best_ms = st.total_ms;
+            }
+        }
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tuned[batch_key(jobs, njobs)] = {best.iterations_per_graph, best.path_budget};
+    }
+    *out = best;
     return AR_OK;
     AR_GUARD_END
 }

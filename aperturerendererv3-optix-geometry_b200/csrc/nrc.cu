@@ -429,49 +429,83 @@ __global__ void __launch_bounds__(kNrcBlock) k_nrc_train_bwd(NrcNet net, const N
     if (lane == 0 && loss_acc != 0.0f) atomicAdd(T.loss, loss_acc);
 }
 
-// Weight gradients dW_l[o][i] = sum over rows of dz_l[row][o] * act_l[row][i]
-// (fp32 SIMT over 128-row chunks, one atomic per weight and chunk).
-constexpr int kWgRows = 64;
-__global__ void __launch_bounds__(256) k_nrc_wgrad(NrcTrainBuffers T, int batch, float* wg)
+// Weight gradients dW_l[o][i] = sum over rows of dz_l[row][o] * act_l[row][i],
+// on the tensor cores: per block a chunk of kWgRows rows of both operands is
+// staged in shared memory (rows padded to 72 bf16), each warp owns 16 output
+// rows o and all 64 inputs i, and the A (dz transposed) and B (act) fragments
+// come from ldmatrix.trans of the row-major tiles.  fp32 accumulators, one
+// atomic per weight and block.
+constexpr int kWgRows = 256;
+constexpr int kSmemWg = 2 * kWgRows * kNrcWRow * 2;   // 73728 B
+
+__device__ __forceinline__ void ldsm_x4_trans(const __nv_bfloat16* p, uint32_t& r0, uint32_t& r1, uint32_t& r2,
+                                              uint32_t& r3)
 {
-    __shared__ float sdz[kWgRows][kNrcHid + 1];
-    __shared__ float sac[kWgRows][kNrcIn + 4];
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(a));
+}
+
+__global__ void __launch_bounds__(kNrcBlock) k_nrc_wgrad(NrcTrainBuffers T, int batch, float* wg)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* sZ = reinterpret_cast<__nv_bfloat16*>(smem);                 // [kWgRows][72]: dz
+    __nv_bfloat16* sX = sZ + kWgRows * kNrcWRow;                                 // [kWgRows][72]: act
     const int l = blockIdx.y;
     const int outs = nrc_w_rows(l);
-    // thread -> (o, 16 consecutive inputs) for 64 outputs; 4 inputs for 16 outputs
-    const int per = outs * kNrcIn / static_cast<int>(blockDim.x);
-    const int o = (static_cast<int>(threadIdx.x) * per) / kNrcIn, i0 = (static_cast<int>(threadIdx.x) * per) % kNrcIn;
-    float acc[16];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int m0 = 16 * warp;                      // this warp's output rows
+    const bool active = m0 < outs;
+    float acc[8][4];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) acc[k] = 0.0f;
+    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
     const __nv_bfloat16* dzl = T.dz + static_cast<int64_t>(l) * batch * kNrcIn;
     const __nv_bfloat16* acl = T.acts + static_cast<int64_t>(l) * batch * kNrcIn;
+    // ldmatrix row addresses: lane -> (8x8 matrix q = lane / 8, row r = lane % 8)
+    const int q = lane >> 3, r = lane & 7;
     for (int r0 = blockIdx.x * kWgRows; r0 < batch; r0 += gridDim.x * kWgRows) {
         const int rows = min(kWgRows, batch - r0);
         __syncthreads();
-        for (int e = threadIdx.x; e < kWgRows * (kNrcIn / 2); e += blockDim.x) {
-            const int r = e / (kNrcIn / 2), c = 2 * (e - r * (kNrcIn / 2));
-            float2 zv = make_float2(0.0f, 0.0f), av = make_float2(0.0f, 0.0f);
-            if (r < rows) {
-                const int64_t off = static_cast<int64_t>(r0 + r) * kNrcIn + c;
-                if (c < outs) zv = unpack_bf16(ld32(dzl + off));
-                av = unpack_bf16(ld32(acl + off));
+        for (int e = threadIdx.x; e < kWgRows * (kNrcIn / 8); e += blockDim.x) {   // 16-byte pieces
+            const int rr = e >> 3, c = (e & 7) * 8;
+            uint4 z = make_uint4(0u, 0u, 0u, 0u), a = z;
+            if (rr < rows) {
+                const int64_t off = static_cast<int64_t>(r0 + rr) * kNrcIn + c;
+                if (c < outs) z = *reinterpret_cast<const uint4*>(dzl + off);
+                a = *reinterpret_cast<const uint4*>(acl + off);
             }
-            sdz[r][c] = zv.x; sdz[r][c + 1] = zv.y;
-            sac[r][c] = av.x; sac[r][c + 1] = av.y;
+            *reinterpret_cast<uint4*>(sZ + rr * kNrcWRow + c) = z;
+            *reinterpret_cast<uint4*>(sX + rr * kNrcWRow + c) = a;
         }
         __syncthreads();
-        for (int r = 0; r < rows; ++r) {
-            const float z = sdz[r][o];
+        if (active) {
+#pragma unroll 2
+            for (int k0 = 0; k0 < kWgRows; k0 += 16) {
+                // A = dz^T (16 outputs x 16 rows): matrices (m0, k0) (m0+8, k0) (m0, k0+8) (m0+8, k0+8)
+                uint32_t a[4];
+                ldsm_x4_trans(sZ + (k0 + ((q >> 1) << 3) + r) * kNrcWRow + m0 + ((q & 1) << 3), a[0], a[1], a[2], a[3]);
 #pragma unroll
-            for (int k = 0; k < 16; ++k)
-                if (k < per) acc[k] += z * sac[r][i0 + k];
+                for (int jp = 0; jp < 4; ++jp) {
+                    // B = act (16 rows x 8 inputs) for n-tiles 2jp, 2jp+1: (k0, n) (k0+8, n) (k0, n+8) (k0+8, n+8)
+                    uint32_t b0, b1, b2, b3;
+                    ldsm_x4_trans(sX + (k0 + ((q & 1) << 3) + r) * kNrcWRow + 16 * jp + ((q >> 1) << 3), b0, b1, b2, b3);
+                    mma_bf16(acc[2 * jp], a, b0, b1);
+                    mma_bf16(acc[2 * jp + 1], a, b2, b3);
+                }
+            }
         }
     }
-    float* dst = wg + nrc_w_offset(l) + o * kNrcIn + i0;
+    if (!active) return;
+    float* dst = wg + nrc_w_offset(l);
 #pragma unroll
-    for (int k = 0; k < 16; ++k)
-        if (k < per) atomicAdd(dst + k, acc[k]);
+    for (int j = 0; j < 8; ++j) {
+        const int col = 8 * j + 2 * t;
+        atomicAdd(dst + (m0 + g) * kNrcIn + col, acc[j][0]);
+        atomicAdd(dst + (m0 + g) * kNrcIn + col + 1, acc[j][1]);
+        atomicAdd(dst + (m0 + g + 8) * kNrcIn + col, acc[j][2]);
+        atomicAdd(dst + (m0 + g + 8) * kNrcIn + col + 1, acc[j][3]);
+    }
 }
 
 // Hash-table gradients: the input gradient of each level's two features,
@@ -488,11 +522,10 @@ __global__ void k_nrc_hash_bwd(NrcNet net, const NrcSample* __restrict__ smp, co
         float w[8];
         nrc_level_corners(net.grid, l, u[0], u[1], u[2], idx, w);
         const float2 d = *reinterpret_cast<const float2*>(T.dx + static_cast<int64_t>(row) * 32 + 2 * l);
+        if (d.x == 0.0f && d.y == 0.0f) continue;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            if (d.x != 0.0f) atomicAdd(tg + 2 * static_cast<int64_t>(idx[c]), w[c] * d.x);
-            if (d.y != 0.0f) atomicAdd(tg + 2 * static_cast<int64_t>(idx[c]) + 1, w[c] * d.y);
-        }
+        for (int c = 0; c < 8; ++c)   // one vector atomic per corner (both features)
+            atomicAdd(reinterpret_cast<float2*>(tg) + idx[c], make_float2(w[c] * d.x, w[c] * d.y));
     }
 }
 
@@ -598,6 +631,7 @@ static cudaError_t set_attrs()
         e = cudaFuncSetAttribute(k_nrc_train_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemW + kSmemIn + kSmemOut);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_nrc_train_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemWt + kSmemIn);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_nrc_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemWg);
     return e;
 }
 
@@ -622,7 +656,7 @@ cudaError_t nrc_train_step(const NrcNet& net, const NrcParams& P, const NrcSampl
     const int grid = std::max(1, std::min((tiles + kWarps - 1) / kWarps, sm_count * 2));
     k_nrc_train_fwd<<<grid, kNrcBlock, kSmemW + kSmemIn + kSmemOut, st>>>(net, samples, count, first, batch, T);
     k_nrc_train_bwd<<<grid, kNrcBlock, kSmemWt + kSmemIn, st>>>(net, samples, count, first, batch, T);
-    k_nrc_wgrad<<<dim3(std::min((batch + kWgRows - 1) / kWgRows, 32), kNrcLayers), 256, 0, st>>>(T, batch, P.w_g);
+    k_nrc_wgrad<<<dim3(std::min((batch + kWgRows - 1) / kWgRows, 32), kNrcLayers), kNrcBlock, kSmemWg, st>>>(T, batch, P.w_g);
     k_nrc_hash_bwd<<<blocks_for(static_cast<int64_t>(batch) * net.grid.levels, 256, sm_count * 8), 256, 0, st>>>(
         net, samples, count, first, batch, T, P.table_g);
     if (!apply) return cudaGetLastError();   // gradients stay in P.w_g / P.table_g (scaled by kNrcLossScale)

@@ -464,6 +464,23 @@ def profile_queues() -> None:
                       "shadow_per_launch": st.shadow_rays / max(st.shadow_launches, 1)}), flush=True)
 
 
+def profile_nrc() -> None:
+    """Six radiance-cache frames (480x270, config-2 scene, training on) for ncu
+    captures of the cache kernels; prints the frame statistics."""
+    objs = scenes.spheres_scene()
+    scene = Scene(objs)
+    cam = scenes.spheres_camera(480, 270)
+    import torch
+    acc = torch.zeros(480 * 270 * 3, dtype=torch.float64, device="cuda")
+    cache = RadianceCache(scene, nrc_config())
+    for f in range(6):
+        st = cache.render_frame(cam, make_params(spp=1, max_depth=DEPTH, frame_offset=f), None, acc.data_ptr(),
+                                train=True, stats=True)
+        print(json.dumps({"frame": f, "ms": round(st.total_ms, 3), "render_ms": round(st.render_ms, 3),
+                          "infer_ms": round(st.infer_ms, 3), "train_ms": round(st.train_ms, 3),
+                          "queries": st.queries, "train_samples": st.train_samples, "loss": st.loss}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -474,11 +491,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--nrc", choices=("off", "small", "full"), default="small",
                     help="radiance-cache time-to-relMSE measurement (small: 480x270, full: 1920x1080)")
+    ap.add_argument("--profile-nrc", action="store_true",
+                    help="six radiance-cache frames at 480x270 (for ncu captures of the cache kernels)")
     ap.add_argument("--profile-queues", action="store_true",
                     help="render the workload once at 1 spp (for ncu captures) and print the per-depth queue sizes")
     args = ap.parse_args()
     if args.profile_queues:
         profile_queues()
+        return
+    if args.profile_nrc:
+        profile_nrc()
         return
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
     if args.impl == "reference":

@@ -402,6 +402,25 @@ typedef struct ar_batch_stats {
 ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_per_graph, int64_t path_budget,
                           ar_batch_stats* stats, void* stream);
 
+/* Result of ar_batch_autotune. */
+typedef struct ar_batch_tuning {
+    int32_t iterations_per_graph;  /* chosen graph length                          */
+    int32_t candidates;            /* configurations timed                         */
+    int64_t path_budget;           /* chosen in-flight path budget                 */
+    float best_ms;                 /* probe time of the chosen configuration       */
+    float default_ms;              /* probe time of the defaults (16, 2^22)        */
+} ar_batch_tuning;
+
+/* Autotuner of ar_render_batch: times the batch's probe (every job at
+ * min(spp, probe_spp) samples into scratch outputs; the jobs' own buffers are
+ * not touched) for graph lengths {4, 8, 16, 32} x path budgets {2^20 .. 2^23}
+ * and picks the fastest in paths per second.  The choice is remembered for
+ * batches of the same shape (job count, pixels, samples, spectral jobs) and
+ * used by ar_render_batch when it is called with iterations_per_graph = 0 and
+ * path_budget = 0.  probe_spp <= 0 takes 4. */
+ar_status ar_batch_autotune(const ar_job* jobs, int32_t njobs, int32_t probe_spp, ar_batch_tuning* out,
+                            void* stream);
+
 /* Running-mean resolve for progressive rendering: out[i] = (float)(accum[i] *
  * scale) for n values (scale = 1 / samples so far).  With ar_render's FP64
  * accum this replaces the reference's per-frame FP32 running mean of the

@@ -48,3 +48,37 @@ def test_batch_rejects_bad_jobs(box_objects):
     s = Scene(box_objects)
     with pytest.raises(ArError):
         render_batch([(s, scenes.box_camera(8, 8), make_params(spp=1), None, None)])
+
+
+@pytest.mark.gpu
+def test_batch_autotune(box_objects, small_spheres_objects):
+    """The autotuner times its probe on scratch outputs (the jobs' buffers keep
+    their contents), returns one of its candidates, the fastest, and the next
+    default render_batch of the same batch shape uses it with unchanged results."""
+    import torch
+    from aperture_b200 import autotune_batch
+    box = Scene(box_objects)
+    sph = Scene(small_spheres_objects)
+    cam_s = scenes.spheres_camera(48, 32)
+    cam_s.position.z = -45.0
+    specs = [(box, scenes.box_camera(40, 30), make_params(spp=8, max_depth=8)),
+             (sph, cam_s, make_params(spp=4, max_depth=10)),
+             (box, scenes.box_camera(17, 23), make_params(spp=16, max_depth=6, frame_offset=9))]
+    outs, jobs = [], []
+    for scene, cam, p in specs:
+        o = torch.full((cam.width * cam.height * 3,), -1.0, dtype=torch.float32, device="cuda")
+        outs.append(o)
+        jobs.append((scene, cam, p, o.data_ptr(), None))
+    t = autotune_batch(jobs, probe_spp=2)
+    torch.cuda.synchronize()
+    assert all(bool((o == -1.0).all()) for o in outs)
+    assert t.candidates == 16
+    assert t.iterations_per_graph in (4, 8, 16, 32)
+    assert t.path_budget in (1 << 20, 1 << 21, 1 << 22, 1 << 23)
+    assert 0 < t.best_ms <= t.default_ms * 1.0001
+    st = render_batch(jobs)
+    torch.cuda.synchronize()
+    assert st.iterations_per_graph == t.iterations_per_graph + (t.iterations_per_graph & 1)
+    for (scene, cam, p), o in zip(specs, outs):
+        ref, _ = scene.render(cam, p)
+        np.testing.assert_allclose(o.cpu().numpy().reshape(cam.height, cam.width, 3), ref, rtol=1e-6, atol=1e-7)
