@@ -158,6 +158,7 @@ void ensure_workspace(ar_scene* s, int64_t pool, int64_t npix)
     const size_t o_p0 = take(sizeof(ar::PathRec) * W), o_p1 = take(sizeof(ar::PathRec) * W);
     const size_t o_hit = take(16 * W), o_qsh = take(4 * W * ar::kShadeBuckets);
     const size_t o_sh = take(sizeof(ar::ShadowRec) * W), o_rt = take(sizeof(ar::RetireRec) * W);
+    const size_t o_ax0 = take(16 * W), o_ax1 = take(16 * W), o_sh3 = take(4 * W);
     const size_t o_b0 = take(16 * N), o_b1 = take(8 * N), o_acc = take(24 * N), o_fout = take(12 * N);
     const size_t o_cnt = take(sizeof(ar::PoolCtl)), o_stats = take(64), o_err = take(64);
     const size_t o_ovf = take(static_cast<size_t>(s->grid_trace) * ar::kTraceBlock * ar::kStackOverflow * 4);
@@ -174,6 +175,9 @@ void ensure_workspace(ar_scene* s, int64_t pool, int64_t npix)
     B.qsh = reinterpret_cast<int32_t*>(b + o_qsh);
     B.shadow = reinterpret_cast<ar::ShadowRec*>(b + o_sh);
     B.retire = reinterpret_cast<ar::RetireRec*>(b + o_rt);
+    B.aux[0] = reinterpret_cast<float4*>(b + o_ax0);
+    B.aux[1] = reinterpret_cast<float4*>(b + o_ax1);
+    B.shadow3 = reinterpret_cast<float*>(b + o_sh3);
     B.capacity = static_cast<int32_t>(pool);
     s->base0 = reinterpret_cast<uint4*>(b + o_b0);
     s->base1 = reinterpret_cast<uint2*>(b + o_b1);
@@ -231,7 +235,8 @@ ar_status check_params(const ar_render_params* p)
     if (p->max_depth <= 0 || p->max_depth > 4096) return fail(AR_ERR_INVALID_ARGUMENT, "max_depth must be in [1, 4096]");
     if (p->rr_depth < 0) return fail(AR_ERR_INVALID_ARGUMENT, "rr_depth must be >= 0");
     if (p->frame_offset < 0) return fail(AR_ERR_INVALID_ARGUMENT, "frame_offset must be >= 0");
-    if (p->spectral != 0 && p->spectral != 1) return fail(AR_ERR_INVALID_ARGUMENT, "spectral must be 0 or 1");
+    if (p->spectral != 0 && p->spectral != 1 && p->spectral != 4)
+        return fail(AR_ERR_INVALID_ARGUMENT, "spectral must be 0, 1 or 4");
     if (p->tri_light_nee != 0 && p->tri_light_nee != 1)
         return fail(AR_ERR_INVALID_ARGUMENT, "tri_light_nee must be 0 or 1");
     return AR_OK;
@@ -270,7 +275,7 @@ ar::FrameParams make_frame(const ar_scene* s, const ar_camera* c, const ar_rende
         fp.tri_light_nee = p->tri_light_nee;
         fp.medium_key = medium_frame_key(fp.seed, fp.frame0);
         if (p->spectral) {
-            fp.spectral = 1;
+            fp.spectral = p->spectral;
             fp.spec.tables = s->spec_tables;
             fp.spec.lut_lam = s->spec_lut_lam;
             fp.spec.lut_rgb = s->spec_lut_rgb;
@@ -732,6 +737,7 @@ void job_alloc(JobWs& w, int64_t pool, int64_t npix, int grid_trace)
     const size_t o_p0 = take(sizeof(ar::PathRec) * W), o_p1 = take(sizeof(ar::PathRec) * W);
     const size_t o_hit = take(16 * W), o_qsh = take(4 * W * ar::kShadeBuckets);
     const size_t o_sh = take(sizeof(ar::ShadowRec) * W), o_rt = take(sizeof(ar::RetireRec) * W);
+    const size_t o_ax0 = take(16 * W), o_ax1 = take(16 * W), o_sh3 = take(4 * W);
     const size_t o_b0 = take(16 * N), o_b1 = take(8 * N), o_acc = take(24 * N);
     const size_t o_cnt = take(sizeof(ar::PoolCtl)), o_stats = take(64), o_err = take(64);
     const size_t o_ovf = take(static_cast<size_t>(grid_trace) * ar::kTraceBlock * ar::kStackOverflow * 4);
@@ -743,6 +749,9 @@ void job_alloc(JobWs& w, int64_t pool, int64_t npix, int grid_trace)
     w.B.qsh = reinterpret_cast<int32_t*>(b + o_qsh);
     w.B.shadow = reinterpret_cast<ar::ShadowRec*>(b + o_sh);
     w.B.retire = reinterpret_cast<ar::RetireRec*>(b + o_rt);
+    w.B.aux[0] = reinterpret_cast<float4*>(b + o_ax0);
+    w.B.aux[1] = reinterpret_cast<float4*>(b + o_ax1);
+    w.B.shadow3 = reinterpret_cast<float*>(b + o_sh3);
     w.B.capacity = static_cast<int32_t>(pool);
     w.base0 = reinterpret_cast<uint4*>(b + o_b0);
     w.base1 = reinterpret_cast<uint2*>(b + o_b1);

@@ -67,6 +67,7 @@ __device__ __forceinline__ uint32_t* thread_overflow(uint32_t* base)
 __device__ __forceinline__ int ibits(float f) { return __float_as_int(f); }
 // pool buffer `c` without dynamic indexing of the kernel-parameter array
 __device__ __forceinline__ PathRec* pool_of(const PathBuffers& B, int c) { return c ? B.pool[1] : B.pool[0]; }
+__device__ __forceinline__ float4* aux_of(const PathBuffers& B, int c) { return c ? B.aux[1] : B.aux[0]; }
 __device__ __forceinline__ float fbits(int i) { return __int_as_float(i); }
 
 // ------------------------------------------------------------------ ray queries
@@ -232,7 +233,12 @@ __global__ void k_regen(FrameParams fp, PathBuffers B, PoolCtl* ctl, int cur, ui
         if (fp.spectral) {  // CalculateRadiance starts with SampleCIE1931(Rand3(seed)) (render.cuh:467)
             const float r0 = r.next(), r1 = r.next(), r2 = r.next();
             const LambdaSample ls = sample_cie1931(r0, r1, r2);
-            pr.mask = make_float4(1.0f, ls.lambda, ls.pdf, fbits(p));
+            if (fp.spectral == 4) {   // hero wavelength + 3 rotations: throughputs 1, hero in the side record
+                pr.mask = make_float4(1.0f, 1.0f, 1.0f, fbits(p));
+                aux_of(B, cur)[base + i] = make_float4(1.0f, 0.0f, ls.lambda, 0.0f);
+            } else {
+                pr.mask = make_float4(1.0f, ls.lambda, ls.pdf, fbits(p));
+            }
         }
         pr.rad = make_float4(0.0f, 0.0f, 0.0f, fbits(sidx));
         pr.rng0 = make_uint4(r.st.d, r.st.v[0], r.st.v[1], r.st.v[2]);
@@ -330,11 +336,25 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_extend(SceneVi
 }
 
 // ------------------------------------------------------------------ shade
+// G-buffer of an RGB material at one wavelength (EvaluateMaterial, spectral).
+__device__ __forceinline__ GB gb_at(const GB& rgb, const SpectralView& sv, const float4& lk, float lambda)
+{
+    GB g = rgb;
+    const float a = interact(sv.lut_rgb, sv.res, lk, rgb.albedo);
+    const float e = interact(sv.lut_rgb, sv.res, lk, rgb.emissive);
+    g.albedo = mk(a, a, a);
+    g.emissive = mk(e, e, e);
+    g.ior = ior_abbe(lambda, rgb.ior, rgb.abbe);
+    g.sigma_a = sigma_tilt(rgb.sigma_a, lambda, rgb.tilt);
+    g.spectral = true;
+    return g;
+}
+
 // One iteration of the CalculateRadiance loop body (render.cuh:541-908) up to
 // the shadow query: Trace's material evaluation and hit offset, emission with
 // MIS, light sampling for NEE, throughput and Russian roulette.  kModel is the
 // shading model of every path of this launch's bucket, -1 = miss.
-template <int kModel, bool kExt, bool kSpec, bool kNrc>
+template <int kModel, bool kExt, int kSpec, bool kNrc>
 __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams fp, PathBuffers B, int cur,
                                                        PoolCtl* ctl, ar_path_record* rec)
 {
@@ -361,13 +381,33 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         // of the RGB arithmetic, the wavelength's basis and D65 weight
         float lambda = 0.0f, lpdf = 0.0f, d65 = 1.0f;
         float4 lk = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (kSpec) {
+        if (kSpec == 1) {
             lambda = pr.mask.y;
             lpdf = pr.mask.z;
             mask = mk(pr.mask.x, pr.mask.x, pr.mask.x);
             radiance = mk(pr.rad.x, pr.rad.x, pr.rad.x);
             lk = query_lambda(fp.spec.lut_lam, lambda);
             d65 = d65_norm(fp.spec.tables, lambda);
+        }
+        f3 d65v = mk(d65, d65, d65);
+        // four wavelengths (extension): lanes x, y, z of the RGB arithmetic carry
+        // wavelengths 0-2, the *3 scalars wavelength 3; directions follow the hero (0)
+        float mask3 = 0.0f, rad3 = 0.0f, d65_3 = 0.0f;
+        float lam4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        float4 lk4[4];
+        if (kSpec == 4) {
+            const float4 ax = aux_of(B, cur)[k];
+            lambda = ax.z;
+            mask3 = ax.x;
+            rad3 = ax.y;
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                lam4[w] = rotate_lambda(lambda, w);
+                lk4[w] = query_lambda(fp.spec.lut_lam, lam4[w]);
+            }
+            lk = lk4[0];
+            d65v = mk(d65_norm(fp.spec.tables, lam4[0]), d65_norm(fp.spec.tables, lam4[1]), d65_norm(fp.spec.tables, lam4[2]));
+            d65_3 = d65_norm(fp.spec.tables, lam4[3]);
         }
         const bool inside = (flags & kFlagInside) != 0;
         const f3 vloc = xyz(pr.vloc);
@@ -381,11 +421,12 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         if (rec) rec[ri].segments = depth + 1;
         // ---- intersection details (re-run of the accepted test)
         f3 pos = mk(0.0f, 0.0f, 0.0f), nrm = mk(0.0f, 0.0f, 0.0f);
-        GB gb;
+        GB gb, gbr;
         int light = -1;
         if (hit) {
             const ObjInfo oi = s.objects[hr.x];
             gb = load_gb(s.materials[oi.material]);
+            gbr = gb;
             if (kSpec) {  // EvaluateMaterial / SampleBSDF at the path's wavelength (material.cuh)
                 const float a = interact(fp.spec.lut_rgb, fp.spec.res, lk, gb.albedo);
                 const float e = interact(fp.spec.lut_rgb, fp.spec.res, lk, gb.emissive);
@@ -472,6 +513,8 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         f3 nvloc = mk(0.0f, 0.0f, 0.0f);
         int nmobj = -1, nmdepth = 0;
         f3 malb = mk(0.0f, 0.0f, 0.0f);  // medium: single-scatter albedo
+        float emis3 = 0.0f, brdf3 = 0.0f, malb3 = 0.0f;  // wavelength 3 (four-wavelength mode)
+        bool dispersed = false;
         if (!hit && !kMed && inside) {
             missThin = true;
             nvloc = cro;
@@ -538,13 +581,38 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             nmobj = hr.x;
             nmdepth = mdepth + 1;
             brdf = eval_bsdf_cos(kModel, crd, next, N, pos, gb, inside, vloc);
+            if (kSpec == 4) {
+                if (kModel != AR_MAT_GLASS) {
+                    emis = mk(interact(fp.spec.lut_rgb, fp.spec.res, lk4[0], gbr.emissive),
+                              interact(fp.spec.lut_rgb, fp.spec.res, lk4[1], gbr.emissive),
+                              interact(fp.spec.lut_rgb, fp.spec.res, lk4[2], gbr.emissive));
+                    emis3 = interact(fp.spec.lut_rgb, fp.spec.res, lk4[3], gbr.emissive);
+                }
+                if (kModel == AR_MAT_GLASS && gbr.abbe > 0.0f && !(flags & kFlagHeroOnly)) {
+                    // dispersive glass: the other wavelengths cannot follow the hero's
+                    // direction; the path continues with the hero alone (its weight
+                    // becomes that of a single-wavelength sample)
+                    dispersed = true;
+                } else if (kModel != AR_MAT_LIGHT && !(flags & kFlagHeroOnly)) {
+                    const float b1 = eval_bsdf_cos(kModel, crd, next, N, pos, gb_at(gbr, fp.spec, lk4[1], lam4[1]), inside, vloc).x;
+                    const float b2 = eval_bsdf_cos(kModel, crd, next, N, pos, gb_at(gbr, fp.spec, lk4[2], lam4[2]), inside, vloc).x;
+                    brdf3 = eval_bsdf_cos(kModel, crd, next, N, pos, gb_at(gbr, fp.spec, lk4[3], lam4[3]), inside, vloc).x;
+                    brdf = mk(brdf.x, b1, b2);
+                }
+            }
         } else if (kMed) {
             // Henyey-Greenstein scattering; phase / pdf = 1, throughput weight = albedo
             const float u1 = g.next(), u2 = g.next();
             next = hg_sample(crd, s.medium.g, u1, u2);
             pdf = hg_phase(s.medium.g, dot(crd, next));
             malb = mk(s.medium.albedo[0], s.medium.albedo[1], s.medium.albedo[2]);
-            if (kSpec) {
+            if (kSpec == 4) {
+                const f3 rgb = malb;
+                malb = mk(interact(fp.spec.lut_rgb, fp.spec.res, lk4[0], rgb), interact(fp.spec.lut_rgb, fp.spec.res, lk4[1], rgb),
+                          interact(fp.spec.lut_rgb, fp.spec.res, lk4[2], rgb));
+                malb3 = interact(fp.spec.lut_rgb, fp.spec.res, lk4[3], rgb);
+                brdf3 = malb3 * pdf;
+            } else if (kSpec) {
                 const float a = interact(fp.spec.lut_rgb, fp.spec.res, lk, malb);
                 malb = mk(a, a, a);
             }
@@ -558,7 +626,13 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             next = crd;
             pdf = 1.0f;
             emis = sky_lighting(crd, fp.sky);
-            if (kSpec) {
+            if (kSpec == 4) {
+                const f3 rgb = emis;
+                emis = mk(interact(fp.spec.lut_rgb, fp.spec.res, lk4[0], rgb), interact(fp.spec.lut_rgb, fp.spec.res, lk4[1], rgb),
+                          interact(fp.spec.lut_rgb, fp.spec.res, lk4[2], rgb));
+                emis3 = interact(fp.spec.lut_rgb, fp.spec.res, lk4[3], rgb);
+                brdf3 = 1.0f;
+            } else if (kSpec) {
                 const float e = interact(fp.spec.lut_rgb, fp.spec.res, lk, emis);
                 emis = mk(e, e, e);
             }
@@ -573,7 +647,10 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         const bool mInside = nInside;  // media state after this segment
         // ---- emission (render.cuh:648-723)
         if (!hit && !kMed) {
-            if (!missThin) radiance = radiance + (mask * emis) * d65;
+            if (!missThin) {
+                radiance = radiance + (mask * emis) * d65v;
+                if (kSpec == 4) rad3 = rad3 + (mask3 * emis3) * d65_3;
+            }
         } else if (hit && light >= 0 && !nrcQuery) {
             float misW = 1.0f;
             if (fp.use_nee && depth > 0 && (flags & kFlagPrevNEE)) {
@@ -581,19 +658,23 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                 const float pL = pdf_light_from_hit(s, hr.x, xyz(pr.prev), pos, nrm, fp.tri_light_nee != 0);
                 if (pL >= 0.0f && pB > 0.0f) misW = power_heuristic(pB, pL);
             }
-            radiance = radiance + ((mask * emis) * d65) * misW;
+            radiance = radiance + ((mask * emis) * d65v) * misW;
+            if (kSpec == 4) rad3 = rad3 + ((mask3 * emis3) * d65_3) * misW;
         }
         const bool brk = (!hit && !kMed && !missThin) || terminate || nrcQuery;
         bool cont = false, shadow = false, cosOK = false;
         f3 pending = mk(0.0f, 0.0f, 0.0f), lightP = mk(0.0f, 0.0f, 0.0f);
+        float pend3 = 0.0f;
         float4 prevOut = pr.prev;
         if (!brk) {
             // ---- NEE (render.cuh:766-827)
             if (!missThin) {
-                const float lum = kSpec ? mask.x : luminance(mask);
+                const float lum = kSpec == 4 ? 0.25f * (mask.x + mask.y + mask.z + mask3)
+                                             : (kSpec ? mask.x : luminance(mask));
                 const float rate = sqrtf(saturate(lum));
                 if (fp.use_nee && nonDelta < 10 && !delta && !mInside && g.next() < rate) {
                     LightSample ls = sample_light(s, pos, g, fp.tri_light_nee != 0);
+                    const f3 lsRgb = ls.emis;
                     if (kSpec) {
                         const float e = interact(fp.spec.lut_rgb, fp.spec.res, lk, ls.emis);
                         ls.emis = mk(e, e, e);
@@ -614,7 +695,26 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                             const float pL = area_to_solid_angle(pos, ls.p, ls.n, ls.pFacet * ls.pA);
                             const float pB = kMed ? hg_phase(s.medium.g, dot(crd, ld))
                                                   : fmaxf(bsdf_pdf(kModel, gb, nrm, crd, ld), 0.0f);
-                            pending = (mask * (contrib * power_heuristic(pL, pB))) * d65;
+                            const float wmis = power_heuristic(pL, pB);
+                            pending = (mask * (contrib * wmis)) * d65v;
+                            if (kSpec == 4) {
+                                const float G4 = G / pATotal;
+                                float f1, f2, f3v;
+                                if (kMed) {
+                                    const float ph = hg_phase(s.medium.g, dot(crd, ld));
+                                    f1 = malb.y * ph; f2 = malb.z * ph; f3v = malb3 * ph;
+                                } else {
+                                    const f3 z0 = mk(0.0f, 0.0f, 0.0f);
+                                    f1 = eval_bsdf_cos(kModel, crd, ld, nrm, pos, gb_at(gbr, fp.spec, lk4[1], lam4[1]), false, z0).x;
+                                    f2 = eval_bsdf_cos(kModel, crd, ld, nrm, pos, gb_at(gbr, fp.spec, lk4[2], lam4[2]), false, z0).x;
+                                    f3v = eval_bsdf_cos(kModel, crd, ld, nrm, pos, gb_at(gbr, fp.spec, lk4[3], lam4[3]), false, z0).x;
+                                }
+                                const f3 c3 = mk(contrib.x,
+                                                 (f1 * interact(fp.spec.lut_rgb, fp.spec.res, lk4[1], lsRgb)) * G4,
+                                                 (f2 * interact(fp.spec.lut_rgb, fp.spec.res, lk4[2], lsRgb)) * G4);
+                                pending = (mask * (c3 * wmis)) * d65v;
+                                pend3 = (mask3 * (((f3v * interact(fp.spec.lut_rgb, fp.spec.res, lk4[3], lsRgb)) * G4) * wmis)) * d65_3;
+                            }
                         }
                         shadow = true;
                         lightP = ls.p;
@@ -633,8 +733,9 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             float qrr = 1.0f;
             bool survived = true;
             if (nonDelta >= fp.rr_depth) {
-                const float lum = kSpec ? mask.x : luminance(mask);
-                const float mx = kSpec ? mask.x : max3(mask);
+                const float lum = kSpec == 4 ? 0.25f * (mask.x + mask.y + mask.z + mask3)
+                                             : (kSpec ? mask.x : luminance(mask));
+                const float mx = kSpec == 4 ? fmaxf(max3(mask), mask3) : (kSpec ? mask.x : max3(mask));
                 const float basic = clampf(lum * 0.5f + mx * 0.5f, 0.05f, 0.95f);
                 qrr = lerpf(basic, 1.0f, mInside ? 0.99f : 0.0f);
                 if (g.next() > qrr) survived = false;
@@ -642,6 +743,15 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             if (survived) {
                 mask = mask * contrib;
                 mask = mask / qrr;
+                if (kSpec == 4) {
+                    mask3 = (mask3 * (brdf3 / fmaxf(pdf, 1e-12f))) / qrr;
+                    if (dispersed) {   // hero alone from here: weight sum_j p(lambda_j) / p(lambda_0)
+                        const float ps = pdf_cie1931(lam4[0]) + pdf_cie1931(lam4[1]) + pdf_cie1931(lam4[2]) + pdf_cie1931(lam4[3]);
+                        mask = mk(mask.x * (ps / pdf_cie1931(lam4[0])), 0.0f, 0.0f);
+                        mask3 = 0.0f;
+                        flags |= kFlagHeroOnly;
+                    }
+                }
                 if (!delta) nonDelta++;
                 cont = depth + 1 < fp.max_depth;
             }
@@ -664,8 +774,9 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             PathRec out;
             out.o = f4(pos, fbits((depth + 1) | (nonDelta << 16)));
             out.d = f4(next, fbits(flags | (nmdepth << 8)));
-            out.mask = kSpec ? make_float4(mask.x, lambda, lpdf, fbits(pixel)) : f4(mask, fbits(pixel));
-            out.rad = kSpec ? make_float4(radiance.x, 0.0f, 0.0f, fbits(sidx)) : f4(radiance, fbits(sidx));
+            out.mask = kSpec == 1 ? make_float4(mask.x, lambda, lpdf, fbits(pixel)) : f4(mask, fbits(pixel));
+            out.rad = kSpec == 1 ? make_float4(radiance.x, 0.0f, 0.0f, fbits(sidx)) : f4(radiance, fbits(sidx));
+            if (kSpec == 4) aux_of(B, 1 - cur)[j] = make_float4(mask3, rad3, lambda, 0.0f);
             out.rng0 = make_uint4(g.st.d, g.st.v[0], g.st.v[1], g.st.v[2]);
             out.rng1 = make_uint4(g.st.v[3], g.st.v[4], static_cast<uint32_t>(nmobj), kNrc ? __float_as_uint(nrcS) : used);
             out.prev = prevOut;
@@ -675,7 +786,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         } else {
             RetireRec out;
             out.rad = f4(radiance, fbits(pixel));
-            out.meta = make_int4(sidx, static_cast<int>(used), ibits(lambda), ibits(lpdf));
+            out.meta = make_int4(sidx, static_cast<int>(used), ibits(lambda), ibits(kSpec == 4 ? rad3 : lpdf));
             B.retire[r] = out;
             target = ~r;
         }
@@ -688,6 +799,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                 ? medium_seed(fp.medium_key, static_cast<uint32_t>(sidx), static_cast<uint32_t>(pixel), static_cast<uint32_t>(depth), 1u) & ~1u
                 : 0u;
             sr.nee = f4(pending, fbits(static_cast<int>(mseed | (cosOK ? 1u : 0u))));
+            if (kSpec == 4) B.shadow3[m] = pend3;
             B.shadow[m] = sr;
         }
     }
@@ -711,6 +823,9 @@ struct ShadowIO {
     const ShadowRec* rec;
     PathRec* next_pool;
     RetireRec* retire;
+    float4* next_aux;         // four-wavelength mode: side records of the next pool
+    const float* pend3;       // four-wavelength mode: pending radiance of wavelength 3
+    int spec4;
     unsigned long long traced;
     __device__ __forceinline__ void finish(int m, bool occ, float tr = 1.0f)
     {
@@ -725,6 +840,7 @@ struct ShadowIO {
             if (add) {
                 const float4 r = p.rad;
                 p.rad = make_float4(r.x + nee.x, r.y + nee.y, r.z + nee.z, r.w);
+                if (spec4) next_aux[target].y += pend3[m] * (kExt ? tr : 1.0f);
             }
             if (occ || cosOK) {
                 const float4 d = p.d;
@@ -734,6 +850,7 @@ struct ShadowIO {
             RetireRec& p = retire[~target];
             const float4 r = p.rad;
             p.rad = make_float4(r.x + nee.x, r.y + nee.y, r.z + nee.z, r.w);
+            if (spec4) p.meta.w = __float_as_int(__int_as_float(p.meta.w) + pend3[m] * (kExt ? tr : 1.0f));
         }
     }
     __device__ __forceinline__ int load(const SceneView&, int m, RayState& r)
@@ -767,7 +884,7 @@ struct ShadowIO {
 
 template <bool kExt>
 __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks - 1) k_shadow(SceneView s, PathBuffers B, int cur, PoolCtl* ctl,
-                                                        unsigned long long* stats, uint32_t* ovf, int* err)
+                                                        unsigned long long* stats, uint32_t* ovf, int* err, int spec4)
 {
     extern __shared__ uint32_t smem[];
     const int n = ctl->shadow_count;
@@ -775,6 +892,9 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks - 1) k_shadow(Sce
     io.rec = B.shadow;
     io.next_pool = pool_of(B, 1 - cur);
     io.retire = B.retire;
+    io.next_aux = aux_of(B, 1 - cur);
+    io.pend3 = B.shadow3;
+    io.spec4 = spec4;
     io.traced = 0;
     traverse_queue<true>(s, io, n, &ctl->fetch_shadow, lane_stack(smem), thread_overflow(ovf), err, &stats[4]);
     unsigned long long c = io.traced;
@@ -799,7 +919,22 @@ __global__ void k_retire(FrameParams fp, PathBuffers B, PoolCtl* ctl, double* ac
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const RetireRec rr = B.retire[i];
         f3 v = xyz(rr.rad);
-        if (fp.spectral) {  // lambdaXYZ * radiance / pdf (render.cuh:966), linear CIE XYZ
+        if (fp.spectral == 4) {
+            // four wavelengths: sum_i XYZ(lambda_i) L_i / sum_j p(lambda_j), the
+            // one-sample estimator of the rotation set (balance heuristic over
+            // which member was the hero)
+            const float h = fbits(rr.meta.z);
+            const float L[4] = {fix_nan_inf(rr.rad.x), fix_nan_inf(rr.rad.y), fix_nan_inf(rr.rad.z), fix_nan_inf(fbits(rr.meta.w))};
+            float ps = 0.0f;
+            f3 acc = mk(0.0f, 0.0f, 0.0f);
+#pragma unroll
+            for (int w = 0; w < 4; ++w) {
+                const float lw = rotate_lambda(h, w);
+                ps += pdf_cie1931(lw);
+                acc = acc + cmf_xyz(fp.spec.tables, lw) * L[w];
+            }
+            v = acc / ps;
+        } else if (fp.spectral) {  // lambdaXYZ * radiance / pdf (render.cuh:966), linear CIE XYZ
             const float lam = fbits(rr.meta.z), lpdf = fbits(rr.meta.w);
             const float r = fix_nan_inf(rr.rad.x);
             const f3 c = cmf_xyz(fp.spec.tables, lam);
@@ -917,7 +1052,7 @@ cudaError_t launch_pool_init(PoolCtl* ctl, int64_t total, cudaStream_t st)
 }
 
 // The five per-material shading launches of one iteration.
-template <bool kExt, bool kSpec, bool kNrc>
+template <bool kExt, int kSpec, bool kNrc>
 void launch_shade(const SceneView& s, const FrameParams& fp, const PathBuffers& B, int c, PoolCtl* ctl,
                   ar_path_record* rec, int grid, cudaStream_t st)
 {
@@ -945,20 +1080,24 @@ cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const P
         if (ext) k_extend<true><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err, fp.medium_key);
         else k_extend<false><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err, fp.medium_key);
         if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend++ + 1], st);
-        if (fp.spectral) {
-            if (ext) launch_shade<true, true, false>(s, fp, B, c, ctl, rec, grid_other, st);
-            else launch_shade<false, true, false>(s, fp, B, c, ctl, rec, grid_other, st);
+        if (fp.spectral == 4) {
+            if (ext) launch_shade<true, 4, false>(s, fp, B, c, ctl, rec, grid_other, st);
+            else launch_shade<false, 4, false>(s, fp, B, c, ctl, rec, grid_other, st);
+        } else if (fp.spectral) {
+            if (ext) launch_shade<true, 1, false>(s, fp, B, c, ctl, rec, grid_other, st);
+            else launch_shade<false, 1, false>(s, fp, B, c, ctl, rec, grid_other, st);
         } else if (fp.nrc.enabled) {
-            if (ext) launch_shade<true, false, true>(s, fp, B, c, ctl, rec, grid_other, st);
-            else launch_shade<false, false, true>(s, fp, B, c, ctl, rec, grid_other, st);
+            if (ext) launch_shade<true, 0, true>(s, fp, B, c, ctl, rec, grid_other, st);
+            else launch_shade<false, 0, true>(s, fp, B, c, ctl, rec, grid_other, st);
         } else {
-            if (ext) launch_shade<true, false, false>(s, fp, B, c, ctl, rec, grid_other, st);
-            else launch_shade<false, false, false>(s, fp, B, c, ctl, rec, grid_other, st);
+            if (ext) launch_shade<true, 0, false>(s, fp, B, c, ctl, rec, grid_other, st);
+            else launch_shade<false, 0, false>(s, fp, B, c, ctl, rec, grid_other, st);
         }
         const bool ts = tm && tm->n_shadow < tm->cap;
         if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow], st);
-        if (ext) k_shadow<true><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
-        else k_shadow<false><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err);
+        const int spec4 = fp.spectral == 4 ? 1 : 0;
+        if (ext) k_shadow<true><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err, spec4);
+        else k_shadow<false><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err, spec4);
         if (ts) cudaEventRecord(tm->shadow_ev[2 * tm->n_shadow++ + 1], st);
         k_retire<<<grid_other, kShadeBlock, 0, st>>>(fp, B, ctl, accum, rec);
         *launches += s.has_medium ? 11 : 10;

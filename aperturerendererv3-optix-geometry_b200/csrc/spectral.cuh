@@ -152,12 +152,23 @@ AR_HD float cmf_z_fit(float l)
 
 struct LambdaSample { float lambda, pdf; };
 
+// Density of sample_cie1931's wavelength: the mixture of a uniform share and
+// the three fitted colour-matching lobes.
+AR_HD float pdf_cie1931(float lambda)
+{
+    const float total = 0.1f + 1.0f + 1.0f + 1.0f;
+    const float uniformRatio = 0.1f / total, xRatio = 1.0f / total, yRatio = 1.0f / total, zRatio = 1.0f / total;
+    const float pMix = uniformRatio * 1.0f / (780.0f - 360.0f) + xRatio * (cmf_x_fit(lambda) / 106.81109281f) +
+                       yRatio * (cmf_y_fit(lambda) / 106.34513640f) + zRatio * (cmf_z_fit(lambda) / 105.88243587f);
+    return fmaxf(pMix, 1e-16f);
+}
+
 // SampleCIE1931 (sample_ciexyz.cuh:288-325): a 0.1 : 1 : 1 : 1 mixture of the
 // uniform density and the three CMF lobes.
 AR_HD LambdaSample sample_cie1931(float r0, float r1, float r2)
 {
     const float total = 0.1f + 1.0f + 1.0f + 1.0f;
-    const float uniformRatio = 0.1f / total, xRatio = 1.0f / total, yRatio = 1.0f / total, zRatio = 1.0f / total;
+    const float uniformRatio = 0.1f / total, xRatio = 1.0f / total, yRatio = 1.0f / total;
     float lambda;
     if (r0 < uniformRatio) {
         lambda = r1 * (780.0f - 360.0f) + 360.0f;
@@ -178,12 +189,20 @@ AR_HD LambdaSample sample_cie1931(float r0, float r1, float r2)
         const float t = 0.0000049890553249f + r1 * (1.0f - 0.0000049890553249f);
         lambda = clamp_lambda(exp_det(6.1114040395252154f + 0.0510000000000000f * ndtri_newton(t)));
     }
-    const float pMix = uniformRatio * 1.0f / (780.0f - 360.0f) + xRatio * (cmf_x_fit(lambda) / 106.81109281f) +
-                       yRatio * (cmf_y_fit(lambda) / 106.34513640f) + zRatio * (cmf_z_fit(lambda) / 105.88243587f);
     LambdaSample s;
     s.lambda = lambda;
-    s.pdf = fmaxf(pMix, 1e-16f);
+    s.pdf = pdf_cie1931(lambda);
     return s;
+}
+
+// Four wavelengths per path (extension; the reference traces one): the hero
+// and its rotations by a quarter of [360, 780] nm (Wilkie et al., "Hero
+// wavelength spectral sampling", 2014).  Wavelength i of a hero h.
+AR_HD float rotate_lambda(float h, int i)
+{
+    float x = h - 360.0f + 105.0f * static_cast<float>(i);
+    if (x >= 420.0f) x -= 420.0f;
+    return 360.0f + x;
 }
 
 // ---------------------------------------------------------------- dispersion

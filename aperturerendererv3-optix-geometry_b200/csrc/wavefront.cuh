@@ -32,6 +32,7 @@ namespace ar {
 enum : int32_t {
     kFlagPrevNEE = 1,      // previousNEEState.previousDidNEE_
     kFlagInside = 2,       // MediaContext::bInsideMedia_
+    kFlagHeroOnly = 4,     // four-wavelength mode: the other wavelengths ended at dispersive glass
 };
 
 constexpr int kModelMedium = 4;   // shade bucket of collisions in the participating medium
@@ -41,8 +42,9 @@ constexpr int32_t kHitMedium = -2; // hit object of a medium collision
 struct alignas(16) PathRec {
     float4 o;     // ray origin xyz; w: depth | nonDeltaDepth << 16 (int bits)
     float4 d;     // ray direction xyz; w: flags | media depth << 8 (int bits)
-    float4 mask;  // throughput rgb (spectral: x throughput, y wavelength, z its pdf); w: pixel (int bits)
-    float4 rad;   // radiance rgb (spectral: x); w: sample index (int bits)
+    float4 mask;  // throughput rgb (spectral: x throughput, y wavelength, z its pdf; four wavelengths:
+                  // wavelengths 0-2); w: pixel (int bits)
+    float4 rad;   // radiance rgb (spectral: x; four wavelengths: 0-2); w: sample index (int bits)
     uint4 rng0;   // xorwow d, v0, v1, v2
     uint4 rng1;   // xorwow v3, v4; z media object; w uniforms consumed (cache mode: spread sum, float bits)
     float4 prev;  // previous NEE vertex xyz; w previous BSDF pdf (cache mode: +inf after a delta event)
@@ -80,6 +82,9 @@ struct PoolCtl {
 
 struct PathBuffers {
     PathRec* pool[2];
+    float4* aux[2];      // four-wavelength mode, per pool index: throughput and radiance of
+                         // wavelength 3, hero wavelength, unused
+    float* shadow3;      // four-wavelength mode: pending radiance of wavelength 3 per shadow segment
     int4* hit;           // per current-pool index: object, prim slot, t bits
     int32_t* qsh;        // shade buckets, kShadeBuckets x capacity
     ShadowRec* shadow;   // capacity entries
@@ -104,7 +109,7 @@ struct FrameParams {
     uint64_t seed;
     uint64_t frame0;         // TOTAL_FRAME_INDEX of the first sample
     float eps_tab[9];        // INTERSECT_EPS(0..8)
-    int32_t spectral;        // 1: one hero wavelength per path, XYZ output
+    int32_t spectral;        // 1: one hero wavelength per path, 4: four wavelengths; XYZ output
     int32_t tri_light_nee;   // 1: NEE also samples triangle lights (extension)
     SpectralView spec;       // tables and lookup tables of the spectral mode
     uint32_t medium_key;     // medium_frame_key(seed, frame0)

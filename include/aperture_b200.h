@@ -128,7 +128,11 @@ typedef struct ar_render_params {
     int32_t wave_paths;    /* paths in flight per wave; 0 = automatic                */
     int32_t spectral;      /* 1 = USE_SPECTRUM_RENDERING: one hero wavelength per path
                               (SampleCIE1931), output linear CIE XYZ; needs
-                              ar_scene_set_spectral.  0 = RGB                        */
+                              ar_scene_set_spectral.  4 = four wavelengths per path
+                              (extension): the hero and its rotations by 105 nm in
+                              [360, 780], one estimate per rotation set (balance
+                              heuristic); dispersive glass continues with the hero
+                              alone.  0 = RGB                                        */
     int32_t tri_light_nee; /* 1 = NEE also samples emissive triangles (uniform area
                               sampling, two-sided, MIS with BSDF hits).  The
                               reference samples cube and sphere lights only
