@@ -149,6 +149,15 @@ def nrc_config(levels=16, log2_entries=19, base_resolution=16, max_resolution=20
     return c
 
 
+class GuideConfig(ctypes.Structure):
+    _fields_ = [("probe_capacity", c_int32), ("log2_table", c_int32)]
+
+
+class GuideStats(ctypes.Structure):
+    _fields_ = [("frames", c_int64), ("probes", c_int64), ("samples", c_int64), ("dropped", c_int64),
+                ("alpha", c_float), ("reserved", c_int32)]
+
+
 class BatchTuning(ctypes.Structure):
     _fields_ = [("iterations_per_graph", c_int32), ("candidates", c_int32), ("path_budget", c_int64),
                 ("best_ms", c_float), ("default_ms", c_float)]
@@ -170,7 +179,8 @@ EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create",
                     "ar_scene_set_spectral", "ar_scene_get_spectral_luts", "ar_render_batch",
                     "ar_scene_set_medium", "ar_nrc_create", "ar_nrc_destroy", "ar_nrc_render_frame",
                     "ar_nrc_get_params", "ar_nrc_set_params", "ar_nrc_infer", "ar_nrc_train", "ar_nrc_gradients",
-                    "ar_batch_autotune")
+                    "ar_batch_autotune", "ar_guide_create", "ar_guide_destroy", "ar_guide_render_frame",
+                    "ar_guide_get_stats", "ar_guide_get_probe")
 
 
 class ArError(RuntimeError):
@@ -226,6 +236,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_scene_set_medium.restype = c_int32
     lib.ar_render_batch.argtypes = [c_void_p, c_int32, c_int32, c_int64, POINTER(BatchStats), c_void_p]
     lib.ar_render_batch.restype = c_int32
+    lib.ar_guide_create.argtypes = [c_void_p, POINTER(GuideConfig), POINTER(c_void_p)]
+    lib.ar_guide_destroy.argtypes = [c_void_p]
+    lib.ar_guide_render_frame.argtypes = [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p, c_void_p]
+    lib.ar_guide_get_stats.argtypes = [c_void_p, POINTER(GuideStats)]
+    lib.ar_guide_get_probe.argtypes = [c_void_p, c_int32, c_void_p]
+    for f in ("ar_guide_create", "ar_guide_destroy", "ar_guide_render_frame", "ar_guide_get_stats", "ar_guide_get_probe"):
+        getattr(lib, f).restype = c_int32
     lib.ar_batch_autotune.argtypes = [c_void_p, c_int32, c_int32, POINTER(BatchTuning), c_void_p]
     lib.ar_batch_autotune.restype = c_int32
     lib.ar_nrc_create.argtypes = [c_void_p, POINTER(NrcConfig), POINTER(c_void_p)]
@@ -531,6 +548,45 @@ class RadianceCache:
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
             _lib.ar_nrc_destroy(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PathGuide:
+    """ar_guide: path-guiding probes of a scene for interactive frames."""
+
+    def __init__(self, scene: "Scene", probe_capacity: int = 0, log2_table: int = 0):
+        lib = load_library()
+        self._scene = scene
+        h = c_void_p()
+        cfg = GuideConfig(probe_capacity, log2_table)
+        _check(lib.ar_guide_create(scene.handle, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+
+    def render_frame(self, camera: Camera, params: RenderParams, out_ptr: int | None, accum_ptr: int | None,
+                     stream: int = 0) -> None:
+        _check(_lib.ar_guide_render_frame(self._h, ctypes.byref(camera), ctypes.byref(params),
+                                          c_void_p(out_ptr) if out_ptr else None,
+                                          c_void_p(accum_ptr) if accum_ptr else None, c_void_p(stream)))
+
+    def stats(self) -> GuideStats:
+        st = GuideStats()
+        _check(_lib.ar_guide_get_stats(self._h, ctypes.byref(st)))
+        return st
+
+    def probe(self, index: int) -> np.ndarray:
+        out = np.empty((88, 4), np.float32)
+        _check(_lib.ar_guide_get_probe(self._h, index, _ptr(out)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.ar_guide_destroy(self._h)
             self._h = c_void_p()
 
     def __del__(self):

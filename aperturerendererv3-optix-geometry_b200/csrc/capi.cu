@@ -83,6 +83,21 @@ private:
     bool changed_ = false;
 };
 
+// The same for destructors: never throws (the runtime may already be shutting
+// down when a handle is released at process exit).
+class QuietDeviceGuard {
+public:
+    explicit QuietDeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev_) == cudaSuccess && prev_ != dev) changed_ = cudaSetDevice(dev) == cudaSuccess;
+        cudaGetLastError();
+    }
+    ~QuietDeviceGuard() { if (changed_) cudaSetDevice(prev_); }
+private:
+    int prev_ = 0;
+    bool changed_ = false;
+};
+
 constexpr int64_t kMaxPool = int64_t(1) << 21;  // paths in flight
 
 }  // namespace
@@ -132,7 +147,7 @@ struct ar_scene {
 
     ~ar_scene()
     {
-        DeviceGuard g(device);
+        QuietDeviceGuard g(device);
         for (void* p : owned) cudaFree(p);
         if (ws) cudaFree(ws);
         if (ev0) cudaEventDestroy(ev0);
@@ -287,7 +302,8 @@ ar::FrameParams make_frame(const ar_scene* s, const ar_camera* c, const ar_rende
 }
 
 ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* p, ar_path_record* rec_dev,
-                     cudaStream_t st, ar_render_stats* stats, const ar::NrcFrame* nrc = nullptr)
+                     cudaStream_t st, ar_render_stats* stats, const ar::NrcFrame* nrc = nullptr,
+                     const ar::GuideView* guide = nullptr)
 {
     using namespace ar;
     if (p->spectral && !s->spec_tables)
@@ -299,6 +315,10 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
     pool = std::max<int64_t>(1, std::min<int64_t>(pool, total));
     fp.pool = static_cast<int32_t>(pool);
     if (nrc) fp.nrc = *nrc;
+    if (guide) {
+        fp.guiding = 1;
+        fp.guide = *guide;
+    }
     ensure_workspace(s, pool, npix);
     PathBuffers B = s->bufs;
     B.capacity = static_cast<int32_t>(pool);
@@ -1139,7 +1159,7 @@ struct ar_nrc {
     }
     ~ar_nrc()
     {
-        DeviceGuard g(scene->device);
+        QuietDeviceGuard g(scene->device);
         for (void* p : owned) cudaFree(p);
         for (cudaEvent_t e : ev)
             if (e) cudaEventDestroy(e);
@@ -1513,6 +1533,156 @@ ar_status ar_batch_autotune(const ar_job* jobs, int32_t njobs, int32_t probe_spp
         g_tuned[batch_key(jobs, njobs)] = {best.iterations_per_graph, best.path_budget};
     }
     *out = best;
+    return AR_OK;
+    AR_GUARD_END
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ path guiding
+struct ar_guide {
+    ar_scene* scene = nullptr;
+    ar::GuideView view{};
+    size_t table_size = 0;
+    int64_t frames = 0;
+    int64_t npix = 0;
+    float* faces = nullptr;
+    std::vector<void*> owned;
+    std::vector<void*> frame_bufs;
+    ~ar_guide()
+    {
+        QuietDeviceGuard g(scene->device);
+        for (void* p : owned) cudaFree(p);
+        for (void* p : frame_bufs) cudaFree(p);
+    }
+};
+
+namespace {
+template <class T>
+T* guide_alloc(std::vector<void*>& v, size_t count, const char* what)
+{
+    T* p = dalloc<T>(count, what);
+    v.push_back(p);
+    return p;
+}
+void guide_ensure_frame(ar_guide* g, int64_t npix)
+{
+    if (npix <= g->npix) return;
+    for (void* p : g->frame_bufs) cudaFree(p);
+    g->frame_bufs.clear();
+    const size_t n = static_cast<size_t>(npix);
+    g->view.events = guide_alloc<float4>(g->frame_bufs, n * ar::kPgEvents * 3, "guiding events");
+    g->view.event_lb = guide_alloc<float4>(g->frame_bufs, n * ar::kPgEvents, "guiding events");
+    g->view.event_count = guide_alloc<int32_t>(g->frame_bufs, n, "guiding events");
+    g->view.sample_cap = static_cast<int32_t>(std::min<int64_t>(npix * ar::kPgCollect, int64_t(1) << 22));
+    g->view.samples = guide_alloc<float4>(g->frame_bufs, static_cast<size_t>(g->view.sample_cap) * 3, "guiding samples");
+    ck(cudaMemset(g->view.event_count, 0, n * sizeof(int32_t)), "memset");
+    g->npix = npix;
+}
+}  // namespace
+
+extern "C" {
+
+ar_status ar_guide_create(ar_scene* s, const ar_guide_config* cfg, ar_guide** out)
+{
+    g_last_error.clear();
+    if (!s || !out) return fail(AR_ERR_INVALID_ARGUMENT, "scene or out is NULL");
+    *out = nullptr;
+    const int cap = cfg && cfg->probe_capacity > 0 ? cfg->probe_capacity : 131072;
+    const int lt = cfg && cfg->log2_table > 0 ? cfg->log2_table : 20;
+    if (cap > (1 << 24)) return fail(AR_ERR_INVALID_ARGUMENT, "probe_capacity above 2^24");
+    if (lt < 10 || lt > 28) return fail(AR_ERR_INVALID_ARGUMENT, "log2_table must be in [10, 28]");
+    AR_GUARD_BEGIN
+    DeviceGuard dg(s->device);
+    std::unique_ptr<ar_guide> g(new ar_guide());
+    g->scene = s;
+    g->table_size = size_t(1) << lt;
+    ar::GuideView& v = g->view;
+    v.capacity = cap;
+    v.table_mask = static_cast<uint32_t>(g->table_size - 1);
+    v.keys = guide_alloc<uint64_t>(g->owned, g->table_size, "guiding table");
+    v.slots = guide_alloc<int32_t>(g->owned, g->table_size, "guiding table");
+    v.probes = guide_alloc<float4>(g->owned, static_cast<size_t>(cap) * ar::kPgStride, "guiding probes");
+    v.accum = guide_alloc<float4>(g->owned, static_cast<size_t>(cap) * ar::kPgRes * ar::kPgRes, "guiding sums");
+    v.counts = guide_alloc<unsigned long long>(g->owned, static_cast<size_t>(cap), "guiding counts");
+    v.frame_counts = guide_alloc<unsigned int>(g->owned, static_cast<size_t>(cap), "guiding counts");
+    v.touched = guide_alloc<int32_t>(g->owned, static_cast<size_t>(cap), "guiding list");
+    v.counters = guide_alloc<int32_t>(g->owned, 6, "guiding counters");
+    float faces[60];
+    ar::pg_face_normals(faces);
+    float* df = guide_alloc<float>(g->owned, 60, "guiding faces");
+    ck(cudaMemcpy(df, faces, sizeof(faces), cudaMemcpyHostToDevice), "copy faces");
+    v.faces = df;
+    ck(ar::pg_clear(v, g->table_size, nullptr), "guiding clear");
+    ck(cudaDeviceSynchronize(), "guiding init");
+    *out = g.release();
+    return AR_OK;
+    AR_GUARD_END
+}
+
+ar_status ar_guide_destroy(ar_guide* g)
+{
+    g_last_error.clear();
+    delete g;
+    return AR_OK;
+}
+
+ar_status ar_guide_render_frame(ar_guide* g, const ar_camera* cam, const ar_render_params* p, float* out_rgb,
+                                double* accum, void* stream)
+{
+    g_last_error.clear();
+    if (!g) return fail(AR_ERR_INVALID_ARGUMENT, "guide is NULL");
+    if (ar_status e = check_camera(cam)) return e;
+    if (ar_status e = check_params(p)) return e;
+    if (p->spp != 1) return fail(AR_ERR_INVALID_ARGUMENT, "guided frames take spp = 1");
+    if (p->spectral) return fail(AR_ERR_UNSUPPORTED, "path guiding is RGB only");
+    if (!out_rgb && !accum) return fail(AR_ERR_INVALID_ARGUMENT, "out_rgb and accum are both NULL");
+    AR_GUARD_BEGIN
+    ar_scene* s = g->scene;
+    DeviceGuard dg(s->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t npix = static_cast<int64_t>(cam->width) * cam->height;
+    guide_ensure_frame(g, npix);
+    g->view.alpha = ar::pg_alpha(g->frames);
+    if (ar_status e = run_render(s, cam, p, nullptr, st, nullptr, nullptr, &g->view)) return e;
+    ck(ar::pg_update(g->view, s->sm_count, st), "guiding update");
+    ++g->frames;
+    const int64_t n = npix * 3;
+    if (out_rgb) ck(ar::launch_mean(s->accum, n, 1.0, out_rgb, st), "mean");
+    if (accum) ck(ar::launch_add(s->accum, n, accum, st), "accumulate");
+    return check_err(s, st);
+    AR_GUARD_END
+}
+
+ar_status ar_guide_get_stats(const ar_guide* g, ar_guide_stats* out)
+{
+    g_last_error.clear();
+    if (!g || !out) return fail(AR_ERR_INVALID_ARGUMENT, "NULL argument");
+    AR_GUARD_BEGIN
+    DeviceGuard dg(g->scene->device);
+    int32_t c[6];
+    ck(cudaMemcpy(c, g->view.counters, sizeof(c), cudaMemcpyDeviceToHost), "copy counters");
+    std::memset(out, 0, sizeof(*out));
+    out->frames = g->frames;
+    out->probes = std::min<int64_t>(c[0], g->view.capacity);
+    out->samples = c[4];
+    out->dropped = c[5];
+    out->alpha = ar::pg_alpha(std::max<int64_t>(0, g->frames - 1));
+    return AR_OK;
+    AR_GUARD_END
+}
+
+ar_status ar_guide_get_probe(const ar_guide* g, int32_t index, float* texels)
+{
+    g_last_error.clear();
+    if (!g || !texels) return fail(AR_ERR_INVALID_ARGUMENT, "NULL argument");
+    AR_GUARD_BEGIN
+    DeviceGuard dg(g->scene->device);
+    int32_t c[4];
+    ck(cudaMemcpy(c, g->view.counters, sizeof(c), cudaMemcpyDeviceToHost), "copy counters");
+    if (index < 0 || index >= std::min(c[0], g->view.capacity)) return fail(AR_ERR_INVALID_ARGUMENT, "probe not allocated");
+    ck(cudaMemcpy(texels, g->view.probes + static_cast<size_t>(index) * ar::kPgStride, sizeof(float4) * ar::kPgStride,
+                  cudaMemcpyDeviceToHost), "copy probe");
     return AR_OK;
     AR_GUARD_END
 }

@@ -354,7 +354,7 @@ __device__ __forceinline__ GB gb_at(const GB& rgb, const SpectralView& sv, const
 // the shadow query: Trace's material evaluation and hit offset, emission with
 // MIS, light sampling for NEE, throughput and Russian roulette.  kModel is the
 // shading model of every path of this launch's bucket, -1 = miss.
-template <int kModel, bool kExt, int kSpec, bool kNrc>
+template <int kModel, bool kExt, int kSpec, bool kNrc, bool kGuide>
 __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams fp, PathBuffers B, int cur,
                                                        PoolCtl* ctl, ar_path_record* rec)
 {
@@ -411,6 +411,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
         }
         const bool inside = (flags & kFlagInside) != 0;
         const f3 vloc = xyz(pr.vloc);
+        const f3 maskIn = mask, radIn = radiance;   // path guiding: values at arrival
         const int4 hr = B.hit[k];
         constexpr bool kMed = kModel == kModelMedium;  // collisions in the participating medium
         constexpr bool hit = kModel >= 0 && !kMed;
@@ -638,6 +639,45 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             }
             nInside = false;
         }
+        // ---- path guiding (render.cuh:555-640): mix the probe's hemisphere
+        // density into the BSDF's, or sample the probe with probability alpha
+        int gProbe = -1;
+        bool guidable = false;
+        f3 gq = mk(0.0f, 0.0f, 0.0f);
+        uint64_t gKey = 0;
+        if (kGuide && hit && (kModel == AR_MAT_DIFFUSE || kModel == AR_MAT_GGX) && !inside && !terminate) {
+            guidable = true;
+            gKey = pg_key(pos, reflect(crd, nrm), fp.guide.faces);
+            gProbe = pg_lookup(fp.guide, gKey);
+            if (gProbe >= 0) {
+                const f3 mq = vmaxs(mask, 1.0e-6f);
+                gq = mq / (mq.x + mq.y + mq.z + 1.0e-6f);
+                const float4* P = fp.guide.probes + static_cast<int64_t>(gProbe) * kPgStride;
+                const float pP = pg_hemi_pdf(P, next, nrm, gq);
+                const float a = fp.guide.alpha;
+                if (pdf > 1.0e-12f && pP > 1.0e-12f) {
+                    if (g.next() < a) {
+                        float u[5];
+#pragma unroll
+                        for (int t = 0; t < 5; ++t) u[t] = g.next();
+                        float pg;
+                        const f3 w = pg_sample_hemi(P, nrm, gq, u, &pg);
+                        if (dot(w, nrm) > 1.0e-12f) {
+                            const float pBs = bsdf_pdf(kModel, gb, nrm, crd, w);
+                            next = w;
+                            brdf = eval_bsdf_cos(kModel, crd, w, nrm, pos, gb, inside, vloc);
+                            pdf = (1.0f - a) * fmaxf(pBs, 1.0e-12f) + a * pg;
+                        } else {
+                            gProbe = -1;
+                        }
+                    } else {
+                        pdf = (1.0f - a) * pdf + a * pP;
+                    }
+                } else {
+                    gProbe = -1;
+                }
+            }
+        }
         if (!kMed) {   // hit offset, always one uniform (render.cuh:156-160)
             const float offEps = eps * fmaxf(1.0f, length(pos));
             const float sg = signf(dot(nrm, next));
@@ -693,8 +733,13 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                             const float G = cosY / d2;
                             const f3 contrib = (fcos * ls.emis) * (G / pATotal);
                             const float pL = area_to_solid_angle(pos, ls.p, ls.n, ls.pFacet * ls.pA);
-                            const float pB = kMed ? hg_phase(s.medium.g, dot(crd, ld))
-                                                  : fmaxf(bsdf_pdf(kModel, gb, nrm, crd, ld), 0.0f);
+                            float pB = kMed ? hg_phase(s.medium.g, dot(crd, ld))
+                                            : fmaxf(bsdf_pdf(kModel, gb, nrm, crd, ld), 0.0f);
+                            if (kGuide && gProbe >= 0) {
+                                const float a = fp.guide.alpha;
+                                pB = (1.0f - a) * pB +
+                                     a * pg_hemi_pdf(fp.guide.probes + static_cast<int64_t>(gProbe) * kPgStride, ld, nrm, gq);
+                            }
                             const float wmis = power_heuristic(pL, pB);
                             pending = (mask * (contrib * wmis)) * d65v;
                             if (kSpec == 4) {
@@ -757,6 +802,18 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             }
         }
         flags = (flags & ~kFlagInside) | (mInside ? kFlagInside : 0);
+        if (kGuide) {   // this event of the pixel's path, for the probes' samples at retirement
+            const int ne = fp.guide.event_count[pixel];
+            if (ne < kPgEvents) {
+                float4* ev = fp.guide.events + (static_cast<int64_t>(pixel) * kPgEvents + ne) * 3;
+                ev[0] = make_float4(__uint_as_float(static_cast<uint32_t>(gKey)), __uint_as_float(static_cast<uint32_t>(gKey >> 32)),
+                                    (guidable && cont) ? 1.0f : 0.0f, 0.0f);
+                ev[1] = f4(next, 0.0f);
+                ev[2] = f4(maskIn, 0.0f);
+                fp.guide.event_lb[static_cast<int64_t>(pixel) * kPgEvents + ne] = f4(radIn, 0.0f);
+                fp.guide.event_count[pixel] = ne + 1;
+            }
+        }
         const uint32_t used = pr.rng1.w + static_cast<uint32_t>(g.used);
         int target;
         const int j = warp_alloc(&ctl->count[1 - cur], cont);
@@ -968,6 +1025,32 @@ __global__ void k_retire(FrameParams fp, PathBuffers B, PoolCtl* ctl, double* ac
                 }
             }
         }
+        if (fp.guiding) {
+            // incident radiance along each guidable vertex's sampled direction:
+            // radiance gathered from the next event on over the throughput that reached it
+            const int ne = fp.guide.event_count[pixel];
+            const f3 L = mk(fix_nan_inf(rr.rad.x), fix_nan_inf(rr.rad.y), fix_nan_inf(rr.rad.z));
+            for (int e = 0; e + 1 < ne; ++e) {
+                const float4* ev = fp.guide.events + (static_cast<int64_t>(pixel) * kPgEvents + e) * 3;
+                const float4 h = ev[0];
+                if (h.z == 0.0f) continue;
+                const float4 tn = fp.guide.events[(static_cast<int64_t>(pixel) * kPgEvents + e + 1) * 3 + 2];
+                const float4 lb = fp.guide.event_lb[static_cast<int64_t>(pixel) * kPgEvents + e + 1];
+                const f3 inc = mk(tn.x > 1e-8f ? fmaxf((L.x - lb.x) / tn.x, 0.0f) : 0.0f,
+                                  tn.y > 1e-8f ? fmaxf((L.y - lb.y) / tn.y, 0.0f) : 0.0f,
+                                  tn.z > 1e-8f ? fmaxf((L.z - lb.z) / tn.z, 0.0f) : 0.0f);
+                const float strength = fminf(luminance(inc), kPgMaxBrightness);
+                if (!(strength >= kPgMinBrightness)) continue;
+                const int si = atomicAdd(&fp.guide.counters[2], 1);
+                if (si < fp.guide.sample_cap) {
+                    float4* o = fp.guide.samples + 3 * static_cast<int64_t>(si);
+                    o[0] = make_float4(h.x, h.y, 0.0f, 0.0f);
+                    o[1] = ev[1];
+                    o[2] = f4(inc, 0.0f);
+                }
+            }
+            fp.guide.event_count[pixel] = 0;
+        }
         double* a = accum + 3 * static_cast<int64_t>(pixel);
         atomicAdd(a + 0, static_cast<double>(x));
         atomicAdd(a + 1, static_cast<double>(y));
@@ -1052,17 +1135,17 @@ cudaError_t launch_pool_init(PoolCtl* ctl, int64_t total, cudaStream_t st)
 }
 
 // The five per-material shading launches of one iteration.
-template <bool kExt, int kSpec, bool kNrc>
+template <bool kExt, int kSpec, bool kNrc, bool kGuide = false>
 void launch_shade(const SceneView& s, const FrameParams& fp, const PathBuffers& B, int c, PoolCtl* ctl,
                   ar_path_record* rec, int grid, cudaStream_t st)
 {
-    k_shade<-1, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_DIFFUSE, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_LIGHT, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_GLASS, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
-    k_shade<AR_MAT_GGX, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<-1, kExt, kSpec, kNrc, kGuide><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_DIFFUSE, kExt, kSpec, kNrc, kGuide><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_LIGHT, kExt, kSpec, kNrc, kGuide><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_GLASS, kExt, kSpec, kNrc, kGuide><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+    k_shade<AR_MAT_GGX, kExt, kSpec, kNrc, kGuide><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
     if (kExt && s.has_medium)
-        k_shade<kModelMedium, kExt, kSpec, kNrc><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
+        k_shade<kModelMedium, kExt, kSpec, kNrc, kGuide><<<grid, kShadeBlock, 0, st>>>(s, fp, B, c, ctl, rec);
 }
 
 cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const PathBuffers& B, PoolCtl* ctl,
@@ -1086,6 +1169,9 @@ cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const P
         } else if (fp.spectral) {
             if (ext) launch_shade<true, 1, false>(s, fp, B, c, ctl, rec, grid_other, st);
             else launch_shade<false, 1, false>(s, fp, B, c, ctl, rec, grid_other, st);
+        } else if (fp.guiding) {
+            if (ext) launch_shade<true, 0, false, true>(s, fp, B, c, ctl, rec, grid_other, st);
+            else launch_shade<false, 0, false, true>(s, fp, B, c, ctl, rec, grid_other, st);
         } else if (fp.nrc.enabled) {
             if (ext) launch_shade<true, 0, true>(s, fp, B, c, ctl, rec, grid_other, st);
             else launch_shade<false, 0, true>(s, fp, B, c, ctl, rec, grid_other, st);

@@ -23,6 +23,7 @@
 #include <cstdint>
 
 #include "../../include/aperture_b200.h"
+#include "guiding.cuh"
 #include "nrc.cuh"
 #include "spectral.cuh"
 #include "traverse.cuh"
@@ -114,6 +115,8 @@ struct FrameParams {
     SpectralView spec;       // tables and lookup tables of the spectral mode
     uint32_t medium_key;     // medium_frame_key(seed, frame0)
     NrcFrame nrc;            // learned radiance cache hooks (enabled = 0: plain tracer)
+    int32_t guiding;         // 1: path guiding with `guide` (interactive frames, one path per pixel)
+    GuideView guide;
 };
 
 }  // namespace ar

@@ -373,6 +373,43 @@ ar_status ar_nrc_train(ar_nrc* nrc, const float* samples, size_t n, int32_t step
 ar_status ar_nrc_gradients(ar_nrc* nrc, const float* samples, size_t n, float* table_grad, float* weight_grad,
                            float* loss);
 
+/* ------------------------------------------------------------------------ */
+/* Path guiding (SceneRenderer's interactive mode with bUsePathGuiding:       */
+/* core/render/render.cuh:545-640, core/guiding, scene.cu:583-744).           */
+/* Probes of incident RGB radiance (8x8 equal-area octahedral maps with mips) */
+/* per (0.05-unit voxel, icosahedron face of the reflected direction), filled */
+/* from the radiance the frame's paths bring back and sampled with           */
+/* probability alpha = 0.5 * min(1, frame / 64)^0.5 (mixture pdf, also in    */
+/* MIS).  Interactive frames: one path per pixel per call, RGB.              */
+/* ------------------------------------------------------------------------ */
+typedef struct ar_guide ar_guide;
+
+typedef struct ar_guide_config {
+    int32_t probe_capacity;     /* probes in the pool (131072)                        */
+    int32_t log2_table;         /* hash-table slots = 2^log2_table (20)               */
+} ar_guide_config;
+
+typedef struct ar_guide_stats {
+    int64_t frames;             /* guided frames rendered                             */
+    int64_t probes;             /* probes allocated (keys seen, capped by capacity)   */
+    int64_t samples;            /* samples of the last frame                          */
+    int64_t dropped;            /* samples of the last frame without a probe          */
+    float alpha;                /* guiding probability of the last frame              */
+    int32_t reserved;
+} ar_guide_stats;
+
+ar_status ar_guide_create(ar_scene* scene, const ar_guide_config* config, ar_guide** out);
+ar_status ar_guide_destroy(ar_guide* guide);
+/* One interactive frame (params->spp must be 1, RGB): render with the current
+ * probes, then add the frame's samples to them.  out_rgb / accum as in
+ * ar_render with AR_MEM_DEVICE (either may be NULL, not both). */
+ar_status ar_guide_render_frame(ar_guide* guide, const ar_camera* camera, const ar_render_params* params,
+                                float* out_rgb, double* accum, void* stream);
+ar_status ar_guide_get_stats(const ar_guide* guide, ar_guide_stats* stats);
+/* Copy of probe `index` (88 float4 texels: 8x8 leaves, 4x4, 2x2, 1x1 mips,
+ * padding), or AR_ERR_INVALID_ARGUMENT when it is not allocated. */
+ar_status ar_guide_get_probe(const ar_guide* guide, int32_t index, float* texels);
+
 /* One job of a batch: a scene (shared between jobs if wanted), a camera, the
  * render parameters and device outputs (mean image and/or FP64 sums added). */
 typedef struct ar_job {

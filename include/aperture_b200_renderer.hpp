@@ -209,6 +209,7 @@ public:
     SceneRenderer(const SceneRenderer&) = delete;
     ~SceneRenderer()
     {
+        MarkNeedResetGuiding();
         if (scene_) ar_scene_destroy(scene_);
         FreeAccum();
     }
@@ -216,7 +217,14 @@ public:
     void SetExposure(float exp) { exposure_ = exp; }
     float GetExposure() const { return exposure_; }
     void MarkAsDirty() { dirty_ = true; }
-    void MarkNeedResetGuiding() {}
+    // Path guiding of the interactive render (the reference's
+    // CalculateRadiance<..., bUsePathGuiding>): off by default here.
+    void SetPathGuiding(bool on) { useGuiding_ = on; }
+    void MarkNeedResetGuiding()
+    {
+        if (guide_) ar_guide_destroy(guide_);
+        guide_ = nullptr;
+    }
 
     // Offline render: linear RGB, row j*size.x + i, mean of sampleNum samples
     // (frames 0 .. sampleNum-1).
@@ -244,14 +252,19 @@ public:
                 denoise::ScreenStatisticsBuffer* screenStatisticsBuffer = nullptr)
     {
         if (oddTarget || evenTarget || radianceSampleBuffer || screenGBuffer || screenStatisticsBuffer)
-            std::cout << "aperture_b200: odd/even, path-guiding and denoiser buffers are not supported; ignored\n";
+            std::cout << "aperture_b200: odd/even, path-guiding sample and denoiser buffers are not supported; ignored\n";
         if (!hdrTarget || size.x <= 0 || size.y <= 0 || !Upload()) return;
         const size_t n = static_cast<size_t>(size.x) * size.y * 3;
         if (!EnsureAccum(n)) return;
         if (frameIndex <= 0 && !ZeroAccum()) return;
         const ar_camera cam = MakeCamera(size, cameraOrigin, cameraDirection);
         const ar_render_params p = MakeParams(1, frameIndex > 0 ? frameIndex : 0);
-        if (!Check(ar_render(scene_, &cam, &p, nullptr, accum_, AR_MEM_DEVICE, nullptr, nullptr))) return;
+        if (useGuiding_) {
+            if (!guide_ && !Check(ar_guide_create(scene_, nullptr, &guide_))) return;
+            if (!Check(ar_guide_render_frame(guide_, &cam, &p, nullptr, accum_, nullptr))) return;
+        } else if (!Check(ar_render(scene_, &cam, &p, nullptr, accum_, AR_MEM_DEVICE, nullptr, nullptr))) {
+            return;
+        }
         const double scale = 1.0 / static_cast<double>((frameIndex > 0 ? frameIndex : 0) + 1);
         if (!Check(ar_accum_resolve(accum_, n, scale, reinterpret_cast<float*>(hdrTarget), AR_MEM_DEVICE, nullptr)))
             return;
@@ -265,6 +278,8 @@ public:
 
 private:
     ar_scene* scene_ = nullptr;
+    ar_guide* guide_ = nullptr;
+    bool useGuiding_ = false;
     bool dirty_ = true;
     float exposure_ = 1.0f;
     double* accum_ = nullptr;
@@ -280,6 +295,7 @@ private:
     bool Upload()
     {
         if (!dirty_ && scene_) return true;
+        MarkNeedResetGuiding();
         if (scene_) {
             ar_scene_destroy(scene_);
             scene_ = nullptr;
