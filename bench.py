@@ -244,6 +244,81 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
     return res
 
 
+def _timed_render(scene: Scene, cam, params, out, stream) -> dict:
+    scene.render_device(cam, params, out.data_ptr(), None, stream.cuda_stream, RenderStats())   # warm-up
+    st = RenderStats()
+    scene.render_device(cam, params, out.data_ptr(), None, stream.cuda_stream, st)
+    stream.synchronize()
+    rays = st.extension_rays + st.shadow_rays
+    return {"ms": round(st.total_ms, 3), "mrays_per_s": round(rays / (st.total_ms / 1e3) / 1e6, 1),
+            "msamples_per_s": round(st.paths / (st.total_ms / 1e3) / 1e6, 2), "paths": st.paths, "rays": rays}
+
+
+def measure_configs(torch, dev, stream, c5_jobs: int) -> dict:
+    """The other benchmark configurations, one timed render each after one
+    warm-up (device time from the library's CUDA events): config 1 (box,
+    256x256, 16 spp), config 3 (box + SDF torus on a 256^3 half grid + 128^3
+    half fBm medium, 1280x720, 256 spp, depth 16, four wavelengths when the
+    spectral tables are present) and config 5 (seeded jobs of uneven
+    resolution, spp, scene size, RGB/spectral in one CUDA graph after the
+    autotuner; c5_jobs of them, triangle counts log-uniform in 10K-500K)."""
+    import spectral_tables
+    from aperture_b200 import autotune_batch, render_batch
+    res = {}
+    out = torch.empty(1280 * 720 * 3, dtype=torch.float32, device=dev)
+    sc1 = Scene(scenes.box_scene(), device=dev.index)
+    r = _timed_render(sc1, scenes.box_camera(256, 256), make_params(spp=16, max_depth=8), out, stream)
+    res["config1"] = dict(workload="box scene (34 triangles + cube light), 256x256, 16 spp, depth 8, RGB", **r)
+    spectral = spectral_tables.available()
+    objs, vols, med = scenes.medium_box_scene(precision=16, grid=256, medium_grid=128)
+    sc3 = Scene(objs, volumes=vols, device=dev.index)
+    sc3.set_medium(**med)
+    if spectral:
+        sc3.set_spectral(64)
+    r = _timed_render(sc3, scenes.box_camera(1280, 720),
+                      make_params(spp=256, max_depth=16, spectral=4 if spectral else 0), out, stream)
+    res["config3"] = dict(workload="box + glass analytic torus + GGX torus on a 256^3 half SDF grid + 128^3 half fBm "
+                                   "medium (sigma_t 2, albedo 0.8, g 0.3), 1280x720, 256 spp, depth 16, "
+                                   + ("4 hero wavelengths, RGB LUT 64^3" if spectral else "RGB (spectral tables absent)"),
+                          **r)
+    rng = np.random.default_rng(0xA11CE + 5)
+    jobs, outs, info = [], [], []
+    cache = {}
+    for j in range(c5_jobs):
+        tris = float(np.exp(rng.uniform(np.log(1e4), np.log(5e5))))
+        nsph = max(8, int(tris // 1280))
+        w = int(np.exp(rng.uniform(np.log(128), np.log(1024))))
+        h = int(np.exp(rng.uniform(np.log(128), np.log(1024))))
+        spp = int(rng.choice([4, 16, 64, 256]))
+        spec = spectral and j % 2 == 1
+        key = (nsph, spec)
+        if key not in cache:
+            sc = Scene(scenes.spheres_scene(seed=0xA11CE + 100 + j, n_spheres=nsph), device=dev.index)
+            if spec:
+                sc.set_spectral(32)
+            cache[key] = sc
+        sc = cache[key]
+        cam = scenes.spheres_camera(w, h)
+        o = torch.empty(w * h * 3, dtype=torch.float32, device=dev)
+        outs.append(o)
+        jobs.append((sc, cam, make_params(spp=spp, max_depth=DEPTH, spectral=1 if spec else 0), o.data_ptr(), None))
+        info.append({"triangles": nsph * 1280 + 2, "width": w, "height": h, "spp": spp, "spectral": bool(spec)})
+    tune = autotune_batch(jobs, probe_spp=4, stream=stream.cuda_stream)
+    render_batch(jobs, stream=stream.cuda_stream)          # warm-up with the tuned knobs
+    st = render_batch(jobs, stream=stream.cuda_stream)
+    res["config5"] = {"workload": f"{c5_jobs} seeded jobs (config-2 generator with 8-390 icospheres), resolutions "
+                                  "log-uniform 128-1024 per axis, spp in {4,16,64,256}, every second job spectral; "
+                                  "one CUDA graph, autotuned (radiance caches per job not included)",
+                      "ms": round(st.total_ms, 3),
+                      "mrays_per_s": round((st.extension_rays + st.shadow_rays) / (st.total_ms / 1e3) / 1e6, 1),
+                      "msamples_per_s": round(st.paths / (st.total_ms / 1e3) / 1e6, 2),
+                      "paths": st.paths, "graph_launches": st.graph_launches,
+                      "autotuned": {"iterations_per_graph": tune.iterations_per_graph, "path_budget": tune.path_budget,
+                                    "probe_ms_best": round(tune.best_ms, 3), "probe_ms_default": round(tune.default_ms, 3)},
+                      "jobs": info}
+    return res
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -386,6 +461,8 @@ def run_ours(args) -> None:
         }
         if world == 1 and args.nrc != "off":
             line["nrc"] = measure_nrc(torch, dev, scene, args.nrc, stream)
+        if world == 1 and args.configs > 0:
+            line["other_configs"] = measure_configs(torch, dev, stream, args.configs)
         if world == 1 and not args.no_cpu:
             cs = cpu_sample(objs, cam, params, args.cpu_seconds, cpu_threads())
             line["cpu_baseline"] = {"value": round(cs["value"], 4), "unit": "Mrays/s", "cores": cpu_threads(),
@@ -489,6 +566,8 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU sample length per measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--configs", type=int, default=16,
+                    help="also time configs 1, 3 and 5 (this many batch jobs); 0 skips")
     ap.add_argument("--nrc", choices=("off", "small", "full"), default="small",
                     help="radiance-cache time-to-relMSE measurement (small: 480x270, full: 1920x1080)")
     ap.add_argument("--profile-nrc", action="store_true",
