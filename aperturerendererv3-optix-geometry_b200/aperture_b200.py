@@ -16,7 +16,7 @@ from ctypes import POINTER, c_char_p, c_double, c_float, c_int32, c_int64, c_siz
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libaperture_b200.so")
+LIB_PATH = os.environ.get("AR_LIBRARY") or os.path.join(HERE, "libaperture_b200.so")   # AR_LIBRARY: another build
 
 AR_OK = 0
 STATUS_NAMES = {0: "AR_OK", 1: "AR_ERR_INVALID_ARGUMENT", 2: "AR_ERR_CUDA", 3: "AR_ERR_OUT_OF_MEMORY",
@@ -179,7 +179,7 @@ EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create",
                     "ar_scene_set_spectral", "ar_scene_get_spectral_luts", "ar_render_batch",
                     "ar_scene_set_medium", "ar_nrc_create", "ar_nrc_destroy", "ar_nrc_render_frame",
                     "ar_nrc_get_params", "ar_nrc_set_params", "ar_nrc_infer", "ar_nrc_train", "ar_nrc_gradients",
-                    "ar_batch_autotune", "ar_guide_create", "ar_guide_destroy", "ar_guide_render_frame",
+                    "ar_batch_autotune", "ar_nrc_set_option", "ar_guide_create", "ar_guide_destroy", "ar_guide_render_frame",
                     "ar_guide_get_stats", "ar_guide_get_probe")
 
 
@@ -254,6 +254,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_nrc_infer.argtypes = [c_void_p, c_void_p, c_size_t, c_void_p]
     lib.ar_nrc_train.argtypes = [c_void_p, c_void_p, c_size_t, c_int32, c_void_p]
     lib.ar_nrc_gradients.argtypes = [c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p]
+    lib.ar_nrc_set_option.argtypes = [c_void_p, c_int32, c_int32]
+    lib.ar_nrc_set_option.restype = c_int32
     for f in ("ar_nrc_create", "ar_nrc_destroy", "ar_nrc_render_frame", "ar_nrc_get_params", "ar_nrc_set_params",
               "ar_nrc_infer", "ar_nrc_train", "ar_nrc_gradients"):
         getattr(lib, f).restype = c_int32
@@ -513,6 +515,10 @@ class RadianceCache:
                                         c_void_p(accum_ptr) if accum_ptr else None, int(train),
                                         ctypes.byref(st) if st is not None else None, c_void_p(stream)))
         return st
+
+    def set_tensor_path(self, tcgen05: bool) -> None:
+        """Inference kernel: tcgen05.mma with tensor-memory accumulators, or mma.sync."""
+        _check(_lib.ar_nrc_set_option(self._h, 1, 1 if tcgen05 else 0))
 
     def params(self):
         t = np.empty(self.table_floats, np.float32)

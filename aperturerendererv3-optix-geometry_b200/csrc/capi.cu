@@ -1145,6 +1145,8 @@ struct ar_nrc {
     ar::NrcSample* samples = nullptr;
     int32_t* counters = nullptr;   // [0] queries, [1] samples, [2..] slot vertex counts
     int slots = 0, sample_cap = 0;
+    int* tc_err = nullptr;         // error word of the tcgen05 inference kernel
+    int tensor_path = 1;           // inference: 1 tcgen05 (default), 0 mma.sync
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<void*> owned;
 
@@ -1184,6 +1186,26 @@ void nrc_ensure_queries(ar_nrc* c, int64_t n)
     if (c->queries) cudaFree(c->queries);
     c->queries = nrc_alloc<ar::NrcQuery>(c, static_cast<size_t>(n), "cache queries");
     c->query_cap = n;
+}
+
+cudaError_t nrc_run_infer(ar_nrc* c, const ar::NrcQuery* q, const int32_t* count, int cap, double* accum,
+                          float* out_rgb, cudaStream_t st)
+{
+    if (c->tensor_path == 1)
+        return ar::nrc_infer_tc(c->net(), q, count, cap, accum, out_rgb, c->tc_err, c->scene->sm_count, st);
+    return ar::nrc_infer(c->net(), q, count, cap, accum, out_rgb, c->scene->sm_count, st);
+}
+
+ar_status nrc_check(ar_nrc* c, cudaStream_t st)
+{
+    int e = 0;
+    ck(cudaMemcpyAsync(&e, c->tc_err, sizeof(int), cudaMemcpyDeviceToHost, st), "copy error word");
+    ck(cudaStreamSynchronize(st), "sync");
+    if (e != 0) {
+        ck(cudaMemsetAsync(c->tc_err, 0, sizeof(int), st), "memset");
+        return fail(AR_ERR_DEVICE_FAULT, "tensor-core inference: an MMA did not complete within its wait limit");
+    }
+    return AR_OK;
 }
 
 ar_status nrc_train_steps(ar_nrc* c, const ar::NrcSample* samples, const int32_t* count, int steps, cudaStream_t st)
@@ -1273,6 +1295,8 @@ ar_status ar_nrc_create(ar_scene* s, const ar_nrc_config* cfg, ar_nrc** out)
     c->tverts = nrc_alloc<ar::NrcTrainVertex>(c.get(), static_cast<size_t>(c->slots) * cfg->max_train_vertices, "cache training vertices");
     c->samples = nrc_alloc<ar::NrcSample>(c.get(), static_cast<size_t>(c->sample_cap), "cache samples");
     c->counters = nrc_alloc<int32_t>(c.get(), static_cast<size_t>(c->slots) + 2, "cache counters");
+    c->tc_err = nrc_alloc<int>(c.get(), 1, "cache error word");
+    ck(cudaMemset(c->tc_err, 0, sizeof(int)), "memset");
     ck(ar::nrc_init_params(P, cfg->seed, nullptr), "cache init");
     for (cudaEvent_t& e : c->ev) ck(cudaEventCreate(&e), "event");
     ck(cudaDeviceSynchronize(), "cache init");
@@ -1326,8 +1350,8 @@ ar_status ar_nrc_render_frame(ar_nrc* c, const ar_camera* cam, const ar_render_p
     ck(cudaEventRecord(c->ev[0], st), "event");
     if (ar_status e = run_render(s, cam, p, nullptr, st, stats ? &rs : nullptr, &f)) return e;
     ck(cudaEventRecord(c->ev[1], st), "event");
-    ck(ar::nrc_infer(c->net(), c->queries, c->counters, static_cast<int>(c->query_cap), s->accum, nullptr,
-                     s->sm_count, st), "cache inference");
+    ck(nrc_run_infer(c, c->queries, c->counters, static_cast<int>(c->query_cap), s->accum, nullptr, st),
+       "cache inference");
     ck(cudaEventRecord(c->ev[2], st), "event");
     if (train) nrc_train_steps(c, c->samples, c->counters + 1, c->cfg.train_steps, st);
     ck(cudaEventRecord(c->ev[3], st), "event");
@@ -1351,8 +1375,19 @@ ar_status ar_nrc_render_frame(ar_nrc* c, const ar_camera* cam, const ar_render_p
         stats->shadow_rays = rs.shadow_rays;
         stats->loss = train && c->cfg.train_steps > 0 ? loss / static_cast<float>(c->cfg.train_steps) : 0.0f;
     }
+    if (ar_status e = nrc_check(c, st)) return e;
     return check_err(s, st);
     AR_GUARD_END
+}
+
+ar_status ar_nrc_set_option(ar_nrc* c, int32_t option, int32_t value)
+{
+    g_last_error.clear();
+    if (!c) return fail(AR_ERR_INVALID_ARGUMENT, "cache is NULL");
+    if (option != AR_NRC_OPT_TENSOR_PATH || (value != 0 && value != 1))
+        return fail(AR_ERR_INVALID_ARGUMENT, "unknown option or value");
+    c->tensor_path = value;
+    return AR_OK;
 }
 
 ar_status ar_nrc_get_params(const ar_nrc* c, float* table, float* weights)
@@ -1404,7 +1439,7 @@ ar_status ar_nrc_infer(ar_nrc* c, const float* vertices, size_t n, float* out_rg
         const int32_t ni = static_cast<int32_t>(n);
         ck(cudaMemcpy(q, h.data(), n * sizeof(ar::NrcQuery), cudaMemcpyHostToDevice), "copy vertices");
         ck(cudaMemcpy(cnt, &ni, 4, cudaMemcpyHostToDevice), "copy count");
-        e = ar::nrc_infer(c->net(), q, cnt, ni, nullptr, out, c->scene->sm_count, nullptr);
+        e = nrc_run_infer(c, q, cnt, ni, nullptr, out, nullptr);
         if (e == cudaSuccess) e = cudaMemcpy(out_rgb, out, n * 12, cudaMemcpyDeviceToHost);
     } catch (...) {
         cudaFree(q); cudaFree(out); cudaFree(cnt);
@@ -1412,7 +1447,7 @@ ar_status ar_nrc_infer(ar_nrc* c, const float* vertices, size_t n, float* out_rg
     }
     cudaFree(q); cudaFree(out); cudaFree(cnt);
     ck(e, "cache inference");
-    return AR_OK;
+    return nrc_check(c, nullptr);
     AR_GUARD_END
 }
 

@@ -182,6 +182,10 @@ cudaError_t nrc_init_params(const NrcParams& P, uint64_t seed, cudaStream_t st);
 cudaError_t nrc_publish(const NrcParams& P, cudaStream_t st);   // bf16 / half copies of the fp32 masters
 cudaError_t nrc_infer(const NrcNet& net, const NrcQuery* q, const int32_t* count, int cap, double* accum,
                       float* out_rgb, int sm_count, cudaStream_t st);
+// The same inference on the tcgen05 tensor cores (nrc_tc.cu); *err gets bit 1
+// when a CTA's MMA wait runs out.
+cudaError_t nrc_infer_tc(const NrcNet& net, const NrcQuery* q, const int32_t* count, int cap, double* accum,
+                         float* out_rgb, int* err, int sm_count, cudaStream_t st);
 cudaError_t nrc_train_step(const NrcNet& net, const NrcParams& P, const NrcSample* samples, const int32_t* count,
                            int first, int batch, const NrcTrainBuffers& T, float lr, int step, int sm_count,
                            cudaStream_t st, bool apply = true);

@@ -1,0 +1,287 @@
+// nrc_tc.cu -- radiance-cache inference on the 5th-generation tensor cores:
+// tcgen05.mma (M = 128 rows per CTA, kind::f16 with bf16 operands, fp32
+// accumulators in tensor memory), one elected thread issuing the MMAs of a
+// layer, completion through tcgen05.commit on an mbarrier, and the epilogue
+// of each layer (ReLU, bf16 pack, or exp at the output) from tcgen05.ld:
+// thread t of the CTA owns row t of the tile, so it reads its 64 accumulator
+// columns from TMEM lane t and writes the next layer's A operand row back to
+// shared memory.
+//
+// Operands live in shared memory in the canonical K-major layout without
+// swizzle: 16-byte core rows of 8 bf16, 8 rows per 128-byte core matrix;
+// element (r, k) of an R-row operand sits at
+//   (k / 8) * (R * 16) + (r / 8) * 128 + (r % 8) * 16 + (k % 8) * 2 bytes,
+// so one K = 16 step of the MMA is the pair of 8-column chunks 2s, 2s + 1:
+// start = chunk 2s, leading-dimension offset (next chunk) = R * 16 bytes,
+// stride-dimension offset (next 8 rows) = 128 bytes.
+//
+// Every wait is bounded: a CTA whose MMA does not complete within the limit
+// sets the error word, skips the rest of its work, and still frees its
+// tensor memory.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "nrc.cuh"
+
+namespace ar {
+
+namespace {
+
+constexpr int kTcRows = 128;                       // rows per CTA tile (M)
+constexpr int kTcThreads = 128;
+constexpr int kTcCols = 64;                        // TMEM columns allocated (fp32 accumulators)
+constexpr int kTcWBytes = 5 * kNrcHid * kNrcIn * 2 + kNrcOut * kNrcIn * 2;   // 43008
+constexpr int kTcABytes = kTcRows * kNrcIn * 2;                               // 16384
+constexpr int kTcSmem = kTcWBytes + kTcABytes + 64;
+constexpr uint32_t kTcSpinLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// byte offset of the 16-byte chunk (row r, k-chunk kc) of an R-row operand
+__host__ __device__ constexpr uint32_t tc_chunk_offset(int R, int r, int kc)
+{
+    return static_cast<uint32_t>(kc * (R * 16) + (r / 8) * 128 + (r % 8) * 16);
+}
+
+// shared-memory matrix descriptor: start, leading/stride byte offsets, version 1, no swizzle
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+           (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: fp32 accumulator, bf16 A and B, both K-major, M x N
+__host__ __device__ constexpr uint32_t tc_idesc(int M, int N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n"
+        :
+        : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" : : "r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t phase)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t"
+        "}"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ void tc_ld64(uint32_t taddr, uint32_t* v)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
+        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31]),
+          "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]),
+          "=r"(v[40]), "=r"(v[41]), "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]),
+          "=r"(v[48]), "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]), "=r"(v[55]),
+          "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]), "=r"(v[61]), "=r"(v[62]), "=r"(v[63])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t pack2(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// the network input of one vertex as 32 bf16 pairs (layout of encode_row in nrc.cu)
+__device__ void tc_encode(const NrcNet& net, const NrcVertex& v, bool valid, uint32_t* r32)
+{
+    if (!valid) {
+#pragma unroll
+        for (int k = 0; k < 32; ++k) r32[k] = 0u;
+        return;
+    }
+    float u[3];
+    nrc_unit_pos(net.grid, v.p, u);
+#pragma unroll 1
+    for (int l = 0; l < kNrcMaxLevels; ++l) {
+        float f0 = 0.0f, f1 = 0.0f;
+        if (l < net.grid.levels) {
+            uint32_t idx[8];
+            float w[8];
+            nrc_level_corners(net.grid, l, u[0], u[1], u[2], idx, w);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const float2 h = __half22float2(__ldg(net.table + idx[c]));
+                f0 += w[c] * h.x;
+                f1 += w[c] * h.y;
+            }
+        }
+        r32[l] = pack2(f0, f1);
+    }
+    float sh[16];
+    nrc_sh16(v.d.x, v.d.y, v.d.z, sh);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r32[16 + k] = pack2(sh[2 * k], sh[2 * k + 1]);
+    r32[24] = pack2(v.d.w, v.a.x);
+    r32[25] = pack2(v.a.y, v.a.z);
+    r32[26] = pack2(v.n.x * 0.5f + 0.5f, v.n.y * 0.5f + 0.5f);
+    r32[27] = pack2(v.n.z * 0.5f + 0.5f, 1.0f);
+#pragma unroll
+    for (int k = 28; k < 32; ++k) r32[k] = 0u;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_nrc_infer_tc(NrcNet net, const NrcQuery* __restrict__ q,
+                                                               const int32_t* count, int cap, double* accum,
+                                                               float* out_rgb, int* err)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char* sW = smem;                                  // 6 weight operands, canonical layout
+    unsigned char* sA = smem + kTcWBytes;                      // 128 x 64 activation operand
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kTcWBytes + kTcABytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcWBytes + kTcABytes + 16);
+    const int t = threadIdx.x, warp = t >> 5;
+
+    // weights [out][in] -> canonical K-major chunks
+    for (int e = t; e < kTcWBytes / 16; e += kTcThreads) {
+        const int l = min(e / (kNrcHid * 8), kNrcLayers - 1);
+        const int local = e - l * (kNrcHid * 8);
+        const int R = nrc_w_rows(l);
+        const int r = local / 8, kc = local % 8;
+        const uint4 v = *reinterpret_cast<const uint4*>(net.w + nrc_w_offset(l) + r * kNrcIn + kc * 8);
+        *reinterpret_cast<uint4*>(sW + l * (kNrcHid * kNrcIn * 2) + tc_chunk_offset(R, r, kc)) = v;
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(smem_addr(mbar)), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     : : "r"(smem_addr(tmem_slot)), "r"(kTcCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+    const uint32_t aBase = smem_addr(sA), wBase = smem_addr(sW), mb = smem_addr(mbar);
+    uint32_t phase = 0;
+    bool failed = false;
+
+    const int n = min(*count, cap);
+    for (int tile = blockIdx.x; tile * kTcRows < n && !failed; tile += gridDim.x) {
+        const int row = tile * kTcRows + t;
+        const bool valid = row < n;
+        NrcQuery qq;
+        if (valid) qq = q[row];
+        {
+            uint32_t r32[32];
+            tc_encode(net, qq.v, valid, r32);
+#pragma unroll
+            for (int kc = 0; kc < 8; ++kc)
+                *reinterpret_cast<uint4*>(sA + tc_chunk_offset(kTcRows, t, kc)) =
+                    make_uint4(r32[4 * kc], r32[4 * kc + 1], r32[4 * kc + 2], r32[4 * kc + 3]);
+        }
+        float out[3] = {0.0f, 0.0f, 0.0f};
+        for (int l = 0; l < kNrcLayers && !failed; ++l) {
+            const int N = nrc_w_rows(l);
+            // generic-proxy writes of the A operand -> visible to the tensor core
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (t == 0) {
+                const uint32_t wl = wBase + static_cast<uint32_t>(l * (kNrcHid * kNrcIn * 2));
+                const uint32_t idesc = tc_idesc(kTcRows, N);
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    const uint64_t da = tc_desc(aBase + static_cast<uint32_t>(2 * s * kTcRows * 16), kTcRows * 16, 128);
+                    const uint64_t db = tc_desc(wl + static_cast<uint32_t>(2 * s * N * 16), static_cast<uint32_t>(N * 16), 128);
+                    tc_mma(tmem, da, db, idesc, s > 0 ? 1u : 0u);
+                }
+                tc_commit(mb);
+            }
+            uint32_t spins = 0;
+            bool late = false;
+            while (!mbar_try_wait(mb, phase)) {
+                if (++spins >= kTcSpinLimit) { late = true; break; }
+            }
+            phase ^= 1u;
+            failed = __syncthreads_or(late ? 1 : 0) != 0;   // the same decision in every thread
+            if (failed) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint32_t v[64];
+            tc_ld64(taddr, v);
+            if (l < kNrcLayers - 1) {
+#pragma unroll
+                for (int kc = 0; kc < 8; ++kc) {
+                    uint32_t p[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        p[j] = pack2(fmaxf(__uint_as_float(v[8 * kc + 2 * j]), 0.0f), fmaxf(__uint_as_float(v[8 * kc + 2 * j + 1]), 0.0f));
+                    *reinterpret_cast<uint4*>(sA + tc_chunk_offset(kTcRows, t, kc)) = make_uint4(p[0], p[1], p[2], p[3]);
+                }
+            } else {
+                out[0] = expf(fminf(__uint_as_float(v[0]), 15.0f));
+                out[1] = expf(fminf(__uint_as_float(v[1]), 15.0f));
+                out[2] = expf(fminf(__uint_as_float(v[2]), 15.0f));
+            }
+        }
+        if (failed) break;
+        if (valid) {
+            if (accum) {
+                const int64_t pix = __float_as_int(qq.v.p.w);
+                atomicAdd(&accum[3 * pix + 0], static_cast<double>(qq.t.x * out[0]));
+                atomicAdd(&accum[3 * pix + 1], static_cast<double>(qq.t.y * out[1]));
+                atomicAdd(&accum[3 * pix + 2], static_cast<double>(qq.t.z * out[2]));
+            }
+            if (out_rgb) {
+                out_rgb[3 * static_cast<int64_t>(row) + 0] = out[0];
+                out_rgb[3 * static_cast<int64_t>(row) + 1] = out[1];
+                out_rgb[3 * static_cast<int64_t>(row) + 2] = out[2];
+            }
+        }
+    }
+    if (failed) atomicOr(err, 2);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(tmem), "r"(kTcCols) : "memory");
+}
+
+}  // namespace
+
+cudaError_t nrc_infer_tc(const NrcNet& net, const NrcQuery* q, const int32_t* count, int cap, double* accum,
+                         float* out_rgb, int* err, int sm_count, cudaStream_t st)
+{
+    cudaError_t e = cudaFuncSetAttribute(k_nrc_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    if (e != cudaSuccess) return e;
+    const int tiles = (cap + kTcRows - 1) / kTcRows;
+    const int grid = std::max(1, std::min(tiles, sm_count * 2));
+    k_nrc_infer_tc<<<grid, kTcThreads, kTcSmem, st>>>(net, q, count, cap, accum, out_rgb, err);
+    return cudaGetLastError();
+}
+
+}  // namespace ar

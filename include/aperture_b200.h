@@ -355,6 +355,11 @@ ar_status ar_nrc_destroy(ar_nrc* nrc);
 ar_status ar_nrc_render_frame(ar_nrc* nrc, const ar_camera* camera, const ar_render_params* params,
                               float* out_rgb, double* accum, int32_t train, ar_nrc_frame_stats* stats,
                               void* stream);
+/* Options: AR_NRC_OPT_TENSOR_PATH selects the inference kernel, 1 (default)
+ * tcgen05.mma with tensor-memory accumulators (128 rows per CTA), 0 the
+ * warp-level mma.sync kernel (32 rows per warp). */
+enum { AR_NRC_OPT_TENSOR_PATH = 1 };
+ar_status ar_nrc_set_option(ar_nrc* nrc, int32_t option, int32_t value);
 /* Parameters as fp32: tables (levels x 2^log2_entries x 2) and MLP weights
  * (21504: layers 0-4 [64][64], layer 5 [16][64], [out][in]); NULL skips. */
 ar_status ar_nrc_get_params(const ar_nrc* nrc, float* table, float* weights);

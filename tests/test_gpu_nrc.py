@@ -119,3 +119,21 @@ def test_nrc_frames_converge_to_plain_image():
     plain, _ = sc.render(cam, make_params(spp=frames, max_depth=8, frame_offset=100000))
     rel_plain = ((plain - ref) ** 2 / (ref ** 2 + 1e-2)).mean()
     print("relMSE cache", rel, "plain", rel_plain)
+
+
+@pytest.mark.gpu
+def test_nrc_tcgen05_inference_equals_mma_sync():
+    """The tcgen05 inference kernel (128-row tiles, tensor-memory accumulators)
+    and the mma.sync kernel compute the same bf16 network with fp32 sums in
+    the same order per output: identical predictions."""
+    _, c, cfg = _cache(log2_entries=15)
+    table, w = _random_params(c, 11)
+    v = _vertices(70_000, 12)      # several tiles per CTA, a ragged last tile
+    c.set_tensor_path(False)
+    a = c.infer(v)
+    c.set_tensor_path(True)
+    b = c.infer(v)
+    assert np.array_equal(a, b)
+    o = N.predict(_geo(cfg), v, table, w)
+    rel = np.abs(b - o) / np.maximum(np.abs(o), 1e-6)
+    assert np.median(rel) < 1e-3 and np.mean(rel) < 5e-3
