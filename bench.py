@@ -541,14 +541,14 @@ def profile_queues() -> None:
                       "shadow_per_launch": st.shadow_rays / max(st.shadow_launches, 1)}), flush=True)
 
 
-def profile_nrc() -> None:
-    """Six radiance-cache frames (480x270, config-2 scene, training on) for ncu
+def profile_nrc(width: int = 480, height: int = 270) -> None:
+    """Six radiance-cache frames (config-2 scene, training on) for ncu
     captures of the cache kernels; prints the frame statistics."""
     objs = scenes.spheres_scene()
     scene = Scene(objs)
-    cam = scenes.spheres_camera(480, 270)
+    cam = scenes.spheres_camera(width, height)
     import torch
-    acc = torch.zeros(480 * 270 * 3, dtype=torch.float64, device="cuda")
+    acc = torch.zeros(width * height * 3, dtype=torch.float64, device="cuda")
     cache = RadianceCache(scene, nrc_config())
     for f in range(6):
         st = cache.render_frame(cam, make_params(spp=1, max_depth=DEPTH, frame_offset=f), None, acc.data_ptr(),
@@ -571,7 +571,8 @@ def main():
     ap.add_argument("--nrc", choices=("off", "small", "full"), default="small",
                     help="radiance-cache time-to-relMSE measurement (small: 480x270, full: 1920x1080)")
     ap.add_argument("--profile-nrc", action="store_true",
-                    help="six radiance-cache frames at 480x270 (for ncu captures of the cache kernels)")
+                    help="six radiance-cache frames (for ncu captures of the cache kernels)")
+    ap.add_argument("--profile-size", default="480x270", help="frame size of --profile-nrc")
     ap.add_argument("--profile-queues", action="store_true",
                     help="render the workload once at 1 spp (for ncu captures) and print the per-depth queue sizes")
     args = ap.parse_args()
@@ -579,7 +580,8 @@ def main():
         profile_queues()
         return
     if args.profile_nrc:
-        profile_nrc()
+        w, h = (int(x) for x in args.profile_size.split("x"))
+        profile_nrc(w, h)
         return
     args.warmup = max(3, args.warmup)  # at least 3 untimed warm-up steps
     if args.impl == "reference":
