@@ -1678,6 +1678,8 @@ ar_status ar_guide_render_frame(ar_guide* g, const ar_camera* cam, const ar_rend
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int64_t npix = static_cast<int64_t>(cam->width) * cam->height;
     guide_ensure_frame(g, npix);
+    // events of a frame that did not complete must not leak into this one
+    ck(cudaMemsetAsync(g->view.event_count, 0, static_cast<size_t>(npix) * sizeof(int32_t), st), "memset");
     g->view.alpha = ar::pg_alpha(g->frames);
     if (ar_status e = run_render(s, cam, p, nullptr, st, nullptr, nullptr, &g->view)) return e;
     ck(ar::pg_update(g->view, s->sm_count, st), "guiding update");
