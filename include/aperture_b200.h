@@ -124,7 +124,8 @@ typedef struct ar_render_params {
     int32_t sky;           /* 1 = SkyLighting, 0 = DISABLE_SKYLIGHT                  */
     int32_t frame_offset;  /* TOTAL_FRAME_INDEX of the first sample                  */
     uint64_t seed;         /* GLOBAL_SEED (reference: 0x9e3779b97f4a7c15)            */
-    int32_t sort_rays;     /* 1 = sort extension rays by material/direction octant  */
+    int32_t sort_rays;     /* reserved (accepted, no effect): shading is always ordered
+                              by material bucket; see the design notes on ray sorting */
     int32_t wave_paths;    /* paths in flight per wave; 0 = automatic                */
     int32_t spectral;      /* 1 = USE_SPECTRUM_RENDERING: one hero wavelength per path
                               (SampleCIE1931), output linear CIE XYZ; needs
