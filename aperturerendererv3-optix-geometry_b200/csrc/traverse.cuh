@@ -265,13 +265,27 @@ __device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b)
     a = lo; b = hi;
 }
 
+// Closest-hit stack entries carry the child's entry distance with the node
+// index: (bits(tnear) & ~mask) | node, mask = all ones up to the highest bit
+// of (num_nodes | 255).  Clearing low bits of a non-negative float rounds it
+// down, so the stored distance never exceeds the true one, and a node popped
+// after a nearer hit was found is dropped without being fetched, by the same
+// test that culls children at push time.  Any-hit queries never lower their
+// limit below what their entries passed and push bare node indices.
+__device__ __forceinline__ uint32_t stack_node_mask(int num_nodes)
+{
+    return 0xFFFFFFFFu >> __clz(static_cast<uint32_t>(num_nodes) | 255u);
+}
+
 // Visit node r.node: test its 8 child boxes, intersect the primitives of hit
 // leaf children nearest first, push hit internal children far to near, pop the
-// next node.  Returns true when the ray is finished (stack empty, any-hit
-// found, or stack overflow reported through *err).
+// next node that can still hold a nearer hit.  Returns true when the ray is
+// finished (stack empty, any-hit found, or stack overflow reported through
+// *err).
 template <bool kAny, bool kCount>
 __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32_t* stack, uint32_t* ovf, int* err)
 {
+    const uint32_t nmask = kAny ? 0u : stack_node_mask(s.num_nodes);
     const WideNode* np = s.nodes + r.node;
     if (kCount) ++r.visits;
     const float4 w0 = ldg4(reinterpret_cast<const char*>(np));
@@ -306,8 +320,9 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
         const float tfar = min3f(tfx, tfy, fminf(tfz, limit)) * kSlabWiden;
         const uint32_t meta = byte_of(k < 4 ? meta0 : meta1, b);
         const bool hit = (tnear <= tfar) && (meta != kMetaEmpty);
-        // tnear >= tmin >= 0, so its bit pattern orders like the value
-        key[k] = hit ? ((__float_as_uint(fmaxf(tnear, 0.0f)) & ~7u) | static_cast<uint32_t>(k)) : 0xFFFFFFFFu;
+        // tnear >= tmin >= 0, so its bit pattern orders like the value; the
+        // low byte carries the child's meta byte (rounding tnear down)
+        key[k] = hit ? ((__float_as_uint(fmaxf(tnear, 0.0f)) & ~0xFFu) | meta) : 0xFFFFFFFFu;
     }
     // visit children nearest first -- sort the 8 keys (Batcher odd-even merge
     // network, 19 comparators).  Any-hit queries profit too: the occluder of a
@@ -324,10 +339,9 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
     for (int k = 0; k < 8; ++k) {
         const uint32_t kk = key[k];
         if (kk == 0xFFFFFFFFu) break;
-        const int slot = static_cast<int>(kk & 7u);
-        const uint32_t meta = byte_of(slot < 4 ? meta0 : meta1, slot & 3);
+        const uint32_t meta = kk & 0xFFu;
         if (meta & kMetaInternal) continue;
-        const float tn = __uint_as_float(kk & ~7u);
+        const float tn = __uint_as_float(kk & ~0xFFu);
         if (!(tn <= fminf(r.best.t, FLT_MAX) * kSlabWiden)) continue;
         const int count = static_cast<int>(meta >> 5) + 1;
         const uint32_t first = prim_base + (meta & 31u);
@@ -359,21 +373,33 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
     for (int k = 7; k >= 0; --k) {
         const uint32_t kk = key[k];
         if (kk == 0xFFFFFFFFu) continue;
-        const int slot = static_cast<int>(kk & 7u);
-        const uint32_t meta = byte_of(slot < 4 ? meta0 : meta1, slot & 3);
+        const uint32_t meta = kk & 0xFFu;
         if (!(meta & kMetaInternal)) continue;
-        const float tn = __uint_as_float(kk & ~7u);
+        const float tn = __uint_as_float(kk & ~0xFFu);
         if (!(tn <= fminf(r.best.t, FLT_MAX) * kSlabWiden)) continue;
         const uint32_t child = child_base + (meta & 7u);
-        if (r.sp < kStackShared) stack[r.sp * 32] = child;
-        else if (r.sp < kStackMax) ovf[r.sp - kStackShared] = child;
+        const uint32_t entry = kAny ? child : ((kk & ~nmask) | child);
+        if (r.sp < kStackShared) stack[r.sp * 32] = entry;
+        else if (r.sp < kStackMax) ovf[r.sp - kStackShared] = entry;
         else { atomicOr(err, 1); return true; }
         ++r.sp;
     }
-    if (r.sp == 0) return true;
-    --r.sp;
-    r.node = (r.sp < kStackShared) ? stack[r.sp * 32] : ovf[r.sp - kStackShared];
-    return false;
+    if (kAny) {
+        if (r.sp == 0) return true;
+        --r.sp;
+        r.node = (r.sp < kStackShared) ? stack[r.sp * 32] : ovf[r.sp - kStackShared];
+        return false;
+    }
+    const float lim = fminf(r.best.t, FLT_MAX) * kSlabWiden;
+    for (;;) {
+        if (r.sp == 0) return true;
+        --r.sp;
+        const uint32_t e = (r.sp < kStackShared) ? stack[r.sp * 32] : ovf[r.sp - kStackShared];
+        if (__uint_as_float(e & ~nmask) <= lim) {
+            r.node = e & nmask;
+            return false;
+        }
+    }
 }
 
 // Persistent traversal loop shared by every ray-query kernel.  Each warp keeps
@@ -389,7 +415,7 @@ __device__ __forceinline__ void traverse_queue(const SceneView& s, IO& io, int n
     RayState r;
     int item = -1;
     unsigned long long visits = 0, tests = 0;
-    bool exhausted = (s.num_nodes == 0 && false);
+    bool exhausted = false;
     for (;;) {
         if (!exhausted) {
             const unsigned idle = __ballot_sync(0xFFFFFFFFu, item < 0);
