@@ -10,8 +10,10 @@
 // mesh are all the mesh position -- scene_helper.h:488-545 -- and degenerate into
 // one leaf per mesh), max 4 primitives per leaf, collapsed greedily (largest
 // surface area first) into 8-wide nodes whose child boxes are quantised to 8
-// bits per plane relative to a power-of-two grid, rounded outwards and padded by
-// one grid step so the decoded box always contains the exact one.
+// bits per plane relative to a power-of-two grid that starts one step below
+// the children's union, rounded outwards and padded by one grid step on both
+// sides, so the decoded box contains the exact one with a margin of a grid
+// step that absorbs the rounding of the kernel's plane decode.
 #include "scene_build.h"
 
 #include <cuda_fp16.h>
@@ -473,9 +475,11 @@ HostScene build_scene(const ar_object_desc* objs, size_t n, const ar_sdf_volume*
         const int ex = grid_exponent(u.lo.x, u.hi.x);
         const int ey = grid_exponent(u.lo.y, u.hi.y);
         const int ez = grid_exponent(u.lo.z, u.hi.z);
-        w.ox = u.lo.x; w.oy = u.lo.y; w.oz = u.lo.z;
-        w.exps = static_cast<uint32_t>(ex + 127) | (static_cast<uint32_t>(ey + 127) << 8) | (static_cast<uint32_t>(ez + 127) << 16);
         const float sx = pow2f(ex), sy = pow2f(ey), sz = pow2f(ez);
+        // the grid starts one step below the union, so that the lowest child
+        // planes get the same one-step padding as every other plane
+        w.ox = u.lo.x - sx; w.oy = u.lo.y - sy; w.oz = u.lo.z - sz;
+        w.exps = static_cast<uint32_t>(ex + 127) | (static_cast<uint32_t>(ey + 127) << 8) | (static_cast<uint32_t>(ez + 127) << 16);
         w.child_base = static_cast<uint32_t>(hs.nodes.size());
         w.prim_base = static_cast<uint32_t>(hs.prims.size());
         uint8_t meta[8];

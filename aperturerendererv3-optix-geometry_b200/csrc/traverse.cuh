@@ -5,11 +5,14 @@
 // of each warp lives in shared memory, interleaved by lane (entry k of lane l at
 // [k * 32 + l]) so pushes and pops are bank-conflict free.  Nodes are 80-byte
 // 8-wide records read with five 128-bit read-only loads; the child boxes are
-// decoded from 8-bit grid coordinates with one FMA per plane:
-//     t(q) = fma(q, scale * inv_dir, (origin - ray_origin) * inv_dir).
-// The box test is conservative (far distance widened by 2^-20 relative), so the
-// set of primitives tested is a superset of the exact one and the closest hit
-// equals a brute-force search.  Ties in t go to the lowest object index; the
+// decoded from 8-bit grid coordinates with one byte permute and one FMA per
+// plane:
+//     t(q) = fma(2^15 + q, a, b),  a = scale * inv_dir,
+//     b = (origin - ray_origin) * inv_dir - 2^15 * a   (once per node).
+// The box test is conservative (every child box is padded by a grid step on
+// all sides, far distance widened by 2^-20 relative), so the set of primitives
+// tested is a superset of the exact one and the closest hit equals a
+// brute-force search.  Ties in t go to the lowest object index; the
 // reference keeps the first primitive its traversal happens to find.
 #pragma once
 
@@ -240,11 +243,13 @@ __device__ __forceinline__ void ray_begin(RayState& r, f3 o, f3 d, float tmin, f
 
 __device__ __forceinline__ uint32_t byte_of(uint32_t w, int k) { return (w >> (8 * k)) & 0xFFu; }
 
-// byte k of w as a float without a conversion instruction: 0x4B0000qq is 2^23 + qq
-__device__ __forceinline__ float byte_float(uint32_t w, int k)
+// byte q = byte k of w placed in bits 8-15 of the float 2^15: the value
+// 2^15 + q, exact, with one byte permute and no conversion instruction.
+__device__ __forceinline__ float byte_biased(uint32_t w, int k)
 {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u + static_cast<uint32_t>(k))) - 8388608.0f;
+    return __uint_as_float(__byte_perm(w, 0x47000000u, 0x7404u + (static_cast<uint32_t>(k) << 4)));
 }
+constexpr float kByteBias = 32768.0f;  // 2^15, the offset byte_biased adds
 
 __device__ __forceinline__ float max3f(float a, float b, float c)
 {
@@ -298,7 +303,12 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
     const float sy = __uint_as_float(((exps >> 8) & 0xFFu) << 23);
     const float sz = __uint_as_float(((exps >> 16) & 0xFFu) << 23);
     const float ax = sx * r.ix, ay = sy * r.iy, az = sz * r.iz;
-    const float bx = (w0.x - r.o.x) * r.ix, by = (w0.y - r.o.y) * r.iy, bz = (w0.z - r.o.z) * r.iz;
+    // plane q at t = q * a + (origin - o) * inv_dir = fma(2^15 + q, a, b) with
+    // b = (origin - o) * inv_dir - 2^15 * a; the extra rounding of b is at most
+    // 2^-24 (|b| + 2^15 |a|), far below the one-grid-step padding of the boxes
+    const float bx = fmaf(-kByteBias, ax, (w0.x - r.o.x) * r.ix);
+    const float by = fmaf(-kByteBias, ay, (w0.y - r.o.y) * r.iy);
+    const float bz = fmaf(-kByteBias, az, (w0.z - r.o.z) * r.iz);
     // w2 = qlo_x | qlo_y, w3 = qlo_z | qhi_x, w4 = qhi_y | qhi_z (8 bytes each)
     const bool nx = r.ix < 0.0f, ny = r.iy < 0.0f, nz = r.iz < 0.0f;
     const uint32_t nx0 = nx ? w3.z : w2.x, nx1 = nx ? w3.w : w2.y, fx0 = nx ? w2.x : w3.z, fx1 = nx ? w2.y : w3.w;
@@ -306,23 +316,25 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
     const uint32_t nz0 = nz ? w4.z : w3.x, nz1 = nz ? w4.w : w3.y, fz0 = nz ? w3.x : w4.z, fz1 = nz ? w3.y : w4.w;
     const uint32_t meta0 = w1.z, meta1 = w1.w;
     const float limit = fminf(r.best.t, FLT_MAX);
+    // every accepted hit has t > 0, so the box test may start at max(tmin, 0),
+    // which also makes every tnear non-negative (its bits order like its value)
+    const float tlow = fmaxf(r.tmin, 0.0f);
     uint32_t key[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int b = k & 3;
-        const float tnx = fmaf(byte_float(k < 4 ? nx0 : nx1, b), ax, bx);
-        const float tfx = fmaf(byte_float(k < 4 ? fx0 : fx1, b), ax, bx);
-        const float tny = fmaf(byte_float(k < 4 ? ny0 : ny1, b), ay, by);
-        const float tfy = fmaf(byte_float(k < 4 ? fy0 : fy1, b), ay, by);
-        const float tnz = fmaf(byte_float(k < 4 ? nz0 : nz1, b), az, bz);
-        const float tfz = fmaf(byte_float(k < 4 ? fz0 : fz1, b), az, bz);
-        const float tnear = max3f(tnx, tny, fmaxf(tnz, r.tmin));
+        const float tnx = fmaf(byte_biased(k < 4 ? nx0 : nx1, b), ax, bx);
+        const float tfx = fmaf(byte_biased(k < 4 ? fx0 : fx1, b), ax, bx);
+        const float tny = fmaf(byte_biased(k < 4 ? ny0 : ny1, b), ay, by);
+        const float tfy = fmaf(byte_biased(k < 4 ? fy0 : fy1, b), ay, by);
+        const float tnz = fmaf(byte_biased(k < 4 ? nz0 : nz1, b), az, bz);
+        const float tfz = fmaf(byte_biased(k < 4 ? fz0 : fz1, b), az, bz);
+        const float tnear = max3f(tnx, tny, fmaxf(tnz, tlow));
         const float tfar = min3f(tfx, tfy, fminf(tfz, limit)) * kSlabWiden;
         const uint32_t meta = byte_of(k < 4 ? meta0 : meta1, b);
         const bool hit = (tnear <= tfar) && (meta != kMetaEmpty);
-        // tnear >= tmin >= 0, so its bit pattern orders like the value; the
-        // low byte carries the child's meta byte (rounding tnear down)
-        key[k] = hit ? ((__float_as_uint(fmaxf(tnear, 0.0f)) & ~0xFFu) | meta) : 0xFFFFFFFFu;
+        // the low byte carries the child's meta byte (rounding tnear down)
+        key[k] = hit ? ((__float_as_uint(tnear) & ~0xFFu) | meta) : 0xFFFFFFFFu;
     }
     // visit children nearest first -- sort the 8 keys (Batcher odd-even merge
     // network, 19 comparators).  Any-hit queries profit too: the occluder of a
