@@ -241,8 +241,6 @@ __device__ __forceinline__ void ray_begin(RayState& r, f3 o, f3 d, float tmin, f
     r.tests = 0;
 }
 
-__device__ __forceinline__ uint32_t byte_of(uint32_t w, int k) { return (w >> (8 * k)) & 0xFFu; }
-
 // byte q = byte k of w placed in bits 8-15 of the float 2^15: the value
 // 2^15 + q, exact, with one byte permute and no conversion instruction.
 __device__ __forceinline__ float byte_biased(uint32_t w, int k)
@@ -331,10 +329,12 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
         const float tfz = fmaf(byte_biased(k < 4 ? fz0 : fz1, b), az, bz);
         const float tnear = max3f(tnx, tny, fmaxf(tnz, tlow));
         const float tfar = min3f(tfx, tfy, fminf(tfz, limit)) * kSlabWiden;
-        const uint32_t meta = byte_of(k < 4 ? meta0 : meta1, b);
-        const bool hit = (tnear <= tfar) && (meta != kMetaEmpty);
-        // the low byte carries the child's meta byte (rounding tnear down)
-        key[k] = hit ? ((__float_as_uint(tnear) & ~0xFFu) | meta) : 0xFFFFFFFFu;
+        // the low byte carries the child's meta byte (rounding tnear down).
+        // Empty slots have inverted boxes (lo 255, hi 0) and fail this test
+        // unless the ray starts some 2^28 grid steps away; their meta byte
+        // kMetaEmpty keeps them out of both loops below either way.
+        key[k] = (tnear <= tfar) ? __byte_perm(__float_as_uint(tnear), k < 4 ? meta0 : meta1, 0x3214u + b)
+                                 : 0xFFFFFFFFu;
     }
     // visit children nearest first -- sort the 8 keys (Batcher odd-even merge
     // network, 19 comparators).  Any-hit queries profit too: the occluder of a
@@ -386,7 +386,7 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
         const uint32_t kk = key[k];
         if (kk == 0xFFFFFFFFu) continue;
         const uint32_t meta = kk & 0xFFu;
-        if (!(meta & kMetaInternal)) continue;
+        if (!(meta & kMetaInternal) || meta == kMetaEmpty) continue;
         const float tn = __uint_as_float(kk & ~0xFFu);
         if (!(tn <= fminf(r.best.t, FLT_MAX) * kSlabWiden)) continue;
         const uint32_t child = child_base + (meta & 7u);
