@@ -150,6 +150,20 @@ __device__ __forceinline__ float isect_analytic_t(const SceneView& s, int obj, f
     return -1.0f;
 }
 
+// The same test out of line, for the traversal loop: analytic primitives are
+// rare leaf entries, and one copy of their code keeps the unrolled leaf loop
+// small.
+static __device__ __noinline__ float isect_analytic_leaf(const ObjInfo* objects, const Analytic* analytic, int obj,
+                                                         f3 ro, f3 rd)
+{
+    const ObjInfo oi = objects[obj];
+    const Analytic& an = analytic[oi.aux];
+    f3 p, n;
+    if (oi.type == 0) return isect_cube<false>(an, ro, rd, &p, &n);
+    if (oi.type == 1) return isect_sphere<false>(an, ro, rd, &p, &n);
+    return -1.0f;
+}
+
 // INTERSECT_EPS(0) = 1e-3 * exp(0) (config.cuh:3): the tolerance of standalone ray queries.
 constexpr float kEpsDepth0 = 1.0e-3f;
 
@@ -262,6 +276,15 @@ __device__ __forceinline__ float min3f(float a, float b, float c)
     return r;
 }
 
+// a[k] for a run-time k without indexing the register array
+__device__ __forceinline__ uint32_t pick8(const uint32_t (&a)[8], int k)
+{
+    const bool k1 = k & 1, k2 = k & 2, k4 = k & 4;
+    const uint32_t b0 = k1 ? a[1] : a[0], b1 = k1 ? a[3] : a[2], b2 = k1 ? a[5] : a[4], b3 = k1 ? a[7] : a[6];
+    const uint32_t c0 = k2 ? b1 : b0, c1 = k2 ? b3 : b2;
+    return k4 ? c1 : c0;
+}
+
 __device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b)
 {
     const uint32_t lo = min(a, b), hi = max(a, b);
@@ -345,18 +368,24 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
     cswap(key[0], key[4]); cswap(key[1], key[5]); cswap(key[2], key[6]); cswap(key[3], key[7]);
     cswap(key[2], key[4]); cswap(key[3], key[5]);
     cswap(key[1], key[2]); cswap(key[3], key[4]); cswap(key[5], key[6]);
-    // leaves, nearest first
-    const uint32_t prim_base = w1.y;
+    // leaves, nearest first, in one rolled loop (a single copy of the
+    // primitive tests): bit k of `leaves` marks a hit leaf at sorted position
+    // k (misses and empty slots carry the internal bit in their low byte)
+    uint32_t leaves = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const uint32_t kk = key[k];
-        if (kk == 0xFFFFFFFFu) break;
+    for (int k = 0; k < 8; ++k) leaves |= ((~key[k] >> 7) & 1u) << k;
+    const uint32_t prim_base = w1.y;
+#pragma unroll 1
+    while (leaves) {
+        const int k = __ffs(leaves) - 1;
+        leaves &= leaves - 1u;
+        const uint32_t kk = pick8(key, k);
         const uint32_t meta = kk & 0xFFu;
-        if (meta & kMetaInternal) continue;
         const float tn = __uint_as_float(kk & ~0xFFu);
-        if (!(tn <= fminf(r.best.t, FLT_MAX) * kSlabWiden)) continue;
+        if (!(tn <= fminf(r.best.t, FLT_MAX) * kSlabWiden)) break;  // later leaves are farther
         const int count = static_cast<int>(meta >> 5) + 1;
         const uint32_t first = prim_base + (meta & 31u);
+#pragma unroll 1
         for (int p = 0; p < count; ++p) {
             const PrimRec* pr = s.prims + first + p;
             if (kCount) ++r.tests;
@@ -368,7 +397,7 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
                 const float4 e2 = ldg4(&pr->e2[0]);
                 t = mt_triangle(r.o, r.d, mk(a.x, a.y, a.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z));
             } else {
-                t = isect_analytic_t(s, obj, r.o, r.d);
+                t = isect_analytic_leaf(s.objects, s.analytic, obj, r.o, r.d);
             }
             if (t < 0.0f || t < r.tmin) continue;
             if (t < r.best.t || (r.best.obj >= 0 && t == r.best.t && obj < r.best.obj)) {
