@@ -397,7 +397,7 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
                 const float4 e2 = ldg4(&pr->e2[0]);
                 t = mt_triangle(r.o, r.d, mk(a.x, a.y, a.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z));
             } else {
-                t = isect_analytic_leaf(s.objects, s.analytic, obj, r.o, r.d);
+                t = isect_analytic_t(s, obj, r.o, r.d);
             }
             if (t < 0.0f || t < r.tmin) continue;
             if (t < r.best.t || (r.best.obj >= 0 && t == r.best.t && obj < r.best.obj)) {
@@ -408,17 +408,23 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
             }
         }
     }
-    // internal children, pushed far to near
-    const uint32_t child_base = w1.x;
+    // internal children, pushed far to near, in one rolled loop over a mask
+    // (misses and empty slots have the low byte kMetaEmpty)
+    uint32_t inner = 0;
 #pragma unroll
-    for (int k = 7; k >= 0; --k) {
-        const uint32_t kk = key[k];
-        if (kk == 0xFFFFFFFFu) continue;
-        const uint32_t meta = kk & 0xFFu;
-        if (!(meta & kMetaInternal) || meta == kMetaEmpty) continue;
-        const float tn = __uint_as_float(kk & ~0xFFu);
-        if (!(tn <= fminf(r.best.t, FLT_MAX) * kSlabWiden)) continue;
-        const uint32_t child = child_base + (meta & 7u);
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t m = key[k] & 0xFFu;
+        inner |= static_cast<uint32_t>(m >= kMetaInternal && m != kMetaEmpty) << k;
+    }
+    const uint32_t child_base = w1.x;
+    const float lim_push = fminf(r.best.t, FLT_MAX) * kSlabWiden;
+#pragma unroll 1
+    while (inner) {
+        const int k = 31 - __clz(inner);
+        inner &= ~(1u << k);
+        const uint32_t kk = pick8(key, k);
+        if (!(__uint_as_float(kk & ~0xFFu) <= lim_push)) continue;
+        const uint32_t child = child_base + (kk & 7u);
         const uint32_t entry = kAny ? child : ((kk & ~nmask) | child);
         if (r.sp < kStackShared) stack[r.sp * 32] = entry;
         else if (r.sp < kStackMax) ovf[r.sp - kStackShared] = entry;
