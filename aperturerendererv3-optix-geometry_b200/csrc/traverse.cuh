@@ -389,12 +389,13 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
         for (int p = 0; p < count; ++p) {
             const PrimRec* pr = s.prims + first + p;
             if (kCount) ++r.tests;
+            // all three words at once: one memory round trip per primitive
             const float4 a = ldg4(&pr->v0[0]);
             const float4 e1 = ldg4(&pr->e1[0]);
+            const float4 e2 = ldg4(&pr->e2[0]);
             const int obj = __float_as_int(a.w);
             float t;
             if (__float_as_int(e1.w) == kPrimTriangle) {
-                const float4 e2 = ldg4(&pr->e2[0]);
                 t = mt_triangle(r.o, r.d, mk(a.x, a.y, a.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z));
             } else {
                 t = isect_analytic_t(s, obj, r.o, r.d);
@@ -450,32 +451,44 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
 }
 
 // Persistent traversal loop shared by every ray-query kernel.  Each warp keeps
-// 32 rays in flight; a lane whose ray finishes takes the next queue entry right
-// away (one atomic per warp per refill), so lanes do not idle until the
-// slowest ray of the warp is done.  IO supplies count(), load() -> item id or
-// -1 when the entry finished without traversal, and store().
+// 32 rays in flight.  Lanes whose rays finish are refilled in batches of at
+// least kRefillMin (or when the whole warp is idle): the refill stores their
+// results and loads new queue entries (one atomic per warp per refill), so the
+// lane-divergent store/load code runs once for several lanes instead of once
+// per finishing lane, while no lane idles for long.  IO supplies load() -> item
+// id or -1 when the entry finished without traversal, and store().
+constexpr int kRefillMin = 8;
+
 template <bool kAny, class IO, bool kCount = false>
 __device__ __forceinline__ void traverse_queue(const SceneView& s, IO& io, int n, int* fetch, uint32_t* stack,
                                                uint32_t* ovf, int* err, unsigned long long* work)
 {
     const unsigned lane = threadIdx.x & 31u;
     RayState r;
-    int item = -1;
+    int item = -1;   // ray in flight
+    int pend = -1;   // finished ray whose result waits in r for the next refill
     unsigned long long visits = 0, tests = 0;
     bool exhausted = false;
     for (;;) {
-        if (!exhausted) {
-            const unsigned idle = __ballot_sync(0xFFFFFFFFu, item < 0);
-            if (idle) {
-                const int leader = __ffs(idle) - 1;
-                int base = 0;
-                if (static_cast<int>(lane) == leader) base = atomicAdd(fetch, __popc(idle));
-                base = __shfl_sync(0xFFFFFFFFu, base, leader);
-                if (base + __popc(idle) >= n) exhausted = true;
-                if (item < 0) {
-                    const int k = base + __popc(idle & ((1u << lane) - 1u));
-                    if (k < n) item = io.load(s, k, r);
-                }
+        const unsigned idle = __ballot_sync(0xFFFFFFFFu, item < 0);
+        const bool refill = !exhausted && idle != 0u && (__popc(idle) >= kRefillMin || idle == 0xFFFFFFFFu);
+        if ((refill || exhausted) && pend >= 0) {
+            io.store(s, pend, r);
+            if (kCount) {
+                visits += r.visits;
+                tests += r.tests;
+            }
+            pend = -1;
+        }
+        if (refill) {
+            const int leader = __ffs(idle) - 1;
+            int base = 0;
+            if (static_cast<int>(lane) == leader) base = atomicAdd(fetch, __popc(idle));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (base + __popc(idle) >= n) exhausted = true;
+            if (item < 0) {
+                const int k = base + __popc(idle & ((1u << lane) - 1u));
+                if (k < n) item = io.load(s, k, r);
             }
         }
         const unsigned busy = __ballot_sync(0xFFFFFFFFu, item >= 0);
@@ -486,11 +499,7 @@ __device__ __forceinline__ void traverse_queue(const SceneView& s, IO& io, int n
         if (item >= 0) {
             const bool done = (s.num_nodes == 0) || ray_step<kAny, kCount>(s, r, stack, ovf, err);
             if (done) {
-                io.store(s, item, r);
-                if (kCount) {
-                    visits += r.visits;
-                    tests += r.tests;
-                }
+                pend = item;
                 item = -1;
             }
         }
