@@ -147,7 +147,7 @@ def cpu_sample(objs, cam: Camera, params: RenderParams, target_s: float, threads
 
 
 # ----------------------------------------------------------------------------- ours
-NRC_SIZES = {"small": (480, 270, 16384, 4096), "full": (1920, 1080, 16384, 4096)}
+NRC_SIZES = {"small": (480, 270, 16384, 4096), "full": (1920, 1080, 16384, 4096), "box": (480, 270, 16384, 4096)}
 
 
 def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
@@ -156,10 +156,20 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
     training), both against an FP64 oracle image of `ref` spp (plain tracer,
     per-pixel FP64 sums on the GPU); then the 300-frame seeded spline camera
     path at 1920x1080 (frames/s, per-stage times).  Device time (CUDA events
-    on the launching stream) excludes the relMSE evaluations."""
+    on the launching stream) excludes the relMSE evaluations.  mode "box": the
+    same time-to-relMSE measurement on the config-3 scene (box, SDF tori, fBm
+    medium, depth 16) in RGB -- the cache is RGB-only -- without the spline path."""
     w, h, ref_spp, target = NRC_SIZES[mode]
     npix = w * h
-    cam = scenes.spheres_camera(w, h)
+    depth = DEPTH
+    if mode == "box":
+        objs, vols, med = scenes.medium_box_scene(precision=16, grid=256, medium_grid=128)
+        scene = Scene(objs, volumes=vols, device=dev.index)
+        scene.set_medium(**med)
+        cam = scenes.box_camera(w, h)
+        depth = 16
+    else:
+        cam = scenes.spheres_camera(w, h)
     out = torch.empty(npix * 3, dtype=torch.float32, device=dev)
 
     def plain(spp_total: int, offset: int, acc):
@@ -168,7 +178,7 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
         for k in range(0, spp_total, chunk):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            scene.render_device(cam, make_params(spp=min(chunk, spp_total - k), max_depth=DEPTH, frame_offset=offset + k),
+            scene.render_device(cam, make_params(spp=min(chunk, spp_total - k), max_depth=depth, frame_offset=offset + k),
                                 out.data_ptr(), acc.data_ptr(), stream.cuda_stream)
             e1.record(stream)
             e1.synchronize()
@@ -197,7 +207,7 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
             for _ in range(check):
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                cache.render_frame(cam, make_params(spp=1, max_depth=DEPTH, frame_offset=30_000_000 + f), None,
+                cache.render_frame(cam, make_params(spp=1, max_depth=depth, frame_offset=30_000_000 + f), None,
                                    acc_n.data_ptr(), train=True, stream=stream.cuda_stream)
                 e1.record(stream)
                 evs.append((e0, e1))
@@ -211,7 +221,9 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
                 break
             check = min(check * 2, 256)
         best = min(c[2] for c in curve)
-        res = {"workload": f"config4 static view: config-2 scene {w}x{h}, max depth {DEPTH}, 1 spp per frame, "
+        what = ("config-3 scene (box + SDF tori + fBm medium), RGB" if mode == "box"
+                else "config4 static view: config-2 scene")
+        res = {"workload": f"{what} {w}x{h}, max depth {depth}, 1 spp per frame, "
                            f"cache trained online (65536 training paths, 4 steps of 16384 per frame)",
                "oracle_spp": ref_spp, "oracle_ms": round(ref_ms, 1),
                "plain_spp": target, "plain_ms": round(plain_ms, 2), "plain_relmse": e_plain,
@@ -219,6 +231,8 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
                "reached": reached is not None,
                "time_to_relmse_speedup": round(plain_ms / reached, 3) if reached else None,
                "curve": [(a, b, round(c, 6)) for a, b, c in curve[:: max(1, len(curve) // 12)]]}
+        if mode == "box":
+            return res
         # the spline camera path at the full config-4 resolution
         cams = scenes.spline_cameras(frames=300)
         acc_s = torch.zeros(1920 * 1080 * 3, dtype=torch.float64, device=dev)
@@ -568,8 +582,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--configs", type=int, default=16,
                     help="also time configs 1, 3 and 5 (this many batch jobs); 0 skips")
-    ap.add_argument("--nrc", choices=("off", "small", "full"), default="small",
-                    help="radiance-cache time-to-relMSE measurement (small: 480x270, full: 1920x1080)")
+    ap.add_argument("--nrc", choices=("off", "small", "full", "box"), default="small",
+                    help="radiance-cache time-to-relMSE measurement (small: 480x270, full: 1920x1080, "
+                         "box: the config-3 scene in RGB at 480x270)")
     ap.add_argument("--profile-nrc", action="store_true",
                     help="six radiance-cache frames (for ncu captures of the cache kernels)")
     ap.add_argument("--profile-size", default="480x270", help="frame size of --profile-nrc")
