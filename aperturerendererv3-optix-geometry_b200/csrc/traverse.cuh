@@ -341,6 +341,7 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
     // which also makes every tnear non-negative (its bits order like its value)
     const float tlow = fmaxf(r.tmin, 0.0f);
     uint32_t key[8];
+    uint32_t hm = 0;  // bit k: slot k's box is hit
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int b = k & 3;
@@ -352,12 +353,17 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
         const float tfz = fmaf(byte_biased(k < 4 ? fz0 : fz1, b), az, bz);
         const float tnear = max3f(tnx, tny, fmaxf(tnz, tlow));
         const float tfar = min3f(tfx, tfy, fminf(tfz, limit)) * kSlabWiden;
-        // the low byte carries the child's meta byte (rounding tnear down).
-        // Empty slots have inverted boxes (lo 255, hi 0) and fail this test
-        // unless the ray starts some 2^28 grid steps away; their meta byte
-        // kMetaEmpty keeps them out of both loops below either way.
-        key[k] = (tnear <= tfar) ? __byte_perm(__float_as_uint(tnear), k < 4 ? meta0 : meta1, 0x3214u + b)
-                                 : 0xFFFFFFFFu;
+        // key: the bits of tnear (rounded down) with the child's meta byte as
+        // the low byte and bit 31 set for internal children, so that the sort
+        // puts every hit leaf (nearest first) before every hit internal child
+        // (nearest first) and the misses last.  Empty slots have inverted
+        // boxes (lo 255, hi 0) and fail this test unless the ray starts some
+        // 2^28 grid steps away; they then sort as internal children, and their
+        // meta byte kMetaEmpty keeps them off the stack.
+        const bool hit = tnear <= tfar;
+        const uint32_t kb = __byte_perm(__float_as_uint(tnear), k < 4 ? meta0 : meta1, 0x3214u + b);
+        key[k] = hit ? ((kb & 0x7FFFFFFFu) | ((kb & 0x80u) << 24)) : 0xFFFFFFFFu;
+        hm |= static_cast<uint32_t>(hit) << k;
     }
     // visit children nearest first -- sort the 8 keys (Batcher odd-even merge
     // network, 19 comparators).  Any-hit queries profit too: the occluder of a
@@ -368,17 +374,17 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
     cswap(key[0], key[4]); cswap(key[1], key[5]); cswap(key[2], key[6]); cswap(key[3], key[7]);
     cswap(key[2], key[4]); cswap(key[3], key[5]);
     cswap(key[1], key[2]); cswap(key[3], key[4]); cswap(key[5], key[6]);
+    // hit leaves occupy sorted positions [0, nl), hit internal children
+    // [nl, nh).  Leaf slots: meta bytes with bit 7 clear, gathered from the two
+    // meta words (bits 7, 15, 23, 31 to bits 0-3 by one multiply-high).
+    const uint32_t ls = ((__umulhi(~meta0 & 0x80808080u, 0x10204080u) >> 3) & 0xFu) |
+                        (((__umulhi(~meta1 & 0x80808080u, 0x10204080u) >> 3) & 0xFu) << 4);
+    const int nh = __popc(hm), nl = __popc(hm & ls);
     // leaves, nearest first, in one rolled loop (a single copy of the
-    // primitive tests): bit k of `leaves` marks a hit leaf at sorted position
-    // k (misses and empty slots carry the internal bit in their low byte)
-    uint32_t leaves = 0;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) leaves |= ((~key[k] >> 7) & 1u) << k;
+    // primitive tests)
     const uint32_t prim_base = w1.y;
 #pragma unroll 1
-    while (leaves) {
-        const int k = __ffs(leaves) - 1;
-        leaves &= leaves - 1u;
+    for (int k = 0; k < nl; ++k) {
         const uint32_t kk = pick8(key, k);
         const uint32_t meta = kk & 0xFFu;
         const float tn = __uint_as_float(kk & ~0xFFu);
@@ -409,21 +415,13 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
             }
         }
     }
-    // internal children, pushed far to near, in one rolled loop over a mask
-    // (misses and empty slots have the low byte kMetaEmpty)
-    uint32_t inner = 0;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const uint32_t m = key[k] & 0xFFu;
-        inner |= static_cast<uint32_t>(m >= kMetaInternal && m != kMetaEmpty) << k;
-    }
+    // internal children, pushed far to near
     const uint32_t child_base = w1.x;
     const float lim_push = fminf(r.best.t, FLT_MAX) * kSlabWiden;
 #pragma unroll 1
-    while (inner) {
-        const int k = 31 - __clz(inner);
-        inner &= ~(1u << k);
-        const uint32_t kk = pick8(key, k);
+    for (int k = nh - 1; k >= nl; --k) {
+        const uint32_t kk = pick8(key, k) & 0x7FFFFFFFu;
+        if ((kk & 0xFFu) == kMetaEmpty) continue;
         if (!(__uint_as_float(kk & ~0xFFu) <= lim_push)) continue;
         const uint32_t child = child_base + (kk & 7u);
         const uint32_t entry = kAny ? child : ((kk & ~nmask) | child);
