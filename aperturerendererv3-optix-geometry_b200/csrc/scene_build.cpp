@@ -71,7 +71,7 @@ struct BNode {
 };
 
 constexpr int kMaxLeaf = 4;
-constexpr int kBins = 16;
+constexpr int kBins = 64;
 
 struct BinaryBuilder {
     const std::vector<Bounds>& pb;
