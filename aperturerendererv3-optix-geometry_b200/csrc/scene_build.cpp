@@ -5,7 +5,7 @@
 // triangle vertices on every test (intersection.cuh:27-29).  Here the transform
 // is applied once, with the same expression, and the leaf records carry the
 // world-space v0, e1 = v1 - v0 and e2 = v2 - v0 -- bit-identical operands of the
-// reference's Moller-Trumbore test.  The BVH is this build's own: binned SAH over
+// reference's Moller-Trumbore test.  The BVH is not the reference's: binned SAH (64 bins) over
 // triangle-bound centroids (the reference bins SceneObject centres, which for a
 // mesh are all the mesh position -- scene_helper.h:488-545 -- and degenerate into
 // one leaf per mesh), max 4 primitives per leaf, collapsed greedily (largest

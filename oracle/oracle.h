@@ -48,7 +48,7 @@ enum {
 /* Query options for or_trace_rays. */
 enum {
     OR_TIE_FIRST_FOUND = 0,   /* reference: strict t < best (intersection.cuh:160) */
-    OR_TIE_LOWEST_INDEX = 1,  /* this build: equal t goes to the lower object index */
+    OR_TIE_LOWEST_INDEX = 1,  /* the GPU core: equal t goes to the lower object index */
     OR_SLAB_REFERENCE = 0,    /* FastAABBHit as written (bvh.cuh:424-470)           */
     OR_SLAB_STANDARD = 2      /* standard slab test (entry <= exit), widened 1 ulp  */
 };
