@@ -291,6 +291,25 @@ __device__ __forceinline__ void cswap(uint32_t& a, uint32_t& b)
     a = lo; b = hi;
 }
 
+// Sort key of a hit child in one byte permute (prmt with sign replication):
+// byte 0 = meta byte b of `meta`, bytes 1-2 = the top 16 bits of tnear, byte 3
+// = the meta byte's bit 7 replicated (0xFF for internal and empty slots, 0 for
+// leaves).  tnear >= 0, so its top 16 bits order like its value.
+__device__ __forceinline__ uint32_t child_key(float tnear, uint32_t meta, int b)
+{
+    uint32_t r;
+    const uint32_t sel = 0x0324u + static_cast<uint32_t>(b) + (static_cast<uint32_t>(0xC + b) << 12);
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(__float_as_uint(tnear)), "r"(meta), "r"(sel));
+    return r;
+}
+
+// The entry distance a key carries, rounded down to 16 bits (bytes 1-2 of
+// the key moved to bytes 2-3 of a float, zeros below).
+__device__ __forceinline__ float key_distance(uint32_t key)
+{
+    return __uint_as_float(__byte_perm(key, 0u, 0x2144u));
+}
+
 // Closest-hit stack entries carry the child's entry distance with the node
 // index: (bits(tnear) & ~mask) | node, mask = all ones up to the highest bit
 // of (num_nodes | 255).  Clearing low bits of a non-negative float rounds it
@@ -353,16 +372,15 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
         const float tfz = fmaf(byte_biased(k < 4 ? fz0 : fz1, b), az, bz);
         const float tnear = max3f(tnx, tny, fmaxf(tnz, tlow));
         const float tfar = min3f(tfx, tfy, fminf(tfz, limit)) * kSlabWiden;
-        // key: the bits of tnear (rounded down) with the child's meta byte as
-        // the low byte and bit 31 set for internal children, so that the sort
-        // puts every hit leaf (nearest first) before every hit internal child
-        // (nearest first) and the misses last.  Empty slots have inverted
+        // key (child_key): the top 16 bits of tnear with the child's meta byte
+        // below and the meta byte's sign above, so that the sort puts every
+        // hit leaf (nearest first) before every hit internal child (nearest
+        // first) and the misses last.  Empty slots have inverted
         // boxes (lo 255, hi 0) and fail this test unless the ray starts some
         // 2^28 grid steps away; they then sort as internal children, and their
         // meta byte kMetaEmpty keeps them off the stack.
         const bool hit = tnear <= tfar;
-        const uint32_t kb = __byte_perm(__float_as_uint(tnear), k < 4 ? meta0 : meta1, 0x3214u + b);
-        key[k] = hit ? ((kb & 0x7FFFFFFFu) | ((kb & 0x80u) << 24)) : 0xFFFFFFFFu;
+        key[k] = hit ? child_key(tnear, k < 4 ? meta0 : meta1, b) : 0xFFFFFFFFu;
         hm |= static_cast<uint32_t>(hit) << k;
     }
     // visit children nearest first -- sort the 8 keys (Batcher odd-even merge
@@ -380,38 +398,49 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
     const uint32_t ls = ((__umulhi(~meta0 & 0x80808080u, 0x10204080u) >> 3) & 0xFu) |
                         (((__umulhi(~meta1 & 0x80808080u, 0x10204080u) >> 3) & 0xFu) << 4);
     const int nh = __popc(hm), nl = __popc(hm & ls);
-    // leaves, nearest first, in one rolled loop (a single copy of the
-    // primitive tests)
+    // leaves, nearest first, in one flat loop over (leaf, primitive) pairs: a
+    // single copy of the primitive tests, and a warp runs as many iterations
+    // as its busiest lane has primitives instead of the sum over leaf ranks of
+    // the per-rank maximum.  A leaf is entered only while its entry distance
+    // does not exceed the current hit (later leaves are farther).
     const uint32_t prim_base = w1.y;
+    int lk = 0, left = 0;
+    uint32_t pidx = 0;
+    if (nl > 0) {
+        const uint32_t kk = key[0];
+        if (key_distance(kk) <= fminf(r.best.t, FLT_MAX) * kSlabWiden) {
+            left = static_cast<int>((kk & 0xFFu) >> 5) + 1;
+            pidx = prim_base + (kk & 31u);
+        }
+    }
 #pragma unroll 1
-    for (int k = 0; k < nl; ++k) {
-        const uint32_t kk = pick8(key, k);
-        const uint32_t meta = kk & 0xFFu;
-        const float tn = __uint_as_float(kk & ~0xFFu);
-        if (!(tn <= fminf(r.best.t, FLT_MAX) * kSlabWiden)) break;  // later leaves are farther
-        const int count = static_cast<int>(meta >> 5) + 1;
-        const uint32_t first = prim_base + (meta & 31u);
-#pragma unroll 1
-        for (int p = 0; p < count; ++p) {
-            const PrimRec* pr = s.prims + first + p;
-            if (kCount) ++r.tests;
-            // all three words at once: one memory round trip per primitive
-            const float4 a = ldg4(&pr->v0[0]);
-            const float4 e1 = ldg4(&pr->e1[0]);
-            const float4 e2 = ldg4(&pr->e2[0]);
-            const int obj = __float_as_int(a.w);
-            float t;
-            if (__float_as_int(e1.w) == kPrimTriangle) {
-                t = mt_triangle(r.o, r.d, mk(a.x, a.y, a.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z));
-            } else {
-                t = isect_analytic_t(s, obj, r.o, r.d);
-            }
-            if (t < 0.0f || t < r.tmin) continue;
-            if (t < r.best.t || (r.best.obj >= 0 && t == r.best.t && obj < r.best.obj)) {
-                r.best.t = t;
-                r.best.obj = obj;
-                r.best.prim = static_cast<int>(first) + p;
-                if (kAny) return true;
+    while (left > 0) {
+        const PrimRec* pr = s.prims + pidx;
+        if (kCount) ++r.tests;
+        // all three words at once: one memory round trip per primitive
+        const float4 a = ldg4(&pr->v0[0]);
+        const float4 e1 = ldg4(&pr->e1[0]);
+        const float4 e2 = ldg4(&pr->e2[0]);
+        const int obj = __float_as_int(a.w);
+        float t;
+        if (__float_as_int(e1.w) == kPrimTriangle) {
+            t = mt_triangle(r.o, r.d, mk(a.x, a.y, a.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z));
+        } else {
+            t = isect_analytic_t(s, obj, r.o, r.d);
+        }
+        if (!(t < 0.0f || t < r.tmin) &&
+            (t < r.best.t || (r.best.obj >= 0 && t == r.best.t && obj < r.best.obj))) {
+            r.best.t = t;
+            r.best.obj = obj;
+            r.best.prim = static_cast<int>(pidx);
+            if (kAny) return true;
+        }
+        ++pidx;
+        if (--left == 0 && ++lk < nl) {
+            const uint32_t kk = pick8(key, lk);
+            if (key_distance(kk) <= fminf(r.best.t, FLT_MAX) * kSlabWiden) {
+                left = static_cast<int>((kk & 0xFFu) >> 5) + 1;
+                pidx = prim_base + (kk & 31u);
             }
         }
     }
@@ -420,11 +449,12 @@ __device__ __forceinline__ bool ray_step(const SceneView& s, RayState& r, uint32
     const float lim_push = fminf(r.best.t, FLT_MAX) * kSlabWiden;
 #pragma unroll 1
     for (int k = nh - 1; k >= nl; --k) {
-        const uint32_t kk = pick8(key, k) & 0x7FFFFFFFu;
+        const uint32_t kk = pick8(key, k);
         if ((kk & 0xFFu) == kMetaEmpty) continue;
-        if (!(__uint_as_float(kk & ~0xFFu) <= lim_push)) continue;
+        const float tn = key_distance(kk);
+        if (!(tn <= lim_push)) continue;
         const uint32_t child = child_base + (kk & 7u);
-        const uint32_t entry = kAny ? child : ((kk & ~nmask) | child);
+        const uint32_t entry = kAny ? child : ((__float_as_uint(tn) & ~nmask) | child);
         if (r.sp < kStackShared) stack[r.sp * 32] = entry;
         else if (r.sp < kStackMax) ovf[r.sp - kStackShared] = entry;
         else { atomicOr(err, 1); return true; }
