@@ -169,7 +169,22 @@ class BatchStats(ctypes.Structure):
                 ("graph_nodes", c_int64), ("kernel_launches", c_int64)]
 
 
+class ScreenGBuffer(ctypes.Structure):
+    """ar_screen_gbuffer: per-pixel guide values of the denoiser (half fields as uint16 bits)."""
+    _fields_ = [("albedo", ctypes.c_uint16 * 3), ("normal", ctypes.c_uint16 * 3), ("metallic", ctypes.c_uint16),
+                ("roughness", ctypes.c_uint16), ("depth", c_float), ("valid_frames", ctypes.c_uint32),
+                ("frames", ctypes.c_uint32), ("shading_model", ctypes.c_uint16 * 6), ("reserved", ctypes.c_uint32 * 2)]
+
+
+class ScreenStats(ctypes.Structure):
+    """ar_screen_stats: per-pixel Box-Cox moments of the denoiser."""
+    _fields_ = [("num", ctypes.c_uint32), ("mean", c_float * 3), ("m2_div_n", c_float * 3),
+                ("m3_div_n", c_float * 3), ("reserved", ctypes.c_uint32 * 2)]
+
+
 OBJECT_DTYPE = np.dtype(ObjectDesc)
+GBUFFER_DTYPE = np.dtype(ScreenGBuffer)
+STATS_DTYPE = np.dtype(ScreenStats)
 RECORD_DTYPE = np.dtype(PathRecord)
 
 EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create", "ar_scene_create_ex",
@@ -180,7 +195,8 @@ EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create",
                     "ar_scene_set_medium", "ar_nrc_create", "ar_nrc_destroy", "ar_nrc_render_frame",
                     "ar_nrc_get_params", "ar_nrc_set_params", "ar_nrc_infer", "ar_nrc_train", "ar_nrc_gradients",
                     "ar_batch_autotune", "ar_nrc_set_option", "ar_guide_create", "ar_guide_destroy", "ar_guide_render_frame",
-                    "ar_guide_get_stats", "ar_guide_get_probe")
+                    "ar_guide_get_stats", "ar_guide_get_probe", "ar_render_frame_denoise", "ar_denoise_record",
+                    "ar_denoise_bilateral")
 
 
 class ArError(RuntimeError):
@@ -242,6 +258,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_guide_get_stats.argtypes = [c_void_p, POINTER(GuideStats)]
     lib.ar_guide_get_probe.argtypes = [c_void_p, c_int32, c_void_p]
     for f in ("ar_guide_create", "ar_guide_destroy", "ar_guide_render_frame", "ar_guide_get_stats", "ar_guide_get_probe"):
+        getattr(lib, f).restype = c_int32
+    lib.ar_render_frame_denoise.argtypes = [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p,
+                                            c_void_p, c_void_p, c_void_p]
+    lib.ar_denoise_record.argtypes = [c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_void_p]
+    lib.ar_denoise_bilateral.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p]
+    for f in ("ar_render_frame_denoise", "ar_denoise_record", "ar_denoise_bilateral"):
         getattr(lib, f).restype = c_int32
     lib.ar_batch_autotune.argtypes = [c_void_p, c_int32, c_int32, POINTER(BatchTuning), c_void_p]
     lib.ar_batch_autotune.restype = c_int32
@@ -561,6 +583,34 @@ class RadianceCache:
             self.close()
         except Exception:
             pass
+
+
+def _dptr(x) -> c_void_p | None:
+    """Device address of a torch tensor (or an int address), None for None."""
+    if x is None:
+        return None
+    return c_void_p(x if isinstance(x, int) else x.data_ptr())
+
+
+def render_frame_denoise(scene: "Scene", camera: Camera, params: RenderParams, out_ptr, accum_ptr, gbuffer, stats,
+                         stream: int = 0) -> None:
+    """ar_render_frame_denoise: one interactive frame (spp = 1) that records the
+    denoiser's guide buffers; device buffers as torch tensors or addresses."""
+    _check(_lib.ar_render_frame_denoise(scene.handle, ctypes.byref(camera), ctypes.byref(params), _dptr(out_ptr),
+                                        _dptr(accum_ptr), _dptr(gbuffer), _dptr(stats), c_void_p(stream)))
+
+
+def denoise_record(hits, samples, n: int, gbuffer, stats, stream: int = 0) -> None:
+    """ar_denoise_record on device buffers (torch tensors or addresses)."""
+    load_library()
+    _check(_lib.ar_denoise_record(_dptr(hits), _dptr(samples), n, _dptr(gbuffer), _dptr(stats), c_void_p(stream)))
+
+
+def denoise_bilateral(hdr_in, hdr_out, gbuffer, stats, width: int, height: int, stream: int = 0) -> None:
+    """ar_denoise_bilateral on device buffers (torch tensors or addresses)."""
+    load_library()
+    _check(_lib.ar_denoise_bilateral(_dptr(hdr_in), _dptr(hdr_out), _dptr(gbuffer), _dptr(stats), width, height,
+                                     c_void_p(stream)))
 
 
 class PathGuide:

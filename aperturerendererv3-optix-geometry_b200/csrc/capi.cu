@@ -303,7 +303,7 @@ ar::FrameParams make_frame(const ar_scene* s, const ar_camera* c, const ar_rende
 
 ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* p, ar_path_record* rec_dev,
                      cudaStream_t st, ar_render_stats* stats, const ar::NrcFrame* nrc = nullptr,
-                     const ar::GuideView* guide = nullptr)
+                     const ar::GuideView* guide = nullptr, const ar::DenoiseView* dn = nullptr)
 {
     using namespace ar;
     if (p->spectral && !s->spec_tables)
@@ -319,6 +319,7 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
         fp.guiding = 1;
         fp.guide = *guide;
     }
+    if (dn) fp.dn = *dn;
     ensure_workspace(s, pool, npix);
     PathBuffers B = s->bufs;
     B.capacity = static_cast<int32_t>(pool);
@@ -1685,6 +1686,30 @@ ar_status ar_guide_render_frame(ar_guide* g, const ar_camera* cam, const ar_rend
     ck(ar::pg_update(g->view, s->sm_count, st), "guiding update");
     ++g->frames;
     const int64_t n = npix * 3;
+    if (out_rgb) ck(ar::launch_mean(s->accum, n, 1.0, out_rgb, st), "mean");
+    if (accum) ck(ar::launch_add(s->accum, n, accum, st), "accumulate");
+    return check_err(s, st);
+    AR_GUARD_END
+}
+
+// ------------------------------------------------------------------ denoiser recording
+ar_status ar_render_frame_denoise(ar_scene* s, const ar_camera* cam, const ar_render_params* p, float* out_rgb,
+                                  double* accum, ar_screen_gbuffer* gbuffer, ar_screen_stats* stats, void* stream)
+{
+    g_last_error.clear();
+    if (!s) return fail(AR_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (ar_status e = check_camera(cam)) return e;
+    if (ar_status e = check_params(p)) return e;
+    if (p->spp != 1) return fail(AR_ERR_INVALID_ARGUMENT, "denoiser frames take spp = 1");
+    if (!out_rgb && !accum) return fail(AR_ERR_INVALID_ARGUMENT, "out_rgb and accum are both NULL");
+    AR_GUARD_BEGIN
+    DeviceGuard dg(s->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ar::DenoiseView dn;
+    dn.gbuf = gbuffer;
+    dn.stat = stats;
+    if (ar_status e = run_render(s, cam, p, nullptr, st, nullptr, nullptr, nullptr, &dn)) return e;
+    const int64_t n = static_cast<int64_t>(cam->width) * cam->height * 3;
     if (out_rgb) ck(ar::launch_mean(s->accum, n, 1.0, out_rgb, st), "mean");
     if (accum) ck(ar::launch_add(s->accum, n, accum, st), "accumulate");
     return check_err(s, st);

@@ -468,6 +468,11 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             }
         }
         if (kMed) pos = cro + crd * fbits(hr.z);  // no surface: the normal stays zero
+        // denoiser guide buffer: the primary hit (RecordScreenGBuffer at depth 0, render.cuh:640-643)
+        if (fp.dn.gbuf && depth == 0) {
+            if (hit) record_gbuffer(fp.dn.gbuf + pixel, true, gb.albedo, nrm, gb.metallic, gb.roughness, fbits(hr.z), kModel);
+            else record_gbuffer(fp.dn.gbuf + pixel, false, nrm, nrm, 0.0f, 0.0f, 0.0f, 0);
+        }
         // ---- learned radiance cache (extension): path spread (Mueller et al. 2021,
         // a = (sum_i sqrt(|x_i-1 - x_i|^2 / (p_i |cos_i|)))^2 against
         // a0 = |x_0 - x_1|^2 / (4 pi |cos_1|)), training vertices, termination
@@ -1003,6 +1008,8 @@ __global__ void k_retire(FrameParams fp, PathBuffers B, PoolCtl* ctl, double* ac
         const float y = fmaxf(clampf(v.y, 0.0f, 1.0e3f), 0.0f);
         const float z = fmaxf(clampf(v.z, 0.0f, 1.0e3f), 0.0f);
         const int pixel = ibits(rr.rad.w);
+        // denoiser moments of the clamped sample (RecordScreenStatisticBuffer, render.cuh:988-991)
+        if (fp.dn.stat) record_stats(fp.dn.stat + pixel, mk(x, y, z));
         int slot;
         if (fp.nrc.enabled && nrc_train_slot(fp.nrc, pixel, &slot)) {
             // training targets: radiance gathered after each recorded vertex,

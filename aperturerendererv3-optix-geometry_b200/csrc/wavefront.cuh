@@ -23,6 +23,7 @@
 #include <cstdint>
 
 #include "../../include/aperture_b200.h"
+#include "denoise.cuh"
 #include "guiding.cuh"
 #include "nrc.cuh"
 #include "spectral.cuh"
@@ -117,6 +118,7 @@ struct FrameParams {
     NrcFrame nrc;            // learned radiance cache hooks (enabled = 0: plain tracer)
     int32_t guiding;         // 1: path guiding with `guide` (interactive frames, one path per pixel)
     GuideView guide;
+    DenoiseView dn;          // denoiser guide buffers (interactive frames, one path per pixel); NULL: off
 };
 
 }  // namespace ar

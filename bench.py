@@ -268,6 +268,45 @@ def _timed_render(scene: Scene, cam, params, out, stream) -> dict:
             "msamples_per_s": round(st.paths / (st.total_ms / 1e3) / 1e6, 2), "paths": st.paths, "rays": rays}
 
 
+def measure_denoise(torch, dev, stream, scene: Scene, frames: int = 8, reps: int = 10) -> dict:
+    """The denoiser on the headline scene at 1920x1080: `frames` interactive
+    frames (spp 1) that record the guide buffers, then the bilateral filter
+    (15 x 15 window) over their mean, timed with CUDA events on the launching
+    stream after two warm-up launches."""
+    from aperture_b200 import denoise_bilateral, render_frame_denoise
+    w, h = WIDTH, HEIGHT
+    n = w * h
+    cam = scenes.spheres_camera(w, h)
+    gbuf = torch.zeros(n * 48, dtype=torch.uint8, device=dev)
+    stats = torch.zeros(n * 48, dtype=torch.uint8, device=dev)
+    acc = torch.zeros(n * 3, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)  # the zero fills run on the default stream
+    s = stream.cuda_stream
+    for f in range(frames):
+        render_frame_denoise(scene, cam, make_params(spp=1, max_depth=DEPTH, frame_offset=f), None, acc, gbuf,
+                             stats, s)
+    with torch.cuda.stream(stream):
+        hdr = (acc / frames).float()
+        out = torch.empty_like(hdr)
+    for _ in range(2):
+        denoise_bilateral(hdr, out, gbuf, stats, w, h, s)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        denoise_bilateral(hdr, out, gbuf, stats, w, h, s)
+    e1.record(stream)
+    stream.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    per_px = 48 + 48 + 12 + 12
+    return {"workload": f"bilateral filter (radius 7, t-test gated) of the config-2 scene at {w}x{h} after "
+                        f"{frames} recorded frames",
+            "ms": round(ms, 4), "mpixels_per_s": round(n / ms / 1e3, 1),
+            "pair_weights_per_s_g": round(n * 225 / ms / 1e6, 2),
+            "algorithmic_bytes_per_pixel": per_px,
+            "achieved_gbs": round(n * per_px / ms / 1e6, 1),
+            "bound": "compute (225 pair weights per pixel from shared memory)"}
+
+
 def measure_configs(torch, dev, stream, c5_jobs: int) -> dict:
     """The other benchmark configurations, one timed render each after one
     warm-up (device time from the library's CUDA events): config 1 (box,
@@ -477,6 +516,8 @@ def run_ours(args) -> None:
             line["nrc"] = measure_nrc(torch, dev, scene, args.nrc, stream)
         if world == 1 and args.configs > 0:
             line["other_configs"] = measure_configs(torch, dev, stream, args.configs)
+        if world == 1 and not args.no_denoise:
+            line["denoise"] = measure_denoise(torch, dev, stream, scene)
         if world == 1 and not args.no_cpu:
             cs = cpu_sample(objs, cam, params, args.cpu_seconds, cpu_threads())
             line["cpu_baseline"] = {"value": round(cs["value"], 4), "unit": "Mrays/s", "cores": cpu_threads(),
@@ -580,6 +621,7 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU sample length per measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-denoise", action="store_true", help="skip the denoiser measurement")
     ap.add_argument("--configs", type=int, default=16,
                     help="also time configs 1, 3 and 5 (this many batch jobs); 0 skips")
     ap.add_argument("--nrc", choices=("off", "small", "full", "box"), default="small",

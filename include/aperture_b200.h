@@ -493,6 +493,74 @@ ar_status ar_tonemap(const float* rgb, size_t n, int32_t tone_type, float exposu
  * Gamma / ACES functions (include/aperture_b200_renderer.hpp). */
 ar_status ar_tone_curve(const float* rgb3, int32_t tone_type, float* out3);
 
+/* ---------------------------------------------------------------- denoiser
+ * Per-pixel guide buffers of the reference's screen-space denoiser and its
+ * bilateral filter (core/denoise/).  Half-precision fields hold IEEE binary16
+ * bit patterns.  Both buffers live on the device, one record per pixel in
+ * row-major order (j*width+i), owned by the caller; zero them (cudaMemset 0)
+ * before the first frame, as the reference's ResetScreenGBuffer does
+ * (core/GUI.hpp:202-230). */
+
+/* Running means over frames of the primary hit: replaces
+ * denoise::ScreenGBuffer (core/denoise/denoise.cuh:35-84).  The reference's
+ * 64-bit frame counters are 32-bit here. */
+typedef struct ar_screen_gbuffer {
+    uint16_t albedo[3];         /* half: material albedo at the primary hit   */
+    uint16_t normal[3];         /* half: shading normal facing the ray         */
+    uint16_t metallic;          /* half                                        */
+    uint16_t roughness;         /* half                                        */
+    float depth;                /* hit distance                                */
+    uint32_t valid_frames;      /* frames whose primary ray hit a surface      */
+    uint32_t frames;            /* frames recorded                             */
+    uint16_t shading_model[6];  /* half: share of frames per shading model
+                                   (AR_MAT_*), [4] = no surface, [5] unused    */
+    uint32_t reserved[2];
+} ar_screen_gbuffer;            /* 48 bytes */
+
+/* Box-Cox (lambda 0.5) moments of the per-frame samples: replaces
+ * denoise::ScreenStatisticsBuffer (core/denoise/denoise_statistic.cuh:11-24). */
+typedef struct ar_screen_stats {
+    uint32_t num;               /* samples recorded                            */
+    float mean[3];              /* mean of BoxCox(sample)                      */
+    float m2_div_n[3];          /* second central moment / num                 */
+    float m3_div_n[3];          /* third central moment / num                  */
+    uint32_t reserved[2];
+} ar_screen_stats;              /* 48 bytes */
+
+/* One interactive frame (params->spp must be 1, RGB or single-wavelength
+ * spectral) that also records, per pixel, the primary hit into `gbuffer`
+ * (denoise::RecordScreenGBuffer at depth 0, core/render/render.cuh:640-643)
+ * and the frame's clamped sample into `stats` (RecordScreenStatisticBuffer,
+ * render.cuh:988-991, core/denoise/denoise_statistic.cuh:37-69).  Either
+ * buffer may be NULL.  out_rgb / accum as in ar_render with AR_MEM_DEVICE
+ * (either may be NULL, not both).  Replaces the recording part of the
+ * interactive SceneRenderer::Render (core/scene.hpp:128-133). */
+ar_status ar_render_frame_denoise(ar_scene* scene, const ar_camera* camera, const ar_render_params* params,
+                                  float* out_rgb, double* accum, ar_screen_gbuffer* gbuffer,
+                                  ar_screen_stats* stats, void* stream);
+
+/* Records one frame from caller-supplied primary-hit attributes and samples
+ * (for a caller with its own primary visibility, and the parity tests):
+ * hits holds 12 floats per pixel -- albedo.xyz, normal.xyz, metallic,
+ * roughness, depth, shading model (AR_MAT_* as a float), hit flag (nonzero =
+ * surface), unused -- and samples 3 floats per pixel (the clamped sample).
+ * Either output may be NULL.  Device pointers; n pixels. */
+ar_status ar_denoise_record(const float* hits, const float* samples, size_t n, ar_screen_gbuffer* gbuffer,
+                            ar_screen_stats* stats, void* stream);
+
+/* Bilateral filter of the reference (denoise::Bilateral16x16<7>,
+ * core/denoise/denoise.cuh:359-443): a 15 x 15 window in log(1 + c) space,
+ * each neighbour weighted by the guide-buffer similarity (ComputeSVGFWeight,
+ * denoise.cuh:185-245), a Gaussian of the pixel offset (sigma 2) and a
+ * skewness-corrected Welch t-test at 0.005 between the two pixels' Box-Cox
+ * moments (ComputeTStatisticFinal, denoise.cuh:341-356); borders clamp.  A
+ * neighbour whose guide weight is not a number (a pixel whose primary ray
+ * never hit has a zero normal) contributes nothing.  hdr_in and hdr_out:
+ * width*height*3 floats; all pointers on the device; hdr_out must not alias
+ * hdr_in. */
+ar_status ar_denoise_bilateral(const float* hdr_in, float* hdr_out, const ar_screen_gbuffer* gbuffer,
+                               const ar_screen_stats* stats, int32_t width, int32_t height, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2640,3 +2640,210 @@ void or_volume_grid(const or_scene* s, int32_t v, float* out)
             return;
         }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Screen-space denoiser (core/denoise/)                                     */
+/* ------------------------------------------------------------------------ */
+/* IEEE binary16 <-> binary32 through _Float16 (round to nearest even). */
+static inline float dn_h2f(uint16_t h) { _Float16 v; memcpy(&v, &h, 2); return (float)v; }
+static inline uint16_t dn_f2h(float f) { _Float16 v = (_Float16)f; uint16_t h; memcpy(&h, &v, 2); return h; }
+/* half - half rounded once to half, as __hsub: the exact difference in double */
+static inline float dn_hsub(uint16_t a, uint16_t b)
+{
+    const _Float16 d = (_Float16)((double)dn_h2f(a) - (double)dn_h2f(b));
+    return (float)d;
+}
+
+#define DN_MODELS 5 /* MAT_MAX + 1 (core/render/object.cuh:45-52) */
+
+/* RecordShadingModel (core/denoise/denoise.cuh:86-104) */
+static void dn_record_model(ar_screen_gbuffer* g, int model)
+{
+    if (g->frames == 0)
+        for (int i = 0; i < DN_MODELS; ++i) g->shading_model[i] = 0;
+    const float affix = 1.0f / (float)(g->frames + 1u);
+    const float pre = (float)g->frames / (float)(g->frames + 1u);
+    for (int i = 0; i < DN_MODELS; ++i) g->shading_model[i] = dn_f2h(dn_h2f(g->shading_model[i]) * pre);
+    g->shading_model[model] = dn_f2h(dn_h2f(g->shading_model[model]) + affix);
+}
+
+/* RecordScreenGBuffer (core/denoise/denoise.cuh:106-166) */
+static void dn_record_gbuffer(ar_screen_gbuffer* g, const float* h)
+{
+    if (h[10] != 0.0f) {
+        int model = (int)h[9];
+        if (model < 0) model = 0;
+        if (model > DN_MODELS - 2) model = DN_MODELS - 2;
+        if (g->valid_frames == 0) {
+            for (int c = 0; c < 3; ++c) g->albedo[c] = g->normal[c] = 0;
+            g->metallic = g->roughness = 0;
+            g->depth = 0.0f;
+        }
+        const float affix = 1.0f / (float)(g->valid_frames + 1u);
+        const float pre = (float)g->valid_frames / (float)(g->valid_frames + 1u);
+        for (int c = 0; c < 3; ++c) {
+            g->albedo[c] = dn_f2h(dn_h2f(g->albedo[c]) * pre);
+            g->normal[c] = dn_f2h(dn_h2f(g->normal[c]) * pre);
+        }
+        g->metallic = dn_f2h(dn_h2f(g->metallic) * pre);
+        g->roughness = dn_f2h(dn_h2f(g->roughness) * pre);
+        g->depth = g->depth * pre;
+        for (int c = 0; c < 3; ++c) {
+            g->albedo[c] = dn_f2h(dn_h2f(g->albedo[c]) + affix * h[c]);
+            g->normal[c] = dn_f2h(dn_h2f(g->normal[c]) + affix * h[3 + c]);
+        }
+        g->metallic = dn_f2h(dn_h2f(g->metallic) + affix * h[6]);
+        g->roughness = dn_f2h(dn_h2f(g->roughness) + affix * h[7]);
+        g->depth = g->depth + affix * h[8];
+        ++g->valid_frames;
+        dn_record_model(g, model);
+    } else {
+        dn_record_model(g, DN_MODELS - 1);
+    }
+    ++g->frames;
+}
+
+/* RecordScreenStatisticBuffer (core/denoise/denoise_statistic.cuh:37-69),
+ * BoxCox05's powf(x, 0.5f) as sqrtf(x) */
+static void dn_record_stats(ar_screen_stats* s, const float* x)
+{
+    const uint32_t n0 = s->num, n1 = n0 + 1u;
+    s->num = n1;
+    const float invN1 = 1.0f / (float)n1;
+    for (int c = 0; c < 3; ++c) {
+        const float bc = (sqrtf(fmaxf(x[c], 0.0f)) - 1.0f) * 2.0f;
+        const float delta = bc - s->mean[c];
+        const float dn = delta * invN1;
+        const double m2 = (double)s->m2_div_n[c] * (double)n0 + (double)(delta * (delta - dn));
+        const float d2 = delta * delta, dn2 = dn * dn;
+        const double m3 = ((double)s->m3_div_n[c] * (double)n0 - 3.0 * ((double)dn * m2)) + (double)(delta * (d2 - dn2));
+        s->mean[c] = s->mean[c] + dn;
+        s->m2_div_n[c] = (float)(m2 / (double)n1);
+        s->m3_div_n[c] = (float)(m3 / (double)n1);
+    }
+}
+
+void or_dn_record(const float* hits, const float* samples, int64_t n, ar_screen_gbuffer* gbuffer,
+                  ar_screen_stats* stats)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        if (gbuffer) dn_record_gbuffer(gbuffer + i, hits + 12 * i);
+        if (stats) dn_record_stats(stats + i, samples + 3 * i);
+    }
+}
+
+/* Per-pixel terms of ComputeTStatistic (denoise.cuh:278-302) and of
+ * ComputeWelchNu (denoise.cuh:326-339), counts in 32-bit unsigned arithmetic. */
+typedef struct { float vth[3], theta[3], u[3], l[3]; } DnT;
+static DnT dn_tstat(const ar_screen_stats* s)
+{
+    DnT r;
+    const uint32_t nm1 = (s->num - 1u) > 1u ? (s->num - 1u) : 1u;
+    const double num = (double)s->num;
+    const double invNm1 = 1.0 / (double)nm1;
+    for (int c = 0; c < 3; ++c) {
+        const float vb = (float)((double)s->m2_div_n[c] * num * invNm1);
+        r.vth[c] = (float)((double)vb / num);
+        r.theta[c] = s->mean[c] + s->m3_div_n[c] / 6.0f / vb;
+        r.u[c] = vb / (float)s->num;
+        r.l[c] = r.u[c] * r.u[c] / (float)nm1;
+    }
+    return r;
+}
+
+/* LookupTQuantile005(floorToInt(nu)) with a saturating conversion (NaN -> 0) */
+static int dn_t_index(float nu)
+{
+    if (!(nu >= 1.0f)) return 0;
+    if (nu >= 1024.0f) return 1023;
+    return (int)floorf(nu) - 1;
+}
+
+/* ComputeSVGFWeight (denoise.cuh:185-245) */
+static float dn_svgf(const ar_screen_gbuffer* a, const ar_screen_gbuffer* b)
+{
+    const float kAlb = 1.0f / (2.0f * 1.0f * 1.0f), kNrm = 1.0f / (2.0f * 0.5f * 0.5f);
+    const float kDep = 1.0f / (2.0f * 0.25f * 0.25f), kMet = 1.0f / (2.0f * 0.5f * 0.5f);
+    const float kRgh = 1.0f / (2.0f * 0.5f * 0.5f), kShd = 1.0f / (2.0f * 0.1f * 0.1f);
+    float w = 0.0f;
+    {
+        const V3 d1 = vsub(v3(dn_h2f(a->albedo[0]), dn_h2f(a->albedo[1]), dn_h2f(a->albedo[2])),
+                           v3(dn_h2f(b->albedo[0]), dn_h2f(b->albedo[1]), dn_h2f(b->albedo[2])));
+        w += dot3(d1, d1) * kAlb;
+    }
+    {
+        const V3 na = vnormalize(v3(dn_h2f(a->normal[0]), dn_h2f(a->normal[1]), dn_h2f(a->normal[2])));
+        const V3 nb = vnormalize(v3(dn_h2f(b->normal[0]), dn_h2f(b->normal[1]), dn_h2f(b->normal[2])));
+        const float d = 1.0f - dot3(na, nb);
+        w += d * d * kNrm;
+    }
+    {
+        const float denom = fmaxf(fmaxf(a->depth, b->depth), 1.0e-6f);
+        const float d = (a->depth - b->depth) / denom;
+        w += d * d * kDep;
+    }
+    const float dm = dn_hsub(a->metallic, b->metallic);
+    w += dm * dm * kMet;
+    const float dr = dn_hsub(a->roughness, b->roughness);
+    w += dr * dr * kRgh;
+    float l1 = 0.0f;
+    for (int i = 0; i < DN_MODELS; ++i) l1 += fabsf(dn_hsub(a->shading_model[i], b->shading_model[i]));
+    const float tv = 0.5f * l1;
+    w += tv * tv * kShd;
+    return om_expf(-w);
+}
+
+/* ComputeTStatisticFinal (denoise.cuh:341-356), A = center */
+static float dn_ttest(const DnT* A, const DnT* B, const float* tq)
+{
+    int pass = 1;
+    for (int c = 0; c < 3; ++c) {
+        const float t = A->theta[c] - B->theta[c];
+        const float t2 = t * t;
+        const float W = (t2 + B->vth[c]) / fmaxf(t2 + A->vth[c] + B->vth[c], 1.0e-6f);
+        const float T = sqrtf(0.5f / (1.0f - W) - 1.0f);
+        const float up = A->u[c] + B->u[c];
+        const float nu = up * up / (A->l[c] + B->l[c]);
+        pass = pass && (T < tq[dn_t_index(nu)]);
+    }
+    return pass ? 1.0f : 0.0f;
+}
+
+/* Bilateral16x16<7> (denoise.cuh:359-443) over the whole image; t_quantiles:
+ * the 1024-entry table of the 0.9975 Student t quantile. */
+void or_dn_bilateral(const float* hdr, float* out, const ar_screen_gbuffer* gb, const ar_screen_stats* st, int width,
+                     int height, const float* t_quantiles)
+{
+    const int R = 7;
+    const float kSpatial = 1.0f / (2.0f * 2.0f * 2.0f);
+    const int64_t np = (int64_t)width * height;
+    DnT* ts = (DnT*)malloc(sizeof(DnT) * (size_t)np);
+    for (int64_t p = 0; p < np; ++p) ts[p] = dn_tstat(st + p);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int oy = 0; oy < height; ++oy) {
+        for (int ox = 0; ox < width; ++ox) {
+            const int64_t ci = (int64_t)oy * width + ox;
+            float acc[3], s[3];
+            for (int c = 0; c < 3; ++c) acc[c] = 0.0f + om_logf(hdr[3 * ci + c] + 1.0f) * 1.0e-6f;
+            float wsum = 0.0f + 1.0e-6f;
+            for (int j = -R; j <= R; ++j) {
+                int ny = oy + j;
+                ny = ny < 0 ? 0 : (ny > height - 1 ? height - 1 : ny);
+                for (int i = -R; i <= R; ++i) {
+                    int nx = ox + i;
+                    nx = nx < 0 ? 0 : (nx > width - 1 ? width - 1 : nx);
+                    const int64_t ni = (int64_t)ny * width + nx;
+                    float weight = dn_svgf(gb + ci, gb + ni) * om_expf((float)(-(i * i + j * j)) * kSpatial) *
+                                   dn_ttest(ts + ci, ts + ni, t_quantiles);
+                    if (weight != weight) weight = 0.0f; /* zero normal of a pixel that never hit */
+                    if (weight == 0.0f) continue;
+                    for (int c = 0; c < 3; ++c) s[c] = om_logf(hdr[3 * ni + c] + 1.0f);
+                    for (int c = 0; c < 3; ++c) acc[c] = acc[c] + s[c] * weight;
+                    wsum = wsum + weight;
+                }
+            }
+            for (int c = 0; c < 3; ++c) out[3 * ci + c] = fmaxf(om_expf(acc[c] / wsum) - 1.0f, 0.0f);
+        }
+    }
+    free(ts);
+}

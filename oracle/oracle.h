@@ -132,6 +132,15 @@ float or_power_heuristic(float a, float b);
 /* Tonemap kernel (scene.cu:180-199): n pixels of RGB (or XYZ) -> 0xAARRGGBB. */
 void or_tonemap(const float* rgb, int64_t n, int tone, float exposure, int xyz_input, uint32_t* out);
 
+/* Screen-space denoiser (core/denoise/): one frame recorded per pixel from
+ * hits (12 floats: albedo.xyz, normal.xyz, metallic, roughness, depth, shading
+ * model, hit flag, unused) and samples (3 floats); either output may be NULL. */
+void or_dn_record(const float* hits, const float* samples, int64_t n, ar_screen_gbuffer* gbuffer,
+                  ar_screen_stats* stats);
+/* Bilateral16x16<7> over the whole image (t_quantiles: 1024 floats). */
+void or_dn_bilateral(const float* hdr, float* out, const ar_screen_gbuffer* gb, const ar_screen_stats* st, int width,
+                     int height, const float* t_quantiles);
+
 /* One object's hit at loop depth `depth` (SDF tolerance INTERSECT_EPS(depth)/2):
  * t = -1 on a miss, with world position and normal. */
 void or_object_isect(const or_scene* s, int32_t obj, const float* rays, int64_t n, int32_t depth, float* t,

@@ -56,6 +56,8 @@ def load():
     lib.or_render_paths.restype = c_int64
     lib.or_render_image.argtypes = [c_void_p, c_void_p, c_void_p, c_int64, c_int64, c_int64, c_void_p,
                                     POINTER(c_int64), POINTER(c_int64), c_int]
+    lib.or_dn_record.argtypes = [c_void_p, c_void_p, c_int64, c_void_p, c_void_p]
+    lib.or_dn_bilateral.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p]
     for f in ("or_sinf", "or_cosf", "or_expf", "or_logf"):
         getattr(lib, f).argtypes = [c_float]
         getattr(lib, f).restype = c_float
@@ -330,3 +332,27 @@ def hg_sample(d, g: float, u2) -> np.ndarray:
 
 def hg_phase(g: float, cos_t: float) -> float:
     return float(load().or_hg_phase(g, cos_t))
+
+
+def dn_record(hits: np.ndarray | None, samples: np.ndarray | None, gbuffer: np.ndarray | None,
+              stats: np.ndarray | None) -> None:
+    """Records one frame into the denoiser buffers in place (numpy record arrays
+    of 48-byte ar_screen_gbuffer / ar_screen_stats): RecordScreenGBuffer and
+    RecordScreenStatisticBuffer (core/denoise/)."""
+    lib = load()
+    n = len(gbuffer) if gbuffer is not None else len(stats)
+    h = np.ascontiguousarray(hits, np.float32) if hits is not None else None
+    sm = np.ascontiguousarray(samples, np.float32) if samples is not None else None
+    lib.or_dn_record(_p(h) if h is not None else None, _p(sm) if sm is not None else None, n,
+                     _p(gbuffer) if gbuffer is not None else None, _p(stats) if stats is not None else None)
+
+
+def dn_bilateral(hdr: np.ndarray, gbuffer: np.ndarray, stats: np.ndarray, width: int, height: int,
+                 t_quantiles: np.ndarray) -> np.ndarray:
+    """Bilateral16x16<7> of core/denoise/denoise.cuh over a whole image."""
+    lib = load()
+    hdr = np.ascontiguousarray(hdr, np.float32).reshape(-1)
+    out = np.empty_like(hdr)
+    tq = np.ascontiguousarray(t_quantiles, np.float32)
+    lib.or_dn_bilateral(_p(hdr), _p(out), _p(gbuffer), _p(stats), width, height, _p(tq))
+    return out

@@ -56,6 +56,7 @@ STRUCTS = {
     "ar_vec3": ab.Vec3, "ar_material": ab.Material, "ar_vertex": ab.Vertex, "ar_object_desc": ab.ObjectDesc,
     "ar_camera": ab.Camera, "ar_render_params": ab.RenderParams, "ar_path_record": ab.PathRecord,
     "ar_scene_info": ab.SceneInfo, "ar_render_stats": ab.RenderStats,
+    "ar_screen_gbuffer": ab.ScreenGBuffer, "ar_screen_stats": ab.ScreenStats,
 }
 
 
