@@ -596,6 +596,16 @@ def profile_queues() -> None:
                       "shadow_per_launch": st.shadow_rays / max(st.shadow_launches, 1)}), flush=True)
 
 
+def profile_denoise() -> None:
+    """Two recorded frames of the headline scene at 1920x1080, then three
+    bilateral-filter launches (for ncu captures of k_bilateral)."""
+    import torch
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    r = measure_denoise(torch, dev, stream, Scene(scenes.spheres_scene()), frames=2, reps=1)
+    print(json.dumps({"profile": "denoise", **r}), flush=True)
+
+
 def profile_nrc(width: int = 480, height: int = 270) -> None:
     """Six radiance-cache frames (config-2 scene, training on) for ncu
     captures of the cache kernels; prints the frame statistics."""
@@ -622,6 +632,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU sample length per measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-denoise", action="store_true", help="skip the denoiser measurement")
+    ap.add_argument("--profile-denoise", action="store_true",
+                    help="record two frames and run the bilateral filter three times (for ncu captures)")
     ap.add_argument("--configs", type=int, default=16,
                     help="also time configs 1, 3 and 5 (this many batch jobs); 0 skips")
     ap.add_argument("--nrc", choices=("off", "small", "full", "box"), default="small",
@@ -635,6 +647,9 @@ def main():
     args = ap.parse_args()
     if args.profile_queues:
         profile_queues()
+        return
+    if args.profile_denoise:
+        profile_denoise()
         return
     if args.profile_nrc:
         w, h = (int(x) for x in args.profile_size.split("x"))
