@@ -9,7 +9,7 @@
 // The pair weight then reads only shared memory, one warp per tile row, so a
 // warp's 32 lanes read 32 consecutive words.  The t-test is evaluated first:
 // a neighbour that fails it has weight 0 and skips the guide-weight
-// exponential.  Every term is computed with the reference's expressions and
+// exponential; its square root is replaced by an exact threshold compare.  Every term is computed with the reference's expressions and
 // order of operations, so the pair weight is the reference's (with the fixed
 // exp/log of detmath.h); the guide weight's half-precision differences round
 // to half as the reference's device code does (__hsub).
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_bilateral(const float* __re
     float* tq = sm + static_cast<size_t>(kWords) * kWin;
     float* spatial = tq + kTQuantiles;
     const int tid = threadIdx.y * kTileX + threadIdx.x;
-    for (int k = tid; k < kTQuantiles; k += kTileX * kTileY) tq[k] = kTQuantile005[k];
+    for (int k = tid; k < kTQuantiles; k += kTileX * kTileY) tq[k] = kTQuantileSqrtThreshold[k];
     for (int k = tid; k < kTaps; k += kTileX * kTileY) {
         const int j = k / (2 * kDnRadius + 1) - kDnRadius, i = k % (2 * kDnRadius + 1) - kDnRadius;
         spatial[k] = exp_det(static_cast<float>(-(i * i + j * j)) * kInvSpatial);
@@ -150,7 +150,10 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_bilateral(const float* __re
 #pragma unroll 1
         for (int i = -kDnRadius; i <= kDnRadius; ++i) {
             const int q = c + j * kWinX + i;
-            // ComputeTStatisticFinal (denoise.cuh:341-356), center = A
+            // ComputeTStatisticFinal (denoise.cuh:341-356), center = A.  The
+            // statistic T = sqrtf(x) is below the quantile exactly when
+            // 0 <= x < (smallest float whose square root reaches it), so the
+            // square root is not taken; the three channels are independent.
             bool pass = true;
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch) {
@@ -158,10 +161,10 @@ __global__ void __launch_bounds__(kTileX * kTileY) k_bilateral(const float* __re
                 const float t = cv[kTh0 + ch] - w[(kTh0 + ch) * kWin + q];
                 const float t2 = t * t;
                 const float W = (t2 + vthB) / fmaxf(t2 + cv[kVth0 + ch] + vthB, 1.0e-6f);
-                const float T = sqrtf(0.5f / (1.0f - W) - 1.0f);
+                const float x = 0.5f / (1.0f - W) - 1.0f;
                 const float up = cv[kU0 + ch] + w[(kU0 + ch) * kWin + q];
                 const float nu = up * up / (cv[kL0 + ch] + w[(kL0 + ch) * kWin + q]);
-                pass = pass && (T < tq[t_index(nu)]);
+                pass &= !(x < 0.0f) & (x < tq[t_index(nu)]);
             }
             if (!pass) continue;
             // ComputeSVGFWeight (denoise.cuh:185-245)

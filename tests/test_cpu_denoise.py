@@ -134,3 +134,18 @@ def test_bilateral_lowers_noise_within_a_region():
     out = oracle.dn_bilateral(noisy, g, st, w, h, np.load(FIXTURE)).reshape(h, w, 3)
     region = (slice(4, h), slice(0, w // 2 - 4))
     assert np.std(out[region]) < 0.5 * np.std(noisy[region])
+
+
+def test_sqrt_thresholds_decide_the_t_test_exactly():
+    """The filter compares x < threshold instead of sqrtf(x) < quantile."""
+    body = open(TABLE_H).read()
+    b = body.split("kTQuantileSqrtThreshold[kTQuantiles] = {", 1)[1].split("}", 1)[0]
+    thr = np.array([float.fromhex(v.strip().rstrip("f")) for v in b.split(",") if v.strip()], np.float32)
+    q = t_table()
+    assert np.all(np.sqrt(thr) >= q) and np.all(np.sqrt(np.nextafter(thr, np.float32(0))) < q)
+    rng = np.random.default_rng(1)
+    for k in range(0, 1024, 31):
+        xs = (thr[k] * (1 + rng.uniform(-1e-5, 1e-5, 4000))).astype(np.float32)
+        xs = np.concatenate([xs, np.float32([0.0, -0.0, -1e-30, np.inf, np.nan])])
+        with np.errstate(invalid="ignore"):
+            assert np.array_equal(np.sqrt(xs) < q[k], ~(xs < 0) & (xs < thr[k]))
