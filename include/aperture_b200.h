@@ -557,7 +557,9 @@ ar_status ar_denoise_record(const float* hits, const float* samples, size_t n, a
  * neighbour whose guide weight is not a number (a pixel whose primary ray
  * never hit has a zero normal) contributes nothing.  hdr_in and hdr_out:
  * width*height*3 floats; all pointers on the device; hdr_out must not alias
- * hdr_in. */
+ * hdr_in.  The call takes 32 bytes per pixel of stream-ordered scratch
+ * (cudaMallocAsync / cudaFreeAsync on `stream`) for the tap mask between its
+ * two passes. */
 ar_status ar_denoise_bilateral(const float* hdr_in, float* hdr_out, const ar_screen_gbuffer* gbuffer,
                                const ar_screen_stats* stats, int32_t width, int32_t height, void* stream);
 
