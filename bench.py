@@ -598,7 +598,7 @@ def profile_queues() -> None:
 
 def profile_denoise() -> None:
     """Two recorded frames of the headline scene at 1920x1080, then three
-    bilateral-filter launches (for ncu captures of k_bilateral)."""
+    bilateral-filter calls (for ncu captures of k_dn_ttest and k_dn_filter)."""
     import torch
     dev = torch.device("cuda", 0)
     stream = torch.cuda.Stream(device=dev)
