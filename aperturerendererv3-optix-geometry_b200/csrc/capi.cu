@@ -254,6 +254,10 @@ ar_status check_params(const ar_render_params* p)
         return fail(AR_ERR_INVALID_ARGUMENT, "spectral must be 0, 1 or 4");
     if (p->tri_light_nee != 0 && p->tri_light_nee != 1)
         return fail(AR_ERR_INVALID_ARGUMENT, "tri_light_nee must be 0 or 1");
+    if (p->sort_rays != 0)
+        return fail(AR_ERR_UNSUPPORTED,
+                    "sort_rays: only 0 is supported (paths are always shaded in material buckets; a direction-octant "
+                    "sort of the extension rays is not built)");
     return AR_OK;
 }
 

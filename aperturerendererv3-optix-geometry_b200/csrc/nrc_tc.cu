@@ -265,7 +265,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nrc_infer_tc(NrcNet net, cons
             }
         }
     }
-    if (failed) atomicOr(err, 2);
+    if (failed) {
+        // A layer's MMAs did not complete within the wait limit and may still be
+        // writing this CTA's tensor-memory columns: wait for that commit once more
+        // (bounded) before the columns are released to other CTAs.  Error bit 2
+        // marks every output of the launch as invalid.
+        uint32_t spins = 0;
+        while (!mbar_try_wait(mb, phase ^ 1u) && ++spins < 4u * kTcSpinLimit) {
+        }
+        atomicOr(err, 2);
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(tmem), "r"(kTcCols) : "memory");

@@ -98,9 +98,6 @@ extern "C" ar_status ar_trace_rays_static(const ar_scene* scene, const float* ra
     if (!rays || !hit_object) return set_error(AR_ERR_INVALID_ARGUMENT, "rays/hit_object is NULL");
     if (reinterpret_cast<uintptr_t>(rays) & 15u)
         return set_error(AR_ERR_INVALID_ARGUMENT, "ray buffer must be 16-byte aligned device memory");
-    if (n > static_cast<size_t>(INT_MAX))
-        return set_error(AR_ERR_INVALID_ARGUMENT,
-                         "ar_trace_rays_static takes at most 2147483647 rays per call; split the batch");
     if (device < 0 || device >= 256) return set_error(AR_ERR_UNSUPPORTED, "device index above 255");
     int prev = 0;
     if (cudaGetDevice(&prev) != cudaSuccess) {
@@ -139,30 +136,51 @@ extern "C" ar_status ar_trace_rays_static(const ar_scene* scene, const float* ra
         blocks = g_blocks_of_device[device];
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    cudaError_t e = cudaMemsetAsync(scratch, 0, kStaticHeaderBytes, st);  // work counter and error word
-    if (e == cudaSuccess) {
-        const size_t smem = static_cast<size_t>(kStackShared) * kTraceBlock * 4;
-        if (view.num_sdf > 0) {
-            StaticRaysIO<true> io;
-            io.rays = reinterpret_cast<const float4*>(rays);
-            io.out_obj = hit_object;
-            io.out_t = hit_t;
-            io.any = any_hit ? 1 : 0;
-            if (any_hit) k_trace_rays_static<true, true><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
-            else k_trace_rays_static<false, true><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
-        } else {
-            StaticRaysIO<false> io;
-            io.rays = reinterpret_cast<const float4*>(rays);
-            io.out_obj = hit_object;
-            io.out_t = hit_t;
-            io.any = any_hit ? 1 : 0;
-            if (any_hit) k_trace_rays_static<true, false><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
-            else k_trace_rays_static<false, false><<<blocks, kTraceBlock, smem, st>>>(view, io, static_cast<int>(n), scratch);
+    const size_t smem = static_cast<size_t>(kStackShared) * kTraceBlock * 4;
+    // The work counter is a 32-bit int that the last fetches of every warp can
+    // carry past the ray count by up to 32 x 4 warps x blocks: chunks of 2^30
+    // rays keep it far below INT_MAX.  The header (counter and error word) is
+    // cleared before each chunk, so with several chunks each chunk's error
+    // word is read back before the next clear.
+    const size_t chunk = size_t(1) << 30;
+    cudaError_t e = cudaSuccess;
+    int err_any = 0;
+    for (size_t first = 0; first < n && e == cudaSuccess && err_any == 0; first += chunk) {
+        const int cnt = static_cast<int>(std::min(chunk, n - first));
+        const float4* r4 = reinterpret_cast<const float4*>(rays) + 2 * first;
+        int32_t* obj = hit_object + first;
+        float* tt = hit_t ? hit_t + first : nullptr;
+        e = cudaMemsetAsync(scratch, 0, kStaticHeaderBytes, st);  // work counter and error word
+        if (e == cudaSuccess) {
+            if (view.num_sdf > 0) {
+                StaticRaysIO<true> io;
+                io.rays = r4;
+                io.out_obj = obj;
+                io.out_t = tt;
+                io.any = any_hit ? 1 : 0;
+                if (any_hit) k_trace_rays_static<true, true><<<blocks, kTraceBlock, smem, st>>>(view, io, cnt, scratch);
+                else k_trace_rays_static<false, true><<<blocks, kTraceBlock, smem, st>>>(view, io, cnt, scratch);
+            } else {
+                StaticRaysIO<false> io;
+                io.rays = r4;
+                io.out_obj = obj;
+                io.out_t = tt;
+                io.any = any_hit ? 1 : 0;
+                if (any_hit) k_trace_rays_static<true, false><<<blocks, kTraceBlock, smem, st>>>(view, io, cnt, scratch);
+                else k_trace_rays_static<false, false><<<blocks, kTraceBlock, smem, st>>>(view, io, cnt, scratch);
+            }
+            e = cudaGetLastError();
         }
-        e = cudaGetLastError();
+        if (n > chunk) {  // several chunks: read this chunk's error word before the next clear
+            int w = 0;
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&w, scratch + 4, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            err_any |= w;
+        }
     }
-    int err_word = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&err_word, scratch + 4, sizeof(int), cudaMemcpyDeviceToHost, st);
+    int err_word = err_any;
+    if (e == cudaSuccess && n <= chunk)
+        e = cudaMemcpyAsync(&err_word, scratch + 4, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         cudaGetLastError();

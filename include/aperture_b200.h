@@ -124,8 +124,9 @@ typedef struct ar_render_params {
     int32_t sky;           /* 1 = SkyLighting, 0 = DISABLE_SKYLIGHT                  */
     int32_t frame_offset;  /* TOTAL_FRAME_INDEX of the first sample                  */
     uint64_t seed;         /* GLOBAL_SEED (reference: 0x9e3779b97f4a7c15)            */
-    int32_t sort_rays;     /* reserved (accepted, no effect): shading is always ordered
-                              by material bucket; see the design notes on ray sorting */
+    int32_t sort_rays;     /* must be 0 (other values: AR_ERR_UNSUPPORTED).  Paths are
+                              always shaded in material buckets; a direction-octant
+                              sort of the extension rays is not built (measured slower) */
     int32_t wave_paths;    /* paths in flight per wave; 0 = automatic                */
     int32_t spectral;      /* 1 = USE_SPECTRUM_RENDERING: one hero wavelength per path
                               (SampleCIE1931), output linear CIE XYZ; needs
@@ -240,12 +241,15 @@ ar_status ar_trace_rays(ar_scene* scene, const float* rays, size_t n, int32_t an
  * the traversal-stack overflow of its persistent threads) is one file-scope
  * __device__ array of 16 MiB that each GPU loading the library holds until the
  * process exits.  rays, hit_object and hit_t (may be NULL) are device
- * pointers; rays 16-byte aligned; at most 2147483647 rays per call (larger
- * batches are rejected with AR_ERR_INVALID_ARGUMENT: split them).  The first
- * call on a device looks up the array's address (cudaGetSymbolAddress); make
- * it before any stream capture.  All calls share the array: calls whose work
- * overlaps on the GPU race -- serialise them (one stream).  Returns after the
- * queries finished (synchronises `stream`).  No counterpart in the reference. */
+ * pointers; rays 16-byte aligned; batches above 2^30 rays run as several
+ * launches of at most 2^30.  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress); make it before any stream capture.  All
+ * calls share the array: calls whose work overlaps on the GPU race --
+ * serialise them (one stream).  Returns after the queries finished
+ * (synchronises `stream`).  While another thread captures a CUDA graph in the
+ * global capture mode, pass a stream created with cudaStreamNonBlocking: work
+ * on the legacy default stream synchronises with every blocking stream, which
+ * invalidates that capture.  No counterpart in the reference. */
 ar_status ar_trace_rays_static(const ar_scene* scene, const float* rays, size_t n, int32_t any_hit,
                                int32_t* hit_object, float* hit_t, void* stream);
 

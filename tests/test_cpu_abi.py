@@ -96,6 +96,18 @@ def test_null_arguments_are_rejected(lib):
     lib.ar_scene_destroy(None)  # no-op
 
 
+def test_sort_rays_is_rejected(lib):
+    """Ray sorting beyond material buckets is not built: asking for it fails
+    with AR_ERR_UNSUPPORTED instead of being ignored (checked on the parameter
+    path shared by every render entry point, before any device work)."""
+    cam = scenes.box_camera(8, 8)
+    p = ab.make_params(spp=1, sort_rays=1)
+    out = np.zeros(64 * 4, np.float32)
+    st = lib.ar_rng_tape(ctypes.byref(cam), ctypes.byref(p), 4, out.ctypes.data, ab.MEM_HOST, None)
+    assert st == 4
+    assert b"sort_rays" in lib.ar_get_last_error_string()
+
+
 def test_scene_create_rejects_bad_input(lib):
     h = ctypes.c_void_p()
     assert lib.ar_scene_create(None, 3, 0, ctypes.byref(h)) == 1

@@ -74,3 +74,42 @@ def test_static_rejects_unaligned_rays(box_objects):
     from aperture_b200 import ArError
     with pytest.raises(ArError):
         scene.trace_rays_static(buf.data_ptr() + 4, 4, False, out.data_ptr(), None)
+
+
+def _static_once(scene, rays, any_hit, with_t):
+    import torch
+    dev = torch.device("cuda", 0)
+    r = torch.from_numpy(np.ascontiguousarray(rays, np.float32)).to(dev)
+    n = rays.shape[0]
+    obj = torch.full((n,), -7, dtype=torch.int32, device=dev)
+    t = torch.full((n,), -7.0, dtype=torch.float32, device=dev) if with_t else None
+    scene.trace_rays_static(r.data_ptr(), n, any_hit, obj.data_ptr(), t.data_ptr() if with_t else None,
+                            torch.cuda.current_stream(dev).cuda_stream)
+    torch.cuda.synchronize(dev)
+    return obj.cpu().numpy(), (t.cpu().numpy() if with_t else None)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("any_hit", [False, True])
+def test_static_matches_allocating_sdf(any_hit):
+    """Scenes with signed-distance objects run the SDF instantiations of the
+    static kernel (sphere tracing after the BVH walk); a second call passes no
+    distance buffer."""
+    objs, vols = scenes.sdf_box_scene(precision=16)
+    scene = Scene(objs, volumes=vols)
+    rays = random_rays(80_000, -0.6, 0.6, 24)
+    if any_hit:
+        rays[:, 7] = np.random.default_rng(25).uniform(0.05, 1.2, len(rays))
+    ref_obj, ref_t = scene.trace_rays(rays, any_hit=any_hit)
+    n = len(objs)
+    assert np.isin(ref_obj, [n - 2, n - 1]).sum() > 300 or any_hit
+    obj, t = _static_once(scene, rays, any_hit, True)
+    obj2, _ = _static_once(scene, rays, any_hit, False)
+    if any_hit:
+        assert np.array_equal(obj >= 0, ref_obj >= 0)
+        assert np.array_equal(obj2 >= 0, ref_obj >= 0)
+    else:
+        assert np.array_equal(obj, ref_obj)
+        assert np.array_equal(obj2, ref_obj)
+        hit = ref_obj >= 0
+        assert np.array_equal(t[hit].view(np.uint32), ref_t[hit].view(np.uint32))
