@@ -12,9 +12,12 @@ Mrays/s: closest-hit plus any-hit BVH queries per second, whole job.
 N > 1 is launched with torch.distributed.run: every rank renders the same
 image with its own sample streams (frame offset rank * spp) and the FP64
 accumulators are summed to rank 0 with one NCCL reduce per step (weak scaling).
-The reference arm times the reference method's CPU implementation of the path
-on the host cores (the reference compiled for the host when oracle/_ref holds
-it, else the C restatement in oracle/) and prints the same JSON line.
+The reference arm times the reference's own path loop on the host cores:
+CalculateRadiance and everything under it, compiled for the host from a
+build-time copy of the reference's sources (oracle/_ref/libref_path.so, made
+by `make -C oracle ref-path`; kind "reference"), or the C restatement in
+oracle/ (kind "port") where that library was not built.  It prints the same
+JSON line.
 """
 from __future__ import annotations
 
@@ -112,18 +115,28 @@ def cpu_threads() -> int:
         return os.cpu_count() or 1
 
 
-def reference_cpu_impl():
-    """The reference's own host build when oracle/_ref has it, else the C restatement."""
-    sys.path.insert(0, ORACLE)
+def reference_cpu_impl(prefer_reference: bool = True):
+    """(scene factory, kind): the reference's own path loop built for the host
+    (oracle/_ref/libref_path.so, host math library) when present and
+    preferred, else the C restatement of oracle/oracle.c."""
+    if ORACLE not in sys.path:
+        sys.path.insert(0, ORACLE)
+    if prefer_reference:
+        import reference_path
+        if reference_path.available(False):
+            return (lambda objs: reference_path.RefPathScene(objs, detmath=False)), "reference"
     import oracle
-    return oracle, "port"
+    return oracle.OracleScene, "port"
 
 
-def cpu_sample(objs, cam: Camera, params: RenderParams, target_s: float, threads: int, osc=None) -> dict:
-    """Render a bounded, image-wide sample of pixels at 1 spp on the host cores."""
-    oracle, kind = reference_cpu_impl()
+def cpu_sample(objs, cam: Camera, params: RenderParams, target_s: float, threads: int, osc=None,
+               prefer_reference: bool = True) -> dict:
+    """Render a bounded, image-wide sample of pixels at 1 spp on the host cores
+    (every step-th pixel; the step shrinks, then spp grows, until one sample
+    takes about target_s / 2 or more)."""
+    factory, kind = reference_cpu_impl(prefer_reference)
     if osc is None:
-        osc = oracle.OracleScene(objs)
+        osc = factory(objs)
     npix = cam.width * cam.height
 
     def run(step: int, spp: int):
@@ -133,7 +146,7 @@ def cpu_sample(objs, cam: Camera, params: RenderParams, target_s: float, threads
         _, e, s = osc.render_image(cam, q, 0, npix, step=step, threads=threads)
         return time.perf_counter() - t0, e, s
 
-    step, spp = 4096, 1                      # start with ~506 pixels spread over the image
+    step, spp = 16384, 1                     # start with ~127 pixels spread over the image
     while True:
         dt, e, s = run(step, spp)
         if dt >= 0.5 * target_s:
@@ -144,6 +157,41 @@ def cpu_sample(objs, cam: Camera, params: RenderParams, target_s: float, threads
             spp = max(spp + 1, int(spp * target_s / max(dt, 1e-3)))
     return {"osc": osc, "value": (e + s) / dt / 1e6, "seconds": dt, "pixels": (npix + step - 1) // step,
             "ext": e, "shadow": s, "kind": kind, "step": step, "spp": spp}
+
+
+CPU_KIND_NOTE = {
+    "reference": "the reference's CalculateRadiance (core/render/render.cuh:460-999) and all it calls, built for the "
+                 "host from its sources (oracle/ref_path_patch.py edits), host math library; per path it scans every "
+                 "object for Overlap (render.cuh:536, intersection.cuh:399-414) and traverses its own BuildBVH, whose "
+                 "triangle proxies sit at the mesh centre",
+    "port": "the C restatement (oracle/oracle.c) with its own binned-SAH BVH over triangle bounds and Overlap "
+            "once per render",
+}
+
+
+def relmse(img, ref) -> float:
+    """mean over pixels and channels of (I - I_ref)^2 / (I_ref^2 + 1e-2)"""
+    return float(((img.double() - ref) ** 2 / (ref * ref + 1e-2)).mean())
+
+
+def fp64_reference(torch, dev, scene: Scene, cam, params: RenderParams, spp: int, offset: int, stream,
+                   chunk: int = 256):
+    """Per-pixel FP64 mean of `spp` samples of the plain tracer (the per-path
+    parity-tested CUDA core), rendered in chunks into an FP64 accumulator on
+    the GPU; sample streams from frame `offset` on, disjoint from the timed
+    renders'.  Returns (image, seconds)."""
+    npix = cam.width * cam.height
+    acc = torch.zeros(npix * 3, dtype=torch.float64, device=dev)
+    out = torch.empty(npix * 3, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for k in range(0, spp, chunk):
+        q = make_params(spp=min(chunk, spp - k), max_depth=params.max_depth, rr_depth=params.rr_depth,
+                        use_nee=params.use_nee, sky=params.sky, spectral=params.spectral,
+                        frame_offset=offset + k)
+        scene.render_device(cam, q, out.data_ptr(), acc.data_ptr(), stream.cuda_stream)
+    stream.synchronize()
+    return acc / spp, time.perf_counter() - t0
 
 
 # ----------------------------------------------------------------------------- ours
@@ -258,14 +306,24 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
     return res
 
 
-def _timed_render(scene: Scene, cam, params, out, stream) -> dict:
+def _timed_render(torch, dev, scene: Scene, cam, params, out, stream, ref_spp: int = 4096) -> dict:
+    """One warm-up render, one render timed by the library's CUDA events, then
+    the relMSE of the timed render's image against an FP64 image of ref_spp
+    samples of the same tracer (outside the timing)."""
     scene.render_device(cam, params, out.data_ptr(), None, stream.cuda_stream, RenderStats())   # warm-up
     st = RenderStats()
     scene.render_device(cam, params, out.data_ptr(), None, stream.cuda_stream, st)
     stream.synchronize()
     rays = st.extension_rays + st.shadow_rays
-    return {"ms": round(st.total_ms, 3), "mrays_per_s": round(rays / (st.total_ms / 1e3) / 1e6, 1),
-            "msamples_per_s": round(st.paths / (st.total_ms / 1e3) / 1e6, 2), "paths": st.paths, "rays": rays}
+    res = {"ms": round(st.total_ms, 3), "mrays_per_s": round(rays / (st.total_ms / 1e3) / 1e6, 1),
+           "msamples_per_s": round(st.paths / (st.total_ms / 1e3) / 1e6, 2), "paths": st.paths, "rays": rays}
+    if ref_spp:
+        npix = cam.width * cam.height
+        ref, secs = fp64_reference(torch, dev, scene, cam, params, ref_spp, 50_000_000, stream)
+        res["relmse"] = relmse(out[: npix * 3], ref)
+        res["relmse_oracle"] = f"FP64 per-pixel mean of {ref_spp} spp of the same tracer, disjoint sample streams " \
+                               f"({secs:.1f} s)"
+    return res
 
 
 def measure_denoise(torch, dev, stream, scene: Scene, frames: int = 8, reps: int = 10) -> dict:
@@ -320,7 +378,7 @@ def measure_configs(torch, dev, stream, c5_jobs: int) -> dict:
     res = {}
     out = torch.empty(1280 * 720 * 3, dtype=torch.float32, device=dev)
     sc1 = Scene(scenes.box_scene(), device=dev.index)
-    r = _timed_render(sc1, scenes.box_camera(256, 256), make_params(spp=16, max_depth=8), out, stream)
+    r = _timed_render(torch, dev, sc1, scenes.box_camera(256, 256), make_params(spp=16, max_depth=8), out, stream)
     res["config1"] = dict(workload="box scene (34 triangles + cube light), 256x256, 16 spp, depth 8, RGB", **r)
     spectral = spectral_tables.available()
     objs, vols, med = scenes.medium_box_scene(precision=16, grid=256, medium_grid=128)
@@ -328,7 +386,7 @@ def measure_configs(torch, dev, stream, c5_jobs: int) -> dict:
     sc3.set_medium(**med)
     if spectral:
         sc3.set_spectral(64)
-    r = _timed_render(sc3, scenes.box_camera(1280, 720),
+    r = _timed_render(torch, dev, sc3, scenes.box_camera(1280, 720),
                       make_params(spp=256, max_depth=16, spectral=4 if spectral else 0), out, stream)
     res["config3"] = dict(workload="box + glass analytic torus + GGX torus on a 256^3 half SDF grid + 128^3 half fBm "
                                    "medium (sigma_t 2, albedo 0.8, g 0.3), 1280x720, 256 spp, depth 16, "
@@ -512,6 +570,11 @@ def run_ours(args) -> None:
             "gpu_launches": int(tot["launches"]),
             "clocks": clocks,
         }
+        ref_img, ref_s = fp64_reference(torch, dev, scene, cam, params, 4096, 50_000_000, stream)
+        line["relmse"] = relmse(out, ref_img)
+        line["relmse_oracle"] = (f"FP64 per-pixel mean of 4096 spp of the same tracer (sample streams disjoint from "
+                                 f"the timed renders', {ref_s:.1f} s); relMSE of one timed step's 64-spp image")
+        del ref_img
         if world == 1 and args.nrc != "off":
             line["nrc"] = measure_nrc(torch, dev, scene, args.nrc, stream)
         if world == 1 and args.configs > 0:
@@ -520,10 +583,16 @@ def run_ours(args) -> None:
             line["denoise"] = measure_denoise(torch, dev, stream, scene)
         if world == 1 and not args.no_cpu:
             cs = cpu_sample(objs, cam, params, args.cpu_seconds, cpu_threads())
-            line["cpu_baseline"] = {"value": round(cs["value"], 4), "unit": "Mrays/s", "cores": cpu_threads(),
-                                    "kind": cs["kind"],
+            line["cpu_baseline"] = {"value": round(cs["value"], 6), "unit": "Mrays/s", "cores": cpu_threads(),
+                                    "kind": cs["kind"], "what": CPU_KIND_NOTE[cs["kind"]],
                                     "sample": f"{cs['pixels']} pixels spread over the image (every {cs['step']}. pixel) at {cs['spp']} spp, "
                                               f"{cs['ext'] + cs['shadow']} queries in {cs['seconds']:.1f} s"}
+            if cs["kind"] == "reference":
+                cp = cpu_sample(objs, cam, params, min(args.cpu_seconds, 6.0), cpu_threads(), prefer_reference=False)
+                line["cpu_baseline_port"] = {"value": round(cp["value"], 4), "unit": "Mrays/s", "cores": cpu_threads(),
+                                             "kind": "port", "what": CPU_KIND_NOTE["port"],
+                                             "sample": f"{cp['pixels']} pixels at {cp['spp']} spp, "
+                                                       f"{cp['ext'] + cp['shadow']} queries in {cp['seconds']:.1f} s"}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -569,14 +638,15 @@ def run_reference(args) -> None:
             sample = cs
     value = qs / sum(secs) / 1e6
     line = {
-        "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": round(value, 6), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * sum(secs) / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
         "config": config_block(world), "impl": "reference",
-        "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": threads, "kind": sample["kind"],
+        "cpu_baseline": {"value": round(value, 6), "unit": "Mrays/s", "cores": threads, "kind": sample["kind"],
+                         "what": CPU_KIND_NOTE[sample["kind"]],
                          "sample": f"per step every {sample['step']}th pixel ({sample['pixels']} pixels) at {sample['spp']} spp "
                                    f"on {threads} host threads (OpenMP)"},
-        "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": round(value, 6), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 

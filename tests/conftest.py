@@ -49,3 +49,11 @@ def box_objects():
 def small_spheres_objects():
     import scenes
     return scenes.spheres_scene(n_spheres=120, n_lights=8, box=20.0)
+
+
+@pytest.fixture(scope="session")
+def config2_objects():
+    """Config 2 at full size: 800 icospheres x 1280 triangles, ground quad,
+    16 emissive spheres (scenes.spheres_scene() defaults)."""
+    import scenes
+    return scenes.spheres_scene()

@@ -1,0 +1,86 @@
+"""The GPU's paths against the reference's own path loop.
+
+The GPU renders with curand XORWOW as core/random.cuh:31-39 seeds it and
+records every path (ar_render_debug_paths); the reference's CalculateRadiance
+(core/render/render.cuh:460-999), compiled for the host from a build-time copy
+of its sources (oracle/_ref/libref_path*.so, see oracle/ref_path_patch.py),
+replays the same random streams from the GPU's tape (ar_rng_tape).
+
+The reference leaves a default G-buffer on triangle hits (white, no emission,
+core/render/intersection.cuh:17, 63) and uses its own first-found tie rule;
+the GPU core shades triangles with their materials and sends ties to the lower
+object index.  The GPU therefore renders the scene whose triangle materials
+equal that default G-buffer, and the reference the scene as given -- the same
+light transport.  Against the reference built with the oracle's fixed
+transcendental functions every path must agree bit for bit (hit object per
+segment, segments, uniforms, shadow rays and their depths, radiance); against
+the reference built with the host math library the path structure must agree
+on >= 99.9 % of the paths and radiance within 1e-5 relative on >= 98.5 % of
+them (last-ulp differences of the math libraries, amplified along a path).
+
+Skipped where the reference libraries were not built (no reference sources
+when `make -C oracle ref-path` ran).
+"""
+import numpy as np
+import pytest
+
+import reference_path
+import scenes
+from aperture_b200 import Scene, make_params, rng_tape
+
+from test_cpu_reference_path_pin import default_gbuffer_materials
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (reference_path.available(True) and reference_path.available(False)),
+                                 reason="reference path libraries not built")]
+
+FIELDS = ("segments", "uniforms", "nee_rays", "nee_depth_mask")
+
+
+def _run(objs, cam, params, per_path=768):
+    g = Scene(default_gbuffer_materials(objs)).debug_paths(cam, params)
+    tape = rng_tape(cam, params, per_path)
+    det, ov = reference_path.RefPathScene(objs, detmath=True).render_paths(cam, params, tape)
+    assert ov == 0, "tape too short"
+    host, ov = reference_path.RefPathScene(objs, detmath=False).render_paths(cam, params, tape)
+    assert ov == 0
+    return g, det, host
+
+
+def _check(g, det, host):
+    for f in FIELDS:
+        bad = np.nonzero(g[f] != det[f])[0]
+        assert bad.size == 0, f"{f}: {bad.size} paths differ, first {bad[:5]}"
+    assert np.array_equal(g["hit_object"], det["hit_object"])
+    assert np.array_equal(g["radiance"].view(np.uint32), det["radiance"].view(np.uint32))
+    same = np.all(g["hit_object"] == host["hit_object"], axis=1)
+    for f in FIELDS:
+        same &= g[f] == host[f]
+    assert same.mean() >= 0.999
+    a, b = g["radiance"].astype(np.float64), host["radiance"].astype(np.float64)
+    err = np.abs(a - b) / np.maximum(np.abs(b), 1e-30)
+    err[(a == 0) & (b == 0)] = 0.0
+    assert (err[same].max(axis=1) <= 1e-5).mean() >= 0.985
+
+
+def test_box_paths_equal_reference_loop(box_objects):
+    g, det, host = _run(box_objects, scenes.box_camera(48, 48), make_params(spp=2, max_depth=8))
+    _check(g, det, host)
+    assert g["segments"].sum() > 15000 and g["nee_rays"].sum() > 10000
+
+
+def test_sphere_field_paths_equal_reference_loop():
+    objs = scenes.spheres_scene(n_spheres=200, n_lights=8, box=60.0, subdivisions=2)
+    cam = scenes.spheres_camera(64, 36)
+    cam.position.z = -35.0
+    g, det, host = _run(objs, cam, make_params(spp=2, max_depth=12))
+    _check(g, det, host)
+    assert g["nee_rays"].sum() > 1000
+
+
+def test_config2_scene_paths_equal_reference_loop(config2_objects):
+    """Config 2 at full size: 800 icospheres x 1280 triangles + ground + 16
+    light spheres (1,024,018 objects), 2,592 paths at depth 12."""
+    cam = scenes.spheres_camera(48, 27)
+    g, det, host = _run(config2_objects, cam, make_params(spp=2, max_depth=12))
+    _check(g, det, host)
