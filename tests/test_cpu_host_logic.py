@@ -93,3 +93,88 @@ def test_two_rank_render_sums_to_single_render(tmp_path):
     t, rays = open(out + ".txt").read().split()
     assert float(t) == 11.0                    # slowest rank
     assert float(rays) == float(e + s)         # queries add over ranks
+
+
+def test_partition_jobs_is_lpt():
+    from sharding import partition_jobs
+    costs = [7, 5, 4, 4, 3, 3, 2, 1]
+    parts = partition_jobs(costs, 3)
+    assert sorted(j for p in parts for j in p) == list(range(len(costs)))
+    loads = [sum(costs[j] for j in p) for p in parts]
+    assert max(loads) == 10 and min(loads) == 9          # LPT on this instance: 10, 10, 9 or better
+    assert partition_jobs(costs, 1) == [list(range(len(costs)))]
+    assert partition_jobs([], 4) == [[], [], [], []]
+    # Graham's bound on random instances, against the trivial lower bound
+    rng = np.random.default_rng(3)
+    for _ in range(50):
+        c = rng.exponential(1.0, int(rng.integers(1, 40))).tolist()
+        w = int(rng.integers(1, 9))
+        p = partition_jobs(c, w)
+        mk = max(sum(c[j] for j in q) for q in p)
+        assert mk <= (4.0 / 3.0) * max(sum(c) / w, max(c)) + 1e-9
+
+
+def _batch_rank_main(rank, world, port, out_dir):
+    import os
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+
+    import oracle
+    import scenes
+    from aperture_b200 import make_params
+    from sharding import job_cost, job_totals, partition_jobs
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        jobs = _batch_jobs()
+        parts = partition_jobs([job_cost(w, h, spp) for (w, h, spp, _) in jobs], world)
+        rays = 0
+        for j in parts[rank]:
+            w, h, spp, seed = jobs[j]
+            acc, e, s = oracle.OracleScene(scenes.box_scene(seed=seed)).render_image(
+                scenes.box_camera(w, h), make_params(spp=spp, max_depth=5), threads=1)
+            rays += e + s
+            np.save(os.path.join(out_dir, f"job{j}_rank{rank}.npy"), acc)
+        t, (total,) = job_totals(float(len(parts[rank])), [rays], dist, torch.device("cpu"))
+        if rank == 0:
+            with open(os.path.join(out_dir, "totals.txt"), "w") as f:
+                f.write(f"{t} {total}\n")
+    finally:
+        dist.destroy_process_group()
+
+
+def _batch_jobs():
+    return [(8, 6, 2, 0xA11CE + 11), (5, 5, 4, 0xA11CE + 12), (12, 4, 1, 0xA11CE + 13), (6, 6, 3, 0xA11CE + 14),
+            (4, 4, 1, 0xA11CE + 15)]
+
+
+def test_two_rank_batch_partition_renders_every_job_once(tmp_path):
+    """Jobs split by partition_jobs over two gloo ranks: every job rendered by
+    exactly one rank, its image equal to a single-process render, no
+    collective on the data path (only the job-time max and ray count sum)."""
+    import os
+
+    import torch.multiprocessing as mp
+
+    import oracle
+    import scenes
+    from aperture_b200 import make_params
+
+    world = 2
+    mp.start_processes(_batch_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       start_method="spawn", join=True)
+    jobs = _batch_jobs()
+    files = sorted(os.listdir(tmp_path))
+    for j, (w, h, spp, seed) in enumerate(jobs):
+        mine = [f for f in files if f.startswith(f"job{j}_")]
+        assert len(mine) == 1, (j, mine)
+        got = np.load(os.path.join(tmp_path, mine[0]))
+        acc, _, _ = oracle.OracleScene(scenes.box_scene(seed=seed)).render_image(
+            scenes.box_camera(w, h), make_params(spp=spp, max_depth=5), threads=1)
+        np.testing.assert_array_equal(got, acc)
+    ranks = {f.split("_rank")[1].split(".")[0] for f in files if f.startswith("job")}
+    assert ranks == {"0", "1"}
