@@ -195,8 +195,8 @@ EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create",
                     "ar_scene_set_medium", "ar_nrc_create", "ar_nrc_destroy", "ar_nrc_render_frame",
                     "ar_nrc_get_params", "ar_nrc_set_params", "ar_nrc_infer", "ar_nrc_train", "ar_nrc_gradients",
                     "ar_batch_autotune", "ar_nrc_set_option", "ar_guide_create", "ar_guide_destroy", "ar_guide_render_frame",
-                    "ar_guide_get_stats", "ar_guide_get_probe", "ar_render_frame_denoise", "ar_denoise_record",
-                    "ar_denoise_bilateral")
+                    "ar_guide_get_stats", "ar_guide_get_probe", "ar_guide_probe_eval", "ar_render_frame_denoise",
+                    "ar_denoise_record", "ar_denoise_bilateral")
 
 
 class ArError(RuntimeError):
@@ -257,7 +257,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_guide_render_frame.argtypes = [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p, c_void_p]
     lib.ar_guide_get_stats.argtypes = [c_void_p, POINTER(GuideStats)]
     lib.ar_guide_get_probe.argtypes = [c_void_p, c_int32, c_void_p]
-    for f in ("ar_guide_create", "ar_guide_destroy", "ar_guide_render_frame", "ar_guide_get_stats", "ar_guide_get_probe"):
+    lib.ar_guide_probe_eval.argtypes = [c_void_p, c_int32] + [c_void_p] * 6 + [c_int64] + [c_void_p] * 4
+    for f in ("ar_guide_create", "ar_guide_destroy", "ar_guide_render_frame", "ar_guide_get_stats", "ar_guide_get_probe",
+              "ar_guide_probe_eval"):
         getattr(lib, f).restype = c_int32
     lib.ar_render_frame_denoise.argtypes = [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p,
                                             c_void_p, c_void_p, c_void_p]
@@ -611,6 +613,25 @@ def denoise_bilateral(hdr_in, hdr_out, gbuffer, stats, width: int, height: int, 
     load_library()
     _check(_lib.ar_denoise_bilateral(_dptr(hdr_in), _dptr(hdr_out), _dptr(gbuffer), _dptr(stats), width, height,
                                      c_void_p(stream)))
+
+
+def guide_probe_eval(texels: np.ndarray, probe_of, normal, query, u5, eval_dir, pos):
+    """ar_guide_probe_eval on host arrays: texels [nprobes, 85, 4]; per query
+    probe index, normal, texel weights, 5 uniforms, evaluation direction and
+    point.  Returns (sample directions [n, 3], sample pdfs, pdfs of eval_dir,
+    (voxel, face) keys as uint64)."""
+    load_library()
+    t = np.ascontiguousarray(texels, np.float32).reshape(-1, 85, 4)
+    po = np.ascontiguousarray(probe_of, np.int32).reshape(-1)
+    n = len(po)
+    arrs = [np.ascontiguousarray(a, np.float32).reshape(n, -1) for a in (normal, query, u5, eval_dir, pos)]
+    d = np.empty((n, 3), np.float32)
+    p = np.empty(n, np.float32)
+    e = np.empty(n, np.float32)
+    k = np.empty(n, np.uint64)
+    _check(_lib.ar_guide_probe_eval(_ptr(t), len(t), _ptr(po), *[_ptr(a) for a in arrs], n, _ptr(d), _ptr(p), _ptr(e),
+                                    _ptr(k)))
+    return d, p, e, k
 
 
 class PathGuide:

@@ -1324,7 +1324,7 @@ ar_status ar_nrc_render_frame(ar_nrc* c, const ar_camera* cam, const ar_render_p
     if (!c) return fail(AR_ERR_INVALID_ARGUMENT, "cache is NULL");
     if (ar_status e = check_camera(cam)) return e;
     if (ar_status e = check_params(p)) return e;
-    if (p->spp != 1) return fail(AR_ERR_INVALID_ARGUMENT, "cache frames take spp = 1");
+    if (p->spp > 64) return fail(AR_ERR_INVALID_ARGUMENT, "cache frames take 1 to 64 samples per pixel");
     if (p->spectral) return fail(AR_ERR_UNSUPPORTED, "the cache is RGB only");
     if (!out_rgb && !accum) return fail(AR_ERR_INVALID_ARGUMENT, "out_rgb and accum are both NULL");
     AR_GUARD_BEGIN
@@ -1332,7 +1332,7 @@ ar_status ar_nrc_render_frame(ar_nrc* c, const ar_camera* cam, const ar_render_p
     DeviceGuard g(s->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int64_t npix = static_cast<int64_t>(cam->width) * cam->height;
-    nrc_ensure_queries(c, npix);
+    nrc_ensure_queries(c, npix * p->spp);   // at most one cache query per path
     ck(cudaMemsetAsync(c->counters, 0, sizeof(int32_t) * (static_cast<size_t>(c->slots) + 2), st), "memset");
     if (stats) ck(cudaMemsetAsync(c->T.loss, 0, sizeof(float), st), "memset");
     ar::NrcFrame f{};
@@ -1361,7 +1361,7 @@ ar_status ar_nrc_render_frame(ar_nrc* c, const ar_camera* cam, const ar_render_p
     if (train) nrc_train_steps(c, c->samples, c->counters + 1, c->cfg.train_steps, st);
     ck(cudaEventRecord(c->ev[3], st), "event");
     const int64_t n = npix * 3;
-    if (out_rgb) ck(ar::launch_mean(s->accum, n, 1.0, out_rgb, st), "mean");
+    if (out_rgb) ck(ar::launch_mean(s->accum, n, 1.0 / static_cast<double>(p->spp), out_rgb, st), "mean");
     if (accum) ck(ar::launch_add(s->accum, n, accum, st), "accumulate");
     if (stats) {
         int32_t cnt[2];
@@ -1690,7 +1690,7 @@ ar_status ar_guide_render_frame(ar_guide* g, const ar_camera* cam, const ar_rend
     ck(ar::pg_update(g->view, s->sm_count, st), "guiding update");
     ++g->frames;
     const int64_t n = npix * 3;
-    if (out_rgb) ck(ar::launch_mean(s->accum, n, 1.0, out_rgb, st), "mean");
+    if (out_rgb) ck(ar::launch_mean(s->accum, n, 1.0 / static_cast<double>(p->spp), out_rgb, st), "mean");
     if (accum) ck(ar::launch_add(s->accum, n, accum, st), "accumulate");
     return check_err(s, st);
     AR_GUARD_END
@@ -1749,6 +1749,70 @@ ar_status ar_guide_get_probe(const ar_guide* g, int32_t index, float* texels)
     if (index < 0 || index >= std::min(c[0], g->view.capacity)) return fail(AR_ERR_INVALID_ARGUMENT, "probe not allocated");
     ck(cudaMemcpy(texels, g->view.probes + static_cast<size_t>(index) * ar::kPgStride, sizeof(float4) * ar::kPgStride,
                   cudaMemcpyDeviceToHost), "copy probe");
+    return AR_OK;
+    AR_GUARD_END
+}
+
+ar_status ar_guide_probe_eval(const float* texels, int32_t nprobes, const int32_t* probe_of, const float* normal3,
+                              const float* query3, const float* u5, const float* eval3, const float* pos3, int64_t n,
+                              float* out_dir3, float* out_pdf, float* out_eval_pdf, uint64_t* out_key)
+{
+    g_last_error.clear();
+    if (n < 0 || nprobes <= 0) return fail(AR_ERR_INVALID_ARGUMENT, "n must be >= 0 and nprobes > 0");
+    if (n == 0) return AR_OK;
+    if (!texels || !probe_of || !normal3 || !query3 || !u5 || !eval3 || !pos3 || !out_dir3 || !out_pdf ||
+        !out_eval_pdf || !out_key)
+        return fail(AR_ERR_INVALID_ARGUMENT, "NULL argument");
+    for (int64_t i = 0; i < n; ++i)
+        if (probe_of[i] < 0 || probe_of[i] >= nprobes) return fail(AR_ERR_INVALID_ARGUMENT, "probe index out of range");
+    AR_GUARD_BEGIN
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(AR_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    const size_t m = static_cast<size_t>(n);
+    std::vector<float4> padded(static_cast<size_t>(nprobes) * ar::kPgStride, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+    for (int32_t p = 0; p < nprobes; ++p)
+        for (int t = 0; t < ar::kPgTexels; ++t) {
+            const float* src = texels + (static_cast<size_t>(p) * ar::kPgTexels + t) * 4;
+            padded[static_cast<size_t>(p) * ar::kPgStride + t] = make_float4(src[0], src[1], src[2], src[3]);
+        }
+    float faces[60];
+    ar::pg_face_normals(faces);
+    std::vector<void*> tmp;
+    struct Free {
+        std::vector<void*>& v;
+        ~Free() { for (void* p : v) cudaFree(p); }
+    } fr{tmp};
+    auto up = [&](const void* src, size_t bytes) {
+        void* d = dalloc<unsigned char>(bytes, "probe eval input");
+        tmp.push_back(d);
+        ck(cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice), "copy probe eval input");
+        return d;
+    };
+    auto dn = [&](size_t bytes) {
+        void* d = dalloc<unsigned char>(bytes, "probe eval output");
+        tmp.push_back(d);
+        return d;
+    };
+    const float4* dp = static_cast<const float4*>(up(padded.data(), padded.size() * sizeof(float4)));
+    const int32_t* dpo = static_cast<const int32_t*>(up(probe_of, m * 4));
+    const float* dn3 = static_cast<const float*>(up(normal3, m * 12));
+    const float* dq3 = static_cast<const float*>(up(query3, m * 12));
+    const float* du5 = static_cast<const float*>(up(u5, m * 20));
+    const float* de3 = static_cast<const float*>(up(eval3, m * 12));
+    const float* dp3 = static_cast<const float*>(up(pos3, m * 12));
+    const float* dfc = static_cast<const float*>(up(faces, sizeof(faces)));
+    float* odir = static_cast<float*>(dn(m * 12));
+    float* opdf = static_cast<float*>(dn(m * 4));
+    float* oepdf = static_cast<float*>(dn(m * 4));
+    unsigned long long* okey = static_cast<unsigned long long*>(dn(m * 8));
+    ck(ar::pg_eval(dp, dpo, dn3, dq3, du5, de3, dp3, n, dfc, odir, opdf, oepdf, okey, nullptr), "probe eval");
+    ck(cudaMemcpy(out_dir3, odir, m * 12, cudaMemcpyDeviceToHost), "copy directions");
+    ck(cudaMemcpy(out_pdf, opdf, m * 4, cudaMemcpyDeviceToHost), "copy pdfs");
+    ck(cudaMemcpy(out_eval_pdf, oepdf, m * 4, cudaMemcpyDeviceToHost), "copy pdfs");
+    ck(cudaMemcpy(out_key, okey, m * 8, cudaMemcpyDeviceToHost), "copy keys");
     return AR_OK;
     AR_GUARD_END
 }

@@ -147,34 +147,67 @@ cudaError_t pg_clear(const GuideView& g, size_t table_size, cudaStream_t st)
 // Unit normals of the 20 faces of the regular icosahedron with vertices
 // (0, +-1, +-phi) and their cyclic permutations: the normalised centroids of
 // the vertex triples at mutual distance 2, in lexicographic triple order.
+// Probe math of the queries of ar_guide_probe_eval: one thread per query.
+__global__ void k_pg_eval(const float4* probes, const int32_t* probe_of, const float* n3, const float* q3,
+                          const float* u5, const float* e3, const float* p3, int64_t n, const float* faces,
+                          float* dir3, float* pdf, float* epdf, unsigned long long* key)
+{
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const float4* pr = probes + static_cast<int64_t>(probe_of[i]) * kPgStride;
+        const f3 nrm = mk(n3[3 * i], n3[3 * i + 1], n3[3 * i + 2]);
+        const f3 q = mk(q3[3 * i], q3[3 * i + 1], q3[3 * i + 2]);
+        const f3 e = mk(e3[3 * i], e3[3 * i + 1], e3[3 * i + 2]);
+        float u[5];
+        for (int k = 0; k < 5; ++k) u[k] = u5[5 * i + k];
+        float p = 0.0f;
+        const f3 w = pg_sample_hemi(pr, nrm, q, u, &p);
+        dir3[3 * i] = w.x; dir3[3 * i + 1] = w.y; dir3[3 * i + 2] = w.z;
+        pdf[i] = p;
+        epdf[i] = pg_hemi_pdf(pr, e, nrm, q);
+        key[i] = pg_key(mk(p3[3 * i], p3[3 * i + 1], p3[3 * i + 2]), e, faces);
+    }
+}
+
+cudaError_t pg_eval(const float4* probes, const int32_t* probe_of, const float* n3, const float* q3, const float* u5,
+                    const float* e3, const float* p3, int64_t n, const float* faces, float* dir3, float* pdf,
+                    float* epdf, unsigned long long* key, cudaStream_t st)
+{
+    const int grid = static_cast<int>(std::min<int64_t>((n + 255) / 256, 4096));
+    if (grid > 0) k_pg_eval<<<grid, 256, 0, st>>>(probes, probe_of, n3, q3, u5, e3, p3, n, faces, dir3, pdf, epdf, key);
+    return cudaGetLastError();
+}
+
+// The 20 face normals of the regular icosahedron in the reference's face
+// numbering (FaceNormal20FromIndex, core/guiding/guiding_bin.cuh:40-66), which
+// probe keys carry.  Each face is given by the signs of its normal's x, y, z:
+// three non-zero signs are a face on a cube diagonal, (+-1, +-1, +-1) / sqrt 3;
+// a zero at axis k puts the long component phi^2 / sqrt(1 + phi^4) on axis
+// (k + 1) % 3 and the short one 1 / sqrt(1 + phi^4) on axis (k + 2) % 3.
+// Values are computed in double and rounded once.
 void pg_face_normals(float* out60)
 {
+    static const signed char sgn[kPgFaces][3] = {
+        {-1, 1, 1}, {0, 1, 1},   {0, 1, -1},  {-1, 1, -1}, {-1, 1, 0},  {1, 1, 1},    {-1, 0, 1},
+        {-1, -1, 0}, {-1, 0, -1}, {1, 1, -1},  {1, -1, 1},  {0, -1, 1},  {0, -1, -1},  {1, -1, -1},
+        {1, -1, 0},  {1, 0, 1},   {-1, -1, 1}, {-1, -1, -1}, {1, 0, -1}, {1, 1, 0}};
     const double phi = (1.0 + std::sqrt(5.0)) / 2.0;
-    std::vector<double> v;
-    for (int s1 = -1; s1 <= 1; s1 += 2)
-        for (int s2 = -1; s2 <= 1; s2 += 2) {
-            const double a = s1, b = s2 * phi;
-            const double cyc[3][3] = {{0, a, b}, {a, b, 0}, {b, 0, a}};
-            for (auto& c : cyc) v.insert(v.end(), {c[0], c[1], c[2]});
+    const double len = std::sqrt(1.0 + phi * phi * phi * phi);
+    const double diag = 1.0 / std::sqrt(3.0), lng = phi * phi / len, shrt = 1.0 / len;
+    for (int f = 0; f < kPgFaces; ++f) {
+        int zero = -1;
+        for (int a = 0; a < 3; ++a)
+            if (sgn[f][a] == 0) zero = a;
+        double v[3];
+        if (zero < 0) {
+            for (int a = 0; a < 3; ++a) v[a] = sgn[f][a] * diag;
+        } else {
+            v[zero] = 0.0;
+            v[(zero + 1) % 3] = sgn[f][(zero + 1) % 3] * lng;
+            v[(zero + 2) % 3] = sgn[f][(zero + 2) % 3] * shrt;
         }
-    const int nv = static_cast<int>(v.size() / 3);
-    auto d2 = [&](int i, int j) {
-        double s = 0;
-        for (int k = 0; k < 3; ++k) s += (v[3 * i + k] - v[3 * j + k]) * (v[3 * i + k] - v[3 * j + k]);
-        return s;
-    };
-    int f = 0;
-    for (int i = 0; i < nv; ++i)
-        for (int j = i + 1; j < nv; ++j)
-            for (int k = j + 1; k < nv; ++k) {
-                if (std::fabs(d2(i, j) - 4.0) > 1e-9 || std::fabs(d2(j, k) - 4.0) > 1e-9 || std::fabs(d2(i, k) - 4.0) > 1e-9) continue;
-                double c[3];
-                for (int a = 0; a < 3; ++a) c[a] = v[3 * i + a] + v[3 * j + a] + v[3 * k + a];
-                const double len = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
-                if (f < kPgFaces)
-                    for (int a = 0; a < 3; ++a) out60[3 * f + a] = static_cast<float>(c[a] / len);
-                ++f;
-            }
+        for (int a = 0; a < 3; ++a) out60[3 * f + a] = static_cast<float>(v[a]);
+    }
 }
 
 }  // namespace ar

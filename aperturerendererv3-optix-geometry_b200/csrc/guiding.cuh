@@ -235,5 +235,8 @@ inline float pg_alpha(int64_t frame)
 cudaError_t pg_update(const GuideView& g, int sm_count, cudaStream_t st);
 cudaError_t pg_clear(const GuideView& g, size_t table_size, cudaStream_t st);
 void pg_face_normals(float* out60);
+cudaError_t pg_eval(const float4* probes, const int32_t* probe_of, const float* n3, const float* q3, const float* u5,
+                    const float* e3, const float* p3, int64_t n, const float* faces, float* dir3, float* pdf,
+                    float* epdf, unsigned long long* key, cudaStream_t st);
 
 }  // namespace ar

@@ -74,7 +74,7 @@ struct NrcSample {                 // a training sample: vertex + target radianc
 // Per-frame parameters of the cache inside the wavefront (FrameParams.nrc).
 struct NrcFrame {
     int32_t enabled;
-    int32_t stride, offset;        // pixel p trains when (p + offset) % stride == 0
+    int32_t stride, offset;        // sample 0 of pixel p trains when (p + offset) % stride == 0
     int32_t max_train_vertices;    // vertices recorded per training path
     float spread_c;                // terminate when spread^2 > c * a0
     int32_t query_cap, sample_cap, slots;

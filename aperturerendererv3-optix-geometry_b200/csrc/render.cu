@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                 nv.n = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
                 nv.a = make_float4(gb.albedo.x, gb.albedo.y, gb.albedo.z, 0.0f);
                 int slot;
-                if (nrc_train_slot(fp.nrc, pixel, &slot)) {
+                if (sidx == 0 && nrc_train_slot(fp.nrc, pixel, &slot)) {   // sample 0 of a training pixel
                     const int kv = fp.nrc.slot_count[slot];
                     if (kv < fp.nrc.max_train_vertices) {
                         NrcTrainVertex tv;
@@ -1011,7 +1011,7 @@ __global__ void k_retire(FrameParams fp, PathBuffers B, PoolCtl* ctl, double* ac
         // denoiser moments of the clamped sample (RecordScreenStatisticBuffer, render.cuh:988-991)
         if (fp.dn.stat) record_stats(fp.dn.stat + pixel, mk(x, y, z));
         int slot;
-        if (fp.nrc.enabled && nrc_train_slot(fp.nrc, pixel, &slot)) {
+        if (fp.nrc.enabled && rr.meta.x == 0 && nrc_train_slot(fp.nrc, pixel, &slot)) {
             // training targets: radiance gathered after each recorded vertex,
             // divided by the throughput that reached it
             const int nvtx = fp.nrc.slot_count[slot];

@@ -198,17 +198,13 @@ def fp64_reference(torch, dev, scene: Scene, cam, params: RenderParams, spp: int
 NRC_SIZES = {"small": (480, 270, 16384, 4096), "full": (1920, 1080, 16384, 4096), "box": (480, 270, 16384, 4096)}
 
 
-def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
-    """Config 4 on the config-2 scene: time to reach the plain tracer's relMSE
-    at `target` spp with the cache-terminated tracer (1 spp per frame, online
-    training), both against an FP64 oracle image of `ref` spp (plain tracer,
-    per-pixel FP64 sums on the GPU); then the 300-frame seeded spline camera
-    path at 1920x1080 (frames/s, per-stage times).  Device time (CUDA events
-    on the launching stream) excludes the relMSE evaluations.  mode "box": the
-    same time-to-relMSE measurement on the config-3 scene (box, SDF tori, fBm
-    medium, depth 16) in RGB -- the cache is RGB-only -- without the spline path."""
+def nrc_setup(torch, dev, scene: Scene, mode: str, stream) -> dict:
+    """The scene, camera and judges of a time-to-relMSE measurement: an FP64
+    oracle image of `ref` spp of the plain tracer (per-pixel FP64 sums on the
+    GPU) and the plain tracer's relMSE after `target` spp with its device
+    time.  mode "box": the config-3 scene (box, SDF tori, fBm medium, depth
+    16) in RGB; otherwise the config-2 scene."""
     w, h, ref_spp, target = NRC_SIZES[mode]
-    npix = w * h
     depth = DEPTH
     if mode == "box":
         objs, vols, med = scenes.medium_box_scene(precision=16, grid=256, medium_grid=128)
@@ -218,6 +214,7 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
         depth = 16
     else:
         cam = scenes.spheres_camera(w, h)
+    npix = w * h
     out = torch.empty(npix * 3, dtype=torch.float32, device=dev)
 
     def plain(spp_total: int, offset: int, acc):
@@ -233,77 +230,126 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream) -> dict:
             ms += e0.elapsed_time(e1)
         return ms
 
-    def relmse(acc, n, ref):
-        img = acc / n
-        return float(((img - ref) ** 2 / (ref * ref + 1e-2)).mean())
-
     with torch.cuda.stream(stream):
         acc_ref = torch.zeros(npix * 3, dtype=torch.float64, device=dev)
         ref_ms = plain(ref_spp, 10_000_000, acc_ref)
         ref = acc_ref / ref_spp
         acc_p = torch.zeros_like(acc_ref)
         plain_ms = plain(target, 20_000_000, acc_p)
-        e_plain = relmse(acc_p, target, ref)
-        cache = RadianceCache(scene, nrc_config())
-        acc_n = torch.zeros_like(acc_ref)
-        t_ms, reached, curve = 0.0, None, []
-        max_ms = 3.0 * plain_ms
-        f = 0
-        check = 16
-        while t_ms < max_ms and f < 65536:
+        e_plain = relmse_sum(acc_p, target, ref)
+    return {"scene": scene, "cam": cam, "depth": depth, "ref": ref, "ref_spp": ref_spp, "ref_ms": ref_ms,
+            "target": target, "plain_ms": plain_ms, "e_plain": e_plain, "mode": mode, "w": w, "h": h}
+
+
+def relmse_sum(acc, n, ref) -> float:
+    """relMSE of the mean of n samples whose FP64 sums are in acc"""
+    img = acc / n
+    return float(((img - ref) ** 2 / (ref * ref + 1e-2)).mean())
+
+
+def nrc_curve(torch, dev, S: dict, stream, k: int = 1, spread_c: float = 0.01, steps: int = 4,
+              max_factor: float = 3.0, seed: int = 1) -> dict:
+    """Time-to-relMSE of the cache-terminated tracer against the plain one:
+    frames of k samples per pixel (cache trained online: 65536 training paths
+    and `steps` optimiser steps of 16384 samples per frame, paths terminated
+    where the spread exceeds sqrt(spread_c) x the primary footprint), run until
+    the relMSE reaches the plain tracer's at `target` spp or the device time
+    reaches max_factor x the plain tracer's.  Device time (CUDA events on the
+    launching stream) excludes the relMSE evaluations."""
+    scene, cam, depth, ref = S["scene"], S["cam"], S["depth"], S["ref"]
+    npix = S["w"] * S["h"]
+    cache = RadianceCache(scene, nrc_config(spread_c=spread_c, train_steps=steps, seed=seed))
+    acc_n = torch.zeros(npix * 3, dtype=torch.float64, device=dev)
+    t_ms, reached, curve = 0.0, None, []
+    max_ms = max_factor * S["plain_ms"]
+    f, samples = 0, 0
+    check = max(1, 16 // k)
+    with torch.cuda.stream(stream):
+        while t_ms < max_ms and samples < 262144:
             evs = []
             for _ in range(check):
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                cache.render_frame(cam, make_params(spp=1, max_depth=depth, frame_offset=30_000_000 + f), None,
+                cache.render_frame(cam, make_params(spp=k, max_depth=depth, frame_offset=30_000_000 + samples), None,
                                    acc_n.data_ptr(), train=True, stream=stream.cuda_stream)
                 e1.record(stream)
                 evs.append((e0, e1))
                 f += 1
+                samples += k
             evs[-1][1].synchronize()
             t_ms += sum(a.elapsed_time(b) for a, b in evs)
-            e = relmse(acc_n, f, ref)
-            curve.append((f, round(t_ms, 2), e))
-            if e <= e_plain:
+            e = relmse_sum(acc_n, samples, ref)
+            curve.append((samples, round(t_ms, 2), e))
+            if e <= S["e_plain"]:
                 reached = t_ms
                 break
-            check = min(check * 2, 256)
-        best = min(c[2] for c in curve)
-        what = ("config-3 scene (box + SDF tori + fBm medium), RGB" if mode == "box"
-                else "config4 static view: config-2 scene")
-        res = {"workload": f"{what} {w}x{h}, max depth {depth}, 1 spp per frame, "
-                           f"cache trained online (65536 training paths, 4 steps of 16384 per frame)",
-               "oracle_spp": ref_spp, "oracle_ms": round(ref_ms, 1),
-               "plain_spp": target, "plain_ms": round(plain_ms, 2), "plain_relmse": e_plain,
-               "cache_frames": f, "cache_ms": round(t_ms, 2), "cache_relmse": curve[-1][2], "cache_best_relmse": best,
-               "reached": reached is not None,
-               "time_to_relmse_speedup": round(plain_ms / reached, 3) if reached else None,
-               "curve": [(a, b, round(c, 6)) for a, b, c in curve[:: max(1, len(curve) // 12)]]}
-        if mode == "box":
-            return res
-        # the spline camera path at the full config-4 resolution
-        cams = scenes.spline_cameras(frames=300)
-        acc_s = torch.zeros(1920 * 1080 * 3, dtype=torch.float64, device=dev)
-        cache2 = RadianceCache(scene, nrc_config(seed=2))
-        tot = {"render": 0.0, "infer": 0.0, "train": 0.0, "total": 0.0, "q": 0, "rays": 0}
-        for k, c in enumerate(cams):
-            st = cache2.render_frame(c, make_params(spp=1, max_depth=DEPTH, frame_offset=40_000_000 + k), None,
-                                     acc_s.data_ptr(), train=True, stats=True, stream=stream.cuda_stream)
-            if k >= 10:
-                tot["render"] += st.render_ms
-                tot["infer"] += st.infer_ms
-                tot["train"] += st.train_ms
-                tot["total"] += st.total_ms
-                tot["q"] += st.queries
-                tot["rays"] += st.extension_rays + st.shadow_rays
-        n = len(cams) - 10
-        res["spline_1920x1080"] = {
-            "frames": len(cams), "timed_frames": n, "ms_per_frame": round(tot["total"] / n, 3),
-            "render_ms": round(tot["render"] / n, 3), "infer_ms": round(tot["infer"] / n, 3),
-            "train_ms": round(tot["train"] / n, 3), "queries_per_frame": int(tot["q"] / n),
-            "tracer_mrays_per_s": round(tot["rays"] / (tot["render"] / 1e3) / 1e6, 1),
-            "last_loss": round(float(st.loss), 5)}
+            check = min(check * 2, max(1, 256 // k))
+    best = min(c[2] for c in curve)
+    return {"spp_per_frame": k, "spread_c": spread_c, "train_steps": steps, "frames": f, "samples": samples,
+            "cache_ms": round(t_ms, 2), "cache_relmse": curve[-1][2], "cache_best_relmse": best,
+            "reached": reached is not None,
+            "time_to_relmse_speedup": round(S["plain_ms"] / reached, 3) if reached else None,
+            "ms_per_sample": round(t_ms / max(samples, 1), 4),
+            "curve": [(a, b, round(c, 7)) for a, b, c in curve[:: max(1, len(curve) // 10)]]}
+
+
+def measure_nrc(torch, dev, scene: Scene, mode: str, stream, k: int = 1, spread_c: float = 0.01, steps: int = 4) -> dict:
+    """Config 4 on the config-2 scene (mode small/full) or the config-3 scene
+    in RGB (mode box): the time-to-relMSE curve of nrc_curve for one setting;
+    for the config-2 scene also the 300-frame seeded spline camera path at
+    1920x1080 (ms per frame, per-stage times)."""
+    S = nrc_setup(torch, dev, scene, mode, stream)
+    what = ("config-3 scene (box + SDF tori + fBm medium), RGB" if mode == "box"
+            else "config4 static view: config-2 scene")
+    res = {"workload": f"{what} {S['w']}x{S['h']}, max depth {S['depth']}, {k} spp per frame, cache trained online "
+                       f"(65536 training paths, {steps} steps of 16384 per frame), spread constant {spread_c}",
+           "oracle_spp": S["ref_spp"], "oracle_ms": round(S["ref_ms"], 1), "plain_spp": S["target"],
+           "plain_ms": round(S["plain_ms"], 2), "plain_relmse": S["e_plain"]}
+    res.update(nrc_curve(torch, dev, S, stream, k, spread_c, steps))
+    if mode == "box":
+        return res
+    # the spline camera path at the full config-4 resolution
+    cams = scenes.spline_cameras(frames=300)
+    acc_s = torch.zeros(1920 * 1080 * 3, dtype=torch.float64, device=dev)
+    cache2 = RadianceCache(S["scene"], nrc_config(seed=2))
+    tot = {"render": 0.0, "infer": 0.0, "train": 0.0, "total": 0.0, "q": 0, "rays": 0}
+    for j, c in enumerate(cams):
+        st = cache2.render_frame(c, make_params(spp=1, max_depth=DEPTH, frame_offset=40_000_000 + j), None,
+                                 acc_s.data_ptr(), train=True, stats=True, stream=stream.cuda_stream)
+        if j >= 10:
+            tot["render"] += st.render_ms
+            tot["infer"] += st.infer_ms
+            tot["train"] += st.train_ms
+            tot["total"] += st.total_ms
+            tot["q"] += st.queries
+            tot["rays"] += st.extension_rays + st.shadow_rays
+    n = len(cams) - 10
+    res["spline_1920x1080"] = {
+        "frames": len(cams), "timed_frames": n, "ms_per_frame": round(tot["total"] / n, 3),
+        "render_ms": round(tot["render"] / n, 3), "infer_ms": round(tot["infer"] / n, 3),
+        "train_ms": round(tot["train"] / n, 3), "queries_per_frame": int(tot["q"] / n),
+        "tracer_mrays_per_s": round(tot["rays"] / (tot["render"] / 1e3) / 1e6, 1),
+        "last_loss": round(float(st.loss), 5)}
     return res
+
+
+def sweep_nrc(torch, dev, stream, mode: str = "box") -> dict:
+    """The cache's time-to-relMSE over spp per frame {1, 4, 16} x spread
+    constant {0.01, 0.1, 1} x optimiser steps per frame {1, 4}, against one
+    oracle and one plain measurement."""
+    S = nrc_setup(torch, dev, None if mode == "box" else Scene(scenes.spheres_scene(), device=dev.index), mode,
+                  stream)
+    runs = []
+    for k in (1, 4, 16):
+        for c in (0.01, 0.1, 1.0):
+            for steps in (1, 4):
+                r = nrc_curve(torch, dev, S, stream, k, c, steps)
+                r.pop("curve")
+                runs.append(r)
+                print(json.dumps({"sweep": r}), flush=True)
+    return {"workload": f"{mode} {S['w']}x{S['h']} depth {S['depth']}", "plain_spp": S["target"],
+            "plain_ms": round(S["plain_ms"], 2), "plain_relmse": S["e_plain"], "oracle_spp": S["ref_spp"],
+            "runs": runs}
 
 
 def _timed_render(torch, dev, scene: Scene, cam, params, out, stream, ref_spp: int = 4096) -> dict:
@@ -576,7 +622,7 @@ def run_ours(args) -> None:
                                  f"the timed renders', {ref_s:.1f} s); relMSE of one timed step's 64-spp image")
         del ref_img
         if world == 1 and args.nrc != "off":
-            line["nrc"] = measure_nrc(torch, dev, scene, args.nrc, stream)
+            line["nrc"] = measure_nrc(torch, dev, scene, args.nrc, stream, args.nrc_spp, args.nrc_c, args.nrc_steps)
         if world == 1 and args.configs > 0:
             line["other_configs"] = measure_configs(torch, dev, stream, args.configs)
         if world == 1 and not args.no_denoise:
@@ -709,6 +755,11 @@ def main():
     ap.add_argument("--nrc", choices=("off", "small", "full", "box"), default="small",
                     help="radiance-cache time-to-relMSE measurement (small: 480x270, full: 1920x1080, "
                          "box: the config-3 scene in RGB at 480x270)")
+    ap.add_argument("--nrc-spp", type=int, default=1, help="samples per pixel of a cache frame")
+    ap.add_argument("--nrc-c", type=float, default=0.01, help="spread constant of the cache's termination rule")
+    ap.add_argument("--nrc-steps", type=int, default=4, help="optimiser steps per cache frame")
+    ap.add_argument("--nrc-sweep", choices=("box", "small"), default=None,
+                    help="time-to-relMSE over spp per frame x spread constant x optimiser steps, then exit")
     ap.add_argument("--profile-nrc", action="store_true",
                     help="six radiance-cache frames (for ncu captures of the cache kernels)")
     ap.add_argument("--profile-size", default="480x270", help="frame size of --profile-nrc")
@@ -717,6 +768,12 @@ def main():
     args = ap.parse_args()
     if args.profile_queues:
         profile_queues()
+        return
+    if args.nrc_sweep:
+        import torch
+        dev = torch.device("cuda", 0)
+        r = sweep_nrc(torch, dev, torch.cuda.Stream(device=dev), args.nrc_sweep)
+        print(json.dumps({"nrc_sweep": r}), flush=True)
         return
     if args.profile_denoise:
         profile_denoise()

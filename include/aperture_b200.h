@@ -352,11 +352,13 @@ typedef struct ar_nrc_frame_stats {
 /* Cache of one scene (the scene must outlive it). */
 ar_status ar_nrc_create(ar_scene* scene, const ar_nrc_config* config, ar_nrc** out);
 ar_status ar_nrc_destroy(ar_nrc* nrc);
-/* One frame of 1 sample per pixel (params->spp must be 1, RGB): paths that
- * end in the cache add throughput x prediction; with train != 0 the frame's
+/* One frame of params->spp samples per pixel (1 to 64, RGB): paths that end
+ * in the cache add throughput x prediction; sample 0 of every training pixel
+ * runs to its end and records training vertices; with train != 0 the frame's
  * training samples then take train_steps optimiser steps.  out_rgb (this
- * frame's image) and accum (FP64 sums added) are device buffers; either may
- * be NULL, not both.  stats may be NULL (then no host synchronisation). */
+ * frame's mean image) and accum (FP64 sums of all spp samples added) are
+ * device buffers; either may be NULL, not both.  stats may be NULL (then no
+ * host synchronisation). */
 ar_status ar_nrc_render_frame(ar_nrc* nrc, const ar_camera* camera, const ar_render_params* params,
                               float* out_rgb, double* accum, int32_t train, ar_nrc_frame_stats* stats,
                               void* stream);
@@ -419,6 +421,22 @@ ar_status ar_guide_get_stats(const ar_guide* guide, ar_guide_stats* stats);
 /* Copy of probe `index` (88 float4 texels: 8x8 leaves, 4x4, 2x2, 1x1 mips,
  * padding), or AR_ERR_INVALID_ARGUMENT when it is not allocated. */
 ar_status ar_guide_get_probe(const ar_guide* guide, int32_t index, float* texels);
+
+/* The probe math of the guided frames evaluated on the current device, for
+ * checks against the reference's Octahedron (core/guiding/octahedron.cuh) and
+ * grid (core/guiding/guiding_bin.cuh).  texels: nprobes x 85 x 4 floats (8x8
+ * leaves, then the 4x4, 2x2 and 1x1 mips; rgb and one unused float).  Per
+ * query i (host arrays): probe probe_of[i], normal normal3, texel weights
+ * query3, five uniforms u5 (three for the mip descent, two for the point in
+ * the leaf texel).  Out: the hemisphere sample's direction and pdf
+ * (SampleOctahedronHemisphere, octahedron.cuh:343-364), the hemisphere pdf of
+ * direction eval3 (OctahedronHemispherePDF, octahedron.cuh:366-380) and the
+ * (voxel, face) key of point pos3 and direction eval3 (19-bit two's-
+ * complement voxel x, y, z in bits 0-56, face index from bit 57; GetVoxelGrid,
+ * guiding_bin.cuh:102-114). */
+ar_status ar_guide_probe_eval(const float* texels, int32_t nprobes, const int32_t* probe_of, const float* normal3,
+                              const float* query3, const float* u5, const float* eval3, const float* pos3, int64_t n,
+                              float* out_dir3, float* out_pdf, float* out_eval_pdf, uint64_t* out_key);
 
 /* One job of a batch: a scene (shared between jobs if wanted), a camera, the
  * render parameters and device outputs (mean image and/or FP64 sums added). */

@@ -105,3 +105,54 @@ def sample_leaf(texels: np.ndarray, q, u3) -> tuple[int, int, float]:
                 pt *= wc
                 break
     return cx, cy, pt
+
+
+# The reference's face numbering (FaceNormal20FromIndex, core/guiding/
+# guiding_bin.cuh:40-66) as the signs of each face normal's x, y, z: three
+# non-zero signs are a cube-diagonal face (+-1, +-1, +-1) / sqrt 3; a zero at
+# axis k puts phi^2 / sqrt(1 + phi^4) on axis (k + 1) % 3 and 1 / sqrt(1 + phi^4)
+# on axis (k + 2) % 3 (the table of csrc/guiding.cu, pg_face_normals).
+FACE_SIGNS = ((-1, 1, 1), (0, 1, 1), (0, 1, -1), (-1, 1, -1), (-1, 1, 0), (1, 1, 1), (-1, 0, 1), (-1, -1, 0),
+              (-1, 0, -1), (1, 1, -1), (1, -1, 1), (0, -1, 1), (0, -1, -1), (1, -1, -1), (1, -1, 0), (1, 0, 1),
+              (-1, -1, 1), (-1, -1, -1), (1, 0, -1), (1, 1, 0))
+
+
+def face_normals() -> np.ndarray:
+    phi = (1.0 + math.sqrt(5.0)) / 2.0
+    ln = math.sqrt(1.0 + phi ** 4)
+    out = np.zeros((20, 3))
+    for f, s in enumerate(FACE_SIGNS):
+        if 0 not in s:
+            out[f] = np.array(s) / math.sqrt(3.0)
+        else:
+            k = s.index(0)
+            out[f, (k + 1) % 3] = s[(k + 1) % 3] * phi * phi / ln
+            out[f, (k + 2) % 3] = s[(k + 2) % 3] / ln
+    return out.astype(np.float32)
+
+
+def voxel_grid(pos, dirs) -> np.ndarray:
+    """(voxel x, y, z of 0.05 units, face whose normal is nearest the direction)"""
+    p = np.asarray(pos, np.float32)
+    d = np.asarray(dirs, np.float64)
+    d = d / np.linalg.norm(d, axis=1, keepdims=True)
+    face = np.argmax(d @ face_normals().astype(np.float64).T, axis=1)
+    g = np.floor(p * np.float32(20.0)).astype(np.int64)
+    return np.concatenate([g, face[:, None]], axis=1)
+
+
+def sample_hemi(texels: np.ndarray, n, q, u5):
+    """SampleOctahedronHemisphere: mip descent with u5[0:3], the point in the
+    leaf texel from 1 - u5[3:5], the mirror about the normal for directions
+    below it; pdf = leaf pdf + pdf of the mirror direction."""
+    n = np.asarray(n, np.float64)
+    cx, cy, pt = sample_leaf(texels, q, u5[:3])
+    su = min(max((cx + (1.0 - u5[3])) / RES, 0.0), 1.0)
+    sv = min(max((cy + (1.0 - u5[4])) / RES, 0.0), 1.0)
+    w = uv_to_dir(su, sv)
+    p = max(pt * RES * RES / (4 * math.pi), 1e-12)
+    m = mirror(w, n)
+    p += float(pdf(texels, m[None], q)[0])
+    if w @ n < 0:
+        w = m
+    return w, p

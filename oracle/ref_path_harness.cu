@@ -291,3 +291,57 @@ int refp_render_image(const ref_path_scene* s, const ar_camera* cam, const ar_re
 }
 
 }  // extern "C"
+
+// ---- path guiding probes (core/guiding/octahedron.cuh, guiding_bin.cuh), for
+// pinning the CUDA core's probe math: the reference's 20 face normals
+// (FaceNormal20FromIndex, guiding_bin.cuh:40-66), its (voxel, face) grid of a
+// point and direction (GetVoxelGrid, guiding_bin.cuh:102-114), and per query
+// SampleOctahedronHemisphere (octahedron.cuh:343-364; three mip-descent
+// uniforms and two for the point in the leaf texel, read from u5) and
+// OctahedronHemispherePDF (octahedron.cuh:366-380) of given probes.
+extern "C" {
+
+void refp_guiding_faces(float* out60)
+{
+    for (int f = 0; f < PATH_GUIDING_FACE_COUNT; ++f) {
+        const float3 n = pg::FaceNormal20FromIndex(f);
+        out60[3 * f] = n.x; out60[3 * f + 1] = n.y; out60[3 * f + 2] = n.z;
+    }
+}
+
+void refp_guiding_voxel(const float* pos3, const float* dir3, int64_t n, int32_t* out4)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        const int4 g = pg::GetVoxelGrid(make_float3(pos3[3 * i], pos3[3 * i + 1], pos3[3 * i + 2]),
+                                        make_float3(dir3[3 * i], dir3[3 * i + 1], dir3[3 * i + 2]));
+        out4[4 * i] = g.x; out4[4 * i + 1] = g.y; out4[4 * i + 2] = g.z; out4[4 * i + 3] = g.w;
+    }
+}
+
+// texels: nprobes x 85 x 4 floats (leaves 8x8, then the 4x4, 2x2, 1x1 mips; rgb + unused)
+void refp_guiding_sample(const float* texels, int32_t nprobes, const int32_t* probe_of, const float* normal3,
+                         const float* query3, const float* u5, const float* eval3, int64_t n, float* out_dir3,
+                         float* out_pdf, float* out_eval_pdf)
+{
+    std::vector<Octahedron> probes(static_cast<size_t>(nprobes));
+    for (int32_t p = 0; p < nprobes; ++p) {
+        std::memset(&probes[p], 0, sizeof(Octahedron));
+        for (int t = 0; t < Octahedron::totalPixelCount_; ++t) {
+            const float* s = texels + (static_cast<size_t>(p) * Octahedron::totalPixelCount_ + t) * 4;
+            probes[p].data_[t] = make_float4(s[0], s[1], s[2], s[3]);
+        }
+    }
+    for (int64_t i = 0; i < n; ++i) {
+        const Octahedron& o = probes[static_cast<size_t>(probe_of[i])];
+        const float3 nrm = make_float3(normal3[3 * i], normal3[3 * i + 1], normal3[3 * i + 2]);
+        const float3 q = make_float3(query3[3 * i], query3[3 * i + 1], query3[3 * i + 2]);
+        PathState st;
+        begin_path(st, u5 + 5 * i, 5, 0);
+        const Sample smp = o.SampleOctahedronHemisphere(&st.rng, nrm, q);
+        out_dir3[3 * i] = smp.direction_.x; out_dir3[3 * i + 1] = smp.direction_.y; out_dir3[3 * i + 2] = smp.direction_.z;
+        out_pdf[i] = smp.pdf_;
+        out_eval_pdf[i] = o.OctahedronHemispherePDF(make_float3(eval3[3 * i], eval3[3 * i + 1], eval3[3 * i + 2]), nrm, q);
+    }
+}
+
+}  // extern "C"

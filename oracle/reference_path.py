@@ -97,3 +97,41 @@ class RefPathScene:
         if st != 0:
             raise ValueError("parameters the reference's RGB path loop cannot express")
         return accum, e.value, s.value
+
+
+def guiding_faces() -> np.ndarray:
+    """The reference's 20 face normals in its numbering (FaceNormal20FromIndex)."""
+    lib = load(False)
+    lib.refp_guiding_faces.argtypes = [c_void_p]
+    out = np.empty((20, 3), np.float32)
+    lib.refp_guiding_faces(out.ctypes.data)
+    return out
+
+
+def guiding_voxel(pos, dirs) -> np.ndarray:
+    """pg::GetVoxelGrid per point and direction: int32 [n, 4] (x, y, z, face)."""
+    lib = load(False)
+    lib.refp_guiding_voxel.argtypes = [c_void_p, c_void_p, c_int64, c_void_p]
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+    out = np.empty((len(p), 4), np.int32)
+    lib.refp_guiding_voxel(p.ctypes.data, d.ctypes.data, len(p), out.ctypes.data)
+    return out
+
+
+def guiding_sample(texels, probe_of, normal, query, u5, eval_dir):
+    """Octahedron::SampleOctahedronHemisphere (uniforms from u5) and
+    OctahedronHemispherePDF of eval_dir for probes given as texels
+    [nprobes, 85, 4]: (directions [n, 3], sample pdfs, pdfs of eval_dir)."""
+    lib = load(False)
+    lib.refp_guiding_sample.argtypes = [c_void_p, c_int] + [c_void_p] * 5 + [c_int64] + [c_void_p] * 3
+    t = np.ascontiguousarray(texels, np.float32).reshape(-1, 85, 4)
+    po = np.ascontiguousarray(probe_of, np.int32).reshape(-1)
+    n = len(po)
+    a = [np.ascontiguousarray(x, np.float32).reshape(n, -1) for x in (normal, query, u5, eval_dir)]
+    d = np.empty((n, 3), np.float32)
+    p = np.empty(n, np.float32)
+    e = np.empty(n, np.float32)
+    lib.refp_guiding_sample(t.ctypes.data, len(t), po.ctypes.data, a[0].ctypes.data, a[1].ctypes.data,
+                            a[2].ctypes.data, a[3].ctypes.data, n, d.ctypes.data, p.ctypes.data, e.ctypes.data)
+    return d, p, e

@@ -49,3 +49,31 @@ def test_mips_are_averages():
     tex = G.build_mips(leaves)
     assert np.allclose(tex[84], leaves.mean(0))
     assert np.allclose(tex[80:84].mean(0), tex[84])
+
+
+def test_probe_math_matches_reference():
+    """The numpy restatement against the reference's own Octahedron and grid,
+    run on the host (tests/golden/reference_guiding.npz): the 20 face normals
+    in the reference's numbering, the (voxel, face) grid of points and
+    directions exactly; hemisphere sample directions within 2e-6 and pdfs
+    within 2e-5 relative (float against float64 arithmetic)."""
+    import os
+    fx = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_guiding.npz"))
+    assert np.array_equal(G.face_normals(), fx["faces"])
+    assert np.array_equal(G.voxel_grid(fx["pos"], fx["eval_dir"]), fx["voxel"])
+    tex = fx["texels"][:, :, :3].astype(np.float64)
+    n = 2000
+    dirs, pdfs, epdfs = [], [], []
+    for i in range(n):
+        t = tex[fx["probe_of"][i]]
+        w, p = G.sample_hemi(t, fx["normal"][i], fx["query"][i], fx["u5"][i].astype(np.float64))
+        dirs.append(w)
+        pdfs.append(p)
+        epdfs.append(float(G.hemi_pdf(t, fx["eval_dir"][i][None].astype(np.float64), fx["normal"][i].astype(np.float64),
+                                      fx["query"][i])[0]))
+    assert np.abs(np.array(dirs) - fx["dir"][:n]).max() < 2e-6
+    assert np.max(np.abs(np.array(pdfs) - fx["pdf"][:n]) / fx["pdf"][:n]) < 2e-5
+    e = fx["epdf"][:n]
+    assert np.array_equal(np.array(epdfs) == 0, e == 0)
+    nz = e > 0
+    assert np.max(np.abs(np.array(epdfs)[nz] - e[nz]) / e[nz]) < 2e-5

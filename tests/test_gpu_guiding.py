@@ -49,3 +49,34 @@ def test_guided_frames_fill_probes_and_converge():
         assert np.allclose(t[80:84].mean(0), t[84], rtol=1e-4)
         q = np.array([0.3, 0.4, 0.3])
         assert abs(np.sum(G.pdf(t[:85], w, q)) * 4 * math.pi / 64 - 1.0) < 1e-4
+
+
+@pytest.mark.gpu
+def test_device_probe_math_matches_reference():
+    """csrc/guiding.cuh on the GPU (ar_guide_probe_eval) against the
+    reference's Octahedron and grid run on the host
+    (tests/golden/reference_guiding.npz, 8,000 queries over 8 probes): the
+    (voxel, face) key of every point and direction equal -- the face in the
+    reference's numbering --, hemisphere sample directions within 2e-6,
+    sample pdfs and pdfs of given directions within 2e-5 relative (the two
+    codes write the equal-area map and the mirror with different float
+    operations)."""
+    import os
+
+    from aperture_b200 import guide_probe_eval
+    fx = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_guiding.npz"))
+    d, p, e, k = guide_probe_eval(fx["texels"], fx["probe_of"], fx["normal"], fx["query"], fx["u5"], fx["eval_dir"],
+                                  fx["pos"])
+    m = (1 << 19) - 1
+    vox = np.stack([(k >> s) & m for s in (0, 19, 38)], 1).astype(np.int64)
+    vox = np.where(vox >= (1 << 18), vox - (1 << 19), vox)
+    face = (k >> 57).astype(np.int64)
+    ref = fx["voxel"].astype(np.int64)
+    assert np.array_equal(vox, ref[:, :3])
+    assert np.array_equal(face, ref[:, 3])
+    assert np.abs(d - fx["dir"]).max() < 2e-6
+    assert np.max(np.abs(p - fx["pdf"]) / fx["pdf"]) < 2e-5
+    ep = fx["epdf"]
+    assert np.array_equal(e == 0, ep == 0)
+    nz = ep > 0
+    assert np.max(np.abs(e[nz] - ep[nz]) / ep[nz]) < 2e-5

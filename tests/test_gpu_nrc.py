@@ -137,3 +137,39 @@ def test_nrc_tcgen05_inference_equals_mma_sync():
     o = N.predict(_geo(cfg), v, table, w)
     rel = np.abs(b - o) / np.maximum(np.abs(o), 1e-6)
     assert np.median(rel) < 1e-3 and np.mean(rel) < 5e-3
+
+
+@pytest.mark.gpu
+def test_nrc_frames_of_several_samples():
+    """A cache frame of k samples per pixel: every sample may end in the cache,
+    sample 0 of the training pixels trains, out_rgb is the mean over the k
+    samples and accum gets their sums.  With the cache frozen (train off),
+    k-sample frames and k times as many one-sample frames estimate the same
+    image."""
+    import torch
+    objs = scenes.box_scene()
+    sc = Scene(objs)
+    cam = scenes.box_camera(48, 48)
+    cfg = nrc_config(bounds=BOUNDS, log2_entries=15, train_paths=1024, train_batch=1024, train_steps=2)
+    c = RadianceCache(sc, cfg)
+    n = 48 * 48 * 3
+    acc = torch.zeros(n, dtype=torch.float64, device="cuda")
+    for f in range(16):   # train a little with 4-sample frames
+        st = c.render_frame(cam, make_params(spp=4, max_depth=8, frame_offset=4 * f), None, acc.data_ptr(),
+                            train=True, stats=(f == 15))
+    assert st.queries > 4 * 500 and 500 < st.train_samples
+    out = torch.empty(n, dtype=torch.float32, device="cuda")
+    acc_k = torch.zeros(n, dtype=torch.float64, device="cuda")
+    acc_1 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    k, frames = 8, 32
+    for f in range(frames):
+        c.render_frame(cam, make_params(spp=k, max_depth=8, frame_offset=1000 + k * f), out.data_ptr(),
+                       acc_k.data_ptr(), train=False)
+    for f in range(frames * k):
+        c.render_frame(cam, make_params(spp=1, max_depth=8, frame_offset=100000 + f), None, acc_1.data_ptr(),
+                       train=False)
+    a = (acc_k / (frames * k)).cpu().numpy()
+    b = (acc_1 / (frames * k)).cpu().numpy()
+    assert np.isfinite(a).all() and abs(a.mean() - b.mean()) < 0.02 * b.mean()
+    last = out.cpu().numpy()
+    assert abs(last.mean() - a.mean()) < 0.1 * a.mean()    # out_rgb is the k-sample mean, not the sum
