@@ -540,6 +540,21 @@ class RadianceCache:
                                         ctypes.byref(st) if st is not None else None, c_void_p(stream)))
         return st
 
+    def set_spectral(self, mode: int) -> None:
+        """Cache mode before the first frame: 0 RGB, 4 four wavelengths per path
+        (16 spectral bins)."""
+        _check(_lib.ar_nrc_set_option(self._h, 2, int(mode)))
+        self.spectral = int(mode)
+
+    @staticmethod
+    def _samples(samples: np.ndarray) -> np.ndarray:
+        """Training samples as rows of 20 floats (16-float rows get 4 zeros)."""
+        s = np.ascontiguousarray(samples, np.float32)
+        s = s.reshape(-1, s.shape[-1]) if s.ndim > 1 else s.reshape(-1, 20)
+        if s.shape[1] == 16:
+            s = np.concatenate([s, np.zeros((len(s), 4), np.float32)], axis=1)
+        return np.ascontiguousarray(s)
+
     def set_tensor_path(self, tcgen05: bool) -> None:
         """Inference kernel: tcgen05.mma with tensor-memory accumulators, or mma.sync."""
         _check(_lib.ar_nrc_set_option(self._h, 1, 1 if tcgen05 else 0))
@@ -557,18 +572,18 @@ class RadianceCache:
 
     def infer(self, vertices: np.ndarray) -> np.ndarray:
         v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 16)
-        out = np.empty((len(v), 3), np.float32)
+        out = np.empty((len(v), 16 if getattr(self, "spectral", 0) else 3), np.float32)
         _check(_lib.ar_nrc_infer(self._h, _ptr(v), len(v), _ptr(out)))
         return out
 
     def train(self, samples: np.ndarray, steps: int) -> np.ndarray:
-        s = np.ascontiguousarray(samples, np.float32).reshape(-1, 16)
+        s = self._samples(samples)
         losses = np.zeros(max(steps, 1), np.float32)
         _check(_lib.ar_nrc_train(self._h, _ptr(s), len(s), steps, _ptr(losses)))
         return losses[:steps]
 
     def gradients(self, samples: np.ndarray):
-        s = np.ascontiguousarray(samples, np.float32).reshape(-1, 16)
+        s = self._samples(samples)
         tg = np.empty(self.table_floats, np.float32)
         wg = np.empty(NRC_PARAMS, np.float32)
         loss = np.zeros(1, np.float32)

@@ -1152,6 +1152,7 @@ struct ar_nrc {
     int slots = 0, sample_cap = 0;
     int* tc_err = nullptr;         // error word of the tcgen05 inference kernel
     int tensor_path = 1;           // inference: 1 tcgen05 (default), 0 mma.sync
+    int spectral = 0;              // 0 RGB cache, 4 four-wavelength cache (16 spectral bins)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<void*> owned;
 
@@ -1162,6 +1163,8 @@ struct ar_nrc {
         n.table = P.table_h;
         n.w = P.w_bf;
         n.wt = P.wt_bf;
+        n.spectral = spectral;
+        n.tables = scene->spec_tables;
         return n;
     }
     ~ar_nrc()
@@ -1292,7 +1295,7 @@ ar_status ar_nrc_create(ar_scene* s, const ar_nrc_config* cfg, ar_nrc** out)
     ar::NrcTrainBuffers& T = c->T;
     T.acts = nrc_alloc<__nv_bfloat16>(c.get(), B * ar::kNrcIn * ar::kNrcLayers, "cache activations");
     T.dz = nrc_alloc<__nv_bfloat16>(c.get(), B * ar::kNrcIn * ar::kNrcLayers, "cache gradients");
-    T.raw = nrc_alloc<float>(c.get(), B * 4, "cache outputs");
+    T.raw = nrc_alloc<float>(c.get(), B * 16, "cache outputs");
     T.dx = nrc_alloc<float>(c.get(), B * 32, "cache input gradients");
     T.loss = nrc_alloc<float>(c.get(), 1, "cache loss");
     c->slots = cfg->train_paths + 1;
@@ -1325,7 +1328,11 @@ ar_status ar_nrc_render_frame(ar_nrc* c, const ar_camera* cam, const ar_render_p
     if (ar_status e = check_camera(cam)) return e;
     if (ar_status e = check_params(p)) return e;
     if (p->spp > 64) return fail(AR_ERR_INVALID_ARGUMENT, "cache frames take 1 to 64 samples per pixel");
-    if (p->spectral) return fail(AR_ERR_UNSUPPORTED, "the cache is RGB only");
+    if (p->spectral != c->spectral)
+        return fail(p->spectral == 1 ? AR_ERR_UNSUPPORTED : AR_ERR_INVALID_ARGUMENT,
+                    "params->spectral must match the cache's mode (AR_NRC_OPT_SPECTRAL: 0 RGB, 4 four wavelengths; "
+                    "one wavelength per path has no cache)");
+    if (c->spectral && !c->scene->spec_tables) return fail(AR_ERR_UNSUPPORTED, "no spectral tables set");
     if (!out_rgb && !accum) return fail(AR_ERR_INVALID_ARGUMENT, "out_rgb and accum are both NULL");
     AR_GUARD_BEGIN
     ar_scene* s = c->scene;
@@ -1337,6 +1344,7 @@ ar_status ar_nrc_render_frame(ar_nrc* c, const ar_camera* cam, const ar_render_p
     if (stats) ck(cudaMemsetAsync(c->T.loss, 0, sizeof(float), st), "memset");
     ar::NrcFrame f{};
     f.enabled = 1;
+    f.spectral = c->spectral;
     f.stride = static_cast<int32_t>(std::max<int64_t>(1, (npix + c->cfg.train_paths - 1) / c->cfg.train_paths));
     f.offset = static_cast<int32_t>(ar::lowbias32(static_cast<uint32_t>(p->frame_offset) * 0x9E3779B9u ^
                                                   static_cast<uint32_t>(p->seed)) % static_cast<uint32_t>(f.stride));
@@ -1389,10 +1397,16 @@ ar_status ar_nrc_set_option(ar_nrc* c, int32_t option, int32_t value)
 {
     g_last_error.clear();
     if (!c) return fail(AR_ERR_INVALID_ARGUMENT, "cache is NULL");
-    if (option != AR_NRC_OPT_TENSOR_PATH || (value != 0 && value != 1))
-        return fail(AR_ERR_INVALID_ARGUMENT, "unknown option or value");
-    c->tensor_path = value;
-    return AR_OK;
+    if (option == AR_NRC_OPT_TENSOR_PATH && (value == 0 || value == 1)) {
+        c->tensor_path = value;
+        return AR_OK;
+    }
+    if (option == AR_NRC_OPT_SPECTRAL && (value == 0 || value == 4)) {
+        if (value == 4 && !c->scene->spec_tables) return fail(AR_ERR_UNSUPPORTED, "no spectral tables set");
+        c->spectral = value;
+        return AR_OK;
+    }
+    return fail(AR_ERR_INVALID_ARGUMENT, "unknown option or value");
 }
 
 ar_status ar_nrc_get_params(const ar_nrc* c, float* table, float* weights)
@@ -1434,7 +1448,7 @@ ar_status ar_nrc_infer(ar_nrc* c, const float* vertices, size_t n, float* out_rg
     int32_t* cnt = nullptr;
     cudaError_t e = cudaSuccess;
     try {
-        out = dalloc<float>(n * 3, "predictions");
+        out = dalloc<float>(n * (c->spectral ? ar::kNrcBins : 3), "predictions");
         cnt = dalloc<int32_t>(1, "count");
         std::vector<ar::NrcQuery> h(n);
         for (size_t i = 0; i < n; ++i) {
@@ -1445,7 +1459,8 @@ ar_status ar_nrc_infer(ar_nrc* c, const float* vertices, size_t n, float* out_rg
         ck(cudaMemcpy(q, h.data(), n * sizeof(ar::NrcQuery), cudaMemcpyHostToDevice), "copy vertices");
         ck(cudaMemcpy(cnt, &ni, 4, cudaMemcpyHostToDevice), "copy count");
         e = nrc_run_infer(c, q, cnt, ni, nullptr, out, nullptr);
-        if (e == cudaSuccess) e = cudaMemcpy(out_rgb, out, n * 12, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(out_rgb, out, n * 4 * (c->spectral ? ar::kNrcBins : 3), cudaMemcpyDeviceToHost);
     } catch (...) {
         cudaFree(q); cudaFree(out); cudaFree(cnt);
         throw;

@@ -230,7 +230,21 @@ __global__ void __launch_bounds__(kNrcBlock) k_nrc_infer(NrcNet net, const NrcQu
         __syncwarp();
         forward_tile(sW, sIn, sOut, nullptr, 0, 0, 0);
         __syncwarp();
-        if (valid) {
+        if (valid && net.spectral) {   // four wavelengths: 16 spectral bins
+            const float* o = sOut + lane * kOutRow;
+            float e[kNrcBins];
+#pragma unroll
+            for (int b = 0; b < kNrcBins; ++b) e[b] = exp_out(o[b]);
+            if (accum) {
+                const int pix = __float_as_int(qq.v.p.w);
+                const f3 c = nrc_spectral_xyz(net.tables, e, qq.v.n.w, qq.t);
+                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 0], static_cast<double>(c.x));
+                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 1], static_cast<double>(c.y));
+                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 2], static_cast<double>(c.z));
+            }
+            if (out_rgb)
+                for (int b = 0; b < kNrcBins; ++b) out_rgb[kNrcBins * static_cast<int64_t>(i) + b] = e[b];
+        } else if (valid) {
             const float* o = sOut + lane * kOutRow;
             const float L0 = exp_out(o[0]), L1 = exp_out(o[1]), L2 = exp_out(o[2]);
             if (accum) {
@@ -276,9 +290,11 @@ __global__ void __launch_bounds__(kNrcBlock) k_nrc_train_fwd(NrcNet net, const N
         __syncwarp();
         forward_tile(sW, sIn, sOut, T.acts, batch, static_cast<int64_t>(tile) * kNrcWarpRows, batch);
         __syncwarp();
-        if (i < batch) {
+        if (i < batch) {   // all 16 raw outputs (rgb uses 0-2)
             const float* o = sOut + lane * kOutRow;
-            reinterpret_cast<float4*>(T.raw)[i] = make_float4(o[0], o[1], o[2], 0.0f);
+            float4* r = reinterpret_cast<float4*>(T.raw) + 4 * static_cast<int64_t>(i);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) r[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
         }
         __syncwarp();
     }
@@ -311,16 +327,43 @@ __global__ void __launch_bounds__(kNrcBlock) k_nrc_train_bwd(NrcNet net, const N
     }
     __syncthreads();
     const int nv = valid_rows(count, first, batch);
-    const float norm = nv > 0 ? 1.0f / (3.0f * static_cast<float>(nv)) : 0.0f;
+    const float norm = nv > 0 ? 1.0f / ((net.spectral ? 4.0f : 3.0f) * static_cast<float>(nv)) : 0.0f;
     float loss_acc = 0.0f;
     for (int tile = blockIdx.x * kWarps + warp; tile * kNrcWarpRows < batch; tile += gridDim.x * kWarps) {
         const int64_t row0 = static_cast<int64_t>(tile) * kNrcWarpRows;
         const int i = static_cast<int>(row0) + lane;
         // output gradient of this lane's row into its shared-memory row (16 columns)
-        float d[3] = {0.0f, 0.0f, 0.0f};
-        if (i < nv) {
+        float d[kNrcBins];
+#pragma unroll
+        for (int b = 0; b < kNrcBins; ++b) d[b] = 0.0f;
+        if (i < nv && net.spectral) {
+            // four wavelengths: pred_i = (1 - f_i) e[b_i] + f_i e[b_i + 1] with e = exp(raw);
+            // the loss gradient of each wavelength flows to its two bins through exp
             const NrcSample s = smp[first + i];
-            const float4 raw = reinterpret_cast<const float4*>(T.raw)[i];
+            const float4* rr = reinterpret_cast<const float4*>(T.raw) + 4 * static_cast<int64_t>(i);
+            float e[kNrcBins];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 v = rr[q];
+                e[4 * q] = exp_out(v.x); e[4 * q + 1] = exp_out(v.y); e[4 * q + 2] = exp_out(v.z); e[4 * q + 3] = exp_out(v.w);
+            }
+            const float tg[4] = {s.v.p.w, s.v.n.w, s.v.a.w, s.x.x};
+            for (int w = 0; w < 4; ++w) {
+                if (tg[w] < 0.0f) continue;   // no throughput reached this wavelength
+                int b;
+                float f;
+                nrc_bin_weights(rotate_lambda(s.x.y, w), &b, &f);
+                const float pred = (1.0f - f) * e[b] + f * e[b + 1];
+                const float den = pred * pred + 0.01f;
+                const float diff = pred - tg[w];
+                loss_acc += diff * diff / den * norm;
+                const float g = (2.0f * diff / den) * norm * kNrcLossScale;
+                d[b] += g * (1.0f - f) * e[b];
+                d[b + 1] += g * f * e[b + 1];
+            }
+        } else if (i < nv) {
+            const NrcSample s = smp[first + i];
+            const float4 raw = reinterpret_cast<const float4*>(T.raw)[4 * static_cast<int64_t>(i)];
             const float tg[3] = {s.v.p.w, s.v.n.w, s.v.a.w};
             const float r3[3] = {raw.x, raw.y, raw.z};
 #pragma unroll
@@ -333,10 +376,8 @@ __global__ void __launch_bounds__(kNrcBlock) k_nrc_train_bwd(NrcNet net, const N
             }
         }
         uint32_t* row = reinterpret_cast<uint32_t*>(sIn + lane * kNrcWRow);
-        row[0] = pack_bf16(d[0], d[1]);
-        row[1] = pack_bf16(d[2], 0.0f);
 #pragma unroll
-        for (int k = 2; k < 8; ++k) row[k] = 0u;
+        for (int k = 0; k < 8; ++k) row[k] = pack_bf16(d[2 * k], d[2 * k + 1]);
         if (i < batch) {   // output-layer gradient for the weight gradient (first 16 columns)
             uint4* dst = reinterpret_cast<uint4*>(T.dz + static_cast<int64_t>(5) * batch * kNrcIn + static_cast<int64_t>(i) * kNrcIn);
             const uint4* src = reinterpret_cast<const uint4*>(row);

@@ -18,6 +18,8 @@
 
 #include <cstdint>
 
+#include "spectral.cuh"
+
 namespace ar {
 
 constexpr int kNrcIn = 64, kNrcHid = 64, kNrcOut = 16;
@@ -43,12 +45,52 @@ struct NrcGrid {
     float bmin[3], inv_ext[3];     // scene box -> [0, 1]^3
 };
 
+// Four-wavelength mode: the 16 network outputs, through exp, are the outgoing
+// spectral radiance at 16 wavelength bins of 26.25 nm over [360, 780] nm (bin
+// centres 373.125 + 26.25 b); a wavelength's value interpolates linearly
+// between the two nearest centres (clamped to the first and last).
+constexpr int kNrcBins = 16;
+constexpr float kNrcLambda0 = 360.0f, kNrcBinWidth = 26.25f;
+
+__host__ __device__ __forceinline__ void nrc_bin_weights(float lambda, int* b0, float* f)
+{
+    float x = (lambda - kNrcLambda0) / kNrcBinWidth - 0.5f;
+    x = x < 0.0f ? 0.0f : (x > static_cast<float>(kNrcBins - 1) ? static_cast<float>(kNrcBins - 1) : x);
+    int b = static_cast<int>(floorf(x));
+    b = b > kNrcBins - 2 ? kNrcBins - 2 : b;
+    *b0 = b;
+    *f = x - static_cast<float>(b);
+}
+
+// The XYZ a four-wavelength path gets from a cache prediction: the hero
+// wavelength's rotation set lambda_i, the predicted radiance L(lambda_i) from
+// the exp'd bins e[16], the path's throughput T_i per wavelength, weighted as
+// the path's own estimate sum_i XYZ(lambda_i) L_i / sum_j p(lambda_j).
+__host__ __device__ __forceinline__ f3 nrc_spectral_xyz(const float* tables, const float* e, float hero, float4 T)
+{
+    const float t[4] = {T.x, T.y, T.z, T.w};
+    float ps = 0.0f;
+    f3 acc = mk(0.0f, 0.0f, 0.0f);
+    for (int w = 0; w < 4; ++w) {
+        const float lw = rotate_lambda(hero, w);
+        ps += pdf_cie1931(lw);
+        int b;
+        float f;
+        nrc_bin_weights(lw, &b, &f);
+        const float L = (1.0f - f) * e[b] + f * e[b + 1];
+        acc = acc + cmf_xyz(tables, lw) * (t[w] * L);
+    }
+    return acc / ps;
+}
+
 // Device view of the network state.
 struct NrcNet {
     NrcGrid grid;
     const __half2* table;          // levels x entries features (forward copy)
     const __nv_bfloat16* w;        // [out][in] per layer, packed
     const __nv_bfloat16* wt;       // [in][out] per layer, packed (backward)
+    int32_t spectral;              // 0: RGB outputs 0-2; 4: four wavelengths, 16 spectral bins
+    const float* tables;           // spectral tables of the scene (colour matching functions), mode 4
 };
 
 // One vertex as the cache sees it: 4 x float4 =
@@ -59,21 +101,24 @@ struct NrcVertex {
 
 // Records that the path tracer writes for the cache.
 struct NrcQuery {                  // a path terminated into the cache
-    NrcVertex v;                   // v.p.w: pixel (int bits)
-    float4 t;                      // throughput rgb
+    NrcVertex v;                   // v.p.w: pixel (int bits); four wavelengths: v.n.w hero wavelength
+    float4 t;                      // throughput rgb, or of wavelengths 0-3
 };
-struct NrcTrainVertex {            // a vertex of a training path
+struct NrcTrainVertex {            // a vertex of a training path (v.n.w: hero wavelength, mode 4)
     NrcVertex v;
-    float4 t;                      // throughput arriving at the vertex
+    float4 t;                      // throughput arriving at the vertex (rgb or wavelengths 0-3)
     float4 lb;                     // radiance gathered before the vertex
 };
 struct NrcSample {                 // a training sample: vertex + target radiance
-    NrcVertex v;                   // target radiance r, g, b in v.p.w, v.n.w, v.a.w
+    NrcVertex v;                   // target radiance r, g, b (wavelengths 0-2) in v.p.w, v.n.w, v.a.w
+    float4 x;                      // four wavelengths: x.x target of wavelength 3, x.y hero wavelength;
+                                   // a negative target (no throughput reached it) is left out of the loss
 };
 
 // Per-frame parameters of the cache inside the wavefront (FrameParams.nrc).
 struct NrcFrame {
     int32_t enabled;
+    int32_t spectral;              // 0 RGB, 4 four wavelengths (the cache's mode)
     int32_t stride, offset;        // sample 0 of pixel p trains when (p + offset) % stride == 0
     int32_t max_train_vertices;    // vertices recorded per training path
     float spread_c;                // terminate when spread^2 > c * a0
@@ -157,7 +202,7 @@ __host__ __device__ __forceinline__ void nrc_unit_pos(const NrcGrid& g, const fl
 // Host launchers (nrc.cu).
 struct NrcTrainBuffers {
     __nv_bfloat16* acts;     // kNrcLayers x [batch][64]: input and hidden activations
-    float* raw;              // [batch][4] raw outputs (pre-exp), rgb
+    float* raw;              // [batch][16] raw outputs (pre-exp): rgb in 0-2, or the 16 spectral bins
     __nv_bfloat16* dz;       // kNrcLayers x [batch][64]: gradients of the pre-activations (scaled)
     float* dx;               // [batch][32] gradient of the hash-grid features (scaled)
     float* loss;             // [1] sum of the relative L2 loss over the step

@@ -244,6 +244,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nrc_infer_tc(NrcNet net, cons
                         p[j] = pack2(fmaxf(__uint_as_float(v[8 * kc + 2 * j]), 0.0f), fmaxf(__uint_as_float(v[8 * kc + 2 * j + 1]), 0.0f));
                     *reinterpret_cast<uint4*>(sA + tc_chunk_offset(kTcRows, t, kc)) = make_uint4(p[0], p[1], p[2], p[3]);
                 }
+            } else if (net.spectral) {   // four wavelengths: the path's XYZ from the 16 spectral bins
+                float e[kNrcBins];
+#pragma unroll
+                for (int b = 0; b < kNrcBins; ++b) e[b] = expf(fminf(__uint_as_float(v[b]), 15.0f));
+                if (valid && accum) {
+                    const f3 c = nrc_spectral_xyz(net.tables, e, qq.v.n.w, qq.t);
+                    out[0] = c.x; out[1] = c.y; out[2] = c.z;
+                }
+                if (valid && out_rgb)
+                    for (int b = 0; b < kNrcBins; ++b) out_rgb[kNrcBins * static_cast<int64_t>(row) + b] = e[b];
             } else {
                 out[0] = expf(fminf(__uint_as_float(v[0]), 15.0f));
                 out[1] = expf(fminf(__uint_as_float(v[1]), 15.0f));
@@ -251,7 +261,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nrc_infer_tc(NrcNet net, cons
             }
         }
         if (failed) break;
-        if (valid) {
+        if (valid && net.spectral) {   // out holds the XYZ contribution already
+            if (accum) {
+                const int64_t pix = __float_as_int(qq.v.p.w);
+                atomicAdd(&accum[3 * pix + 0], static_cast<double>(out[0]));
+                atomicAdd(&accum[3 * pix + 1], static_cast<double>(out[1]));
+                atomicAdd(&accum[3 * pix + 2], static_cast<double>(out[2]));
+            }
+        } else if (valid) {
             if (accum) {
                 const int64_t pix = __float_as_int(qq.v.p.w);
                 atomicAdd(&accum[3 * pix + 0], static_cast<double>(qq.t.x * out[0]));

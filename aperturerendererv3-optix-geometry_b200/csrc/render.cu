@@ -493,16 +493,19 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
                 }
                 nv.p = make_float4(pos.x, pos.y, pos.z, fbits(pixel));
                 nv.d = make_float4(-crd.x, -crd.y, -crd.z, kModel == AR_MAT_GGX ? gb.roughness : 1.0f);
-                nv.n = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
-                nv.a = make_float4(gb.albedo.x, gb.albedo.y, gb.albedo.z, 0.0f);
+                // four wavelengths: the hero wavelength rides in n.w, the features
+                // keep the material's RGB albedo
+                nv.n = make_float4(nrm.x, nrm.y, nrm.z, kSpec == 4 ? lambda : 0.0f);
+                const f3 alb = kSpec ? gbr.albedo : gb.albedo;
+                nv.a = make_float4(alb.x, alb.y, alb.z, 0.0f);
                 int slot;
                 if (sidx == 0 && nrc_train_slot(fp.nrc, pixel, &slot)) {   // sample 0 of a training pixel
                     const int kv = fp.nrc.slot_count[slot];
                     if (kv < fp.nrc.max_train_vertices) {
                         NrcTrainVertex tv;
                         tv.v = nv;
-                        tv.t = f4(mask, 0.0f);
-                        tv.lb = f4(radiance, 0.0f);
+                        tv.t = f4(mask, kSpec == 4 ? mask3 : 0.0f);
+                        tv.lb = f4(radiance, kSpec == 4 ? rad3 : 0.0f);
                         fp.nrc.train_vertices[static_cast<int64_t>(slot) * fp.nrc.max_train_vertices + kv] = tv;
                         fp.nrc.slot_count[slot] = kv + 1;
                     }
@@ -828,7 +831,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(SceneView s, FrameParams 
             if (nrcQuery && qi < fp.nrc.query_cap) {
                 NrcQuery qq;
                 qq.v = nv;
-                qq.t = f4(mask, 0.0f);
+                qq.t = f4(mask, kSpec == 4 ? mask3 : 0.0f);
                 fp.nrc.queries[qi] = qq;
             }
         }
@@ -1016,7 +1019,32 @@ __global__ void k_retire(FrameParams fp, PathBuffers B, PoolCtl* ctl, double* ac
             // divided by the throughput that reached it
             const int nvtx = fp.nrc.slot_count[slot];
             const f3 L = mk(fix_nan_inf(rr.rad.x), fix_nan_inf(rr.rad.y), fix_nan_inf(rr.rad.z));
-            for (int k = 0; k < nvtx; ++k) {
+            if (fp.nrc.spectral == 4) {
+                // four wavelengths: a target per wavelength, negative (left out of the
+                // loss) where no throughput reached the vertex (hero-only after dispersion)
+                const float L3 = fix_nan_inf(fbits(rr.meta.w));
+                for (int k = 0; k < nvtx; ++k) {
+                    const NrcTrainVertex tv = fp.nrc.train_vertices[static_cast<int64_t>(slot) * fp.nrc.max_train_vertices + k];
+                    const float Lw[4] = {L.x, L.y, L.z, L3};
+                    const float T[4] = {tv.t.x, tv.t.y, tv.t.z, tv.t.w};
+                    const float B4[4] = {tv.lb.x, tv.lb.y, tv.lb.z, tv.lb.w};
+                    float tg[4];
+#pragma unroll
+                    for (int w = 0; w < 4; ++w)
+                        tg[w] = T[w] > 1e-6f ? fminf(fmaxf((Lw[w] - B4[w]) / T[w], 0.0f), 1.0e3f) : -1.0f;
+                    const int si = atomicAdd(fp.nrc.sample_count, 1);
+                    if (si < fp.nrc.sample_cap) {
+                        NrcSample sm;
+                        sm.v = tv.v;
+                        sm.v.p.w = tg[0];
+                        sm.v.n.w = tg[1];
+                        sm.v.a.w = tg[2];
+                        sm.x = make_float4(tg[3], tv.v.n.w, 0.0f, 0.0f);
+                        fp.nrc.samples[si] = sm;
+                    }
+                }
+            }
+            for (int k = 0; k < (fp.nrc.spectral == 4 ? 0 : nvtx); ++k) {
                 const NrcTrainVertex tv = fp.nrc.train_vertices[static_cast<int64_t>(slot) * fp.nrc.max_train_vertices + k];
                 const f3 tgt = mk(tv.t.x > 1e-6f ? (L.x - tv.lb.x) / tv.t.x : 0.0f,
                                   tv.t.y > 1e-6f ? (L.y - tv.lb.y) / tv.t.y : 0.0f,
@@ -1028,6 +1056,7 @@ __global__ void k_retire(FrameParams fp, PathBuffers B, PoolCtl* ctl, double* ac
                     sm.v.p.w = fminf(fmaxf(tgt.x, 0.0f), 1.0e3f);
                     sm.v.n.w = fminf(fmaxf(tgt.y, 0.0f), 1.0e3f);
                     sm.v.a.w = fminf(fmaxf(tgt.z, 0.0f), 1.0e3f);
+                    sm.x = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                     fp.nrc.samples[si] = sm;
                 }
             }
@@ -1170,7 +1199,10 @@ cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const P
         if (ext) k_extend<true><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err, fp.medium_key);
         else k_extend<false><<<grid_trace, kTraceBlock, kTraceSmem, st>>>(s, B, c, ctl, stats, ovf, err, fp.medium_key);
         if (te) cudaEventRecord(tm->extend_ev[2 * tm->n_extend++ + 1], st);
-        if (fp.spectral == 4) {
+        if (fp.spectral == 4 && fp.nrc.enabled) {
+            if (ext) launch_shade<true, 4, true>(s, fp, B, c, ctl, rec, grid_other, st);
+            else launch_shade<false, 4, true>(s, fp, B, c, ctl, rec, grid_other, st);
+        } else if (fp.spectral == 4) {
             if (ext) launch_shade<true, 4, false>(s, fp, B, c, ctl, rec, grid_other, st);
             else launch_shade<false, 4, false>(s, fp, B, c, ctl, rec, grid_other, st);
         } else if (fp.spectral) {

@@ -195,7 +195,8 @@ def fp64_reference(torch, dev, scene: Scene, cam, params: RenderParams, spp: int
 
 
 # ----------------------------------------------------------------------------- ours
-NRC_SIZES = {"small": (480, 270, 16384, 4096), "full": (1920, 1080, 16384, 4096), "box": (480, 270, 16384, 4096)}
+NRC_SIZES = {"small": (480, 270, 16384, 4096), "full": (1920, 1080, 16384, 4096), "box": (480, 270, 16384, 4096),
+             "config3": (1280, 720, 16384, 4096)}
 
 
 def nrc_setup(torch, dev, scene: Scene, mode: str, stream) -> dict:
@@ -206,12 +207,16 @@ def nrc_setup(torch, dev, scene: Scene, mode: str, stream) -> dict:
     16) in RGB; otherwise the config-2 scene."""
     w, h, ref_spp, target = NRC_SIZES[mode]
     depth = DEPTH
-    if mode == "box":
+    spectral = 0
+    if mode in ("box", "config3"):
         objs, vols, med = scenes.medium_box_scene(precision=16, grid=256, medium_grid=128)
         scene = Scene(objs, volumes=vols, device=dev.index)
         scene.set_medium(**med)
         cam = scenes.box_camera(w, h)
         depth = 16
+        if mode == "config3":
+            scene.set_spectral(64)
+            spectral = 4
     else:
         cam = scenes.spheres_camera(w, h)
     npix = w * h
@@ -223,7 +228,8 @@ def nrc_setup(torch, dev, scene: Scene, mode: str, stream) -> dict:
         for k in range(0, spp_total, chunk):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            scene.render_device(cam, make_params(spp=min(chunk, spp_total - k), max_depth=depth, frame_offset=offset + k),
+            scene.render_device(cam, make_params(spp=min(chunk, spp_total - k), max_depth=depth, frame_offset=offset + k,
+                                                 spectral=spectral),
                                 out.data_ptr(), acc.data_ptr(), stream.cuda_stream)
             e1.record(stream)
             e1.synchronize()
@@ -238,7 +244,8 @@ def nrc_setup(torch, dev, scene: Scene, mode: str, stream) -> dict:
         plain_ms = plain(target, 20_000_000, acc_p)
         e_plain = relmse_sum(acc_p, target, ref)
     return {"scene": scene, "cam": cam, "depth": depth, "ref": ref, "ref_spp": ref_spp, "ref_ms": ref_ms,
-            "target": target, "plain_ms": plain_ms, "e_plain": e_plain, "mode": mode, "w": w, "h": h}
+            "target": target, "plain_ms": plain_ms, "e_plain": e_plain, "mode": mode, "w": w, "h": h,
+            "spectral": spectral}
 
 
 def relmse_sum(acc, n, ref) -> float:
@@ -259,6 +266,8 @@ def nrc_curve(torch, dev, S: dict, stream, k: int = 1, spread_c: float = 0.01, s
     scene, cam, depth, ref = S["scene"], S["cam"], S["depth"], S["ref"]
     npix = S["w"] * S["h"]
     cache = RadianceCache(scene, nrc_config(spread_c=spread_c, train_steps=steps, seed=seed))
+    if S["spectral"]:
+        cache.set_spectral(S["spectral"])
     acc_n = torch.zeros(npix * 3, dtype=torch.float64, device=dev)
     t_ms, reached, curve = 0.0, None, []
     max_ms = max_factor * S["plain_ms"]
@@ -270,7 +279,8 @@ def nrc_curve(torch, dev, S: dict, stream, k: int = 1, spread_c: float = 0.01, s
             for _ in range(check):
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-                cache.render_frame(cam, make_params(spp=k, max_depth=depth, frame_offset=30_000_000 + samples), None,
+                cache.render_frame(cam, make_params(spp=k, max_depth=depth, frame_offset=30_000_000 + samples,
+                                                    spectral=S["spectral"]), None,
                                    acc_n.data_ptr(), train=True, stream=stream.cuda_stream)
                 e1.record(stream)
                 evs.append((e0, e1))
@@ -299,8 +309,9 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream, k: int = 1, spread_
     for the config-2 scene also the 300-frame seeded spline camera path at
     1920x1080 (ms per frame, per-stage times)."""
     S = nrc_setup(torch, dev, scene, mode, stream)
-    what = ("config-3 scene (box + SDF tori + fBm medium), RGB" if mode == "box"
-            else "config4 static view: config-2 scene")
+    what = {"box": "config-3 scene (box + SDF tori + fBm medium), RGB",
+            "config3": "config 3: box + SDF tori (256^3 half grid) + 128^3 half fBm medium, four wavelengths per path "
+                       "(four-wavelength cache, 16 spectral bins)"}.get(mode, "config4 static view: config-2 scene")
     res = {"workload": f"{what} {S['w']}x{S['h']}, max depth {S['depth']}, {k} spp per frame, cache trained online "
                        f"(65536 training paths, {steps} steps of 16384 per frame), spread constant {spread_c}",
            "oracle_spp": S["ref_spp"], "oracle_ms": round(S["ref_ms"], 1), "plain_spp": S["target"],
@@ -308,10 +319,20 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream, k: int = 1, spread_
     res.update(nrc_curve(torch, dev, S, stream, k, spread_c, steps))
     if mode == "box":
         return res
-    # the spline camera path at the full config-4 resolution
+    if mode == "config3":
+        res["config4_spline"] = spline_path(torch, dev, Scene(scenes.spheres_scene(), device=dev.index), stream)
+        return res
+    res["spline_1920x1080"] = spline_path(torch, dev, S["scene"], stream)
+    return res
+
+
+def spline_path(torch, dev, scene: Scene, stream) -> dict:
+    """Config 4's 300-frame seeded spline camera path at 1920x1080 on the
+    config-2 scene, 1 spp per frame with the cache trained online: ms per frame
+    and per stage (the first 10 frames untimed)."""
     cams = scenes.spline_cameras(frames=300)
     acc_s = torch.zeros(1920 * 1080 * 3, dtype=torch.float64, device=dev)
-    cache2 = RadianceCache(S["scene"], nrc_config(seed=2))
+    cache2 = RadianceCache(scene, nrc_config(seed=2))
     tot = {"render": 0.0, "infer": 0.0, "train": 0.0, "total": 0.0, "q": 0, "rays": 0}
     for j, c in enumerate(cams):
         st = cache2.render_frame(c, make_params(spp=1, max_depth=DEPTH, frame_offset=40_000_000 + j), None,
@@ -324,21 +345,20 @@ def measure_nrc(torch, dev, scene: Scene, mode: str, stream, k: int = 1, spread_
             tot["q"] += st.queries
             tot["rays"] += st.extension_rays + st.shadow_rays
     n = len(cams) - 10
-    res["spline_1920x1080"] = {
+    return {
         "frames": len(cams), "timed_frames": n, "ms_per_frame": round(tot["total"] / n, 3),
         "render_ms": round(tot["render"] / n, 3), "infer_ms": round(tot["infer"] / n, 3),
         "train_ms": round(tot["train"] / n, 3), "queries_per_frame": int(tot["q"] / n),
         "tracer_mrays_per_s": round(tot["rays"] / (tot["render"] / 1e3) / 1e6, 1),
         "last_loss": round(float(st.loss), 5)}
-    return res
 
 
 def sweep_nrc(torch, dev, stream, mode: str = "box") -> dict:
     """The cache's time-to-relMSE over spp per frame {1, 4, 16} x spread
     constant {0.01, 0.1, 1} x optimiser steps per frame {1, 4}, against one
     oracle and one plain measurement."""
-    S = nrc_setup(torch, dev, None if mode == "box" else Scene(scenes.spheres_scene(), device=dev.index), mode,
-                  stream)
+    S = nrc_setup(torch, dev, None if mode in ("box", "config3") else Scene(scenes.spheres_scene(), device=dev.index),
+                  mode, stream)
     runs = []
     for k in (1, 4, 16):
         for c in (0.01, 0.1, 1.0):
@@ -752,13 +772,14 @@ def main():
                     help="record two frames and run the bilateral filter three times (for ncu captures)")
     ap.add_argument("--configs", type=int, default=16,
                     help="also time configs 1, 3 and 5 (this many batch jobs); 0 skips")
-    ap.add_argument("--nrc", choices=("off", "small", "full", "box"), default="small",
-                    help="radiance-cache time-to-relMSE measurement (small: 480x270, full: 1920x1080, "
-                         "box: the config-3 scene in RGB at 480x270)")
+    ap.add_argument("--nrc", choices=("off", "small", "full", "box", "config3"), default="config3",
+                    help="radiance-cache time-to-relMSE measurement (config3: the config-3 scene with four "
+                         "wavelengths at 1280x720, plus config 4's spline path; small / full: the config-2 scene "
+                         "at 480x270 / 1920x1080; box: the config-3 scene in RGB at 480x270)")
     ap.add_argument("--nrc-spp", type=int, default=1, help="samples per pixel of a cache frame")
     ap.add_argument("--nrc-c", type=float, default=0.01, help="spread constant of the cache's termination rule")
     ap.add_argument("--nrc-steps", type=int, default=4, help="optimiser steps per cache frame")
-    ap.add_argument("--nrc-sweep", choices=("box", "small"), default=None,
+    ap.add_argument("--nrc-sweep", choices=("box", "small", "config3"), default=None,
                     help="time-to-relMSE over spp per frame x spread constant x optimiser steps, then exit")
     ap.add_argument("--profile-nrc", action="store_true",
                     help="six radiance-cache frames (for ncu captures of the cache kernels)")

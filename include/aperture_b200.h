@@ -364,19 +364,28 @@ ar_status ar_nrc_render_frame(ar_nrc* nrc, const ar_camera* camera, const ar_ren
                               void* stream);
 /* Options: AR_NRC_OPT_TENSOR_PATH selects the inference kernel, 1 (default)
  * tcgen05.mma with tensor-memory accumulators (128 rows per CTA), 0 the
- * warp-level mma.sync kernel (32 rows per warp). */
-enum { AR_NRC_OPT_TENSOR_PATH = 1 };
+ * warp-level mma.sync kernel (32 rows per warp).  AR_NRC_OPT_SPECTRAL sets
+ * the cache's mode before its first frame: 0 (default) RGB, 4 for frames of
+ * four wavelengths per path (params->spectral = 4; needs the scene's spectral
+ * tables): the 16 outputs are then the outgoing spectral radiance at 16
+ * wavelength bins of 26.25 nm over [360, 780] nm, interpolated linearly at
+ * each of the path's wavelengths, and the cache adds the path's XYZ estimate. */
+enum { AR_NRC_OPT_TENSOR_PATH = 1, AR_NRC_OPT_SPECTRAL = 2 };
 ar_status ar_nrc_set_option(ar_nrc* nrc, int32_t option, int32_t value);
 /* Parameters as fp32: tables (levels x 2^log2_entries x 2) and MLP weights
  * (21504: layers 0-4 [64][64], layer 5 [16][64], [out][in]); NULL skips. */
 ar_status ar_nrc_get_params(const ar_nrc* nrc, float* table, float* weights);
 ar_status ar_nrc_set_params(ar_nrc* nrc, const float* table, const float* weights);
 /* Direct use of the network: n vertices of 16 floats (position, pad;
- * direction, roughness; normal, pad; albedo, pad) -> n x 3 predictions; and
- * `steps` optimiser steps over n training samples (the vertex layout with
- * the target radiance in the three pad floats: r at 3, g at 11, b at 15),
- * batches taken in order, the mean loss of each step to losses[steps].  Host
- * buffers. */
+ * direction, roughness; normal, pad; albedo, pad) -> n x 3 predictions (RGB
+ * cache) or n x 16 spectral bins (four-wavelength cache); and `steps`
+ * optimiser steps over n training samples of 20 floats (the vertex layout
+ * with the target radiance in the three pad floats: r at 3, g at 11, b at
+ * 15; then 4 floats, unused by the RGB cache; the four-wavelength cache reads
+ * the targets of wavelengths 0-2 from the pads, that of wavelength 3 from
+ * float 16 and the hero wavelength from float 17, a negative target being
+ * left out), batches taken in order, the mean loss of each step to
+ * losses[steps].  Host buffers. */
 ar_status ar_nrc_infer(ar_nrc* nrc, const float* vertices, size_t n, float* out_rgb);
 ar_status ar_nrc_train(ar_nrc* nrc, const float* samples, size_t n, int32_t steps, float* losses);
 /* Gradients of the mean relative L2 loss over n <= train_batch samples with

@@ -163,6 +163,74 @@ def predict(geo: Geometry, v: np.ndarray, table: np.ndarray, W: np.ndarray) -> n
     return np.exp(np.minimum(raw[:, :3], 15.0)).astype(np.float32)
 
 
+# Four-wavelength cache: 16 spectral bins of 26.25 nm over [360, 780] nm,
+# linear interpolation between bin centres (csrc/nrc.cuh, nrc_bin_weights),
+# the path's wavelengths the hero and its rotations by 105 nm in [360, 780].
+BINS, LAMBDA0, BIN_WIDTH = 16, 360.0, 26.25
+
+
+def rotate_lambda(h, i):
+    """csrc/spectral.cuh rotate_lambda, in float32"""
+    x = (np.asarray(h, np.float32) - np.float32(360.0)) + np.float32(105.0) * np.float32(i)
+    x = np.where(x >= np.float32(420.0), x - np.float32(420.0), x).astype(np.float32)
+    return (np.float32(360.0) + x).astype(np.float32)
+
+
+def bin_weights(lam):
+    x = (np.asarray(lam, np.float32) - np.float32(LAMBDA0)) / np.float32(BIN_WIDTH) - np.float32(0.5)
+    x = np.clip(x, 0.0, BINS - 1).astype(np.float32)
+    b = np.minimum(np.floor(x).astype(np.int64), BINS - 2)
+    return b, (x - b.astype(np.float32)).astype(np.float32)
+
+
+def predict_bins(geo: Geometry, v: np.ndarray, table: np.ndarray, W: np.ndarray) -> np.ndarray:
+    X, _ = encode(geo, v, table)
+    raw, _ = forward(X, layer_weights(W))
+    return np.exp(np.minimum(raw, 15.0)).astype(np.float32)
+
+
+def loss_and_gradients_spectral(geo: Geometry, s: np.ndarray, table: np.ndarray, W: np.ndarray):
+    """The four-wavelength loss over samples s (n, 20; targets of wavelengths
+    0-2 at 3, 11, 15, of wavelength 3 at 16, hero wavelength at 17; negative
+    targets left out): relative L2 of the interpolated bins per wavelength,
+    normalised by 4 n, and its gradients (bf16 roundings as the GPU's)."""
+    n = len(s)
+    X, cw = encode(geo, s[:, :16], table)
+    Ws = layer_weights(W)
+    raw, acts = forward(X, Ws)
+    e = np.exp(np.minimum(raw, 15.0))
+    tg = s[:, [3, 11, 15, 16]].astype(np.float32)
+    norm = 1.0 / (4.0 * n)
+    d = np.zeros((n, OUT))
+    loss = 0.0
+    for w in range(4):
+        b, f = bin_weights(rotate_lambda(s[:, 17], w))
+        rows = np.arange(n)
+        pred = (1.0 - f) * e[rows, b] + f * e[rows, b + 1]
+        ok = tg[:, w] >= 0
+        den = pred * pred + 0.01
+        diff = pred - tg[:, w]
+        loss += float(np.sum(np.where(ok, diff * diff / den, 0.0)) * norm)
+        g = np.where(ok, 2.0 * diff / den * norm, 0.0)
+        np.add.at(d, (rows, b), g * (1.0 - f) * e[rows, b])
+        np.add.at(d, (rows, b + 1), g * f * e[rows, b + 1])
+    g = bf16(d.astype(np.float32))
+    grads = [None] * LAYERS
+    for l in range(LAYERS - 1, -1, -1):
+        grads[l] = g.T @ acts[l]
+        dIn = g @ Ws[l]
+        if l == 0:
+            dX = dIn
+            break
+        g = bf16(np.where(acts[l] > 0, dIn, 0.0).astype(np.float32))
+    dW = np.concatenate([gr.reshape(-1) for gr in grads])
+    dT = np.zeros((geo.levels * geo.entries, 2), np.float64)
+    for l, (idx, w) in enumerate(cw):
+        for c in range(8):
+            np.add.at(dT, idx[:, c], w[:, c:c + 1].astype(np.float64) * dX[:, 2 * l:2 * l + 2])
+    return loss, dT, dW
+
+
 def loss_and_gradients(geo: Geometry, s: np.ndarray, table: np.ndarray, W: np.ndarray, exact: bool = False,
                        den_fixed: np.ndarray | None = None):
     """Mean relative L2 loss over samples s (n, 16; targets at 3, 11, 15) and its

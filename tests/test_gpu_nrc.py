@@ -173,3 +173,76 @@ def test_nrc_frames_of_several_samples():
     assert np.isfinite(a).all() and abs(a.mean() - b.mean()) < 0.02 * b.mean()
     last = out.cpu().numpy()
     assert abs(last.mean() - a.mean()) < 0.1 * a.mean()    # out_rgb is the k-sample mean, not the sum
+
+
+def _spectral_cache(**kw):
+    import spectral_tables
+    if not spectral_tables.available():
+        pytest.skip("spectral tables not built")
+    cfg = nrc_config(bounds=BOUNDS, **kw)
+    sc = Scene(scenes.box_scene())
+    sc.set_spectral(32)
+    c = RadianceCache(sc, cfg)
+    c.set_spectral(4)
+    return sc, c, cfg
+
+
+@pytest.mark.gpu
+def test_nrc_spectral_inference_equals_oracle():
+    """Four-wavelength cache: the 16 exp'd spectral bins of the tcgen05 and
+    mma.sync kernels are identical and agree with the numpy restatement."""
+    _, c, cfg = _spectral_cache(log2_entries=15)
+    table, w = _random_params(c, 21)
+    v = _vertices(6000, 22)
+    c.set_tensor_path(True)
+    a = c.infer(v)
+    c.set_tensor_path(False)
+    b = c.infer(v)
+    assert a.shape == (6000, 16) and np.array_equal(a, b)
+    o = N.predict_bins(_geo(cfg), v, table, w)
+    rel = np.abs(a - o) / np.maximum(np.abs(o), 1e-6)
+    assert np.median(rel) < 1e-3 and np.mean(rel) < 5e-3
+
+
+@pytest.mark.gpu
+def test_nrc_spectral_gradients_equal_oracle():
+    """Four-wavelength loss (per-wavelength relative L2 of the interpolated
+    bins, negative targets left out) and its gradients against the numpy
+    restatement."""
+    _, c, cfg = _spectral_cache(log2_entries=15, train_batch=2048)
+    table, w = _random_params(c, 23, 0.3, 0.2)
+    rng = np.random.default_rng(24)
+    s = np.zeros((2000, 20), np.float32)
+    s[:, :16] = _vertices(2000, 25)
+    s[:, [3, 11, 15, 16]] = rng.uniform(0.05, 3.0, (2000, 4))
+    s[rng.random(2000) < 0.1, 16] = -1.0            # wavelength 3 without throughput
+    s[:, 17] = rng.uniform(360.0, 780.0, 2000)       # hero wavelength
+    tg, wg, loss = c.gradients(s)
+    lo, dT, dW = N.loss_and_gradients_spectral(_geo(cfg), s, table, w)
+    assert abs(loss - lo) <= 2e-3 * abs(lo)
+    assert np.linalg.norm(wg - dW) <= 2e-2 * np.linalg.norm(dW)
+    dT = dT.reshape(-1)
+    assert np.linalg.norm(tg - dT) <= 2e-2 * np.linalg.norm(dT)
+
+
+@pytest.mark.gpu
+def test_nrc_spectral_frames_converge_to_plain_image():
+    """Frames of four wavelengths per path with the four-wavelength cache: the
+    XYZ image converges to the plain four-wavelength tracer's within a few
+    percent per channel (the cache's bias), with paths ending in the cache."""
+    import torch
+    sc, c, cfg = _spectral_cache(log2_entries=16, train_paths=2048, train_batch=2048, train_steps=2)
+    cam = scenes.box_camera(48, 48)
+    ref, _ = sc.render(cam, make_params(spp=1024, max_depth=8, spectral=4))
+    acc = torch.zeros(48 * 48 * 3, dtype=torch.float64, device="cuda")
+    frames = 128
+    st = None
+    for f in range(frames):
+        st = c.render_frame(cam, make_params(spp=2, max_depth=8, spectral=4, frame_offset=2 * f), None,
+                            acc.data_ptr(), train=True, stats=(f == frames - 1))
+    assert st.queries > 500 and st.train_samples > 500
+    img = (acc / (2 * frames)).cpu().numpy().reshape(48, 48, 3)
+    m, r = img.mean(axis=(0, 1)), ref.reshape(48, 48, 3).mean(axis=(0, 1))
+    assert np.all(np.abs(m - r) < 0.05 * r), (m, r)
+    with pytest.raises(Exception):   # a frame of another mode than the cache's
+        c.render_frame(cam, make_params(spp=1, max_depth=8), None, acc.data_ptr(), train=False)
