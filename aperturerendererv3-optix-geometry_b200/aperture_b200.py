@@ -166,7 +166,7 @@ class BatchTuning(ctypes.Structure):
 class BatchStats(ctypes.Structure):
     _fields_ = [("total_ms", c_float), ("iterations_per_graph", c_int32), ("paths", c_int64),
                 ("extension_rays", c_int64), ("shadow_rays", c_int64), ("graph_launches", c_int64),
-                ("graph_nodes", c_int64), ("kernel_launches", c_int64)]
+                ("graph_nodes", c_int64), ("kernel_launches", c_int64), ("loop_passes", c_int64)]
 
 
 class ScreenGBuffer(ctypes.Structure):

@@ -787,19 +787,48 @@ void job_alloc(JobWs& w, int64_t pool, int64_t npix, int grid_trace)
     w.ovf = reinterpret_cast<uint32_t*>(b + o_ovf);
 }
 
+// Device-side end test of the batch loop: after each pass of the loop body
+// every job's retired-path count is compared with its total; the conditional
+// handle keeps the WHILE node looping while a job has paths left and the pass
+// count is below its bound (then the error word gets bit 0 and the loop ends).
+struct BatchDrain {
+    const ar::PoolCtl* const* ctl;  // per job
+    const int64_t* total;           // per job
+    int32_t jobs;
+    int32_t max_passes;
+    int32_t* passes;                // [0] passes run, [1] error word
+};
+
+__global__ void k_batch_drain(BatchDrain d, cudaGraphConditionalHandle h)
+{
+    __shared__ int open;
+    if (threadIdx.x == 0) open = 0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < d.jobs; j += blockDim.x)
+        if (d.ctl[j]->retired < d.total[j]) atomicOr(&open, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int n = d.passes[0] + 1;
+        d.passes[0] = n;
+        const bool again = open != 0 && n < d.max_passes;
+        if (open != 0 && !again) d.passes[1] |= 1;
+        cudaGraphSetConditional(h, again ? 1u : 0u);
+    }
+}
+
 struct BatchResources {
     std::vector<JobWs> jobs;
+    void* drain_mem = nullptr;      // BatchDrain tables and counters
     cudaEvent_t fork = nullptr;
     cudaStream_t orch = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int64_t* retired_host = nullptr;
     ~BatchResources()
     {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (fork) cudaEventDestroy(fork);
-        if (retired_host) cudaFreeHost(retired_host);
+        if (drain_mem) cudaFree(drain_mem);
         if (orch) cudaStreamDestroy(orch);
         for (JobWs& w : jobs) {
             if (w.done) cudaEventDestroy(w.done);
@@ -884,7 +913,6 @@ ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_
     struct Ev { cudaEvent_t a, b; ~Ev() { cudaEventDestroy(a); cudaEventDestroy(b); } } evs{t0, t1};
     BatchResources R;
     R.jobs.resize(static_cast<size_t>(njobs));
-    ck(cudaMallocHost(&R.retired_host, sizeof(int64_t) * njobs), "pinned poll buffer");
     ck(cudaEventCreateWithFlags(&R.fork, cudaEventDisableTiming), "event");
     // the batch runs on a stream of its own (the legacy default stream cannot
     // be captured), ordered after the caller's stream
@@ -918,9 +946,51 @@ ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_
         ck(cudaEventRecord(w.done, w.st), "event record");
         ck(cudaStreamWaitEvent(st, w.done, 0), "join");
     }
-    // One graph: K wavefront iterations of every job, each job on its own
-    // branch, plus the copy of every job's retired count.
-    ck(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int64_t maxDepth = 0, maxRatio = 0;
+    for (int j = 0; j < njobs; ++j) {
+        maxDepth = std::max<int64_t>(maxDepth, jobs[j].params.max_depth);
+        const int64_t admit = std::max<int64_t>(1, std::min<int64_t>(R.jobs[j].pool, R.jobs[j].npix));
+        maxRatio = std::max<int64_t>(maxRatio, R.jobs[j].total / admit + 2);
+    }
+    const int64_t maxPasses = (maxRatio * (maxDepth + 2)) / K + 2;
+    // The drain test's tables: per job its pool control block and path total.
+    {
+        const size_t nj = static_cast<size_t>(njobs);
+        R.drain_mem = dalloc<unsigned char>(nj * 16 + 64, "batch drain tables");
+        std::vector<const ar::PoolCtl*> ctls(nj);
+        std::vector<int64_t> totals(nj);
+        for (size_t j = 0; j < nj; ++j) {
+            ctls[j] = R.jobs[j].ctl;
+            totals[j] = R.jobs[j].total;
+        }
+        unsigned char* m = static_cast<unsigned char*>(R.drain_mem);
+        ck(cudaMemcpyAsync(m, ctls.data(), nj * 8, cudaMemcpyHostToDevice, st), "drain tables");
+        ck(cudaMemcpyAsync(m + nj * 8, totals.data(), nj * 8, cudaMemcpyHostToDevice, st), "drain tables");
+        ck(cudaMemsetAsync(m + nj * 16, 0, 64, st), "drain counters");
+    }
+    BatchDrain dr;
+    dr.ctl = reinterpret_cast<const ar::PoolCtl* const*>(R.drain_mem);
+    dr.total = reinterpret_cast<const int64_t*>(static_cast<unsigned char*>(R.drain_mem) + njobs * 8);
+    dr.jobs = njobs;
+    dr.max_passes = static_cast<int32_t>(std::min<int64_t>(maxPasses, INT32_MAX));
+    dr.passes = reinterpret_cast<int32_t*>(static_cast<unsigned char*>(R.drain_mem) + njobs * 16);
+    // One graph, launched once: a WHILE conditional node whose body runs K
+    // wavefront iterations of every job (each job on its own branch) and then
+    // the drain test, which sets the node's condition on the device -- no host
+    // round trip between passes.
+    ck(cudaGraphCreate(&R.graph, 0), "graph create");
+    cudaGraphConditionalHandle cond;
+    ck(cudaGraphConditionalHandleCreate(&cond, R.graph, 1, cudaGraphCondAssignDefault), "conditional handle");
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t loop;
+    ck(cudaGraphAddNode(&loop, R.graph, nullptr, 0, &cp), "conditional node");
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    ck(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+       "begin capture");
     ck(cudaEventRecord(R.fork, st), "fork");
     int64_t launches = 0;
     for (int j = 0; j < njobs; ++j) {
@@ -931,32 +1001,22 @@ ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_
                                  w.ovf, w.err, w.accum, nullptr, K, &w.cur, jb.scene->grid_trace,
                                  jb.scene->sm_count * 4, w.st, &launches, nullptr),
            "capture iterations");
-        ck(cudaMemcpyAsync(R.retired_host + j, &w.ctl->retired, sizeof(int64_t), cudaMemcpyDeviceToHost, w.st),
-           "capture poll");
         ck(cudaEventRecord(w.done, w.st), "join");
         ck(cudaStreamWaitEvent(st, w.done, 0), "join");
     }
-    ck(cudaStreamEndCapture(st, &R.graph), "end capture");
+    k_batch_drain<<<1, 256, 0, st>>>(dr, cond);
+    ck(cudaGetLastError(), "drain test");
+    cudaGraph_t captured = nullptr;
+    ck(cudaStreamEndCapture(st, &captured), "end capture");
     ck(cudaGraphInstantiate(&R.exec, R.graph, 0), "graph instantiate");
     size_t nodes = 0;
-    cudaGraphGetNodes(R.graph, nullptr, &nodes);
-    int64_t maxDepth = 0, maxRatio = 0;
-    for (int j = 0; j < njobs; ++j) {
-        maxDepth = std::max<int64_t>(maxDepth, jobs[j].params.max_depth);
-        const int64_t admit = std::max<int64_t>(1, std::min<int64_t>(R.jobs[j].pool, R.jobs[j].npix));
-        maxRatio = std::max<int64_t>(maxRatio, R.jobs[j].total / admit + 2);
-    }
-    const int64_t maxReplays = (maxRatio * (maxDepth + 2)) / K + 2;
-    int64_t replays = 0;
-    for (;;) {
-        ck(cudaGraphLaunch(R.exec, st), "graph launch");
-        ck(cudaStreamSynchronize(st), "sync");
-        ++replays;
-        bool all = true;
-        for (int j = 0; j < njobs; ++j) all = all && (R.retired_host[j] >= R.jobs[j].total);
-        if (all) break;
-        if (replays > maxReplays) return fail(AR_ERR_DEVICE_FAULT, "batch path pools did not drain");
-    }
+    cudaGraphGetNodes(body, nullptr, &nodes);
+    ck(cudaGraphLaunch(R.exec, st), "graph launch");
+    int32_t dres[2] = {0, 0};
+    ck(cudaMemcpyAsync(dres, dr.passes, sizeof(dres), cudaMemcpyDeviceToHost, st), "pass count");
+    ck(cudaStreamSynchronize(st), "sync");
+    if (dres[1] != 0) return fail(AR_ERR_DEVICE_FAULT, "batch path pools did not drain");
+    const int64_t replays = dres[0];
     // outputs, counters, error words
     unsigned long long ext = 0, sh = 0;
     for (int j = 0; j < njobs; ++j) {
@@ -985,7 +1045,8 @@ ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_
         stats->paths = totalAll;
         stats->extension_rays = static_cast<int64_t>(ext);
         stats->shadow_rays = static_cast<int64_t>(sh);
-        stats->graph_launches = replays;
+        stats->graph_launches = 1;
+        stats->loop_passes = replays;
         stats->graph_nodes = static_cast<int64_t>(nodes);
         stats->kernel_launches = launches * replays;
         stats->iterations_per_graph = K;

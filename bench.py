@@ -40,7 +40,7 @@ sys.path.insert(0, PKG)
 
 import scenes  # noqa: E402
 from aperture_b200 import Camera, RadianceCache, RenderParams, RenderStats, Scene, make_params, nrc_config  # noqa: E402
-from sharding import job_totals, rank_frame_offset, reduce_accumulators  # noqa: E402
+from sharding import job_totals, partition_jobs, rank_frame_offset, reduce_accumulators  # noqa: E402
 
 METRIC = "Mrays/s"
 WIDTH, HEIGHT, SPP, DEPTH = 1920, 1080, 64, 12
@@ -431,16 +431,113 @@ def measure_denoise(torch, dev, stream, scene: Scene, frames: int = 8, reps: int
             "bound": "compute (225 pair weights per pixel from shared memory)"}
 
 
+def measure_config5(torch, dev, stream, njobs: int = 64) -> dict:
+    """Config 5: njobs seeded render jobs -- resolutions log-uniform in
+    128-1024 per axis, spp uniform in {4, 16, 64, 256}, scenes from the
+    config-2 generator with triangle counts log-uniform in 10K-2M and their own
+    seeds, every second job four wavelengths per path, every other pair of jobs
+    with a radiance cache of its own.  The jobs without a cache run in one
+    launch of the batch graph (device-side loop) after the autotuner; each
+    cache job renders its samples as cache frames of 4 samples with online
+    training (four-wavelength cache for the spectral ones).  Per job: paths,
+    rays, Mrays/s of its part; relMSE against a 4096-spp FP64 image of the
+    plain tracer for every eighth job."""
+    import concurrent.futures as cf
+
+    import spectral_tables
+    from aperture_b200 import autotune_batch, render_batch
+    from sharding import job_cost
+    spectral_ok = spectral_tables.available()
+    rng = np.random.default_rng(0xA11CE + 5)
+    specs = []
+    for j in range(njobs):
+        tris = float(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        nsph = max(8, int(round(tris / 1280)))
+        w = int(np.exp(rng.uniform(np.log(128), np.log(1024))))
+        h = int(np.exp(rng.uniform(np.log(128), np.log(1024))))
+        spp = int(rng.choice([4, 16, 64, 256]))
+        specs.append({"job": j, "triangles": nsph * 1280 + 2, "spheres": nsph, "width": w, "height": h, "spp": spp,
+                      "spectral": 4 if (spectral_ok and j % 2 == 1) else 0, "cache": (j // 2) % 2 == 1})
+    t0 = time.perf_counter()
+
+    def build(sp):
+        sc = Scene(scenes.spheres_scene(seed=0xA11CE + 100 + sp["job"], n_spheres=sp["spheres"]), device=dev.index)
+        if sp["spectral"]:
+            sc.set_spectral(32)
+        return sc
+
+    with cf.ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 4)) as ex:
+        built = list(ex.map(build, specs))
+    build_s = time.perf_counter() - t0
+    outs = [torch.empty(sp["width"] * sp["height"] * 3, dtype=torch.float32, device=dev) for sp in specs]
+    torch.cuda.synchronize(dev)
+    plain = [k for k, sp in enumerate(specs) if not sp["cache"]]
+    jobs = [(built[k], scenes.spheres_camera(specs[k]["width"], specs[k]["height"]),
+             make_params(spp=specs[k]["spp"], max_depth=DEPTH, spectral=specs[k]["spectral"]), outs[k].data_ptr(), None)
+            for k in plain]
+    tune = autotune_batch(jobs, probe_spp=4, stream=stream.cuda_stream)
+    render_batch(jobs, stream=stream.cuda_stream)          # warm-up with the tuned knobs
+    st = render_batch(jobs, stream=stream.cuda_stream)
+    batch_rays = st.extension_rays + st.shadow_rays
+    # cache jobs: frames of 4 samples per pixel, cache trained online
+    cache_ms, cache_rays, cache_paths = 0.0, 0, 0
+    for k, sp in enumerate(specs):
+        if not sp["cache"]:
+            continue
+        cam = scenes.spheres_camera(sp["width"], sp["height"])
+        c = RadianceCache(built[k], nrc_config(seed=k + 1))
+        if sp["spectral"]:
+            c.set_spectral(4)
+        acc = torch.zeros(sp["width"] * sp["height"] * 3, dtype=torch.float64, device=dev)
+        ms = 0.0
+        for f in range(0, sp["spp"], 4):
+            fs = c.render_frame(cam, make_params(spp=4, max_depth=DEPTH, spectral=sp["spectral"], frame_offset=f),
+                                None, acc.data_ptr(), train=True, stats=True, stream=stream.cuda_stream)
+            ms += fs.total_ms
+            cache_rays += fs.extension_rays + fs.shadow_rays
+        cache_paths += sp["width"] * sp["height"] * sp["spp"]
+        cache_ms += ms
+        sp["cache_ms"] = round(ms, 3)
+        outs[k].copy_((acc / sp["spp"]).float())
+    # relMSE of every eighth job against a 4096-spp FP64 image of the plain tracer
+    for k in range(0, njobs, 8):
+        sp = specs[k]
+        cam = scenes.spheres_camera(sp["width"], sp["height"])
+        ref, _ = fp64_reference(torch, dev, built[k], cam,
+                                make_params(spp=4096, max_depth=DEPTH, spectral=sp["spectral"]), 4096, 60_000_000,
+                                stream)
+        sp["relmse"] = relmse(outs[k], ref)
+    costs = [job_cost(sp["width"], sp["height"], sp["spp"], sp["triangles"], sp["spectral"], sp["cache"])
+             for sp in specs]
+    total_ms = st.total_ms + cache_ms
+    return {"workload": f"{njobs} seeded jobs: config-2 generator with 10K-2M triangles (log-uniform), resolutions "
+                        "log-uniform 128-1024 per axis, spp in {4,16,64,256}, every second job four wavelengths, "
+                        "half the jobs with their own radiance cache (frames of 4 spp, trained online); jobs "
+                        "without a cache in one launch of the batch graph (device-side loop), autotuned",
+            "jobs": njobs, "ms": round(total_ms, 3),
+            "mrays_per_s": round((batch_rays + cache_rays) / (total_ms / 1e3) / 1e6, 1),
+            "batch": {"jobs": len(plain), "ms": round(st.total_ms, 3),
+                      "mrays_per_s": round(batch_rays / (st.total_ms / 1e3) / 1e6, 1),
+                      "msamples_per_s": round(st.paths / (st.total_ms / 1e3) / 1e6, 2), "paths": st.paths,
+                      "graph_launches": st.graph_launches, "loop_passes": st.loop_passes,
+                      "autotuned": {"iterations_per_graph": tune.iterations_per_graph, "path_budget": tune.path_budget,
+                                    "probe_ms_best": round(tune.best_ms, 3),
+                                    "probe_ms_default": round(tune.default_ms, 3)}},
+            "cache_jobs": {"jobs": njobs - len(plain), "ms": round(cache_ms, 3), "paths": cache_paths,
+                           "mrays_per_s": round(cache_rays / max(cache_ms / 1e3, 1e-9) / 1e6, 1)},
+            "scene_build_s": round(build_s, 1),
+            "lpt_2gpu_makespan_share": round(max(sum(costs[j] for j in p) for p in partition_jobs(costs, 2))
+                                             / sum(costs), 4),
+            "per_job": specs}
+
+
 def measure_configs(torch, dev, stream, c5_jobs: int) -> dict:
     """The other benchmark configurations, one timed render each after one
     warm-up (device time from the library's CUDA events): config 1 (box,
     256x256, 16 spp), config 3 (box + SDF torus on a 256^3 half grid + 128^3
     half fBm medium, 1280x720, 256 spp, depth 16, four wavelengths when the
-    spectral tables are present) and config 5 (seeded jobs of uneven
-    resolution, spp, scene size, RGB/spectral in one CUDA graph after the
-    autotuner; c5_jobs of them, triangle counts log-uniform in 10K-500K)."""
+    spectral tables are present) and config 5 (measure_config5, c5_jobs jobs)."""
     import spectral_tables
-    from aperture_b200 import autotune_batch, render_batch
     res = {}
     out = torch.empty(1280 * 720 * 3, dtype=torch.float32, device=dev)
     sc1 = Scene(scenes.box_scene(), device=dev.index)
@@ -458,41 +555,8 @@ def measure_configs(torch, dev, stream, c5_jobs: int) -> dict:
                                    "medium (sigma_t 2, albedo 0.8, g 0.3), 1280x720, 256 spp, depth 16, "
                                    + ("4 hero wavelengths, RGB LUT 64^3" if spectral else "RGB (spectral tables absent)"),
                           **r)
-    rng = np.random.default_rng(0xA11CE + 5)
-    jobs, outs, info = [], [], []
-    cache = {}
-    for j in range(c5_jobs):
-        tris = float(np.exp(rng.uniform(np.log(1e4), np.log(5e5))))
-        nsph = max(8, int(tris // 1280))
-        w = int(np.exp(rng.uniform(np.log(128), np.log(1024))))
-        h = int(np.exp(rng.uniform(np.log(128), np.log(1024))))
-        spp = int(rng.choice([4, 16, 64, 256]))
-        spec = spectral and j % 2 == 1
-        key = (nsph, spec)
-        if key not in cache:
-            sc = Scene(scenes.spheres_scene(seed=0xA11CE + 100 + j, n_spheres=nsph), device=dev.index)
-            if spec:
-                sc.set_spectral(32)
-            cache[key] = sc
-        sc = cache[key]
-        cam = scenes.spheres_camera(w, h)
-        o = torch.empty(w * h * 3, dtype=torch.float32, device=dev)
-        outs.append(o)
-        jobs.append((sc, cam, make_params(spp=spp, max_depth=DEPTH, spectral=1 if spec else 0), o.data_ptr(), None))
-        info.append({"triangles": nsph * 1280 + 2, "width": w, "height": h, "spp": spp, "spectral": bool(spec)})
-    tune = autotune_batch(jobs, probe_spp=4, stream=stream.cuda_stream)
-    render_batch(jobs, stream=stream.cuda_stream)          # warm-up with the tuned knobs
-    st = render_batch(jobs, stream=stream.cuda_stream)
-    res["config5"] = {"workload": f"{c5_jobs} seeded jobs (config-2 generator with 8-390 icospheres), resolutions "
-                                  "log-uniform 128-1024 per axis, spp in {4,16,64,256}, every second job spectral; "
-                                  "one CUDA graph, autotuned (radiance caches per job not included)",
-                      "ms": round(st.total_ms, 3),
-                      "mrays_per_s": round((st.extension_rays + st.shadow_rays) / (st.total_ms / 1e3) / 1e6, 1),
-                      "msamples_per_s": round(st.paths / (st.total_ms / 1e3) / 1e6, 2),
-                      "paths": st.paths, "graph_launches": st.graph_launches,
-                      "autotuned": {"iterations_per_graph": tune.iterations_per_graph, "path_budget": tune.path_budget,
-                                    "probe_ms_best": round(tune.best_ms, 3), "probe_ms_default": round(tune.default_ms, 3)},
-                      "jobs": info}
+    if c5_jobs > 0:
+        res["config5"] = measure_config5(torch, dev, stream, c5_jobs)
     return res
 
 
@@ -770,7 +834,7 @@ def main():
     ap.add_argument("--no-denoise", action="store_true", help="skip the denoiser measurement")
     ap.add_argument("--profile-denoise", action="store_true",
                     help="record two frames and run the bilateral filter three times (for ncu captures)")
-    ap.add_argument("--configs", type=int, default=16,
+    ap.add_argument("--configs", type=int, default=64,
                     help="also time configs 1, 3 and 5 (this many batch jobs); 0 skips")
     ap.add_argument("--nrc", choices=("off", "small", "full", "box", "config3"), default="config3",
                     help="radiance-cache time-to-relMSE measurement (config3: the config-3 scene with four "

@@ -463,17 +463,20 @@ typedef struct ar_batch_stats {
     int64_t paths;
     int64_t extension_rays;
     int64_t shadow_rays;
-    int64_t graph_launches;/* replays of the batch graph                       */
-    int64_t graph_nodes;   /* nodes of the batch graph                         */
-    int64_t kernel_launches;/* kernels run (graph nodes x replays)             */
+    int64_t graph_launches;/* launches of the batch graph (1)                  */
+    int64_t graph_nodes;   /* nodes of the loop body                           */
+    int64_t kernel_launches;/* kernels run (body kernels x loop passes)         */
+    int64_t loop_passes;   /* passes of the device-side loop                   */
 } ar_batch_stats;
 
 /* Many render jobs of uneven resolution, scene and spp at once (config 5 of
  * the benchmark; the reference renders one camera at a time, scene.cu:276-306).
- * Every job keeps its own wavefront pool; one CUDA graph holds
- * iterations_per_graph (0 = 16; rounded up to even) wavefront iterations of
- * every job, each job on its own branch so small jobs run side by side, and is
- * replayed until every job has retired all of its paths.  path_budget (0 =
+ * Every job keeps its own wavefront pool; the batch is ONE launch of a CUDA
+ * graph whose WHILE conditional node repeats a body of iterations_per_graph
+ * (0 = 16; rounded up to even) wavefront iterations of every job -- each job
+ * on its own branch so small jobs run side by side -- followed by a drain test
+ * that sets the node's condition on the device until every job has retired
+ * all of its paths (no host round trip between passes).  path_budget (0 =
  * 2^22) paths in flight are shared among the jobs by their share of the work
  * (a job's own params.wave_paths overrides).  All scenes on one device.
  * Outputs are written on `stream`; the call returns when they are complete. */
