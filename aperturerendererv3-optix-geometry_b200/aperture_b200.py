@@ -196,7 +196,7 @@ EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create",
                     "ar_nrc_get_params", "ar_nrc_set_params", "ar_nrc_infer", "ar_nrc_train", "ar_nrc_gradients",
                     "ar_batch_autotune", "ar_nrc_set_option", "ar_guide_create", "ar_guide_destroy", "ar_guide_render_frame",
                     "ar_guide_get_stats", "ar_guide_get_probe", "ar_guide_probe_eval", "ar_render_frame_denoise",
-                    "ar_denoise_record", "ar_denoise_bilateral")
+                    "ar_denoise_record", "ar_denoise_bilateral", "ar_scene_set_spectral_ex", "ar_spectral_rgb_lut")
 
 
 class ArError(RuntimeError):
@@ -257,6 +257,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_guide_render_frame.argtypes = [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p, c_void_p]
     lib.ar_guide_get_stats.argtypes = [c_void_p, POINTER(GuideStats)]
     lib.ar_guide_get_probe.argtypes = [c_void_p, c_int32, c_void_p]
+    lib.ar_scene_set_spectral_ex.argtypes = [c_void_p, c_void_p, c_size_t, c_int32, c_int32]
+    lib.ar_spectral_rgb_lut.argtypes = [c_void_p, c_size_t, c_int32, c_int32, c_void_p, c_void_p]
+    lib.ar_scene_set_spectral_ex.restype = c_int32
+    lib.ar_spectral_rgb_lut.restype = c_int32
     lib.ar_guide_probe_eval.argtypes = [c_void_p, c_int32] + [c_void_p] * 6 + [c_int64] + [c_void_p] * 4
     for f in ("ar_guide_create", "ar_guide_destroy", "ar_guide_render_frame", "ar_guide_get_stats", "ar_guide_get_probe",
               "ar_guide_probe_eval"):
@@ -342,14 +346,15 @@ class Scene:
         self._h = h
         self.num_objects = len(objects)
 
-    def set_spectral(self, lut_res: int = 64, tables: np.ndarray | None = None) -> None:
+    def set_spectral(self, lut_res: int = 64, tables: np.ndarray | None = None, method: int = 0) -> None:
         """Enable spectral rendering: the reference's tables (spectral_tables.load()
-        unless given) and an lut_res^3 RGB lookup table built on the device."""
+        unless given) and an lut_res^3 RGB lookup table built on the device
+        (method LUT_SIMT, or LUT_TENSOR on the tcgen05 tensor cores)."""
         if tables is None:
             import spectral_tables
             tables = spectral_tables.load()[0]
         t = np.ascontiguousarray(tables, np.float32)
-        _check(_lib.ar_scene_set_spectral(self._h, _ptr(t), t.size, lut_res))
+        _check(_lib.ar_scene_set_spectral_ex(self._h, _ptr(t), t.size, lut_res, int(method)))
         self.lut_res = lut_res
 
     def set_medium(self, density, bounds_min=None, bounds_max=None, sigma_t_max: float = 0.0, albedo=None,
@@ -492,6 +497,25 @@ def _job_array(jobs):
         arr[k].out_rgb = out_ptr
         arr[k].accum = acc_ptr
     return arr
+
+
+LUT_SIMT, LUT_TENSOR = 0, 1
+
+
+def spectral_rgb_lut(res: int, method: int, tables: np.ndarray | None = None, out=None):
+    """ar_spectral_rgb_lut: the res^3 x 4 RGB lookup table built on the current
+    device into a torch tensor (allocated unless given); returns (table, ms)."""
+    import torch
+    load_library()
+    if tables is None:
+        import spectral_tables
+        tables = spectral_tables.load()[0]
+    t = np.ascontiguousarray(tables, np.float32)
+    if out is None:
+        out = torch.empty(res * res * res * 4, dtype=torch.float32, device="cuda")
+    ms = ctypes.c_float(0.0)
+    _check(_lib.ar_spectral_rgb_lut(_ptr(t), t.size, res, int(method), c_void_p(out.data_ptr()), ctypes.byref(ms)))
+    return out, ms.value
 
 
 def autotune_batch(jobs, probe_spp: int = 4, stream: int = 0) -> BatchTuning:

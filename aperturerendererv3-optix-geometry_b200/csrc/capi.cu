@@ -622,6 +622,13 @@ ar_status ar_render(ar_scene* s, const ar_camera* cam, const ar_render_params* p
 
 ar_status ar_scene_set_spectral(ar_scene* s, const float* tables, size_t count, int32_t lut_res)
 {
+    return ar_scene_set_spectral_ex(s, tables, count, lut_res, AR_LUT_SIMT);
+}
+
+ar_status ar_scene_set_spectral_ex(ar_scene* s, const float* tables, size_t count, int32_t lut_res, int32_t method)
+{
+    if (method != AR_LUT_SIMT && method != AR_LUT_TENSOR)
+        return fail(AR_ERR_INVALID_ARGUMENT, "method must be AR_LUT_SIMT or AR_LUT_TENSOR");
     g_last_error.clear();
     if (!s) return fail(AR_ERR_INVALID_ARGUMENT, "scene is NULL");
     if (!tables) return fail(AR_ERR_INVALID_ARGUMENT, "tables is NULL");
@@ -647,6 +654,16 @@ ar_status ar_scene_set_spectral(ar_scene* s, const float* tables, size_t count, 
     s->owned.push_back(rgb);
     ck(cudaMemcpy(tab, tables, count * sizeof(float), cudaMemcpyHostToDevice), "copy spectral tables");
     ck(ar::launch_spectral_luts(tab, lut_res, lam, rgb, s->sm_count, nullptr), "spectral tables");
+    if (method == AR_LUT_TENSOR) {   // the RGB table again, on the tensor cores
+        int* err = dalloc<int>(1, "error word");
+        ck(cudaMemset(err, 0, sizeof(int)), "memset");
+        cudaError_t e = ar::launch_spectral_rgb_lut_tc(tab, lut_res, rgb, err, s->sm_count, nullptr);
+        int h = 0;
+        if (e == cudaSuccess) e = cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+        cudaFree(err);
+        ck(e, "spectral rgb table on the tensor cores");
+        if (h) return fail(AR_ERR_DEVICE_FAULT, "tensor-core table build: an MMA did not complete within its wait limit");
+    }
     ck(cudaDeviceSynchronize(), "spectral tables");
     s->spec_tables = tab;
     s->spec_lut_lam = lam;
@@ -1825,6 +1842,47 @@ ar_status ar_guide_get_probe(const ar_guide* g, int32_t index, float* texels)
     if (index < 0 || index >= std::min(c[0], g->view.capacity)) return fail(AR_ERR_INVALID_ARGUMENT, "probe not allocated");
     ck(cudaMemcpy(texels, g->view.probes + static_cast<size_t>(index) * ar::kPgStride, sizeof(float4) * ar::kPgStride,
                   cudaMemcpyDeviceToHost), "copy probe");
+    return AR_OK;
+    AR_GUARD_END
+}
+
+ar_status ar_spectral_rgb_lut(const float* tables, size_t count, int32_t res, int32_t method, float* out_device,
+                              float* ms)
+{
+    g_last_error.clear();
+    if (!tables || !out_device) return fail(AR_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (count != static_cast<size_t>(ar::kTabFloats))
+        return fail(AR_ERR_INVALID_ARGUMENT, "tables must hold " + std::to_string(ar::kTabFloats) + " floats");
+    if (res < 2 || res > 1024) return fail(AR_ERR_INVALID_ARGUMENT, "res must be in [2, 1024]");
+    if (method != AR_LUT_SIMT && method != AR_LUT_TENSOR)
+        return fail(AR_ERR_INVALID_ARGUMENT, "method must be AR_LUT_SIMT or AR_LUT_TENSOR");
+    if (reinterpret_cast<uintptr_t>(out_device) & 15u) return fail(AR_ERR_INVALID_ARGUMENT, "out must be 16-byte aligned");
+    AR_GUARD_BEGIN
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(AR_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    float* tab = dalloc<float>(count, "spectral tables");
+    float4* lam = dalloc<float4>(ar::kLambdaLutRes, "spectral lambda table");
+    int* err = dalloc<int>(1, "error word");
+    struct Free { void* a; void* b; void* c; ~Free() { cudaFree(a); cudaFree(b); cudaFree(c); } } fr{tab, lam, err};
+    ck(cudaMemcpy(tab, tables, count * sizeof(float), cudaMemcpyHostToDevice), "copy spectral tables");
+    ck(cudaMemset(err, 0, sizeof(int)), "memset");
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    struct Ev { cudaEvent_t a, b; ~Ev() { cudaEventDestroy(a); cudaEventDestroy(b); } } ev{e0, e1};
+    float4* out = reinterpret_cast<float4*>(out_device);
+    ck(cudaEventRecord(e0, nullptr), "event");
+    if (method == AR_LUT_TENSOR) ck(ar::launch_spectral_rgb_lut_tc(tab, res, out, err, sms, nullptr), "table build");
+    else ck(ar::launch_spectral_luts(tab, res, lam, out, sms, nullptr), "table build");
+    ck(cudaEventRecord(e1, nullptr), "event");
+    ck(cudaEventSynchronize(e1), "sync");
+    int h = 0;
+    ck(cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost), "error word");
+    if (h) return fail(AR_ERR_DEVICE_FAULT, "tensor-core table build: an MMA did not complete within its wait limit");
+    if (ms) cudaEventElapsedTime(ms, e0, e1);
     return AR_OK;
     AR_GUARD_END
 }

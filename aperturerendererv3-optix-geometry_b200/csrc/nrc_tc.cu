@@ -7,13 +7,8 @@
 // columns from TMEM lane t and writes the next layer's A operand row back to
 // shared memory.
 //
-// Operands live in shared memory in the canonical K-major layout without
-// swizzle: 16-byte core rows of 8 bf16, 8 rows per 128-byte core matrix;
-// element (r, k) of an R-row operand sits at
-//   (k / 8) * (R * 16) + (r / 8) * 128 + (r % 8) * 16 + (k % 8) * 2 bytes,
-// so one K = 16 step of the MMA is the pair of 8-column chunks 2s, 2s + 1:
-// start = chunk 2s, leading-dimension offset (next chunk) = R * 16 bytes,
-// stride-dimension offset (next 8 rows) = 128 bytes.
+// Operands live in shared memory in the canonical K-major layout of
+// tcgen05.cuh.
 //
 // Every wait is bounded: a CTA whose MMA does not complete within the limit
 // sets the error word, skips the rest of its work, and still frees its
@@ -23,6 +18,7 @@
 #include <algorithm>
 
 #include "nrc.cuh"
+#include "tcgen05.cuh"
 
 namespace ar {
 
@@ -35,79 +31,6 @@ constexpr int kTcWBytes = 5 * kNrcHid * kNrcIn * 2 + kNrcOut * kNrcIn * 2;   // 
 constexpr int kTcABytes = kTcRows * kNrcIn * 2;                               // 16384
 constexpr int kTcSmem = kTcWBytes + kTcABytes + 64;
 constexpr uint32_t kTcSpinLimit = 1u << 22;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
-
-// byte offset of the 16-byte chunk (row r, k-chunk kc) of an R-row operand
-__host__ __device__ constexpr uint32_t tc_chunk_offset(int R, int r, int kc)
-{
-    return static_cast<uint32_t>(kc * (R * 16) + (r / 8) * 128 + (r % 8) * 16);
-}
-
-// shared-memory matrix descriptor: start, leading/stride byte offsets, version 1, no swizzle
-__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
-{
-    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
-           (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
-}
-
-// instruction descriptor of kind::f16: fp32 accumulator, bf16 A and B, both K-major, M x N
-__host__ __device__ constexpr uint32_t tc_idesc(int M, int N)
-{
-    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) | (static_cast<uint32_t>(M >> 4) << 24);
-}
-
-__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
-{
-    asm volatile(
-        "{\n\t"
-        ".reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
-        "}\n"
-        :
-        : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-}
-
-__device__ __forceinline__ void tc_commit(uint32_t mbar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" : : "r"(mbar) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t phase)
-{
-    uint32_t done;
-    asm volatile(
-        "{\n\t"
-        ".reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P1;\n\t"
-        "}"
-        : "=r"(done)
-        : "r"(mbar), "r"(phase)
-        : "memory");
-    return done != 0;
-}
-
-__device__ __forceinline__ void tc_ld64(uint32_t taddr, uint32_t* v)
-{
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
-        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
-        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31]),
-          "=r"(v[32]), "=r"(v[33]), "=r"(v[34]), "=r"(v[35]), "=r"(v[36]), "=r"(v[37]), "=r"(v[38]), "=r"(v[39]),
-          "=r"(v[40]), "=r"(v[41]), "=r"(v[42]), "=r"(v[43]), "=r"(v[44]), "=r"(v[45]), "=r"(v[46]), "=r"(v[47]),
-          "=r"(v[48]), "=r"(v[49]), "=r"(v[50]), "=r"(v[51]), "=r"(v[52]), "=r"(v[53]), "=r"(v[54]), "=r"(v[55]),
-          "=r"(v[56]), "=r"(v[57]), "=r"(v[58]), "=r"(v[59]), "=r"(v[60]), "=r"(v[61]), "=r"(v[62]), "=r"(v[63])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi)
 {

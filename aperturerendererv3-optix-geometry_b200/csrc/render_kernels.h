@@ -40,6 +40,10 @@ cudaError_t launch_iterations(const SceneView& s, const FrameParams& fp, const P
 // Spectral lookup tables from the network weights in `tab` (device memory).
 cudaError_t launch_spectral_luts(const float* tab, int res, float4* lut_lam, float4* lut_rgb, int sm_count,
                                  cudaStream_t st);
+// The RGB table alone on the tensor cores (spectral_tc.cu); *err gets bit 0
+// when a CTA's MMA wait runs out.
+cudaError_t launch_spectral_rgb_lut_tc(const float* tab, int res, float4* lut, int* err, int sm_count,
+                                       cudaStream_t st);
 cudaError_t launch_mean(const double* accum, int64_t n, double inv, float* out, cudaStream_t st);
 cudaError_t launch_add(const double* src, int64_t n, double* dst, cudaStream_t st);
 

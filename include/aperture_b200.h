@@ -278,6 +278,22 @@ ar_status ar_rng_tape(const ar_camera* camera, const ar_render_params* params, i
  * SPECTRUM_RGB_LUT_RES is 512) are then built on the scene's device. */
 ar_status ar_scene_set_spectral(ar_scene* scene, const float* tables, size_t count, int32_t lut_res);
 
+/* Builders of the RGB lookup table: AR_LUT_SIMT evaluates the network one
+ * thread per entry in fp32 (fmaf in the reference's input order; the table
+ * the oracle reproduces bit for bit, used by ar_scene_set_spectral);
+ * AR_LUT_TENSOR runs every layer as a 128 x 32 x 32 product on the tcgen05
+ * tensor cores with three-term bf16 splits of both operands (fp32 accuracy,
+ * other summation order: entries within a few fp32 ulps of the SIMT table). */
+enum { AR_LUT_SIMT = 0, AR_LUT_TENSOR = 1 };
+ar_status ar_scene_set_spectral_ex(ar_scene* scene, const float* tables, size_t count, int32_t lut_res,
+                                   int32_t method);
+/* The RGB lookup table alone (res^3 x 4 floats, x fastest) into a 16-byte
+ * aligned device buffer of the current device, built by `method`; *ms (may be
+ * NULL) gets the device time of the build.  res in [2, 1024].  No counterpart
+ * in the reference beyond PrecomputeRGBLUTKernel (spectrum_lut.cuh:12-38). */
+ar_status ar_spectral_rgb_lut(const float* tables, size_t count, int32_t res, int32_t method, float* out_device,
+                              float* ms);
+
 /* Copies of the spectral lookup tables (840 x 4 and lut_res^3 x 4 floats, x
  * fastest); either pointer may be NULL. */
 ar_status ar_scene_get_spectral_luts(const ar_scene* scene, float* lambda_lut, float* rgb_lut);
