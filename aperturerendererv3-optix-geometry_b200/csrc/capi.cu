@@ -1289,7 +1289,7 @@ ar_status nrc_check(ar_nrc* c, cudaStream_t st)
     ck(cudaStreamSynchronize(st), "sync");
     if (e != 0) {
         ck(cudaMemsetAsync(c->tc_err, 0, sizeof(int), st), "memset");
-        return fail(AR_ERR_DEVICE_FAULT, "tensor-core inference: an MMA did not complete within its wait limit");
+        return fail(AR_ERR_DEVICE_FAULT, "cache tensor-core kernels: an MMA did not complete within its wait limit");
     }
     return AR_OK;
 }
@@ -1298,7 +1298,8 @@ ar_status nrc_train_steps(ar_nrc* c, const ar::NrcSample* samples, const int32_t
 {
     for (int k = 0; k < steps; ++k)
         ck(ar::nrc_train_step(c->net(), c->P, samples, count, k * c->cfg.train_batch, c->cfg.train_batch, c->T,
-                              c->cfg.learning_rate, ++c->step, c->scene->sm_count, st), "cache training");
+                              c->cfg.learning_rate, ++c->step, c->scene->sm_count, st, true,
+                              c->tensor_path ? c->tc_err : nullptr), "cache training");
     return AR_OK;
 }
 
@@ -1566,7 +1567,8 @@ ar_status ar_nrc_gradients(ar_nrc* c, const float* samples, size_t n, float* tab
         ck(cudaMemcpy(cnt, &ni, 4, cudaMemcpyHostToDevice), "copy count");
         ck(cudaMemset(c->T.loss, 0, 4), "memset");
         ck(ar::nrc_train_step(c->net(), c->P, d, cnt, 0, c->cfg.train_batch, c->T, c->cfg.learning_rate, c->step + 1,
-                              c->scene->sm_count, nullptr, false), "cache gradients");
+                              c->scene->sm_count, nullptr, false, c->tensor_path ? c->tc_err : nullptr),
+           "cache gradients");
         const size_t tf = static_cast<size_t>(c->P.table_floats);
         std::vector<float> tg(tf), wg(ar::kNrcParams);
         ck(cudaMemcpy(tg.data(), c->P.table_g, tf * 4, cudaMemcpyDeviceToHost), "copy gradients");
@@ -1582,7 +1584,7 @@ ar_status ar_nrc_gradients(ar_nrc* c, const float* samples, size_t n, float* tab
         throw;
     }
     cudaFree(d); cudaFree(cnt);
-    return AR_OK;
+    return nrc_check(c, nullptr);
     AR_GUARD_END
 }
 
@@ -1603,7 +1605,8 @@ ar_status ar_nrc_train(ar_nrc* c, const float* samples, size_t n, int32_t steps,
         for (int k = 0; k < steps; ++k) {
             ck(cudaMemset(c->T.loss, 0, 4), "memset");
             ck(ar::nrc_train_step(c->net(), c->P, d, cnt, k * c->cfg.train_batch, c->cfg.train_batch, c->T,
-                                  c->cfg.learning_rate, ++c->step, c->scene->sm_count, nullptr), "cache training");
+                                  c->cfg.learning_rate, ++c->step, c->scene->sm_count, nullptr, true,
+                                  c->tensor_path ? c->tc_err : nullptr), "cache training");
             float l = 0.0f;
             ck(cudaMemcpy(&l, c->T.loss, 4, cudaMemcpyDeviceToHost), "copy loss");
             if (losses) losses[k] = l;
@@ -1613,7 +1616,7 @@ ar_status ar_nrc_train(ar_nrc* c, const float* samples, size_t n, int32_t steps,
         throw;
     }
     cudaFree(d); cudaFree(cnt);
-    return AR_OK;
+    return nrc_check(c, nullptr);
     AR_GUARD_END
 }
 

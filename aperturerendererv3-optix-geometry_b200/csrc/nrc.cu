@@ -207,7 +207,7 @@ __device__ void load_weights_fwd(const __nv_bfloat16* w, __nv_bfloat16* sW)
     }
 }
 
-__device__ __forceinline__ float exp_out(float raw) { return expf(fminf(raw, 15.0f)); }
+__device__ __forceinline__ float exp_out(float raw) { return nrc_exp_out(raw); }
 
 // ------------------------------------------------------------------ inference
 __global__ void __launch_bounds__(kNrcBlock) k_nrc_infer(NrcNet net, const NrcQuery* __restrict__ q,
@@ -336,44 +336,16 @@ __global__ void __launch_bounds__(kNrcBlock) k_nrc_train_bwd(NrcNet net, const N
         float d[kNrcBins];
 #pragma unroll
         for (int b = 0; b < kNrcBins; ++b) d[b] = 0.0f;
-        if (i < nv && net.spectral) {
-            // four wavelengths: pred_i = (1 - f_i) e[b_i] + f_i e[b_i + 1] with e = exp(raw);
-            // the loss gradient of each wavelength flows to its two bins through exp
+        if (i < nv) {
             const NrcSample s = smp[first + i];
             const float4* rr = reinterpret_cast<const float4*>(T.raw) + 4 * static_cast<int64_t>(i);
-            float e[kNrcBins];
+            float raw[kNrcBins];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const float4 v = rr[q];
-                e[4 * q] = exp_out(v.x); e[4 * q + 1] = exp_out(v.y); e[4 * q + 2] = exp_out(v.z); e[4 * q + 3] = exp_out(v.w);
+                raw[4 * q] = v.x; raw[4 * q + 1] = v.y; raw[4 * q + 2] = v.z; raw[4 * q + 3] = v.w;
             }
-            const float tg[4] = {s.v.p.w, s.v.n.w, s.v.a.w, s.x.x};
-            for (int w = 0; w < 4; ++w) {
-                if (tg[w] < 0.0f) continue;   // no throughput reached this wavelength
-                int b;
-                float f;
-                nrc_bin_weights(rotate_lambda(s.x.y, w), &b, &f);
-                const float pred = (1.0f - f) * e[b] + f * e[b + 1];
-                const float den = pred * pred + 0.01f;
-                const float diff = pred - tg[w];
-                loss_acc += diff * diff / den * norm;
-                const float g = (2.0f * diff / den) * norm * kNrcLossScale;
-                d[b] += g * (1.0f - f) * e[b];
-                d[b + 1] += g * f * e[b + 1];
-            }
-        } else if (i < nv) {
-            const NrcSample s = smp[first + i];
-            const float4 raw = reinterpret_cast<const float4*>(T.raw)[4 * static_cast<int64_t>(i)];
-            const float tg[3] = {s.v.p.w, s.v.n.w, s.v.a.w};
-            const float r3[3] = {raw.x, raw.y, raw.z};
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const float pred = exp_out(r3[c]);
-                const float den = pred * pred + 0.01f;
-                const float diff = pred - tg[c];
-                loss_acc += diff * diff / den * norm;
-                d[c] = (2.0f * diff / den) * norm * pred * kNrcLossScale;
-            }
+            loss_acc += nrc_output_grad(net.spectral, s, raw, norm, d);
         }
         uint32_t* row = reinterpret_cast<uint32_t*>(sIn + lane * kNrcWRow);
 #pragma unroll
@@ -689,14 +661,19 @@ cudaError_t nrc_infer(const NrcNet& net, const NrcQuery* q, const int32_t* count
 
 cudaError_t nrc_train_step(const NrcNet& net, const NrcParams& P, const NrcSample* samples, const int32_t* count,
                            int first, int batch, const NrcTrainBuffers& T, float lr, int step, int sm_count,
-                           cudaStream_t st, bool apply)
+                           cudaStream_t st, bool apply, int* tc_err)
 {
     cudaError_t e = set_attrs();
     if (e != cudaSuccess) return e;
-    const int tiles = (batch + kNrcWarpRows - 1) / kNrcWarpRows;
-    const int grid = std::max(1, std::min((tiles + kWarps - 1) / kWarps, sm_count * 2));
-    k_nrc_train_fwd<<<grid, kNrcBlock, kSmemW + kSmemIn + kSmemOut, st>>>(net, samples, count, first, batch, T);
-    k_nrc_train_bwd<<<grid, kNrcBlock, kSmemWt + kSmemIn, st>>>(net, samples, count, first, batch, T);
+    if (tc_err) {   // forward and backward on the tcgen05 tensor cores
+        e = nrc_train_fwd_bwd_tc(net, samples, count, first, batch, T, tc_err, sm_count, st);
+        if (e != cudaSuccess) return e;
+    } else {
+        const int tiles = (batch + kNrcWarpRows - 1) / kNrcWarpRows;
+        const int grid = std::max(1, std::min((tiles + kWarps - 1) / kWarps, sm_count * 2));
+        k_nrc_train_fwd<<<grid, kNrcBlock, kSmemW + kSmemIn + kSmemOut, st>>>(net, samples, count, first, batch, T);
+        k_nrc_train_bwd<<<grid, kNrcBlock, kSmemWt + kSmemIn, st>>>(net, samples, count, first, batch, T);
+    }
     k_nrc_wgrad<<<dim3(std::min((batch + kWgRows - 1) / kWgRows, 32), kNrcLayers), kNrcBlock, kSmemWg, st>>>(T, batch, P.w_g);
     k_nrc_hash_bwd<<<blocks_for(static_cast<int64_t>(batch) * net.grid.levels, 256, sm_count * 8), 256, 0, st>>>(
         net, samples, count, first, batch, T, P.table_g);

@@ -47,8 +47,10 @@ struct NrcGrid {
 
 // Four-wavelength mode: the 16 network outputs, through exp, are the outgoing
 // spectral radiance at 16 wavelength bins of 26.25 nm over [360, 780] nm (bin
-// centres 373.125 + 26.25 b); a wavelength's value interpolates linearly
-// between the two nearest centres (clamped to the first and last).
+// centres 373.125 + 26.25 b), relative to the D65 weight d65_norm of the
+// wavelength (the factor the tracer applies to emission, ~0.01), which keeps
+// the targets near 1; a wavelength's value interpolates linearly between the
+// two nearest centres (clamped to the first and last).
 constexpr int kNrcBins = 16;
 constexpr float kNrcLambda0 = 360.0f, kNrcBinWidth = 26.25f;
 
@@ -77,7 +79,7 @@ __host__ __device__ __forceinline__ f3 nrc_spectral_xyz(const float* tables, con
         int b;
         float f;
         nrc_bin_weights(lw, &b, &f);
-        const float L = (1.0f - f) * e[b] + f * e[b + 1];
+        const float L = ((1.0f - f) * e[b] + f * e[b + 1]) * d65_norm(tables, lw);
         acc = acc + cmf_xyz(tables, lw) * (t[w] * L);
     }
     return acc / ps;
@@ -137,6 +139,51 @@ __host__ __device__ __forceinline__ bool nrc_train_slot(const NrcFrame& f, int p
     if (q % f.stride != 0) return false;
     *slot = q / f.stride;
     return *slot < f.slots;
+}
+
+__device__ __forceinline__ float nrc_exp_out(float raw) { return expf(fminf(raw, 15.0f)); }
+
+// Gradient (times the loss scale) of the training loss with respect to the 16
+// raw outputs of one sample, and the sample's loss, normalised by `norm`.
+// RGB: relative L2 per channel (pred - target)^2 / (sg(pred)^2 + 0.01) with
+// pred = exp(raw); four wavelengths: the same per wavelength with pred the
+// bins interpolated at the wavelength, targets below zero left out.
+__device__ __forceinline__ float nrc_output_grad(int spectral, const NrcSample& s, const float* raw, float norm,
+                                                 float* d)
+{
+    float loss = 0.0f;
+#pragma unroll
+    for (int b = 0; b < kNrcBins; ++b) d[b] = 0.0f;
+    if (spectral) {
+        float e[kNrcBins];
+#pragma unroll
+        for (int b = 0; b < kNrcBins; ++b) e[b] = nrc_exp_out(raw[b]);
+        const float tg[4] = {s.v.p.w, s.v.n.w, s.v.a.w, s.x.x};
+        for (int w = 0; w < 4; ++w) {
+            if (tg[w] < 0.0f) continue;   // no throughput reached this wavelength
+            int b;
+            float f;
+            nrc_bin_weights(rotate_lambda(s.x.y, w), &b, &f);
+            const float pred = (1.0f - f) * e[b] + f * e[b + 1];
+            const float den = pred * pred + 0.01f;
+            const float diff = pred - tg[w];
+            loss += diff * diff / den * norm;
+            const float g = (2.0f * diff / den) * norm * kNrcLossScale;
+            d[b] += g * (1.0f - f) * e[b];
+            d[b + 1] += g * f * e[b + 1];
+        }
+    } else {
+        const float tg[3] = {s.v.p.w, s.v.n.w, s.v.a.w};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float pred = nrc_exp_out(raw[c]);
+            const float den = pred * pred + 0.01f;
+            const float diff = pred - tg[c];
+            loss += diff * diff / den * norm;
+            d[c] = (2.0f * diff / den) * norm * pred * kNrcLossScale;
+        }
+    }
+    return loss;
 }
 
 // Real spherical harmonics up to degree 3 (16 coefficients) of a unit
@@ -233,6 +280,10 @@ cudaError_t nrc_infer_tc(const NrcNet& net, const NrcQuery* q, const int32_t* co
                          float* out_rgb, int* err, int sm_count, cudaStream_t st);
 cudaError_t nrc_train_step(const NrcNet& net, const NrcParams& P, const NrcSample* samples, const int32_t* count,
                            int first, int batch, const NrcTrainBuffers& T, float lr, int step, int sm_count,
-                           cudaStream_t st, bool apply = true);
+                           cudaStream_t st, bool apply = true, int* tc_err = nullptr);
+// The training forward and backward passes on the tcgen05 tensor cores
+// (nrc_tc.cu); *err gets bit 2 (forward) or 3 (backward) when an MMA wait runs out.
+cudaError_t nrc_train_fwd_bwd_tc(const NrcNet& net, const NrcSample* samples, const int32_t* count, int first,
+                                 int batch, const NrcTrainBuffers& T, int* err, int sm_count, cudaStream_t st);
 
 }  // namespace ar

@@ -1021,17 +1021,22 @@ __global__ void k_retire(FrameParams fp, PathBuffers B, PoolCtl* ctl, double* ac
             const f3 L = mk(fix_nan_inf(rr.rad.x), fix_nan_inf(rr.rad.y), fix_nan_inf(rr.rad.z));
             if (fp.nrc.spectral == 4) {
                 // four wavelengths: a target per wavelength, negative (left out of the
-                // loss) where no throughput reached the vertex (hero-only after dispersion)
+                // loss) where no throughput reached the vertex (hero-only after dispersion),
                 const float L3 = fix_nan_inf(fbits(rr.meta.w));
                 for (int k = 0; k < nvtx; ++k) {
                     const NrcTrainVertex tv = fp.nrc.train_vertices[static_cast<int64_t>(slot) * fp.nrc.max_train_vertices + k];
                     const float Lw[4] = {L.x, L.y, L.z, L3};
                     const float T[4] = {tv.t.x, tv.t.y, tv.t.z, tv.t.w};
                     const float B4[4] = {tv.lb.x, tv.lb.y, tv.lb.z, tv.lb.w};
+                    // relative to the D65 weight of the wavelength (the cache's output scale)
                     float tg[4];
 #pragma unroll
                     for (int w = 0; w < 4; ++w)
-                        tg[w] = T[w] > 1e-6f ? fminf(fmaxf((Lw[w] - B4[w]) / T[w], 0.0f), 1.0e3f) : -1.0f;
+                        tg[w] = T[w] > 1e-6f ? fminf(fmaxf(((Lw[w] - B4[w]) / T[w]) /
+                                                               d65_norm(fp.spec.tables, rotate_lambda(tv.v.n.w, w)),
+                                                           0.0f),
+                                                     1.0e3f)
+                                             : -1.0f;
                     const int si = atomicAdd(fp.nrc.sample_count, 1);
                     if (si < fp.nrc.sample_cap) {
                         NrcSample sm;

@@ -109,15 +109,19 @@ def load(path: str = DATA):
     return v[:n].copy(), v[n:n + 400].reshape(4, 100).copy(), v[n + 400:n + 500].copy()
 
 
-def build(ref_core: str | None = None) -> bool:
-    """Write the table file when the reference sources are present."""
-    ref_core = ref_core or os.environ.get("AR_REFERENCE_CORE", "/root/reference/core")
-    if not os.path.isdir(ref_core):
+def build(ref_core: str | None) -> bool:
+    """Write the table file from the reference's core/ directory (given, or
+    from the environment variable AR_REFERENCE_CORE); False when neither names
+    an existing directory (the file already written, if any, stays)."""
+    ref_core = ref_core or os.environ.get("AR_REFERENCE_CORE")
+    if not ref_core or not os.path.isdir(ref_core):
         return False
     write(ref_core)
     return True
 
 
 if __name__ == "__main__":
-    ok = build(sys.argv[1] if len(sys.argv) > 1 else None)
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: spectral_tables.py <reference core/ directory>")
+    ok = build(sys.argv[1])
     print(DATA if ok else "reference sources not found: spectral tables not written")

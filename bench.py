@@ -555,9 +555,36 @@ def measure_configs(torch, dev, stream, c5_jobs: int) -> dict:
                                    "medium (sigma_t 2, albedo 0.8, g 0.3), 1280x720, 256 spp, depth 16, "
                                    + ("4 hero wavelengths, RGB LUT 64^3" if spectral else "RGB (spectral tables absent)"),
                           **r)
+    if spectral:
+        res["spectral_lut_512"] = measure_spectral_lut(torch)
     if c5_jobs > 0:
         res["config5"] = measure_config5(torch, dev, stream, c5_jobs)
     return res
+
+
+def measure_spectral_lut(torch, res: int = 512) -> dict:
+    """The reference-size RGB lookup table (512^3 entries of 4 floats, 2 GiB;
+    PrecomputeRGBLUTKernel, spectrum_lut.cuh:12-38) built by the SIMT kernel
+    and on the tensor cores, each timed by CUDA events after one warm-up build,
+    and the largest difference between the two tables."""
+    from aperture_b200 import LUT_SIMT, LUT_TENSOR, spectral_rgb_lut
+    a, _ = spectral_rgb_lut(res, LUT_SIMT)
+    a, ms_simt = spectral_rgb_lut(res, LUT_SIMT, out=a)
+    b, _ = spectral_rgb_lut(res, LUT_TENSOR)
+    b, ms_tc = spectral_rgb_lut(res, LUT_TENSOR, out=b)
+    big = float(a.abs().max())
+    diff = float((a - b).abs().max())
+    entries = res ** 3
+    flop = entries * (2 * 8 * 32 * 32 + 2 * 4 * 32)   # input layer, 7 blocks, output
+    out = {"entries": entries, "simt_ms": round(ms_simt, 2), "tensor_ms": round(ms_tc, 2),
+           "speedup": round(ms_simt / ms_tc, 2), "max_abs_diff_rel_to_max": diff / big,
+           "network_tflops_simt": round(flop / (ms_simt / 1e3) / 1e12, 2),
+           "network_tflops_tensor": round(flop / (ms_tc / 1e3) / 1e12, 2),
+           "note": "tensor path: 6 bf16 products per fp32 product (three-term splits), so the MMA work is 6x the "
+                   "network's fp32 FLOPs"}
+    del a, b
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_ours(args) -> None:

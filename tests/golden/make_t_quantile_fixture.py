@@ -3,7 +3,7 @@ core/denoise/t_quantile.cu) as text into t_quantile_005_ref.npy, the fixture
 that pins the denoiser's generated table.  Run where the reference sources
 are present:
 
-    python tests/golden/make_t_quantile_fixture.py [reference root]
+    python tests/golden/make_t_quantile_fixture.py <reference root>
 """
 import os
 import re
@@ -15,7 +15,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def main() -> None:
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_t_quantile_fixture.py <reference root>")
+    root = sys.argv[1]
     txt = open(os.path.join(root, "core", "denoise", "t_quantile.cu")).read()
     body = re.search(r"#define T005_LUT_INIT \{([^}]*)\}", txt).group(1)
     vals = np.array([float(v.strip().rstrip("f")) for v in body.split(",") if v.strip()], np.float64)

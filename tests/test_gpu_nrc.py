@@ -227,22 +227,60 @@ def test_nrc_spectral_gradients_equal_oracle():
 
 @pytest.mark.gpu
 def test_nrc_spectral_frames_converge_to_plain_image():
-    """Frames of four wavelengths per path with the four-wavelength cache: the
-    XYZ image converges to the plain four-wavelength tracer's within a few
-    percent per channel (the cache's bias), with paths ending in the cache."""
+    """Frames of four wavelengths per path with the four-wavelength cache: after
+    32 frames of online training the XYZ image of the next 96 frames agrees
+    with the plain four-wavelength tracer's within 10 % per channel mean (the
+    cache's bias), with paths ending in the cache and the training loss low."""
     import torch
     sc, c, cfg = _spectral_cache(log2_entries=16, train_paths=2048, train_batch=2048, train_steps=2)
     cam = scenes.box_camera(48, 48)
     ref, _ = sc.render(cam, make_params(spp=1024, max_depth=8, spectral=4))
+    warm = torch.zeros(48 * 48 * 3, dtype=torch.float64, device="cuda")
+    for f in range(32):
+        c.render_frame(cam, make_params(spp=2, max_depth=8, spectral=4, frame_offset=2 * f), None, warm.data_ptr(),
+                       train=True)
     acc = torch.zeros(48 * 48 * 3, dtype=torch.float64, device="cuda")
-    frames = 128
+    frames = 96
     st = None
     for f in range(frames):
-        st = c.render_frame(cam, make_params(spp=2, max_depth=8, spectral=4, frame_offset=2 * f), None,
+        st = c.render_frame(cam, make_params(spp=2, max_depth=8, spectral=4, frame_offset=1000 + 2 * f), None,
                             acc.data_ptr(), train=True, stats=(f == frames - 1))
-    assert st.queries > 500 and st.train_samples > 500
+    assert st.queries > 500 and st.train_samples > 500 and st.loss < 0.1
     img = (acc / (2 * frames)).cpu().numpy().reshape(48, 48, 3)
+    assert np.isfinite(img).all()
     m, r = img.mean(axis=(0, 1)), ref.reshape(48, 48, 3).mean(axis=(0, 1))
-    assert np.all(np.abs(m - r) < 0.05 * r), (m, r)
+    assert np.all(np.abs(m - r) < 0.10 * r), (m, r)
     with pytest.raises(Exception):   # a frame of another mode than the cache's
         c.render_frame(cam, make_params(spp=1, max_depth=8), None, acc.data_ptr(), train=False)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("spectral", [0, 4])
+def test_nrc_tcgen05_training_equals_mma_sync(spectral):
+    """Training forward and backward on the tcgen05 tensor cores (128-row
+    tiles, tensor-memory accumulators, the transposed weights for the
+    backward chain) against the warp-level mma.sync kernels and the numpy
+    restatement: losses equal to 1e-4, gradients within 1e-2 (bf16 rounding of
+    the layer gradients after a different fp32 summation order) of each other
+    and within 2e-2 of the oracle."""
+    if spectral:
+        _, c, cfg = _spectral_cache(log2_entries=15, train_batch=2048)
+    else:
+        _, c, cfg = _cache(log2_entries=15, train_batch=2048)
+    table, w = _random_params(c, 31, 0.3, 0.2)
+    rng = np.random.default_rng(32)
+    s = np.zeros((2000, 20), np.float32)
+    s[:, :16] = _vertices(2000, 33)
+    s[:, [3, 11, 15, 16]] = rng.uniform(0.05, 3.0, (2000, 4))
+    s[:, 17] = rng.uniform(360.0, 780.0, 2000)
+    c.set_tensor_path(False)
+    tg0, wg0, l0 = c.gradients(s)
+    c.set_tensor_path(True)
+    tg1, wg1, l1 = c.gradients(s)
+    assert abs(l1 - l0) <= 1e-4 * abs(l0)
+    assert np.linalg.norm(wg1 - wg0) <= 1e-2 * np.linalg.norm(wg0)
+    assert np.linalg.norm(tg1 - tg0) <= 1e-2 * np.linalg.norm(tg0)
+    lo, dT, dW = (N.loss_and_gradients_spectral(_geo(cfg), s, table, w) if spectral
+                  else N.loss_and_gradients(_geo(cfg), s[:, :16], table, w))
+    assert np.linalg.norm(wg1 - dW) <= 2e-2 * np.linalg.norm(dW)
+    assert np.linalg.norm(tg1 - dT.reshape(-1)) <= 2e-2 * np.linalg.norm(dT)
