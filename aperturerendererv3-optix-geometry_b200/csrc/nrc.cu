@@ -238,9 +238,9 @@ __global__ void __launch_bounds__(kNrcBlock) k_nrc_infer(NrcNet net, const NrcQu
             if (accum) {
                 const int pix = __float_as_int(qq.v.p.w);
                 const f3 c = nrc_spectral_xyz(net.tables, e, qq.v.n.w, qq.t);
-                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 0], static_cast<double>(c.x));
-                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 1], static_cast<double>(c.y));
-                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 2], static_cast<double>(c.z));
+                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 0], nrc_contrib(c.x));
+                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 1], nrc_contrib(c.y));
+                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 2], nrc_contrib(c.z));
             }
             if (out_rgb)
                 for (int b = 0; b < kNrcBins; ++b) out_rgb[kNrcBins * static_cast<int64_t>(i) + b] = e[b];
@@ -249,9 +249,9 @@ __global__ void __launch_bounds__(kNrcBlock) k_nrc_infer(NrcNet net, const NrcQu
             const float L0 = exp_out(o[0]), L1 = exp_out(o[1]), L2 = exp_out(o[2]);
             if (accum) {
                 const int pix = __float_as_int(qq.v.p.w);
-                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 0], static_cast<double>(qq.t.x * L0));
-                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 1], static_cast<double>(qq.t.y * L1));
-                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 2], static_cast<double>(qq.t.z * L2));
+                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 0], nrc_contrib(qq.t.x * L0));
+                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 1], nrc_contrib(qq.t.y * L1));
+                atomicAdd(&accum[3 * static_cast<int64_t>(pix) + 2], nrc_contrib(qq.t.z * L2));
             }
             if (out_rgb) {
                 out_rgb[3 * static_cast<int64_t>(i) + 0] = L0;
@@ -549,16 +549,16 @@ __global__ void k_nrc_adam_mlp(float* p, float* m, float* v, float* gr, __nv_bfl
 {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < kNrcParams; e += gridDim.x * blockDim.x) {
         float w = p[e];
-        if (update) {
-            const float gg = gr[e] * inv_scale;
+        const float gg = gr[e] * inv_scale;
+        if (update && gg - gg == 0.0f) {   // a non-finite gradient element skips its update
             const float mm = b1 * m[e] + (1.0f - b1) * gg;
             const float vv = b2 * v[e] + (1.0f - b2) * gg * gg;
             m[e] = mm;
             v[e] = vv;
             w -= lr_t * mm / (sqrtf(vv) + eps);
             p[e] = w;
-            gr[e] = 0.0f;
         }
+        if (update) gr[e] = 0.0f;
         const int l = min(e / (kNrcHid * kNrcIn), kNrcLayers - 1);
         const int local = e - nrc_w_offset(l);
         const int rows = nrc_w_rows(l);
@@ -582,6 +582,8 @@ __global__ void k_nrc_adam_table(float* p, float* m, float* v, float* gr, __half
             if (g2.x == 0.0f && g2.y == 0.0f) continue;
             float2 m2 = reinterpret_cast<float2*>(m)[e], v2 = reinterpret_cast<float2*>(v)[e];
             const float gx = g2.x * inv_scale, gy = g2.y * inv_scale;
+            reinterpret_cast<float2*>(gr)[e] = make_float2(0.0f, 0.0f);
+            if (!(gx - gx == 0.0f && gy - gy == 0.0f)) continue;   // non-finite: skip the entry's update
             m2.x = b1 * m2.x + (1.0f - b1) * gx;
             m2.y = b1 * m2.y + (1.0f - b1) * gy;
             v2.x = b2 * v2.x + (1.0f - b2) * gx * gx;
@@ -591,7 +593,6 @@ __global__ void k_nrc_adam_table(float* p, float* m, float* v, float* gr, __half
             reinterpret_cast<float2*>(m)[e] = m2;
             reinterpret_cast<float2*>(v)[e] = v2;
             reinterpret_cast<float2*>(p)[e] = w;
-            reinterpret_cast<float2*>(gr)[e] = make_float2(0.0f, 0.0f);
         }
         th[e] = __floats2half2_rn(w.x, w.y);
     }

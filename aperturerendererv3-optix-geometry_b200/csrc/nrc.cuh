@@ -57,9 +57,10 @@ constexpr float kNrcLambda0 = 360.0f, kNrcBinWidth = 26.25f;
 __host__ __device__ __forceinline__ void nrc_bin_weights(float lambda, int* b0, float* f)
 {
     float x = (lambda - kNrcLambda0) / kNrcBinWidth - 0.5f;
-    x = x < 0.0f ? 0.0f : (x > static_cast<float>(kNrcBins - 1) ? static_cast<float>(kNrcBins - 1) : x);
+    x = x > 0.0f ? x : 0.0f;   // not-a-number as bin 0
+    x = x < static_cast<float>(kNrcBins - 1) ? x : static_cast<float>(kNrcBins - 1);
     int b = static_cast<int>(floorf(x));
-    b = b > kNrcBins - 2 ? kNrcBins - 2 : b;
+    b = b < 0 ? 0 : (b > kNrcBins - 2 ? kNrcBins - 2 : b);
     *b0 = b;
     *f = x - static_cast<float>(b);
 }
@@ -142,6 +143,13 @@ __host__ __device__ __forceinline__ bool nrc_train_slot(const NrcFrame& f, int p
 }
 
 __device__ __forceinline__ float nrc_exp_out(float raw) { return expf(fminf(raw, 15.0f)); }
+
+// A cache contribution to a pixel, bounded as the tracer bounds a sample
+// (RADIANCE_CLAMP 1e3 per channel, not-a-number as 0; render.cuh:966-969).
+__device__ __forceinline__ double nrc_contrib(float v)
+{
+    return (v >= 0.0f) ? static_cast<double>(fminf(v, 1.0e3f)) : 0.0;
+}
 
 // Gradient (times the loss scale) of the training loss with respect to the 16
 // raw outputs of one sample, and the sample's loss, normalised by `norm`.
@@ -243,7 +251,16 @@ __host__ __device__ __forceinline__ void nrc_unit_pos(const NrcGrid& g, const fl
     u[0] = (p.x - g.bmin[0]) * g.inv_ext[0];
     u[1] = (p.y - g.bmin[1]) * g.inv_ext[1];
     u[2] = (p.z - g.bmin[2]) * g.inv_ext[2];
-    for (int k = 0; k < 3; ++k) u[k] = u[k] < 0.0f ? 0.0f : (u[k] > 1.0f ? 1.0f : u[k]);
+    for (int k = 0; k < 3; ++k) u[k] = u[k] > 0.0f ? (u[k] < 1.0f ? u[k] : 1.0f) : 0.0f;   // not-a-number as 0
+}
+
+// A recorded vertex the cache may train on: every input finite.
+__host__ __device__ __forceinline__ bool nrc_vertex_finite(const NrcVertex& v)
+{
+    const float s = (v.p.x - v.p.x) + (v.p.y - v.p.y) + (v.p.z - v.p.z) + (v.d.x - v.d.x) + (v.d.y - v.d.y) +
+                    (v.d.z - v.d.z) + (v.n.x - v.n.x) + (v.n.y - v.n.y) + (v.n.z - v.n.z) + (v.n.w - v.n.w) +
+                    (v.a.x - v.a.x) + (v.a.y - v.a.y) + (v.a.z - v.a.z);
+    return s == 0.0f;   // x - x is 0 for finite x, not-a-number for infinities and not-a-number
 }
 
 // Host launchers (nrc.cu).

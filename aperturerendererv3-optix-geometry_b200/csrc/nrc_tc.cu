@@ -187,16 +187,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nrc_infer_tc(NrcNet net, cons
         if (valid && net.spectral) {   // out holds the XYZ contribution already
             if (accum) {
                 const int64_t pix = __float_as_int(qq.v.p.w);
-                atomicAdd(&accum[3 * pix + 0], static_cast<double>(out[0]));
-                atomicAdd(&accum[3 * pix + 1], static_cast<double>(out[1]));
-                atomicAdd(&accum[3 * pix + 2], static_cast<double>(out[2]));
+                atomicAdd(&accum[3 * pix + 0], nrc_contrib(out[0]));
+                atomicAdd(&accum[3 * pix + 1], nrc_contrib(out[1]));
+                atomicAdd(&accum[3 * pix + 2], nrc_contrib(out[2]));
             }
         } else if (valid) {
             if (accum) {
                 const int64_t pix = __float_as_int(qq.v.p.w);
-                atomicAdd(&accum[3 * pix + 0], static_cast<double>(qq.t.x * out[0]));
-                atomicAdd(&accum[3 * pix + 1], static_cast<double>(qq.t.y * out[1]));
-                atomicAdd(&accum[3 * pix + 2], static_cast<double>(qq.t.z * out[2]));
+                atomicAdd(&accum[3 * pix + 0], nrc_contrib(qq.t.x * out[0]));
+                atomicAdd(&accum[3 * pix + 1], nrc_contrib(qq.t.y * out[1]));
+                atomicAdd(&accum[3 * pix + 2], nrc_contrib(qq.t.z * out[2]));
             }
             if (out_rgb) {
                 out_rgb[3 * static_cast<int64_t>(row) + 0] = out[0];

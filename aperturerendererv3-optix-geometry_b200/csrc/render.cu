@@ -1025,6 +1025,7 @@ __global__ void k_retire(FrameParams fp, PathBuffers B, PoolCtl* ctl, double* ac
                 const float L3 = fix_nan_inf(fbits(rr.meta.w));
                 for (int k = 0; k < nvtx; ++k) {
                     const NrcTrainVertex tv = fp.nrc.train_vertices[static_cast<int64_t>(slot) * fp.nrc.max_train_vertices + k];
+                    if (!nrc_vertex_finite(tv.v)) continue;   // a non-finite input would poison the whole step
                     const float Lw[4] = {L.x, L.y, L.z, L3};
                     const float T[4] = {tv.t.x, tv.t.y, tv.t.z, tv.t.w};
                     const float B4[4] = {tv.lb.x, tv.lb.y, tv.lb.z, tv.lb.w};
@@ -1051,6 +1052,7 @@ __global__ void k_retire(FrameParams fp, PathBuffers B, PoolCtl* ctl, double* ac
             }
             for (int k = 0; k < (fp.nrc.spectral == 4 ? 0 : nvtx); ++k) {
                 const NrcTrainVertex tv = fp.nrc.train_vertices[static_cast<int64_t>(slot) * fp.nrc.max_train_vertices + k];
+                if (!nrc_vertex_finite(tv.v)) continue;
                 const f3 tgt = mk(tv.t.x > 1e-6f ? (L.x - tv.lb.x) / tv.t.x : 0.0f,
                                   tv.t.y > 1e-6f ? (L.y - tv.lb.y) / tv.t.y : 0.0f,
                                   tv.t.z > 1e-6f ? (L.z - tv.lb.z) / tv.t.z : 0.0f);

@@ -875,11 +875,21 @@ def main():
     ap.add_argument("--profile-nrc", action="store_true",
                     help="six radiance-cache frames (for ncu captures of the cache kernels)")
     ap.add_argument("--profile-size", default="480x270", help="frame size of --profile-nrc")
+    ap.add_argument("--profile-lut", type=int, default=0,
+                    help="build the spectral RGB lookup table of this resolution by both methods (for ncu captures)")
     ap.add_argument("--profile-queues", action="store_true",
                     help="render the workload once at 1 spp (for ncu captures) and print the per-depth queue sizes")
     args = ap.parse_args()
     if args.profile_queues:
         profile_queues()
+        return
+    if args.profile_lut:
+        import torch
+        from aperture_b200 import LUT_SIMT, LUT_TENSOR, spectral_rgb_lut
+        a, ms_a = spectral_rgb_lut(args.profile_lut, LUT_SIMT)
+        b, ms_b = spectral_rgb_lut(args.profile_lut, LUT_TENSOR)
+        print(json.dumps({"profile": "spectral lut", "res": args.profile_lut, "simt_ms": ms_a, "tensor_ms": ms_b,
+                          "max_abs_diff": float((a - b).abs().max())}), flush=True)
         return
     if args.nrc_sweep:
         import torch
