@@ -867,8 +867,9 @@ def main():
                     help="radiance-cache time-to-relMSE measurement (config3: the config-3 scene with four "
                          "wavelengths at 1280x720, plus config 4's spline path; small / full: the config-2 scene "
                          "at 480x270 / 1920x1080; box: the config-3 scene in RGB at 480x270)")
-    ap.add_argument("--nrc-spp", type=int, default=1, help="samples per pixel of a cache frame")
-    ap.add_argument("--nrc-c", type=float, default=0.01, help="spread constant of the cache's termination rule")
+    # defaults: the best of the 18 settings of the config-3 sweep (--nrc-sweep config3)
+    ap.add_argument("--nrc-spp", type=int, default=16, help="samples per pixel of a cache frame")
+    ap.add_argument("--nrc-c", type=float, default=1.0, help="spread constant of the cache's termination rule")
     ap.add_argument("--nrc-steps", type=int, default=4, help="optimiser steps per cache frame")
     ap.add_argument("--nrc-sweep", choices=("box", "small", "config3"), default=None,
                     help="time-to-relMSE over spp per frame x spread constant x optimiser steps, then exit")
