@@ -948,7 +948,7 @@ struct ShadowIO {
 };
 
 template <bool kExt>
-__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks - 1) k_shadow(SceneView s, PathBuffers B, int cur, PoolCtl* ctl,
+__global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_shadow(SceneView s, PathBuffers B, int cur, PoolCtl* ctl,
                                                         unsigned long long* stats, uint32_t* ovf, int* err, int spec4)
 {
     extern __shared__ uint32_t smem[];
