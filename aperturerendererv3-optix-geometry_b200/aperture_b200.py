@@ -160,7 +160,8 @@ class GuideStats(ctypes.Structure):
 
 class BatchTuning(ctypes.Structure):
     _fields_ = [("iterations_per_graph", c_int32), ("candidates", c_int32), ("path_budget", c_int64),
-                ("best_ms", c_float), ("default_ms", c_float)]
+                ("best_ms", c_float), ("default_ms", c_float), ("trace_blocks_per_sm", c_int32),
+                ("shade_blocks_per_sm", c_int32)]
 
 
 class BatchStats(ctypes.Structure):

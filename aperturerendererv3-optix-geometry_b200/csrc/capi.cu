@@ -881,8 +881,21 @@ BatchKey batch_key(const ar_job* jobs, int32_t njobs)
     }
     return k;
 }
+// Launch knobs of a batch: graph length, in-flight path budget, resident
+// blocks per SM of each job's traversal kernels and of its shading, path
+// generation and retirement kernels (0: the defaults -- the traversal
+// kernels' occupancy and 4).  Jobs run as parallel graph branches, so smaller
+// grids let kernels of several jobs share the GPU.
+struct BatchKnobs {
+    int32_t iterations = 0;
+    int64_t budget = 0;
+    int32_t trace_bps = 0;
+    int32_t shade_bps = 0;
+};
 std::mutex g_tune_mutex;
-std::map<BatchKey, std::pair<int32_t, int64_t>> g_tuned;
+std::map<BatchKey, BatchKnobs> g_tuned;
+
+ar_status render_batch(const ar_job* jobs, int32_t njobs, BatchKnobs kn, ar_batch_stats* stats, void* stream);
 }  // namespace
 
 extern "C" {
@@ -891,6 +904,25 @@ ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_
                           ar_batch_stats* stats, void* stream)
 {
     g_last_error.clear();
+    if (njobs <= 0 || !jobs) return fail(AR_ERR_INVALID_ARGUMENT, "jobs is NULL or empty");
+    BatchKnobs kn;
+    kn.iterations = iterations_per_graph;
+    kn.budget = path_budget;
+    if (iterations_per_graph == 0 && path_budget == 0) {   // autotuned knobs for this batch shape
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tuned.find(batch_key(jobs, njobs));
+        if (it != g_tuned.end()) kn = it->second;
+    }
+    return render_batch(jobs, njobs, kn, stats, stream);
+}
+
+}  // extern "C"
+
+namespace {
+ar_status render_batch(const ar_job* jobs, int32_t njobs, BatchKnobs kn, ar_batch_stats* stats, void* stream)
+{
+    const int32_t iterations_per_graph = kn.iterations;
+    const int64_t path_budget = kn.budget;
     if (njobs <= 0 || !jobs) return fail(AR_ERR_INVALID_ARGUMENT, "jobs is NULL or empty");
     if (iterations_per_graph < 0 || iterations_per_graph > 256)
         return fail(AR_ERR_INVALID_ARGUMENT, "iterations_per_graph must be in [0, 256]");
@@ -905,14 +937,8 @@ ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_
         if (jb.params.spectral && !jb.scene->spec_tables)
             return fail(AR_ERR_UNSUPPORTED, "job " + std::to_string(j) + ": spectral tables not set");
     }
-    if (iterations_per_graph == 0 && path_budget == 0) {   // autotuned defaults for this batch shape
-        std::lock_guard<std::mutex> lock(g_tune_mutex);
-        auto it = g_tuned.find(batch_key(jobs, njobs));
-        if (it != g_tuned.end()) {
-            iterations_per_graph = it->second.first;
-            path_budget = it->second.second;
-        }
-    }
+    if (kn.trace_bps < 0 || kn.trace_bps > 64 || kn.shade_bps < 0 || kn.shade_bps > 64)
+        return fail(AR_ERR_INVALID_ARGUMENT, "blocks per SM must be in [0, 64]");
     AR_GUARD_BEGIN
     DeviceGuard g(s0->device);
     cudaStream_t user = static_cast<cudaStream_t>(stream);
@@ -1014,9 +1040,13 @@ ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_
         JobWs& w = R.jobs[j];
         const ar_job& jb = jobs[j];
         ck(cudaStreamWaitEvent(w.st, R.fork, 0), "fork");
+        // persistent traversal kernels fetch work dynamically: any grid up to
+        // the one the overflow slabs were sized for is complete
+        const int gt = kn.trace_bps > 0 ? std::min(jb.scene->grid_trace, jb.scene->sm_count * kn.trace_bps)
+                                        : jb.scene->grid_trace;
+        const int go = jb.scene->sm_count * (kn.shade_bps > 0 ? kn.shade_bps : 4);
         ck(ar::launch_iterations(jb.scene->view, w.fp, w.B, w.ctl, w.base0, w.base1, jb.scene->jump_table, w.stats,
-                                 w.ovf, w.err, w.accum, nullptr, K, &w.cur, jb.scene->grid_trace,
-                                 jb.scene->sm_count * 4, w.st, &launches, nullptr),
+                                 w.ovf, w.err, w.accum, nullptr, K, &w.cur, gt, go, w.st, &launches, nullptr),
            "capture iterations");
         ck(cudaEventRecord(w.done, w.st), "join");
         ck(cudaStreamWaitEvent(st, w.done, 0), "join");
@@ -1071,6 +1101,9 @@ ar_status ar_render_batch(const ar_job* jobs, int32_t njobs, int32_t iterations_
     return AR_OK;
     AR_GUARD_END
 }
+}  // namespace
+
+extern "C" {
 
 ar_status ar_accum_resolve(const double* accum, size_t n, double scale, float* out, int32_t mem_kind, void* stream)
 {
@@ -1646,27 +1679,53 @@ ar_status ar_batch_autotune(const ar_job* jobs, int32_t njobs, int32_t probe_spp
     }
     const int32_t ks[4] = {4, 8, 16, 32};
     const int64_t bs[4] = {int64_t(1) << 20, int64_t(1) << 21, int64_t(1) << 22, int64_t(1) << 23};
+    const int32_t tbs[3] = {0, 4, 2};   // traversal blocks per SM (0: the kernels' occupancy)
+    const int32_t sbs[3] = {4, 2, 1};   // shading / generation / retirement blocks per SM
     ar_batch_stats st;
     // first use of every workspace (allocations, graph set-up) outside the timing
-    if (ar_status e = ar_render_batch(probe.data(), njobs, 16, bs[2], &st, stream)) return e;
-    ar_batch_tuning best{16, 0, bs[2], 0.0f, 0.0f};
+    BatchKnobs cur;
+    cur.iterations = 16;
+    cur.budget = bs[2];
+    if (ar_status e = render_batch(probe.data(), njobs, cur, &st, stream)) return e;
+    ar_batch_tuning best{16, 0, bs[2], 0.0f, 0.0f, 0, 4};
+    BatchKnobs bestk = cur;
     double best_rate = -1.0;
+    auto run = [&](const BatchKnobs& k) -> ar_status {
+        if (ar_status e = render_batch(probe.data(), njobs, k, &st, stream)) return e;
+        const double rate = static_cast<double>(st.paths) / std::max(1e-6, static_cast<double>(st.total_ms));
+        if (k.iterations == 16 && k.budget == bs[2] && k.trace_bps == 0 && k.shade_bps == 0) best.default_ms = st.total_ms;
+        ++best.candidates;
+        if (rate > best_rate) {
+            best_rate = rate;
+            bestk = k;
+            best.best_ms = st.total_ms;
+        }
+        return AR_OK;
+    };
+    // graph length x path budget at the default grids, then the grids at the best of those
     for (int32_t k : ks)
         for (int64_t b : bs) {
-            if (ar_status e = ar_render_batch(probe.data(), njobs, k, b, &st, stream)) return e;
-            const double rate = static_cast<double>(st.paths) / std::max(1e-6, static_cast<double>(st.total_ms));
-            if (k == 16 && b == bs[2]) best.default_ms = st.total_ms;
-            ++best.candidates;
-            if (rate > best_rate) {
-                best_rate = rate;
-                best.iterations_per_graph = k;
-                best.path_budget = b;
-                best.best_ms = st.total_ms;
-            }
+            BatchKnobs c;
+            c.iterations = k;
+            c.budget = b;
+            if (ar_status e = run(c)) return e;
         }
+    const BatchKnobs base = bestk;
+    for (int32_t t : tbs)
+        for (int32_t sb : sbs) {
+            if (t == 0 && sb == 4) continue;   // measured above
+            BatchKnobs c = base;
+            c.trace_bps = t;
+            c.shade_bps = sb;
+            if (ar_status e = run(c)) return e;
+        }
+    best.iterations_per_graph = bestk.iterations;
+    best.path_budget = bestk.budget;
+    best.trace_blocks_per_sm = bestk.trace_bps;
+    best.shade_blocks_per_sm = bestk.shade_bps > 0 ? bestk.shade_bps : 4;
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
-        g_tuned[batch_key(jobs, njobs)] = {best.iterations_per_graph, best.path_budget};
+        g_tuned[batch_key(jobs, njobs)] = bestk;
     }
     *out = best;
     return AR_OK;

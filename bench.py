@@ -438,7 +438,7 @@ def measure_config5(torch, dev, stream, njobs: int = 64) -> dict:
     seeds, every second job four wavelengths per path, every other pair of jobs
     with a radiance cache of its own.  The jobs without a cache run in one
     launch of the batch graph (device-side loop) after the autotuner; each
-    cache job renders its samples as cache frames of 4 samples with online
+    cache job renders its samples as cache frames of up to 16 samples with online
     training (four-wavelength cache for the spectral ones).  Per job: paths,
     rays, Mrays/s of its part; relMSE against a 4096-spp FP64 image of the
     plain tracer for every eighth job."""
@@ -479,7 +479,7 @@ def measure_config5(torch, dev, stream, njobs: int = 64) -> dict:
     render_batch(jobs, stream=stream.cuda_stream)          # warm-up with the tuned knobs
     st = render_batch(jobs, stream=stream.cuda_stream)
     batch_rays = st.extension_rays + st.shadow_rays
-    # cache jobs: frames of 4 samples per pixel, cache trained online
+    # cache jobs: frames of up to 16 samples per pixel, cache trained online
     cache_ms, cache_rays, cache_paths = 0.0, 0, 0
     for k, sp in enumerate(specs):
         if not sp["cache"]:
@@ -490,8 +490,9 @@ def measure_config5(torch, dev, stream, njobs: int = 64) -> dict:
             c.set_spectral(4)
         acc = torch.zeros(sp["width"] * sp["height"] * 3, dtype=torch.float64, device=dev)
         ms = 0.0
-        for f in range(0, sp["spp"], 4):
-            fs = c.render_frame(cam, make_params(spp=4, max_depth=DEPTH, spectral=sp["spectral"], frame_offset=f),
+        for f in range(0, sp["spp"], 16):   # frames of 16 spp (the best frame size of the cache sweep)
+            fs = c.render_frame(cam, make_params(spp=min(16, sp["spp"] - f), max_depth=DEPTH, spectral=sp["spectral"],
+                                                 frame_offset=f),
                                 None, acc.data_ptr(), train=True, stats=True, stream=stream.cuda_stream)
             ms += fs.total_ms
             cache_rays += fs.extension_rays + fs.shadow_rays
@@ -512,7 +513,7 @@ def measure_config5(torch, dev, stream, njobs: int = 64) -> dict:
     total_ms = st.total_ms + cache_ms
     return {"workload": f"{njobs} seeded jobs: config-2 generator with 10K-2M triangles (log-uniform), resolutions "
                         "log-uniform 128-1024 per axis, spp in {4,16,64,256}, every second job four wavelengths, "
-                        "half the jobs with their own radiance cache (frames of 4 spp, trained online); jobs "
+                        "half the jobs with their own radiance cache (frames of up to 16 spp, trained online); jobs "
                         "without a cache in one launch of the batch graph (device-side loop), autotuned",
             "jobs": njobs, "ms": round(total_ms, 3),
             "mrays_per_s": round((batch_rays + cache_rays) / (total_ms / 1e3) / 1e6, 1),
@@ -521,6 +522,8 @@ def measure_config5(torch, dev, stream, njobs: int = 64) -> dict:
                       "msamples_per_s": round(st.paths / (st.total_ms / 1e3) / 1e6, 2), "paths": st.paths,
                       "graph_launches": st.graph_launches, "loop_passes": st.loop_passes,
                       "autotuned": {"iterations_per_graph": tune.iterations_per_graph, "path_budget": tune.path_budget,
+                                  "trace_blocks_per_sm": tune.trace_blocks_per_sm,
+                                  "shade_blocks_per_sm": tune.shade_blocks_per_sm, "candidates": tune.candidates,
                                     "probe_ms_best": round(tune.best_ms, 3),
                                     "probe_ms_default": round(tune.default_ms, 3)}},
             "cache_jobs": {"jobs": njobs - len(plain), "ms": round(cache_ms, 3), "paths": cache_paths,

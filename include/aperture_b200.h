@@ -506,14 +506,20 @@ typedef struct ar_batch_tuning {
     int64_t path_budget;           /* chosen in-flight path budget                 */
     float best_ms;                 /* probe time of the chosen configuration       */
     float default_ms;              /* probe time of the defaults (16, 2^22)        */
+    int32_t trace_blocks_per_sm;   /* chosen traversal grid per job (0: occupancy) */
+    int32_t shade_blocks_per_sm;   /* chosen shading/generation/retirement grid    */
 } ar_batch_tuning;
 
 /* Autotuner of ar_render_batch: times the batch's probe (every job at
  * min(spp, probe_spp) samples into scratch outputs; the jobs' own buffers are
- * not touched) for graph lengths {4, 8, 16, 32} x path budgets {2^20 .. 2^23}
- * and picks the fastest in paths per second.  The choice is remembered for
- * batches of the same shape (job count, pixels, samples, spectral jobs) and
- * used by ar_render_batch when it is called with iterations_per_graph = 0 and
+ * not touched) for graph lengths {4, 8, 16, 32} x path budgets {2^20 .. 2^23},
+ * then, at the fastest of those, for each job's kernel grids: traversal
+ * blocks per SM {occupancy, 4, 2} x shading / path generation / retirement
+ * blocks per SM {4, 2, 1} (jobs run as parallel graph branches, so smaller
+ * grids let several jobs' kernels share the GPU); 24 candidates, the fastest
+ * in paths per second wins.  The choice is remembered for batches of the same
+ * shape (job count, pixels, samples, spectral jobs) and used by
+ * ar_render_batch when it is called with iterations_per_graph = 0 and
  * path_budget = 0.  probe_spp <= 0 takes 4. */
 ar_status ar_batch_autotune(const ar_job* jobs, int32_t njobs, int32_t probe_spp, ar_batch_tuning* out,
                             void* stream);

@@ -54,8 +54,10 @@ def test_batch_rejects_bad_jobs(box_objects):
 @pytest.mark.gpu
 def test_batch_autotune(box_objects, small_spheres_objects):
     """The autotuner times its probe on scratch outputs (the jobs' buffers keep
-    their contents), returns one of its candidates, the fastest, and the next
-    default render_batch of the same batch shape uses it with unchanged results."""
+    their contents) over graph lengths x path budgets and then the per-job
+    kernel grids, returns one of its candidates, the fastest, and the next
+    default render_batch of the same batch shape uses it (grids included) with
+    unchanged results."""
     import torch
     from aperture_b200 import autotune_batch
     box = Scene(box_objects)
@@ -73,9 +75,11 @@ def test_batch_autotune(box_objects, small_spheres_objects):
     t = autotune_batch(jobs, probe_spp=2)
     torch.cuda.synchronize()
     assert all(bool((o == -1.0).all()) for o in outs)
-    assert t.candidates == 16
+    assert t.candidates == 24
     assert t.iterations_per_graph in (4, 8, 16, 32)
     assert t.path_budget in (1 << 20, 1 << 21, 1 << 22, 1 << 23)
+    assert t.trace_blocks_per_sm in (0, 4, 2)
+    assert t.shade_blocks_per_sm in (4, 2, 1)
     assert 0 < t.best_ms <= t.default_ms * 1.0001
     st = render_batch(jobs)
     torch.cuda.synchronize()
