@@ -5,15 +5,16 @@
 // triangle vertices on every test (intersection.cuh:27-29).  Here the transform
 // is applied once, with the same expression, and the leaf records carry the
 // world-space v0, e1 = v1 - v0 and e2 = v2 - v0 -- bit-identical operands of the
-// reference's Moller-Trumbore test.  The BVH is not the reference's: SAH (exact sweep for small
-// ranges, 256 bins above) over triangle-bound centroids (the reference bins SceneObject centres, which for a
-// mesh are all the mesh position -- scene_helper.h:488-545 -- and degenerate into
-// one leaf per mesh), max 4 primitives per leaf, collapsed greedily (largest
-// surface area first) into 8-wide nodes whose child boxes are quantised to 8
-// bits per plane relative to a power-of-two grid that starts one step below
-// the children's union, rounded outwards and padded by one grid step on both
-// sides, so the decoded box contains the exact one with a margin of a grid
-// step that absorbs the rounding of the kernel's plane decode.
+// reference's Moller-Trumbore test.  The BVH is not the reference's: SAH (exact
+// sweep for small ranges, 256 bins above) over triangle-bound centroids (the
+// reference bins SceneObject centres, which for a mesh are all the mesh
+// position -- scene_helper.h:488-545 -- and degenerate into one leaf per mesh),
+// max 4 primitives per leaf, collapsed along an SAH-optimal plan (dynamic
+// programming over the binary tree) into 8-wide nodes whose child boxes are
+// quantised to 8 bits per plane relative to a power-of-two grid that starts one
+// step below the children's union, rounded outwards and padded by one grid step
+// on both sides, so the decoded box contains the exact one with a margin of a
+// grid step that absorbs the rounding of the kernel's plane decode.
 #include "scene_build.h"
 
 #include <cuda_fp16.h>
@@ -80,6 +81,105 @@ constexpr int kBins = 256;
 // a visit of an 8-wide node costs several triangle tests.
 constexpr int kSweepMax = 64;
 constexpr float kTraversalCost = 0.25f;
+// Collapse costs (per unit of surface area): a wide-node visit and a
+// primitive test.  On the 1M-triangle sphere field the greedy collapse
+// (expand the child of largest area until 8 slots) left 3.8 of 8 slots used
+// per node; this plan fills 5.9 and traces 2 % faster.  A cheaper primitive
+// (0.3, 0.15: leaves of merged subtrees, 7.8 slots) was 1-3 % slower than
+// greedy; 1, 3 and 10 within 0.2 % of each other.
+constexpr float kCollapseNode = 1.0f;
+constexpr float kCollapsePrim = 3.0f;
+
+// SAH-optimal collapse of the binary tree into 8-wide nodes (dynamic
+// programming over the binary nodes, after Ylitie, Karras and Laine 2017):
+// C(n, i) is the least cost of subtree n spread over at most i child slots of
+// the wide node above it, C(n, 1) the cheaper of n as one leaf slot (at most
+// kMaxLeaf primitives, A(n) * p(n) * kCollapsePrim) and n as a wide node of
+// its own (A(n) * kCollapseNode + D(n, 8)), with D(n, j) the best split of j
+// slots between n's two children.
+struct CollapsePlan {
+    const std::vector<BNode>& bn;
+    std::vector<float> cost;          // [node * 9 + i], i = 1..8
+    std::vector<int8_t> how;          // [node * 9 + i]: -1 as with i - 1 slots; i = 1: 0 leaf, 1 wide node; else 2 split
+    std::vector<int8_t> split;        // [node * 9 + i]: slots of the left child in D(n, i)
+    std::vector<int> prims, first;
+
+    explicit CollapsePlan(const std::vector<BNode>& b) : bn(b)
+    {
+        const size_t n = bn.size();
+        cost.assign(n * 9, FLT_MAX);
+        how.assign(n * 9, 0);
+        split.assign(n * 9, 0);
+        prims.assign(n, 0);
+        first.assign(n, 0);
+        std::vector<float> dist(9);
+        std::vector<int8_t> dsplit(9);
+        for (int64_t v = static_cast<int64_t>(n) - 1; v >= 0; --v) {   // children (larger indices) first
+            const BNode& b = bn[v];
+            const float area = b.b.area();
+            float* c = &cost[v * 9];
+            if (b.leaf()) {
+                prims[v] = b.count;
+                first[v] = b.begin;
+                for (int i = 1; i <= 8; ++i) {
+                    c[i] = area * static_cast<float>(b.count) * kCollapsePrim;
+                    how[v * 9 + i] = 0;
+                }
+                continue;
+            }
+            prims[v] = prims[b.left] + prims[b.right];
+            first[v] = first[b.left];
+            // D(v, j): j slots split between the children
+            for (int j = 2; j <= 8; ++j) {
+                float best = FLT_MAX;
+                int8_t bk = 1;
+                for (int k = 1; k < j; ++k) {
+                    const float t = cost[b.left * 9 + k] + cost[b.right * 9 + (j - k)];
+                    if (t < best) { best = t; bk = static_cast<int8_t>(k); }
+                }
+                dist[j] = best;
+                dsplit[j] = bk;
+            }
+            const float asLeaf = prims[v] <= kMaxLeaf ? area * static_cast<float>(prims[v]) * kCollapsePrim : FLT_MAX;
+            const float asNode = area * kCollapseNode + dist[8];
+            c[1] = std::min(asLeaf, asNode);
+            how[v * 9 + 1] = asLeaf <= asNode ? 0 : 1;
+            split[v * 9 + 8] = dsplit[8];   // the slot split of v as a wide node, D(v, 8)
+            for (int i = 2; i <= 8; ++i) {
+                if (c[i - 1] <= dist[i]) { c[i] = c[i - 1]; how[v * 9 + i] = -1; }
+                else { c[i] = dist[i]; how[v * 9 + i] = 2; split[v * 9 + i] = dsplit[i]; }
+            }
+        }
+    }
+
+    struct Slot { int node; bool leaf; };
+
+    // the child slots of subtree v spread over at most i slots
+    void forest(int v, int i, std::vector<Slot>& out) const
+    {
+        if (bn[v].leaf()) {
+            out.push_back({v, true});
+            return;
+        }
+        while (i > 1 && how[v * 9 + i] == -1) --i;
+        if (i == 1) {
+            out.push_back({v, how[v * 9 + 1] == 0});
+            return;
+        }
+        const int k = split[v * 9 + i];
+        forest(bn[v].left, k, out);
+        forest(bn[v].right, i - k, out);
+    }
+
+    // the child slots of v as a wide node
+    void children(int v, std::vector<Slot>& out) const
+    {
+        const int k = split[v * 9 + 8];
+        forest(bn[v].left, k, out);
+        forest(bn[v].right, 8 - k, out);
+    }
+};
+
 
 struct BinaryBuilder {
     const std::vector<Bounds>& pb;
@@ -481,8 +581,9 @@ HostScene build_scene(const ar_object_desc* objs, size_t n, const ar_sdf_volume*
     bb.build(0, np);
     const std::vector<BNode>& bn = bb.nodes;
 
-    // ---------------- collapse to 8-wide, breadth first so that the internal
-    // children of a node are contiguous
+    // ---------------- collapse to 8-wide along the SAH-optimal plan, breadth
+    // first so that the internal children of a node are contiguous
+    const CollapsePlan plan(bn);
     struct Item { int wide; int bnode; };
     std::deque<Item> q;
     hs.nodes.emplace_back();
@@ -492,22 +593,11 @@ HostScene build_scene(const ar_object_desc* objs, size_t n, const ar_sdf_volume*
     while (!q.empty()) {
         const Item it = q.front();
         q.pop_front();
+        std::vector<CollapsePlan::Slot> slots;
+        if (bn[it.bnode].leaf()) slots.push_back({it.bnode, true});
+        else plan.children(it.bnode, slots);
         std::vector<int> ch;
-        if (bn[it.bnode].leaf()) ch.push_back(it.bnode);
-        else { ch.push_back(bn[it.bnode].left); ch.push_back(bn[it.bnode].right); }
-        while (ch.size() < static_cast<size_t>(kWide)) {
-            int best = -1;
-            float bestA = -1.0f;
-            for (size_t k = 0; k < ch.size(); ++k) {
-                if (bn[ch[k]].leaf()) continue;
-                const float a = bn[ch[k]].b.area();
-                if (a > bestA) { bestA = a; best = static_cast<int>(k); }
-            }
-            if (best < 0) break;
-            const int c = ch[best];
-            ch[best] = bn[c].left;
-            ch.insert(ch.begin() + best + 1, bn[c].right);
-        }
+        for (const auto& sl : slots) ch.push_back(sl.node);
         WideNode w;
         std::memset(&w, 0, sizeof(w));
         Bounds u;
@@ -530,11 +620,12 @@ HostScene build_scene(const ar_object_desc* objs, size_t n, const ar_sdf_volume*
             quantise(w.ox, sx, c.b.lo.x, c.b.hi.x, &w.qlo_x[k], &w.qhi_x[k]);
             quantise(w.oy, sy, c.b.lo.y, c.b.hi.y, &w.qlo_y[k], &w.qhi_y[k]);
             quantise(w.oz, sz, c.b.lo.z, c.b.hi.z, &w.qlo_z[k], &w.qhi_z[k]);
-            if (c.leaf()) {
-                if (c.count < 1 || c.count > kMaxLeaf) throw std::runtime_error("bad leaf size");
-                meta[k] = static_cast<uint8_t>(((c.count - 1) << 5) | poff);
-                for (int p = 0; p < c.count; ++p) hs.prims.push_back(precs[idx[c.begin + p]]);
-                poff += c.count;
+            if (slots[k].leaf) {
+                const int cnt = plan.prims[ch[k]], beg = plan.first[ch[k]];
+                if (cnt < 1 || cnt > kMaxLeaf) throw std::runtime_error("bad leaf size");
+                meta[k] = static_cast<uint8_t>(((cnt - 1) << 5) | poff);
+                for (int p = 0; p < cnt; ++p) hs.prims.push_back(precs[idx[beg + p]]);
+                poff += cnt;
             } else {
                 meta[k] = static_cast<uint8_t>(kMetaInternal | rank);
                 q.push_back({static_cast<int>(hs.nodes.size()), ch[k]});
