@@ -20,7 +20,8 @@ LIB_PATH = os.environ.get("AR_LIBRARY") or os.path.join(HERE, "libaperture_b200.
 
 AR_OK = 0
 STATUS_NAMES = {0: "AR_OK", 1: "AR_ERR_INVALID_ARGUMENT", 2: "AR_ERR_CUDA", 3: "AR_ERR_OUT_OF_MEMORY",
-                4: "AR_ERR_UNSUPPORTED", 5: "AR_ERR_DEVICE_FAULT", 6: "AR_ERR_NO_DEVICE"}
+                4: "AR_ERR_UNSUPPORTED", 5: "AR_ERR_DEVICE_FAULT", 6: "AR_ERR_NO_DEVICE",
+                7: "AR_ERR_INTERNAL"}
 OBJ_CUBE, OBJ_SPHERE, OBJ_SDF, OBJ_TRIANGLE = 0, 1, 2, 3
 MAT_DIFFUSE, MAT_LIGHT, MAT_GLASS, MAT_GGX = 0, 1, 2, 3
 MEM_HOST, MEM_DEVICE = 0, 1
@@ -103,6 +104,11 @@ class PathRecord(ctypes.Structure):
 class SceneInfo(ctypes.Structure):
     _fields_ = [("objects", c_int64), ("triangles", c_int64), ("lights", c_int64), ("wide_nodes", c_int64),
                 ("prim_refs", c_int64), ("device_bytes", c_int64), ("device", c_int32), ("camera_inside", c_int32)]
+
+
+class BvhInfo(ctypes.Structure):
+    _fields_ = [("wide_nodes", c_int64), ("prim_refs", c_int64), ("leaf_slots", c_int64), ("internal_slots", c_int64),
+                ("stack_bound", c_int32), ("depth", c_int32)]
 
 
 class RenderStats(ctypes.Structure):
@@ -190,7 +196,7 @@ RECORD_DTYPE = np.dtype(PathRecord)
 
 EXPORTED_SYMBOLS = ("ar_version", "ar_get_last_error_string", "ar_scene_create", "ar_scene_create_ex",
                     "ar_scene_destroy",
-                    "ar_scene_get_info", "ar_render", "ar_trace_rays", "ar_trace_rays_static",
+                    "ar_scene_get_info", "ar_bvh_build_info", "ar_render", "ar_trace_rays", "ar_trace_rays_static",
                     "ar_render_debug_paths", "ar_rng_tape", "ar_tonemap", "ar_accum_resolve", "ar_tone_curve",
                     "ar_scene_set_spectral", "ar_scene_get_spectral_luts", "ar_render_batch",
                     "ar_scene_set_medium", "ar_nrc_create", "ar_nrc_destroy", "ar_nrc_render_frame",
@@ -227,6 +233,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.ar_scene_destroy.restype = None
     lib.ar_scene_get_info.argtypes = [c_void_p, POINTER(SceneInfo)]
     lib.ar_scene_get_info.restype = c_int32
+    lib.ar_bvh_build_info.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, POINTER(BvhInfo)]
+    lib.ar_bvh_build_info.restype = c_int32
     lib.ar_render.argtypes = [c_void_p, POINTER(Camera), POINTER(RenderParams), c_void_p, c_void_p, c_int32,
                               c_void_p, POINTER(RenderStats)]
     lib.ar_render.restype = c_int32
@@ -450,6 +458,18 @@ class Scene:
         _check(_lib.ar_render_debug_paths(self._h, ctypes.byref(camera), ctypes.byref(params), _ptr(rec), MEM_HOST,
                                           None))
         return rec
+
+
+def bvh_build_info(objects: np.ndarray, volumes=None) -> BvhInfo:
+    """The shape of the BVH Scene(objects, volumes=volumes) would build, built
+    on the host alone (no device); raises if the structure check fails."""
+    lib = load_library()
+    objects = np.ascontiguousarray(objects, dtype=OBJECT_DTYPE)
+    info = BvhInfo()
+    arr = (SdfVolume * len(volumes))(*[v for v, _ in volumes]) if volumes else None
+    _check(lib.ar_bvh_build_info(_ptr(objects) if len(objects) else None, len(objects), arr,
+                                 len(volumes) if volumes else 0, ctypes.byref(info)))
+    return info
 
 
 def rng_tape(camera: Camera, params: RenderParams, per_path: int) -> np.ndarray:

@@ -585,6 +585,53 @@ ar_status ar_scene_get_info(const ar_scene* s, ar_scene_info* info)
     return AR_OK;
 }
 
+ar_status ar_bvh_build_info(const ar_object_desc* objects, size_t count, const ar_sdf_volume* volumes,
+                            size_t volume_count, ar_bvh_info* info)
+{
+    g_last_error.clear();
+    if (!info) return fail(AR_ERR_INVALID_ARGUMENT, "info is NULL");
+    std::memset(info, 0, sizeof(*info));
+    if (count > 0 && !objects) return fail(AR_ERR_INVALID_ARGUMENT, "objects is NULL");
+    if (volume_count > 0 && !volumes) return fail(AR_ERR_INVALID_ARGUMENT, "volumes is NULL");
+    try {
+        const ar::HostScene hs = ar::build_scene(objects, count, volumes, volume_count);
+        // every primitive record in exactly one leaf slot, every child index in range
+        std::vector<uint8_t> seen(hs.prims.size(), 0);
+        for (size_t w = 0; w < hs.nodes.size(); ++w) {
+            const ar::WideNode& nd = hs.nodes[w];
+            for (int k = 0; k < ar::kWide; ++k) {
+                const uint32_t m = ((k < 4 ? nd.meta_lo : nd.meta_hi) >> (8 * (k & 3))) & 0xFFu;
+                if (m == ar::kMetaEmpty) continue;
+                if (m & ar::kMetaInternal) {
+                    const uint64_t c = static_cast<uint64_t>(nd.child_base) + (m & 7u);
+                    if (c == 0 || c >= hs.nodes.size())
+                        return fail(AR_ERR_INTERNAL, "BVH: child index out of range");
+                    ++info->internal_slots;
+                } else {
+                    const uint32_t cnt = ((m >> 5) & 3u) + 1u;
+                    for (uint32_t q = 0; q < cnt; ++q) {
+                        const uint64_t pi = static_cast<uint64_t>(nd.prim_base) + (m & 31u) + q;
+                        if (pi >= hs.prims.size() || seen[pi]++)
+                            return fail(AR_ERR_INTERNAL, "BVH: primitive record out of range or shared");
+                    }
+                    ++info->leaf_slots;
+                }
+            }
+        }
+        for (uint8_t v : seen)
+            if (v != 1) return fail(AR_ERR_INTERNAL, "BVH: primitive record in no leaf");
+        info->wide_nodes = static_cast<int64_t>(hs.nodes.size());
+        info->prim_refs = static_cast<int64_t>(hs.prims.size());
+        info->stack_bound = hs.stack_bound;
+        info->depth = hs.wide_depth;
+        return AR_OK;
+    } catch (const std::bad_alloc&) {
+        return fail(AR_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(AR_ERR_INVALID_ARGUMENT, e.what());
+    }
+}
+
 ar_status ar_render(ar_scene* s, const ar_camera* cam, const ar_render_params* p, float* out_rgb, double* accum,
                     int32_t mem_kind, void* stream, ar_render_stats* stats)
 {

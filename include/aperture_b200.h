@@ -32,7 +32,8 @@ typedef enum ar_status {
     AR_ERR_OUT_OF_MEMORY = 3,    /* device or host allocation failed             */
     AR_ERR_UNSUPPORTED = 4,      /* feature not available for this scene/config  */
     AR_ERR_DEVICE_FAULT = 5,     /* a kernel reported an internal error word     */
-    AR_ERR_NO_DEVICE = 6         /* no CUDA device / extension not usable        */
+    AR_ERR_NO_DEVICE = 6,        /* no CUDA device / extension not usable        */
+    AR_ERR_INTERNAL = 7          /* a consistency check of the library failed    */
 } ar_status;
 
 /* EObjectType (core/render/object.cuh:29-35). */
@@ -211,6 +212,25 @@ ar_status ar_scene_create_ex(const ar_object_desc* objects, size_t count, const 
 void ar_scene_destroy(ar_scene* scene);
 
 ar_status ar_scene_get_info(const ar_scene* scene, ar_scene_info* info);
+
+/* Shape of the BVH that ar_scene_create_ex builds for these objects, built on
+ * the host alone (no device, nothing uploaded): the 8-wide nodes, primitive
+ * records, occupied child slots and the exact worst-case traversal stack
+ * depth.  The call also checks the structure -- every primitive record in
+ * exactly one leaf slot, every child index in range -- and returns
+ * AR_ERR_INTERNAL if it does not hold.  Invalid objects give the same
+ * AR_ERR_INVALID_ARGUMENT as ar_scene_create_ex. */
+typedef struct ar_bvh_info {
+    int64_t wide_nodes;
+    int64_t prim_refs;
+    int64_t leaf_slots;      /* child slots holding a leaf (1-4 primitive records) */
+    int64_t internal_slots;  /* child slots holding a wide node (= wide_nodes - 1)  */
+    int32_t stack_bound;     /* deepest traversal stack any ray can need           */
+    int32_t depth;           /* wide levels                                        */
+} ar_bvh_info;
+
+ar_status ar_bvh_build_info(const ar_object_desc* objects, size_t count, const ar_sdf_volume* volumes,
+                            size_t volume_count, ar_bvh_info* info);
 
 /* Offline render: spp samples per pixel, FP64 accumulation, mean written as
  * linear RGB float3 rows (index j*width+i).  Replaces
