@@ -627,6 +627,10 @@ ar_status ar_bvh_build_info(const ar_object_desc* objects, size_t count, const a
         return AR_OK;
     } catch (const std::bad_alloc&) {
         return fail(AR_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::domain_error& e) {
+        return fail(AR_ERR_UNSUPPORTED, e.what());
+    } catch (const std::runtime_error& e) {   // the builder's own consistency checks
+        return fail(AR_ERR_INTERNAL, e.what());
     } catch (const std::exception& e) {
         return fail(AR_ERR_INVALID_ARGUMENT, e.what());
     }

@@ -311,7 +311,7 @@ int grid_exponent(float lo, float hi)
         std::frexp(ext / 250.0, &ee);  // ext/250 < 2^ee
         e = std::max(e, ee);
     }
-    if (e > 126) throw std::runtime_error("scene coordinates too large for the quantised BVH");
+    if (e > 126) throw std::domain_error("scene coordinates too large for the quantised BVH");
     return e;
 }
 
@@ -327,7 +327,7 @@ void quantise(float origin, float scale, float lo, float hi, uint8_t* qlo, uint8
     while (ql > 0 && std::fma(static_cast<float>(ql), scale, origin) > lo) --ql;
     while (qh < 255 && std::fma(static_cast<float>(qh), scale, origin) < hi) ++qh;
     if (std::fma(static_cast<float>(ql), scale, origin) > lo || std::fma(static_cast<float>(qh), scale, origin) < hi)
-        throw std::runtime_error("BVH quantisation could not enclose a child box");
+        throw std::domain_error("BVH quantisation could not enclose a child box");
     *qlo = static_cast<uint8_t>(ql);
     *qhi = static_cast<uint8_t>(qh);
 }

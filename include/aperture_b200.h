@@ -218,8 +218,9 @@ ar_status ar_scene_get_info(const ar_scene* scene, ar_scene_info* info);
  * records, occupied child slots and the exact worst-case traversal stack
  * depth.  The call also checks the structure -- every primitive record in
  * exactly one leaf slot, every child index in range -- and returns
- * AR_ERR_INTERNAL if it does not hold.  Invalid objects give the same
- * AR_ERR_INVALID_ARGUMENT as ar_scene_create_ex. */
+ * AR_ERR_INTERNAL if it does not hold.  Invalid objects give
+ * AR_ERR_INVALID_ARGUMENT and coordinates beyond the quantised grid's range
+ * AR_ERR_UNSUPPORTED, as in ar_scene_create_ex. */
 typedef struct ar_bvh_info {
     int64_t wide_nodes;
     int64_t prim_refs;
