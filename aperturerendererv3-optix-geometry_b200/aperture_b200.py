@@ -413,9 +413,15 @@ class Scene:
         return si
 
     def render(self, camera: Camera, params: RenderParams, accum: np.ndarray | None = None,
-               stream: int = 0, want_stats: bool = True):
-        """Host-buffer render; returns (image[h, w, 3] float32, RenderStats)."""
-        out = np.empty((camera.height, camera.width, 3), np.float32)
+               stream: int = 0, want_stats: bool = True, out: np.ndarray | None = None):
+        """Host-buffer render; returns (image[h, w, 3] float32, RenderStats).
+        out: a caller-owned float32 host array of h*w*3 values to write into
+        (page-locked memory makes the copy back a direct DMA)."""
+        if out is None:
+            out = np.empty((camera.height, camera.width, 3), np.float32)
+        else:
+            assert out.dtype == np.float32 and out.flags.c_contiguous and out.size == camera.height * camera.width * 3
+            out = out.reshape(camera.height, camera.width, 3)
         st = RenderStats()
         acc_ptr = None
         if accum is not None:
