@@ -5,9 +5,9 @@
 // residual blocks of width 32 with ReLU, a 4-wide output -- at every voxel
 // centre of the unit colour cube; 512^3 voxels in the reference).
 //
-// A CTA owns 128 voxels, one per thread; every layer is one 128 x 32 x 32
+// A tile is 128 voxels, one per thread; every layer is one 128 x 32 x 32
 // matrix product on tcgen05.mma (kind::f16) with fp32 accumulators in tensor
-// memory.  The MMA takes bf16 operands, so fp32 accuracy comes from splitting
+// memory.  A CTA of 256 threads runs two tiles side by side.  The MMA takes bf16 operands, so fp32 accuracy comes from splitting
 // both operands into three bf16 terms, x = x0 + x1 + x2 (x0 = bf16(x),
 // x1 = bf16(x - x0), x2 = bf16(x - x0 - x1): 24 significant bits), and
 // accumulating the six products whose order is at most 2 (x2 w0, x1 w1,
@@ -43,7 +43,7 @@ constexpr int kLutWLayer = kLutN * kLutK * 2;                 // bytes of one bf
 constexpr int kLutWOut = kLutNOut * kLutK * 2;
 constexpr int kLutWBytes = 3 * ((kLutLayers - 1) * kLutWLayer + kLutWOut);   // three splits
 constexpr int kLutABytes = kLutRows * kLutK * 2;              // one bf16 split of the activations
-constexpr int kLutSmem = kLutWBytes + 3 * kLutABytes + 64;
+constexpr int kLutSmem = kLutWBytes + 6 * kLutABytes + 64;   // weights, two tiles' A operands, barriers
 constexpr int kLutCols = 32;                                  // TMEM columns (fp32 accumulators)
 constexpr uint32_t kLutSpinLimit = 1u << 22;
 
@@ -86,18 +86,39 @@ __device__ __forceinline__ void store_row(unsigned char* sA, int t, const float*
 
 namespace {
 
-__global__ void __launch_bounds__(kLutRows) k_lut_rgb_tc(const float* __restrict__ tab, int res,
-                                                         float4* __restrict__ lut, int* err)
+// Synchronisation of one 128-thread half of the CTA (named barrier 1 + half).
+__device__ __forceinline__ void half_sync(int half)
+{
+    asm volatile("bar.sync %0, 128;" : : "r"(1 + half) : "memory");
+}
+// The same barrier with an OR over the half's predicates.
+__device__ __forceinline__ bool half_sync_or(int half, bool v)
+{
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred q, p;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.or.pred p, %2, 128, q;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(r) : "r"(v ? 1u : 0u), "r"(1 + half) : "memory");
+    return r != 0;
+}
+
+// Two halves of 128 threads run two tiles side by side: each half has its own
+// A operand, mbarrier and 32 tensor-memory columns and synchronises on a named
+// barrier of its own, so one half's epilogue (tcgen05.ld, bias, ReLU, split,
+// store) overlaps the other half's MMAs.  The weights are shared.
+__global__ void __launch_bounds__(2 * kLutRows) k_lut_rgb_tc(const float* __restrict__ tab, int res,
+                                                             float4* __restrict__ lut, int* err)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char* sW = smem;
-    unsigned char* sA = smem + kLutWBytes;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kLutWBytes + 3 * kLutABytes);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kLutWBytes + 3 * kLutABytes + 16);
-    const int t = threadIdx.x, warp = t >> 5;
+    const int half = threadIdx.x >> 7;                 // which tile of the pair
+    const int t = threadIdx.x & (kLutRows - 1);        // row within the tile
+    const int warp = threadIdx.x >> 5;
+    unsigned char* sA = smem + kLutWBytes + half * 3 * kLutABytes;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kLutWBytes + 6 * kLutABytes) + half;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kLutWBytes + 6 * kLutABytes + 16);
 
     // weights [out][in] of every layer as three bf16 splits, B operands (N rows x K)
-    for (int e = t; e < kLutLayers * kLutN * kLutK; e += kLutRows) {
+    for (int e = threadIdx.x; e < kLutLayers * kLutN * kLutK; e += 2 * kLutRows) {
         const int l = e / (kLutN * kLutK), rem = e - l * (kLutN * kLutK);
         const int n = rem / kLutK, k = rem - n * kLutK;
         const int R = l == kLutLayers - 1 ? kLutNOut : kLutN;
@@ -112,26 +133,27 @@ __global__ void __launch_bounds__(kLutRows) k_lut_rgb_tc(const float* __restrict
             *reinterpret_cast<__nv_bfloat16*>(sW + lut_w_offset(l, j) + tc_chunk_offset(R, n, k / 8) + (k % 8) * 2) =
                 s3[j];
     }
-    if (t == 0) {
+    if (t == 0) {   // thread 0 of each half: its mbarrier
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(smem_addr(mbar)), "r"(1) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     : : "r"(smem_addr(tmem_slot)), "r"(kLutCols) : "memory");
+                     : : "r"(smem_addr(tmem_slot)), "r"(2 * kLutCols) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+    const uint32_t tmem = *tmem_slot + static_cast<uint32_t>(half * kLutCols);   // this half's columns
+    const uint32_t taddr = tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16);  // lanes of this warp's rows
     const uint32_t aBase = smem_addr(sA), wBase = smem_addr(sW), mb = smem_addr(mbar);
     uint32_t phase = 0;
     bool failed = false;
     const int64_t total = static_cast<int64_t>(res) * res * res;
     const float invRes = 1.0f / static_cast<float>(res);
-    for (int64_t tile = blockIdx.x; tile * kLutRows < total && !failed; tile += gridDim.x) {
+    for (int64_t tile = 2 * static_cast<int64_t>(blockIdx.x) + half; tile * kLutRows < total && !failed;
+         tile += 2 * static_cast<int64_t>(gridDim.x)) {
         const int64_t vx = tile * kLutRows + t;
         const bool valid = vx < total;
         const int64_t v = valid ? vx : total - 1;
@@ -156,7 +178,7 @@ __global__ void __launch_bounds__(kLutRows) k_lut_rgb_tc(const float* __restrict
             store_row(sA, t, h);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncthreads();
+            half_sync(half);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (t == 0) {
                 const uint32_t idesc = tc_idesc(kLutRows, N);
@@ -179,7 +201,7 @@ __global__ void __launch_bounds__(kLutRows) k_lut_rgb_tc(const float* __restrict
                 if (++spins >= kLutSpinLimit) { late = true; break; }
             }
             phase ^= 1u;
-            failed = __syncthreads_or(late ? 1 : 0) != 0;
+            failed = half_sync_or(half, late);   // the same decision in every thread of the half
             if (failed) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             uint32_t acc[kLutN];
@@ -207,7 +229,8 @@ __global__ void __launch_bounds__(kLutRows) k_lut_rgb_tc(const float* __restrict
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(tmem), "r"(kLutCols) : "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(*tmem_slot), "r"(2 * kLutCols) : "memory");
 }
 
 }  // namespace
@@ -219,8 +242,8 @@ cudaError_t launch_spectral_rgb_lut_tc(const float* tab, int res, float4* lut, i
     if (e != cudaSuccess) return e;
     const int64_t total = static_cast<int64_t>(res) * res * res;
     const int64_t tiles = (total + kLutRows - 1) / kLutRows;
-    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sm_count) * 2)));
-    k_lut_rgb_tc<<<grid, kLutRows, kLutSmem, st>>>(tab, res, lut, err);
+    const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((tiles + 1) / 2, int64_t(sm_count) * 2)));
+    k_lut_rgb_tc<<<grid, 2 * kLutRows, kLutSmem, st>>>(tab, res, lut, err);
     return cudaGetLastError();
 }
 
