@@ -354,13 +354,13 @@ def spline_path(torch, dev, scene: Scene, stream) -> dict:
 
 
 def sweep_nrc(torch, dev, stream, mode: str = "box") -> dict:
-    """The cache's time-to-relMSE over spp per frame {1, 4, 16} x spread
-    constant {0.01, 0.1, 1} x optimiser steps per frame {1, 4}, against one
-    oracle and one plain measurement."""
+    """The cache's time-to-relMSE over spp per frame {1, 4, 16} ({16, 64} for
+    the 1920x1080 mode "full") x spread constant {0.01, 0.1, 1} x optimiser
+    steps per frame {1, 4}, against one oracle and one plain measurement."""
     S = nrc_setup(torch, dev, None if mode in ("box", "config3") else Scene(scenes.spheres_scene(), device=dev.index),
                   mode, stream)
     runs = []
-    for k in (1, 4, 16):
+    for k in ((16, 64) if mode == "full" else (1, 4, 16)):
         for c in (0.01, 0.1, 1.0):
             for steps in (1, 4):
                 r = nrc_curve(torch, dev, S, stream, k, c, steps)
@@ -879,7 +879,7 @@ def main():
     ap.add_argument("--nrc-spp", type=int, default=16, help="samples per pixel of a cache frame")
     ap.add_argument("--nrc-c", type=float, default=1.0, help="spread constant of the cache's termination rule")
     ap.add_argument("--nrc-steps", type=int, default=4, help="optimiser steps per cache frame")
-    ap.add_argument("--nrc-sweep", choices=("box", "small", "config3"), default=None,
+    ap.add_argument("--nrc-sweep", choices=("box", "small", "full", "config3"), default=None,
                     help="time-to-relMSE over spp per frame x spread constant x optimiser steps, then exit")
     ap.add_argument("--profile-nrc", action="store_true",
                     help="six radiance-cache frames (for ncu captures of the cache kernels)")
