@@ -108,6 +108,7 @@ struct ar_scene {
     ar::SceneView view{};
     int grid_trace = 0;
     const uint32_t* jump_table = nullptr;  // A^(2^32) lookup table of the XORWOW register
+    const uint32_t* jump_table67 = nullptr;  // A^(2^67): one curand subsequence
     int64_t objects = 0, triangles = 0, lights = 0, nodes = 0, prims = 0;
     int64_t device_bytes = 0;
     std::vector<void*> owned;
@@ -338,7 +339,7 @@ ar_status run_render(ar_scene* s, const ar_camera* cam, const ar_render_params* 
     // seed and image) starts from the states the previous one left.
     if (!(s->rng_valid && s->rng_seed == fp.seed && s->rng_width == fp.width && s->rng_height == fp.height &&
           s->rng_next_frame == fp.frame0))
-        ck(launch_rng_init(fp, s->base0, s->base1, st), "rng init");
+        ck(launch_rng_init(fp, s->base0, s->base1, s->jump_table67, st), "rng init");
     s->rng_valid = false;
     ck(launch_pool_init(s->ctl, total, st), "pool init");
     int64_t launches = 2;
@@ -518,6 +519,8 @@ ar_status ar_scene_create_ex(const ar_object_desc* objects, size_t count, const 
         {
             static const std::vector<uint32_t> jt = ar::xorwow_jump_table_2p32();
             s->jump_table = static_cast<const uint32_t*>(own(upload(jt, "rng jump table"), jt.size() * 4));
+            static const std::vector<uint32_t> js = ar::xorwow_jump_table_pow2(67);
+            s->jump_table67 = static_cast<const uint32_t*>(own(upload(js, "rng subsequence table"), js.size() * 4));
         }
         {
             // SDF volumes, then the SDF records pointing at them (device and host copies)
@@ -1035,7 +1038,7 @@ ar_status render_batch(const ar_job* jobs, int32_t njobs, BatchKnobs kn, ar_batc
         ck(cudaMemsetAsync(w.accum, 0, sizeof(double) * 3 * w.npix, w.st), "memset");
         ck(cudaMemsetAsync(w.stats, 0, 64, w.st), "memset");
         ck(cudaMemsetAsync(w.err, 0, 64, w.st), "memset");
-        ck(ar::launch_rng_init(w.fp, w.base0, w.base1, w.st), "rng init");
+        ck(ar::launch_rng_init(w.fp, w.base0, w.base1, jb.scene->jump_table67, w.st), "rng init");
         ck(ar::launch_pool_init(w.ctl, w.total, w.st), "pool init");
         ck(cudaEventRecord(w.done, w.st), "event record");
         ck(cudaStreamWaitEvent(st, w.done, 0), "join");

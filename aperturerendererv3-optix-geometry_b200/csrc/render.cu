@@ -106,15 +106,34 @@ __global__ void __launch_bounds__(kTraceBlock, kTraceMinBlocks) k_trace_rays(Sce
 
 // ------------------------------------------------------------------ RNG
 // curand_init(GLOBAL_SEED, pixelIndex, TOTAL_FRAME_INDEX * 2^32) (random.cuh:35-38)
-__global__ void k_rng_init(FrameParams fp, uint4* base0, uint2* base1)
+// Every pixel's state of InitRand: curand_init(seed, s, frame0 * 2^32) with s
+// its reference pixel index.  One thread per 8x4 pixel block, i.e. per run of
+// 32 consecutive s: curand_init for the block's first pixel, then each next
+// pixel's register as A^(2^67) times the previous one (subsequences are 2^67
+// draws apart; the Weyl counter moves by 362437 * 2^67 = 0 mod 2^32), which
+// replaces 31 of every 32 general skip-aheads by a table jump.
+__global__ void k_rng_init(FrameParams fp, uint4* base0, uint2* base1, const uint32_t* __restrict__ jump67)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= fp.npix) return;
-    const int i = p % fp.width, j = p / fp.width;
-    curandStateXORWOW_t st;
-    curand_init(fp.seed, ref_pixel_index(i, j, fp.grid_x), fp.frame0 << 32, &st);
-    base0[p] = make_uint4(st.d, st.v[0], st.v[1], st.v[2]);
-    base1[p] = make_uint2(st.v[3], st.v[4]);
+    __shared__ uint32_t jt[kJumpWords];
+    for (int k = threadIdx.x; k < kJumpWords; k += blockDim.x) jt[k] = jump67[k];
+    __syncthreads();
+    const int grid_y = (fp.height + 3) / 4;
+    const int nblk = fp.grid_x * grid_y;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nblk; b += gridDim.x * blockDim.x) {
+        curandStateXORWOW_t st;
+        curand_init(fp.seed, 32ull * static_cast<unsigned long long>(b), fp.frame0 << 32, &st);
+        uint32_t v[5] = {st.v[0], st.v[1], st.v[2], st.v[3], st.v[4]};
+        const int bx = b % fp.grid_x, by = b / fp.grid_x;
+        for (int w = 0; w < 32; ++w) {   // w = tx + 8 ty: ref_pixel_index order within the block
+            if (w > 0) xorwow_jump(v, jt);   // A^(2^67): the next subsequence
+            const int i = 8 * bx + (w & 7), j = 4 * by + (w >> 3);
+            if (i < fp.width && j < fp.height) {
+                const int p = j * fp.width + i;
+                base0[p] = make_uint4(st.d, v[0], v[1], v[2]);
+                base1[p] = make_uint2(v[3], v[4]);
+            }
+        }
+    }
 }
 
 // out[(s * npix + p) * per_path + k] = k-th uniform of pixel p at sample s
@@ -204,7 +223,7 @@ __global__ void k_regen(FrameParams fp, PathBuffers B, PoolCtl* ctl, int cur, ui
         rng_from(r, a, make_uint4(b.x, b.y, 0u, 0u));
         {   // advance the per-pixel state to the next frame: offset + 2^32
             uint32_t nv[5] = {a.y, a.z, a.w, b.x, b.y};
-            xorwow_jump_2p32(nv, jt);
+            xorwow_jump(nv, jt);
             base0[p] = make_uint4(a.x, nv[0], nv[1], nv[2]);
             base1[p] = make_uint2(nv[3], nv[4]);
         }
@@ -1159,9 +1178,10 @@ cudaError_t launch_trace_rays(const SceneView& s, const float4* rays, int n, int
     return cudaGetLastError();
 }
 
-cudaError_t launch_rng_init(const FrameParams& fp, uint4* b0, uint2* b1, cudaStream_t st)
+cudaError_t launch_rng_init(const FrameParams& fp, uint4* b0, uint2* b1, const uint32_t* jump67, cudaStream_t st)
 {
-    k_rng_init<<<(fp.npix + 255) / 256, 256, 0, st>>>(fp, b0, b1);
+    const int nblk = fp.grid_x * ((fp.height + 3) / 4);
+    k_rng_init<<<(nblk + 127) / 128, 128, 0, st>>>(fp, b0, b1, jump67);
     return cudaGetLastError();
 }
 

@@ -19,7 +19,7 @@ cudaError_t set_intersect_eps(const float* tab9);
 int trace_grid(int sm_count);
 cudaError_t launch_trace_rays(const SceneView& s, const float4* rays, int n, int any, int32_t* obj, float* t,
                               PoolCtl* ctl, uint32_t* ovf, int* err, int grid, cudaStream_t st);
-cudaError_t launch_rng_init(const FrameParams& fp, uint4* b0, uint2* b1, cudaStream_t st);
+cudaError_t launch_rng_init(const FrameParams& fp, uint4* b0, uint2* b1, const uint32_t* jump67, cudaStream_t st);
 cudaError_t launch_rng_tape(const FrameParams& fp, int spp, int per_path, float* out, cudaStream_t st);
 
 // Optional event pairs around every traversal launch: ev[2k], ev[2k+1].

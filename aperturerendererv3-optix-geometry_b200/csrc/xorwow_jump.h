@@ -1,4 +1,4 @@
-// xorwow_jump.h -- jump a XORWOW state ahead by 2^32 draws.
+// xorwow_jump.h -- jump a XORWOW state ahead by 2^32 (or 2^67) draws.
 //
 // The reference seeds every frame of every pixel with
 // curand_init(seed, pixel, frame * 2^32) (core/random.cuh:31-39), so frame f+1
@@ -92,9 +92,10 @@ inline Bits160 xorwow_jump_apply(const std::vector<uint32_t>& table, const Bits1
 inline std::vector<uint32_t> xorwow_jump_table_2p32() { return xorwow_jump_table_pow2(32); }
 
 #ifdef __CUDACC__
-// v (the five register words, curand order v[0..4]) <- A^(2^32) v, with the
-// table staged in shared memory.
-__device__ __forceinline__ void xorwow_jump_2p32(uint32_t v[5], const uint32_t* __restrict__ table)
+// v (the five register words, curand order v[0..4]) <- M v for the jump M of
+// a table built by xorwow_jump_table_pow2 (A^(2^32): one frame; A^(2^67): one
+// curand subsequence), with the table staged in shared memory.
+__device__ __forceinline__ void xorwow_jump(uint32_t v[5], const uint32_t* __restrict__ table)
 {
     uint32_t r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
 #pragma unroll
