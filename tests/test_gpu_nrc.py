@@ -115,10 +115,19 @@ def test_nrc_frames_converge_to_plain_image():
     rel = ((img - ref) ** 2 / (ref ** 2 + 1e-2)).mean()
     assert queries > 1000
     assert rel < 0.02, rel
-    # the cache removes most of the noise of the plain tracer at equal frames
+    # what the trained network gains: the plain tracer at the same number of
+    # samples, and the same frames with a cache that is never trained
     plain, _ = sc.render(cam, make_params(spp=frames, max_depth=8, frame_offset=100000))
     rel_plain = ((plain - ref) ** 2 / (ref ** 2 + 1e-2)).mean()
-    print("relMSE cache", rel, "plain", rel_plain)
+    c0 = RadianceCache(sc, cfg)
+    acc0 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    for f in range(frames):
+        c0.render_frame(cam, make_params(spp=1, max_depth=8, frame_offset=f), None, acc0.data_ptr(), train=False)
+    img0 = (acc0 / frames).cpu().numpy().reshape(64, 64, 3)
+    rel_untrained = ((img0 - ref) ** 2 / (ref ** 2 + 1e-2)).mean()
+    print("relMSE cache", rel, "plain", rel_plain, "untrained cache", rel_untrained)
+    assert rel < rel_plain, (rel, rel_plain)
+    assert rel < 0.5 * rel_untrained, (rel, rel_untrained)
 
 
 @pytest.mark.gpu
