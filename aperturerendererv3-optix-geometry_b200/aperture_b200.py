@@ -420,7 +420,8 @@ class Scene:
         if out is None:
             out = np.empty((camera.height, camera.width, 3), np.float32)
         else:
-            assert out.dtype == np.float32 and out.flags.c_contiguous and out.size == camera.height * camera.width * 3
+            if not (out.dtype == np.float32 and out.flags.c_contiguous and out.size == camera.height * camera.width * 3):
+                raise ValueError("out must be a C-contiguous float32 array of height * width * 3 values")
             out = out.reshape(camera.height, camera.width, 3)
         st = RenderStats()
         acc_ptr = None
