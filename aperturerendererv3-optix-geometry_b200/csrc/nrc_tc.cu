@@ -1,11 +1,11 @@
 // nrc_tc.cu -- radiance-cache inference on the 5th-generation tensor cores:
-// tcgen05.mma (M = 128 rows per CTA, kind::f16 with bf16 operands, fp32
+// tcgen05.mma (M = 128 rows per tile, kind::f16 with bf16 operands, fp32
 // accumulators in tensor memory), one elected thread issuing the MMAs of a
 // layer, completion through tcgen05.commit on an mbarrier, and the epilogue
 // of each layer (ReLU, bf16 pack, or exp at the output) from tcgen05.ld:
-// thread t of the CTA owns row t of the tile, so it reads its 64 accumulator
-// columns from TMEM lane t and writes the next layer's A operand row back to
-// shared memory.
+// thread t of a 128-thread tile group owns row t of the tile, so it reads its
+// 64 accumulator columns from TMEM lane t and writes the next layer's A
+// operand row back to shared memory.  Inference runs two tiles per CTA.
 //
 // Operands live in shared memory in the canonical K-major layout of
 // tcgen05.cuh.
@@ -30,6 +30,7 @@ constexpr int kTcCols = 64;                        // TMEM columns allocated (fp
 constexpr int kTcWBytes = 5 * kNrcHid * kNrcIn * 2 + kNrcOut * kNrcIn * 2;   // 43008
 constexpr int kTcABytes = kTcRows * kNrcIn * 2;                               // 16384
 constexpr int kTcSmem = kTcWBytes + kTcABytes + 64;
+constexpr int kTcInferSmem = kTcWBytes + 2 * kTcABytes + 64;                  // two tiles per CTA
 constexpr uint32_t kTcSpinLimit = 1u << 22;
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi)
@@ -76,19 +77,23 @@ __device__ void tc_encode(const NrcNet& net, const NrcVertex& v, bool valid, uin
     for (int k = 28; k < 32; ++k) r32[k] = 0u;
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) k_nrc_infer_tc(NrcNet net, const NrcQuery* __restrict__ q,
+// Two halves of 128 threads run two query tiles side by side, each with its
+// own A operand, mbarrier, 64 tensor-memory columns and named barrier: one
+// half's hash-grid gathers and epilogues overlap the other half's MMAs.
+__global__ void __launch_bounds__(2 * kTcRows, 2) k_nrc_infer_tc(NrcNet net, const NrcQuery* __restrict__ q,
                                                                const int32_t* count, int cap, double* accum,
                                                                float* out_rgb, int* err)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char* sW = smem;                                  // 6 weight operands, canonical layout
-    unsigned char* sA = smem + kTcWBytes;                      // 128 x 64 activation operand
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kTcWBytes + kTcABytes);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcWBytes + kTcABytes + 16);
-    const int t = threadIdx.x, warp = t >> 5;
+    const int half = threadIdx.x >> 7;                         // which tile of the pair
+    const int t = threadIdx.x & (kTcRows - 1), warp = threadIdx.x >> 5;
+    unsigned char* sA = smem + kTcWBytes + half * kTcABytes;   // this half's 128 x 64 activation operand
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + kTcWBytes + 2 * kTcABytes) + half;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kTcWBytes + 2 * kTcABytes + 16);
 
     // weights [out][in] -> canonical K-major chunks
-    for (int e = t; e < kTcWBytes / 16; e += kTcThreads) {
+    for (int e = threadIdx.x; e < kTcWBytes / 16; e += 2 * kTcRows) {
         const int l = min(e / (kNrcHid * 8), kNrcLayers - 1);
         const int local = e - l * (kNrcHid * 8);
         const int R = nrc_w_rows(l);
@@ -102,20 +107,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nrc_infer_tc(NrcNet net, cons
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     : : "r"(smem_addr(tmem_slot)), "r"(kTcCols) : "memory");
+                     : : "r"(smem_addr(tmem_slot)), "r"(2 * kTcCols) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+    const uint32_t tmem = *tmem_slot + static_cast<uint32_t>(half * kTcCols);     // this half's columns
+    const uint32_t taddr = tmem + (static_cast<uint32_t>((warp & 3) * 32) << 16);  // lanes of this warp's rows
     const uint32_t aBase = smem_addr(sA), wBase = smem_addr(sW), mb = smem_addr(mbar);
     uint32_t phase = 0;
     bool failed = false;
 
     const int n = min(*count, cap);
-    for (int tile = blockIdx.x; tile * kTcRows < n && !failed; tile += gridDim.x) {
+    for (int tile = 2 * blockIdx.x + half; tile * kTcRows < n && !failed; tile += 2 * gridDim.x) {
         const int row = tile * kTcRows + t;
         const bool valid = row < n;
         NrcQuery qq;
@@ -134,7 +139,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nrc_infer_tc(NrcNet net, cons
             // generic-proxy writes of the A operand -> visible to the tensor core
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncthreads();
+            half_sync(half);
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (t == 0) {
                 const uint32_t wl = wBase + static_cast<uint32_t>(l * (kNrcHid * kNrcIn * 2));
@@ -153,7 +158,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nrc_infer_tc(NrcNet net, cons
                 if (++spins >= kTcSpinLimit) { late = true; break; }
             }
             phase ^= 1u;
-            failed = __syncthreads_or(late ? 1 : 0) != 0;   // the same decision in every thread
+            failed = half_sync_or(half, late);   // the same decision in every thread of the half
             if (failed) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             uint32_t v[64];
@@ -217,7 +222,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nrc_infer_tc(NrcNet net, cons
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(tmem), "r"(kTcCols) : "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(*tmem_slot), "r"(2 * kTcCols) : "memory");
 }
 
 // ------------------------------------------------------------------ training
@@ -500,11 +506,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_nrc_train_bwd_tc(NrcNet net, 
 cudaError_t nrc_infer_tc(const NrcNet& net, const NrcQuery* q, const int32_t* count, int cap, double* accum,
                          float* out_rgb, int* err, int sm_count, cudaStream_t st)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_nrc_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    cudaError_t e = cudaFuncSetAttribute(k_nrc_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcInferSmem);
     if (e != cudaSuccess) return e;
     const int tiles = (cap + kTcRows - 1) / kTcRows;
-    const int grid = std::max(1, std::min(tiles, sm_count * 2));
-    k_nrc_infer_tc<<<grid, kTcThreads, kTcSmem, st>>>(net, q, count, cap, accum, out_rgb, err);
+    const int grid = std::max(1, std::min((tiles + 1) / 2, sm_count * 2));
+    k_nrc_infer_tc<<<grid, 2 * kTcRows, kTcInferSmem, st>>>(net, q, count, cap, accum, out_rgb, err);
     return cudaGetLastError();
 }
 

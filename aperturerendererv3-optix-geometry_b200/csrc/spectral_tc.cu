@@ -86,21 +86,6 @@ __device__ __forceinline__ void store_row(unsigned char* sA, int t, const float*
 
 namespace {
 
-// Synchronisation of one 128-thread half of the CTA (named barrier 1 + half).
-__device__ __forceinline__ void half_sync(int half)
-{
-    asm volatile("bar.sync %0, 128;" : : "r"(1 + half) : "memory");
-}
-// The same barrier with an OR over the half's predicates.
-__device__ __forceinline__ bool half_sync_or(int half, bool v)
-{
-    uint32_t r;
-    asm volatile("{\n\t.reg .pred q, p;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.or.pred p, %2, 128, q;\n\t"
-                 "selp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(r) : "r"(v ? 1u : 0u), "r"(1 + half) : "memory");
-    return r != 0;
-}
-
 // Two halves of 128 threads run two tiles side by side: each half has its own
 // A operand, mbarrier and 32 tensor-memory columns and synchronises on a named
 // barrier of its own, so one half's epilogue (tcgen05.ld, bias, ReLU, split,

@@ -106,4 +106,21 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t* v)
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Kernels that run two 128-row tiles per CTA side by side (threads 0-127 and
+// 128-255) synchronise each half on a named barrier of its own (1 + half),
+// so one half's epilogue overlaps the other half's MMAs.
+__device__ __forceinline__ void half_sync(int half)
+{
+    asm volatile("bar.sync %0, 128;" : : "r"(1 + half) : "memory");
+}
+// The same barrier with an OR over the half's predicates.
+__device__ __forceinline__ bool half_sync_or(int half, bool v)
+{
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred q, p;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.or.pred p, %2, 128, q;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(r) : "r"(v ? 1u : 0u), "r"(1 + half) : "memory");
+    return r != 0;
+}
+
 }  // namespace ar
