@@ -17,7 +17,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
 def test_xorwow_frame_jump_table(tmp_path):
-    """A^(2^16) against explicit steps, A^(2^32) against 2^16 jumps of 2^16."""
+    """A^(2^16) against explicit steps, A^(2^32) against 2^16 jumps of 2^16,
+    A^(2^33) and A^(2^67) (the subsequence jump of the per-pixel
+    initialisation) against two jumps of half the distance."""
     exe = tmp_path / "xorwow_jump_check"
     subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe),
                     os.path.join(HERE, "native", "xorwow_jump_check.cpp")], check=True)
